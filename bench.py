@@ -1,0 +1,310 @@
+"""Benchmark: Leiden RB(1.0), seed 7, on the 4M-node Gaussian kNN graph.
+
+Workload (the large single-graph configuration): 4,000,000 points x 30 dims
+f32 from a 100-component Gaussian mixture (sigma ~ U[0.7, 1.5], centres
+N(0, 4I)); exact kNN k = 10; Gaussian connectivities with per-point sigma =
+distance to the k-th neighbour; union-symmetrised u32 / f32 CSR handed over
+with from_csr_parts. A "step" is one full leiden() call on that graph.
+
+  value      undirected edges / s of leiden() with the graph resident in HBM
+             (edge_count / device time of the run, CUDA events on the
+             library's stream), summed over ranks (replicas only: a single
+             graph does not shard).
+  e2e        the same metric through the public C ABI with host buffers:
+             from_csr_parts (H2D + device finish) + leiden + labels D2H.
+  cpu_baseline  the CPU oracle (single-threaded restatement of the
+             reference's Leiden) on the same graph.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "single-clustering_b200"))
+
+import numpy as np  # noqa: E402
+
+N_POINTS = 4_000_000
+DIMS = 30
+COMPONENTS = 100
+K = 10
+GRAPH_SEED = 7
+LEIDEN_SEED = 7
+METRIC = "Leiden s/run & edges/s @4M nodes (dQ<=1e-3); sweep+warm-start vs plain GPU"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- workload
+def knn_graph_torch(n, d, comps, seed, k, device):
+    """Synthetic input only: exact fp32 brute-force kNN with torch, Gaussian
+    weights with sigma = k-th neighbour distance, union symmetrisation."""
+    import torch
+    from sc_gpu import synth
+    X, _ = synth.gaussian_mixture(n, d, comps, seed, sigma=(0.7, 1.5))
+    x = torch.from_numpy(X).to(device)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    norms = (x * x).sum(1)
+    idx = torch.empty((n, k + 1), dtype=torch.int64, device=device)
+    dist = torch.empty((n, k + 1), dtype=torch.float32, device=device)
+    chunk = 512
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        d2 = norms[s:e, None] + norms[None, :] - 2.0 * (x[s:e] @ x.T)
+        v, i = torch.topk(d2, k + 1, dim=1, largest=False, sorted=True)
+        idx[s:e] = i
+        dist[s:e] = v.clamp_min_(0).sqrt_()
+    sig = dist[:, k]
+    rows = torch.arange(n, device=device).repeat_interleave(k)
+    cols = idx[:, 1:].reshape(-1)
+    dd = dist[:, 1:].reshape(-1)
+    si, sj = sig[rows], sig[cols]
+    den = si * si + sj * sj
+    w = torch.sqrt(2 * si * sj / den) * torch.exp(-dd * dd / den)
+    keep = rows != cols
+    rows, cols, w = rows[keep], cols[keep], w[keep]
+    lo, hi = torch.minimum(rows, cols), torch.maximum(rows, cols)
+    key = lo * n + hi
+    key, order = torch.sort(key, stable=True)
+    w = w[order]
+    first = torch.ones_like(key, dtype=torch.bool)
+    first[1:] = key[1:] != key[:-1]
+    key, w = key[first], w[first]
+    lo, hi = key // n, key % n
+    r = torch.cat([lo, hi])
+    c = torch.cat([hi, lo])
+    ww = torch.cat([w, w]).float()
+    k2, order = torch.sort(r * n + c)
+    r, c, ww = r[order], c[order], ww[order]
+    ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(torch.bincount(r, minlength=n), 0)
+    out = (ptr.cpu().numpy().astype(np.uint64), c.to(torch.int32).cpu().numpy().view(np.uint32).copy(),
+           ww.cpu().numpy())
+    del x, norms, idx, dist
+    torch.cuda.empty_cache()
+    return out
+
+
+def make_graph(args, device):
+    if args.graph == "lattice":
+        from sc_gpu import synth
+        return synth.knn_like_graph(args.n, k=K, seed=GRAPH_SEED)
+    return knn_graph_torch(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                     timeout=5).stdout.strip()
+                if out:
+                    self.samples.append([x.strip() for x in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = sorted(float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit())
+        mx = max(float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()) if sm else None
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 5 + i and s[5 + i].lower() in ("active", "0x1", "1")})
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+# ---------------------------------------------------------------- arms
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def run_cpu_baseline(ptr, nbr, w, seed):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    g = O.Graph.from_csr_parts(ptr, nbr, w)
+    t = time.perf_counter()
+    lab, ncl = g.leiden(seed=seed, resolution=1.0)
+    dt = time.perf_counter() - t
+    return g, lab, dt
+
+
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=N_POINTS)
+    ap.add_argument("--graph", default="gmm", choices=["gmm", "lattice"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    device = torch.device("cuda", local_rank)
+
+    workload = {"workload": f"leiden_rb1_seed{LEIDEN_SEED}_knn{K}_gmm{args.n}x{DIMS}",
+                "n_points": args.n, "dims": DIMS, "components": COMPONENTS, "k": K,
+                "graph": args.graph, "sigma": "kth", "symmetrisation": "union",
+                "objective": "rb", "resolution": 1.0, "seed": LEIDEN_SEED,
+                "l2": "inputs larger than L2 (graph > 126 MB)", "parallelism": f"replicas{args.gpus}"}
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        ptr, nbr, w = make_graph(args, device)
+        g, lab, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
+        m = g.edge_count()
+        eps = m / dt
+        line = {"metric": METRIC, "value": eps, "unit": "edges/s", "impl": "reference", "n_gpus": args.gpus,
+                "steps": 1, "warmup": 0, "ms_per_step": dt * 1e3, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
+                "modularity": g.modularity(lab),
+                "cpu_baseline": {"value": eps, "unit": "edges/s", "cores": 1, "kind": "port",
+                                 "sample": "one full leiden() run on the whole graph",
+                                 "cpu": cpu_model(), "nproc": os.cpu_count()},
+                "e2e": {"value": eps, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line), flush=True)
+        return
+
+    import sc_gpu
+    t0 = time.perf_counter()
+    ptr, nbr, w = make_graph(args, device)
+    log(f"graph built in {time.perf_counter() - t0:.1f}s: n={len(ptr) - 1} entries={len(nbr)}")
+    g = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
+    m = g.edge_count()
+    cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(1.0), seed=LEIDEN_SEED)
+
+    for _ in range(args.warmup):
+        sc_gpu.leiden(g, cfg)
+    clocks = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    dev_ms = 0.0
+    stats = None
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        c = sc_gpu.leiden(g, cfg)
+        stats = sc_gpu.last_run_stats(local_rank)
+        dev_ms += stats["ms_total"]
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms_step = dev_ms / args.steps
+    if dist:
+        tt = torch.tensor([ms_step], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_step = float(tt.item())
+    value = world * m / (ms_step / 1e3)
+    q = sc_gpu.modularity(g, c.labels())
+
+    # e2e through the C ABI with host buffers
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 2))
+    for _ in range(e2e_steps):
+        g2 = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
+        c2 = sc_gpu.leiden(g2, cfg)
+        del g2
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t) / e2e_steps
+    h2d = ptr.nbytes + nbr.nbytes + w.nbytes
+    d2h = len(ptr) * 8 - 8
+
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    hbm, peak_kind = peaks()
+    lm_gbs = stats["alg_bytes_local_move"] / (stats["ms_local_move"] / 1e3) / 1e9 if stats["ms_local_move"] else 0
+    line = {"metric": METRIC, "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
+            "s_per_run": ms_step / 1e3, "edge_count": m, "modularity": q, "n_clusters": c.n_clusters(),
+            "wall_s_per_step": wall / args.steps,
+            "phases_ms": {k: stats[k] for k in ("ms_local_move", "ms_refine", "ms_aggregate", "ms_other")},
+            "run_stats": {k: stats[k] for k in ("passes", "levels", "local_move_sweeps", "moves")},
+            "gpu_launches": int(stats["kernel_launches"]) * args.steps,
+            "roofline": {"bound": "hbm", "kernel": "local-move sweeps (decide + apply)",
+                         "achieved": lm_gbs, "peak": hbm, "unit": "GB/s",
+                         "frac": lm_gbs / hbm if hbm else None, "traffic": None,
+                         "peak_kind": peak_kind},
+            "clocks": clk,
+            "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
+    if not args.no_cpu_baseline:
+        og, lab_o, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
+        q_o = og.modularity(lab_o)
+        line["cpu_baseline"] = {"value": m / dt, "unit": "edges/s", "cores": 1, "kind": "port",
+                                "sample": "one full leiden() run of the CPU oracle on the same graph",
+                                "s_per_run": dt, "modularity": q_o, "cpu": cpu_model(),
+                                "nproc": os.cpu_count()}
+        line["dQ_vs_cpu"] = q - q_o
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,279 @@
+/*
+ * sc_gpu.h — C ABI of the B200 (sm_100a) implementation of single-clustering's
+ * Leiden hot path and its Gaussian kNN graph builder.
+ *
+ * Every entry point mirrors one Rust API of single-clustering v0.7.0; the
+ * reference item each one replaces is cited beside it as `file:line` relative
+ * to the single-clustering source tree.
+ *
+ * Conventions
+ *   - Every function returns an `sc_status`. `SC_OK` is success; the codes 1..10
+ *     map one-to-one onto the variants of `ClusteringError` (src/error.rs:7-68),
+ *     the rest are device / argument failures the Rust API has no variant for.
+ *   - Input arrays are HOST pointers owned by the caller unless the name says
+ *     `_device`; the library copies them to the GPU. Outputs are host buffers
+ *     the caller sized.
+ *   - Ids are `uint32_t` inside the adjacency (`u32`, csr_network.rs:35-36),
+ *     offsets and labels are `uint64_t` (`usize`), weights `float` in storage
+ *     and `double` in every per-node quantity and every piece of arithmetic.
+ *   - One `sc_ctx` per host thread. A context owns one CUDA stream, a memory
+ *     pool, a device status word and the last error. Graph handles are
+ *     immutable after construction and may be shared between contexts on the
+ *     same device.
+ *   - The library never aborts the process: device-side guards (bounded waits,
+ *     bounds checks) set a status word that the host turns into SC_E_TIMEOUT /
+ *     SC_E_INTERNAL.
+ */
+#ifndef SC_GPU_H
+#define SC_GPU_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SC_GPU_ABI_VERSION 1
+
+/* Status codes. 1..10 follow ClusteringError (src/error.rs:7-68) in order. */
+typedef enum sc_status {
+    SC_OK = 0,
+    SC_E_NODE_INDEX_OUT_OF_RANGE = 1,     /* NodeIndexOutOfRange { node, n_nodes }        */
+    SC_E_NON_FINITE_WEIGHT = 2,           /* NonFiniteWeight { edge }                     */
+    SC_E_NEGATIVE_WEIGHT = 3,             /* NegativeWeight { edge, weight }              */
+    SC_E_INVALID_NODE_WEIGHT = 4,         /* InvalidNodeWeight { node, weight }           */
+    SC_E_NODE_WEIGHT_LENGTH_MISMATCH = 5, /* NodeWeightLengthMismatch { got, expected }   */
+    SC_E_MEMBERSHIP_LENGTH_MISMATCH = 6,  /* MembershipLengthMismatch { got, expected }   */
+    SC_E_INVALID_CONFIG = 7,              /* InvalidConfig(String)                        */
+    SC_E_TOO_MANY_NODES = 8,              /* TooManyNodes { n_nodes }                     */
+    SC_E_INVALID_CSR = 9,                 /* InvalidCsr(String)                           */
+    SC_E_ASYMMETRIC_GRAPH = 10,           /* AsymmetricGraph { degree_sum, expected }     */
+    SC_E_INVALID_ARGUMENT = 20,           /* null handle / pointer, bad enum value        */
+    SC_E_CUDA = 21,                       /* a CUDA runtime call failed                   */
+    SC_E_OUT_OF_MEMORY = 22,              /* device allocation failed                     */
+    SC_E_TIMEOUT = 23,                    /* a bounded device wait gave up                */
+    SC_E_INTERNAL = 24,                   /* an internal invariant failed (a bug)         */
+    SC_E_UNSUPPORTED = 25                 /* shape outside what a kernel supports         */
+} sc_status;
+
+/* Payload of the last error, field meaning follows the ClusteringError variant. */
+typedef struct sc_error_info {
+    int32_t code;          /* sc_status of the failure                                */
+    uint64_t node;         /* NodeIndexOutOfRange.node, InvalidNodeWeight.node        */
+    uint64_t n_nodes;      /* NodeIndexOutOfRange.n_nodes, TooManyNodes.n_nodes       */
+    uint64_t edge_from;    /* NonFiniteWeight/NegativeWeight .edge.0                  */
+    uint64_t edge_to;      /* NonFiniteWeight/NegativeWeight .edge.1                  */
+    double weight;         /* NegativeWeight.weight, InvalidNodeWeight.weight         */
+    uint64_t got;          /* *LengthMismatch.got                                     */
+    uint64_t expected_len; /* *LengthMismatch.expected                                */
+    double degree_sum;     /* AsymmetricGraph.degree_sum                              */
+    double expected;       /* AsymmetricGraph.expected                                */
+    char message[256];     /* Display text of the error, NUL-terminated               */
+} sc_error_info;
+
+/* ObjectiveKind (src/community_search/leiden/objective.rs:188-199). */
+typedef enum sc_objective { SC_OBJECTIVE_RB = 0, SC_OBJECTIVE_CPM = 1 } sc_objective;
+
+/*
+ * LeidenConfig (src/community_search/leiden/mod.rs:49-106), field for field.
+ * `Option<T>` fields are a has_ flag plus the value.
+ */
+typedef struct sc_leiden_config {
+    int32_t objective;              /* sc_objective                         */
+    double resolution;              /* ObjectiveKind::{Rb,Cpm}.resolution   */
+    int32_t has_seed;               /* seed: Option<u64>                    */
+    uint64_t seed;
+    uint64_t n_iterations;          /* default 2                            */
+    uint64_t max_levels;            /* default 64                           */
+    double tolerance;               /* default 1e-9                         */
+    int32_t refine;                 /* default 1; 0 = Louvain               */
+    double refine_randomness;       /* default 0.01                         */
+    uint64_t patience;              /* default 2                            */
+    int32_t has_max_community_weight;
+    double max_community_weight;
+} sc_leiden_config;
+
+/* Per-run counters of the last sc_leiden* call on a context (host-side copy). */
+typedef struct sc_run_stats {
+    uint64_t passes;                /* passes actually run                        */
+    uint64_t levels;                /* levels summed over passes                  */
+    uint64_t local_move_sweeps;     /* local-moving sweeps summed over levels     */
+    uint64_t moves;                 /* committed local moves                      */
+    uint64_t kernel_launches;       /* kernels this library launched for the run  */
+    double ms_local_move;           /* device time per phase, CUDA events         */
+    double ms_refine;
+    double ms_aggregate;
+    double ms_other;
+    double ms_total;
+    double alg_bytes_local_move;    /* algorithmic bytes of the local-move sweeps */
+    double alg_bytes_refine;
+    double alg_bytes_aggregate;
+} sc_run_stats;
+
+typedef struct sc_ctx sc_ctx;
+typedef struct sc_graph sc_graph;
+
+/* ---- context ------------------------------------------------------------ */
+uint32_t sc_abi_version(void);
+sc_status sc_ctx_create(int32_t device, sc_ctx** out);
+void sc_ctx_destroy(sc_ctx* ctx);
+/* Display text of the last error on this context ("" after success). */
+const char* sc_last_error_message(const sc_ctx* ctx);
+sc_status sc_last_error_info(const sc_ctx* ctx, sc_error_info* out);
+sc_status sc_last_run_stats(const sc_ctx* ctx, sc_run_stats* out);
+/* Blocks until all work of the context's stream is done. */
+sc_status sc_ctx_synchronize(sc_ctx* ctx);
+/* LeidenConfig::default() (src/community_search/leiden/mod.rs:92-106). */
+void sc_leiden_config_default(sc_leiden_config* cfg);
+
+/* ---- graph construction ------------------------------------------------- */
+/*
+ * CSRNetwork::from_csr_parts (src/network/csr_network.rs:185-256) followed by
+ * finish (:262-351) and check_degree_sum (:712-723), computed on the GPU.
+ * Each Vec of the Rust signature is a pointer plus its length, so every length
+ * check of the reference is reproduced. node_weights may be NULL (= None).
+ */
+sc_status sc_graph_from_csr(sc_ctx* ctx,
+                            const uint64_t* node_ptrs, uint64_t n_node_ptrs,
+                            const uint32_t* neighbors, uint64_t n_neighbors,
+                            const float* weights, uint64_t n_weights,
+                            const double* node_weights, uint64_t n_node_weights,
+                            sc_graph** out);
+
+/* Same contract, inputs already in this device's memory (kNN output hand-off). */
+sc_status sc_graph_from_csr_device(sc_ctx* ctx,
+                                   const uint64_t* node_ptrs_device, uint64_t n_node_ptrs,
+                                   const uint32_t* neighbors_device, uint64_t n_neighbors,
+                                   const float* weights_device, uint64_t n_weights,
+                                   const double* node_weights_device, uint64_t n_node_weights,
+                                   sc_graph** out);
+
+/*
+ * CSRNetwork::from_edges / from_edges_with_node_weights
+ * (src/network/csr_network.rs:104-167). Edge i is (from[i], to[i], weights[i]);
+ * weights are given as double (W::to_f64) and stored `as f32`. node_weights may
+ * be NULL, meaning unit weights over n_nodes nodes.
+ */
+sc_status sc_graph_from_edges(sc_ctx* ctx, uint64_t n_nodes,
+                              const uint64_t* from, const uint64_t* to,
+                              const double* weights, uint64_t n_edges,
+                              const double* node_weights, sc_graph** out);
+
+/*
+ * CSRNetwork::from_csr_matrix (src/network/csr_network.rs:360-391): reads only
+ * entries with row <= col and non-zero value, then from_edges.
+ */
+sc_status sc_graph_from_csr_matrix(sc_ctx* ctx,
+                                   const uint64_t* row_ptrs, uint64_t n_rows,
+                                   const uint64_t* col_indices, const double* values,
+                                   uint64_t nnz, const double* node_weights,
+                                   sc_graph** out);
+
+void sc_graph_destroy(sc_graph* g);
+
+/* node_count, stored entries, edge_count, total_weight, has_self_loops
+ * (src/network/csr_network.rs:407-442, :648-652). */
+sc_status sc_graph_info(const sc_graph* g, uint64_t* n_nodes, uint64_t* n_entries,
+                        uint64_t* edge_count, double* total_weight, int32_t* any_self_loops);
+
+/* to_csr_parts (src/network/csr_network.rs:484-490): node_ptrs n+1, neighbors
+ * and weights n_entries each. Any pointer may be NULL to skip it. */
+sc_status sc_graph_copy_csr(sc_ctx* ctx, const sc_graph* g, uint64_t* node_ptrs,
+                            uint32_t* neighbors, float* weights);
+
+/* node_weights (csr_network.rs:493-495) and strengths (:428-430), n each. */
+sc_status sc_graph_copy_node_data(sc_ctx* ctx, const sc_graph* g, double* node_weights,
+                                  double* strengths);
+
+/* validate_symmetry (src/network/csr_network.rs:627-646); SC_E_INVALID_CSR on failure. */
+sc_status sc_graph_validate_symmetry(sc_ctx* ctx, const sc_graph* g);
+
+/*
+ * CSRNetwork::aggregate (src/network/csr_network.rs:516-608) with the grouping
+ * VectorGrouping::from_assignments(groups) (src/network/grouping.rs:154-172),
+ * i.e. group ids are first renumbered by ascending rank.
+ */
+sc_status sc_aggregate(sc_ctx* ctx, const sc_graph* g, const uint64_t* groups,
+                       uint64_t n_groups_len, sc_graph** out);
+
+/* ---- evaluation --------------------------------------------------------- */
+/* modularity (src/community_search/leiden/objective.rs:221-244). */
+sc_status sc_modularity(sc_ctx* ctx, const sc_graph* g, const uint64_t* labels,
+                        uint64_t n_labels, double resolution, double* out);
+
+/* Partition::from_membership (partition.rs:75-112) then Rb::quality (objective.rs:108-119)
+ * or Cpm::quality (:171-178). */
+sc_status sc_quality(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership,
+                     uint64_t n_membership, int32_t objective, double resolution, double* out);
+
+/*
+ * Partition::from_membership aggregates (partition.rs:75-112): per slot
+ * c < slots = max(membership)+1, size, weight, strength and internal. Any output
+ * may be NULL. *slots_out receives the slot count.
+ */
+sc_status sc_partition_stats(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership,
+                             uint64_t n_membership, uint64_t* slots_out, uint32_t* size,
+                             double* weight, double* strength, double* internal,
+                             uint64_t capacity);
+
+/* ---- Leiden ------------------------------------------------------------- */
+/* leiden(&graph, &config) (src/community_search/leiden/mod.rs:168-204).
+ * labels_out has node_count entries, consecutive from 0. */
+sc_status sc_leiden(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg,
+                    uint64_t* labels_out, uint64_t* n_clusters_out);
+
+/* leiden starting from `initial` labels instead of singletons: the `initial`
+ * argument of run_once (src/community_search/leiden/mod.rs:207-220). */
+sc_status sc_leiden_from(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg,
+                         const uint64_t* initial, uint64_t n_initial,
+                         uint64_t* labels_out, uint64_t* n_clusters_out);
+
+/*
+ * Many independent leiden() calls in one batched launch sequence: instance i
+ * runs `cfgs[i]` on `graphs[i]` (graphs may repeat) and writes labels_out at
+ * label_offsets[i] (caller computes offsets; each instance needs node_count
+ * entries). No reference counterpart as one call; semantically a loop over
+ * leiden (src/community_search/leiden/mod.rs:168).
+ */
+sc_status sc_leiden_batch(sc_ctx* ctx, const sc_graph* const* graphs,
+                          const sc_leiden_config* cfgs, uint64_t count,
+                          const uint64_t* label_offsets, uint64_t* labels_out,
+                          uint64_t* n_clusters_out);
+
+/* ---- kNN graph builder --------------------------------------------------- */
+typedef enum sc_knn_sigma { SC_SIGMA_MEDIAN = 0, SC_SIGMA_KTH = 1 } sc_knn_sigma;
+typedef enum sc_knn_sym { SC_SYM_LOWER_ID = 0, SC_SYM_UNION = 1 } sc_knn_sym;
+typedef enum sc_knn_precision { SC_KNN_FP32 = 0, SC_KNN_BF16 = 1, SC_KNN_FP8 = 2 } sc_knn_precision;
+
+typedef struct sc_knn_opts {
+    int32_t sigma;        /* sc_knn_sigma; median = reference (neighborhood/mod.rs:105-124, :480-499) */
+    int32_t sym;          /* sc_knn_sym;   lower_id = reference (neighborhood/mod.rs:138-163)         */
+    int32_t precision;    /* sc_knn_precision of the candidate distance contraction                 */
+    int32_t rerank_factor;/* candidates kept per row before the exact FP32 re-rank = factor * (k+1)  */
+    int32_t squared_kiddo;/* 1: kd-tree path semantics (squared distances, sigma = sqrt(median d^2)) */
+} sc_knn_opts;
+
+void sc_knn_opts_default(sc_knn_opts* opts);
+
+/*
+ * knn_arrayd_kiddo_gaussian / knn_arrayd_hnswlib_gaussian
+ * (src/neighborhood/mod.rs:51-202, :359-578), exact on the GPU. X is row-major
+ * n x d float. Outputs (host):
+ *   knn_index   n*(k+1) neighbour ids per row, self first, ascending distance
+ *   knn_dist    n*(k+1) distances (squared when opts.squared_kiddo), may be NULL
+ * and the connectivities CSR, which is returned as a graph handle built with
+ * from_csr_parts semantics when `graph_out` is non-NULL, and/or copied to host
+ * when conn_ptrs is non-NULL (conn_nnz receives the entry count; conn_nbrs /
+ * conn_w must then hold conn_capacity entries).
+ */
+sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k,
+                          const sc_knn_opts* opts, uint32_t* knn_index, float* knn_dist,
+                          uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                          uint64_t conn_capacity, uint64_t* conn_nnz, sc_graph** graph_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SC_GPU_H */

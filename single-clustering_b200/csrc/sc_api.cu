@@ -1,0 +1,427 @@
+// sc_api.cu — the extern "C" boundary (include/sc_gpu.h). Every entry point
+// catches library failures and turns them into an sc_status plus the context's
+// last-error record; nothing escapes as a C++ exception or an abort.
+#include <random>
+
+#include "sc_prims.cuh"
+
+struct sc_ctx {
+    sc::Ctx c;
+};
+struct sc_graph {
+    sc::DevGraph* g = nullptr;
+};
+
+namespace {
+
+sc_status fill_error(sc_ctx* ctx, const sc_error_info& info) {
+    if (ctx) {
+        ctx->c.last.code = (sc_status)info.code;
+        ctx->c.last.info = info;
+    }
+    return (sc_status)info.code;
+}
+
+template <class F>
+sc_status guarded(sc_ctx* ctx, F&& f) {
+    if (!ctx) return SC_E_INVALID_ARGUMENT;
+    ctx->c.last = sc::Error{};
+    ctx->c.launches = 0;
+    try {
+        SC_CUDA(cudaSetDevice(ctx->c.device));
+        f(ctx->c);
+        return SC_OK;
+    } catch (sc::Failure& fl) {
+        return fill_error(ctx, fl.info);
+    } catch (std::bad_alloc&) {
+        sc_error_info i{};
+        i.code = SC_E_OUT_OF_MEMORY;
+        std::snprintf(i.message, sizeof i.message, "host allocation failed");
+        return fill_error(ctx, i);
+    } catch (...) {
+        sc_error_info i{};
+        i.code = SC_E_INTERNAL;
+        std::snprintf(i.message, sizeof i.message, "unexpected internal exception");
+        return fill_error(ctx, i);
+    }
+}
+
+[[noreturn]] void bad_arg(const char* what) { sc::fail(SC_E_INVALID_ARGUMENT, "invalid argument: %s", what); }
+
+void require(bool ok, const char* what) {
+    if (!ok) bad_arg(what);
+}
+
+void check_membership_len(uint64_t got, uint64_t expected) {
+    if (got != expected) {
+        sc_error_info i{};
+        i.code = SC_E_MEMBERSHIP_LENGTH_MISMATCH;
+        i.got = got;
+        i.expected_len = expected;
+        sc::fail_info(i);
+    }
+}
+
+void require_same_device(sc::Ctx& c, const sc::DevGraph& g) {
+    if (c.device != g.device) bad_arg("graph lives on another device than the context");
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t sc_abi_version(void) { return SC_GPU_ABI_VERSION; }
+
+sc_status sc_ctx_create(int32_t device, sc_ctx** out) {
+    if (!out) return SC_E_INVALID_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        return SC_E_CUDA;
+    }
+    if (device < 0 || device >= count) return SC_E_INVALID_ARGUMENT;
+    std::unique_ptr<sc_ctx> ctx(new sc_ctx());
+    sc::Ctx& c = ctx->c;
+    c.device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return SC_E_CUDA;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
+    if (cudaDeviceGetDefaultMemPool(&c.pool, device) != cudaSuccess) return SC_E_CUDA;
+    uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
+    cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+    if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
+    cudaMemset(c.d_status, 0, sizeof(uint32_t));
+    cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    c.smem_optin = (size_t)optin;
+    *out = ctx.release();
+    return SC_OK;
+}
+
+void sc_ctx_destroy(sc_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->c.device);
+    if (ctx->c.stream) {
+        cudaStreamSynchronize(ctx->c.stream);
+        cudaStreamDestroy(ctx->c.stream);
+    }
+    if (ctx->c.d_status) cudaFree(ctx->c.d_status);
+    delete ctx;
+}
+
+const char* sc_last_error_message(const sc_ctx* ctx) {
+    if (!ctx) return "null context";
+    return ctx->c.last.info.message;
+}
+
+sc_status sc_last_error_info(const sc_ctx* ctx, sc_error_info* out) {
+    if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
+    *out = ctx->c.last.info;
+    return SC_OK;
+}
+
+sc_status sc_last_run_stats(const sc_ctx* ctx, sc_run_stats* out) {
+    if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
+    *out = ctx->c.stats;
+    return SC_OK;
+}
+
+sc_status sc_ctx_synchronize(sc_ctx* ctx) {
+    return guarded(ctx, [&](sc::Ctx& c) { SC_CUDA(cudaStreamSynchronize(c.stream)); });
+}
+
+void sc_leiden_config_default(sc_leiden_config* cfg) {
+    if (!cfg) return;
+    std::memset(cfg, 0, sizeof *cfg);
+    cfg->objective = SC_OBJECTIVE_RB;
+    cfg->resolution = 1.0;
+    cfg->has_seed = 1;
+    cfg->seed = 42;
+    cfg->n_iterations = 2;
+    cfg->max_levels = 64;
+    cfg->tolerance = 1e-9;
+    cfg->refine = 1;
+    cfg->refine_randomness = 0.01;
+    cfg->patience = 2;
+    cfg->has_max_community_weight = 0;
+    cfg->max_community_weight = 0.0;
+}
+
+sc_status sc_graph_from_csr(sc_ctx* ctx, const uint64_t* node_ptrs, uint64_t n_node_ptrs,
+                            const uint32_t* neighbors, uint64_t n_neighbors, const float* weights,
+                            uint64_t n_weights, const double* node_weights, uint64_t n_node_weights,
+                            sc_graph** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(out != nullptr, "out is NULL");
+        require(n_node_ptrs == 0 || node_ptrs, "node_ptrs is NULL");
+        require(n_neighbors == 0 || neighbors, "neighbors is NULL");
+        require(n_weights == 0 || weights, "weights is NULL");
+        *out = nullptr;
+        sc::DevGraph* g = sc::graph_from_csr(c, node_ptrs, n_node_ptrs, neighbors, n_neighbors, weights,
+                                             n_weights, node_weights, n_node_weights, false);
+        *out = new sc_graph{g};
+    });
+}
+
+sc_status sc_graph_from_csr_device(sc_ctx* ctx, const uint64_t* node_ptrs, uint64_t n_node_ptrs,
+                                   const uint32_t* neighbors, uint64_t n_neighbors,
+                                   const float* weights, uint64_t n_weights,
+                                   const double* node_weights, uint64_t n_node_weights,
+                                   sc_graph** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(out != nullptr, "out is NULL");
+        require(n_node_ptrs == 0 || node_ptrs, "node_ptrs is NULL");
+        *out = nullptr;
+        sc::DevGraph* g = sc::graph_from_csr(c, node_ptrs, n_node_ptrs, neighbors, n_neighbors, weights,
+                                             n_weights, node_weights, n_node_weights, true);
+        *out = new sc_graph{g};
+    });
+}
+
+sc_status sc_graph_from_edges(sc_ctx* ctx, uint64_t n_nodes, const uint64_t* from, const uint64_t* to,
+                              const double* weights, uint64_t n_edges, const double* node_weights,
+                              sc_graph** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(out != nullptr, "out is NULL");
+        require(n_edges == 0 || (from && to && weights), "edge arrays are NULL");
+        *out = nullptr;
+        sc::DevGraph* g = sc::graph_from_edges(c, n_nodes, from, to, weights, n_edges, node_weights);
+        *out = new sc_graph{g};
+    });
+}
+
+sc_status sc_graph_from_csr_matrix(sc_ctx* ctx, const uint64_t* row_ptrs, uint64_t n_rows,
+                                   const uint64_t* col_indices, const double* values, uint64_t nnz,
+                                   const double* node_weights, sc_graph** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(out != nullptr, "out is NULL");
+        require(row_ptrs != nullptr, "row_ptrs is NULL");
+        *out = nullptr;
+        // upper triangle, non-zero values (csr_network.rs:382-388), in triplet order
+        std::vector<uint64_t> f, t;
+        std::vector<double> w;
+        f.reserve(nnz / 2 + 1);
+        t.reserve(nnz / 2 + 1);
+        w.reserve(nnz / 2 + 1);
+        for (uint64_t r = 0; r < n_rows; ++r)
+            for (uint64_t e = row_ptrs[r]; e < row_ptrs[r + 1]; ++e)
+                if (r <= col_indices[e] && values[e] != 0.0) {
+                    f.push_back(r);
+                    t.push_back(col_indices[e]);
+                    w.push_back(values[e]);
+                }
+        sc::DevGraph* g = sc::graph_from_edges(c, n_rows, f.data(), t.data(), w.data(), f.size(),
+                                               node_weights);
+        *out = new sc_graph{g};
+    });
+}
+
+void sc_graph_destroy(sc_graph* g) {
+    if (!g) return;
+    delete g->g;
+    delete g;
+}
+
+sc_status sc_graph_info(const sc_graph* g, uint64_t* n_nodes, uint64_t* n_entries, uint64_t* edge_count,
+                        double* total_weight, int32_t* any_self_loops) {
+    if (!g || !g->g) return SC_E_INVALID_ARGUMENT;
+    if (n_nodes) *n_nodes = g->g->n;
+    if (n_entries) *n_entries = g->g->E;
+    if (edge_count) *edge_count = g->g->edge_count;
+    if (total_weight) *total_weight = g->g->total_weight;
+    if (any_self_loops) *any_self_loops = g->g->any_self_loops ? 1 : 0;
+    return SC_OK;
+}
+
+sc_status sc_graph_copy_csr(sc_ctx* ctx, const sc_graph* g, uint64_t* node_ptrs, uint32_t* neighbors,
+                            float* weights) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g, "graph is NULL");
+        require_same_device(c, *g->g);
+        sc::graph_copy_csr(c, *g->g, node_ptrs, neighbors, weights);
+    });
+}
+
+sc_status sc_graph_copy_node_data(sc_ctx* ctx, const sc_graph* g, double* node_weights, double* strengths) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g, "graph is NULL");
+        require_same_device(c, *g->g);
+        sc::graph_copy_node_data(c, *g->g, node_weights, strengths);
+    });
+}
+
+sc_status sc_graph_validate_symmetry(sc_ctx* ctx, const sc_graph* g) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g, "graph is NULL");
+        require_same_device(c, *g->g);
+        sc::graph_validate_symmetry(c, *g->g);
+    });
+}
+
+sc_status sc_aggregate(sc_ctx* ctx, const sc_graph* g, const uint64_t* groups, uint64_t n_groups_len,
+                       sc_graph** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && out, "graph or out is NULL");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        check_membership_len(n_groups_len, G.n);
+        *out = nullptr;
+        sc::DBuf<uint64_t> dg(c, G.n);
+        sc::DBuf<uint32_t> ids(c, G.n);
+        sc::h2d(c, dg.get(), groups, G.n);
+        uint32_t ng = sc::renumber_u64_labels(c, dg.get(), G.n, ids.get(), nullptr);
+        sc::DevGraph* a = sc::graph_aggregate(c, G, ids.get(), ng);
+        *out = new sc_graph{a};
+    });
+}
+
+sc_status sc_modularity(sc_ctx* ctx, const sc_graph* g, const uint64_t* labels, uint64_t n_labels,
+                        double resolution, double* out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && out, "graph or out is NULL");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        check_membership_len(n_labels, G.n);
+        sc::DBuf<uint64_t> dl(c, G.n);
+        sc::DBuf<uint32_t> ids(c, G.n);
+        sc::h2d(c, dl.get(), labels, G.n);
+        uint32_t C = sc::renumber_u64_labels(c, dl.get(), G.n, ids.get(), nullptr);
+        *out = sc::modularity(c, G, ids.get(), C, resolution);
+    });
+}
+
+sc_status sc_quality(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
+                     int32_t objective, double resolution, double* out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && out, "graph or out is NULL");
+        require(objective == SC_OBJECTIVE_RB || objective == SC_OBJECTIVE_CPM, "unknown objective");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        check_membership_len(n_membership, G.n);
+        sc::DBuf<uint64_t> dl(c, G.n);
+        sc::DBuf<uint32_t> ids(c, G.n);
+        sc::h2d(c, dl.get(), membership, G.n);
+        uint32_t C = sc::renumber_u64_labels(c, dl.get(), G.n, ids.get(), nullptr);
+        *out = sc::quality(c, G, ids.get(), C, objective, resolution);
+    });
+}
+
+sc_status sc_partition_stats(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership,
+                             uint64_t n_membership, uint64_t* slots_out, uint32_t* size, double* weight,
+                             double* strength, double* internal, uint64_t capacity) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && slots_out, "graph or slots_out is NULL");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        check_membership_len(n_membership, G.n);
+        uint64_t slots = 0;
+        for (uint64_t i = 0; i < G.n; ++i) slots = std::max<uint64_t>(slots, membership[i] + 1);
+        *slots_out = slots;
+        require(slots <= capacity, "capacity is smaller than max(membership)+1");
+        sc::DBuf<uint64_t> dl(c, G.n);
+        sc::DBuf<uint32_t> ids(c, G.n);
+        sc::h2d(c, dl.get(), membership, G.n);
+        uint32_t C = sc::renumber_u64_labels(c, dl.get(), G.n, ids.get(), nullptr);
+        sc::PartStats st;
+        sc::partition_stats(c, G, ids.get(), C, st, internal != nullptr);
+        std::vector<uint32_t> hs(C);
+        std::vector<double> hw(C), hst(C), hin(C);
+        sc::d2h(c, hs.data(), st.size.get(), C);
+        sc::d2h(c, hw.data(), st.weight.get(), C);
+        sc::d2h(c, hst.data(), st.strength.get(), C);
+        sc::d2h(c, hin.data(), st.internal.get(), C);
+        sc::sync(c);
+        // compact id r corresponds to the r-th smallest distinct label
+        std::vector<uint64_t> distinct(membership, membership + G.n);
+        std::sort(distinct.begin(), distinct.end());
+        distinct.erase(std::unique(distinct.begin(), distinct.end()), distinct.end());
+        if (size) std::fill(size, size + slots, 0u);
+        if (weight) std::fill(weight, weight + slots, 0.0);
+        if (strength) std::fill(strength, strength + slots, 0.0);
+        if (internal) std::fill(internal, internal + slots, 0.0);
+        for (uint64_t r = 0; r < distinct.size(); ++r) {
+            uint64_t s = distinct[r];
+            if (size) size[s] = hs[r];
+            if (weight) weight[s] = hw[r];
+            if (strength) strength[s] = hst[r];
+            if (internal) internal[s] = hin[r];
+        }
+    });
+}
+
+sc_status sc_leiden(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg, uint64_t* labels_out,
+                    uint64_t* n_clusters_out) {
+    return sc_leiden_from(ctx, g, cfg, nullptr, 0, labels_out, n_clusters_out);
+}
+
+sc_status sc_leiden_from(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg,
+                         const uint64_t* initial, uint64_t n_initial, uint64_t* labels_out,
+                         uint64_t* n_clusters_out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && cfg && n_clusters_out, "graph, config or n_clusters_out is NULL");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        require(G.n == 0 || labels_out, "labels_out is NULL");
+        if (initial) check_membership_len(n_initial, G.n);
+        sc::DBuf<uint32_t> lab(c, G.n);
+        uint64_t ncl = 0;
+        sc::leiden(c, G, *cfg, initial, lab.get(), &ncl);
+        if (G.n) {
+            std::vector<uint32_t> h(G.n);
+            sc::d2h(c, h.data(), lab.get(), G.n);
+            sc::sync(c);
+            for (uint64_t i = 0; i < G.n; ++i) labels_out[i] = h[i];
+        }
+        *n_clusters_out = ncl;
+    });
+}
+
+sc_status sc_leiden_batch(sc_ctx* ctx, const sc_graph* const* graphs, const sc_leiden_config* cfgs,
+                          uint64_t count, const uint64_t* label_offsets, uint64_t* labels_out,
+                          uint64_t* n_clusters_out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(count == 0 || (graphs && cfgs && label_offsets && labels_out && n_clusters_out),
+                "batch arrays are NULL");
+        for (uint64_t i = 0; i < count; ++i) {
+            require(graphs[i] && graphs[i]->g, "a graph of the batch is NULL");
+            require_same_device(c, *graphs[i]->g);
+            const sc::DevGraph& G = *graphs[i]->g;
+            sc::DBuf<uint32_t> lab(c, G.n);
+            uint64_t ncl = 0;
+            sc::leiden(c, G, cfgs[i], nullptr, lab.get(), &ncl);
+            std::vector<uint32_t> h(G.n);
+            sc::d2h(c, h.data(), lab.get(), G.n);
+            sc::sync(c);
+            for (uint64_t j = 0; j < G.n; ++j) labels_out[label_offsets[i] + j] = h[j];
+            n_clusters_out[i] = ncl;
+        }
+    });
+}
+
+void sc_knn_opts_default(sc_knn_opts* o) {
+    if (!o) return;
+    o->sigma = SC_SIGMA_MEDIAN;
+    o->sym = SC_SYM_LOWER_ID;
+    o->precision = SC_KNN_BF16;
+    o->rerank_factor = 2;
+    o->squared_kiddo = 0;
+}
+
+sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k,
+                          const sc_knn_opts* opts, uint32_t* knn_index, float* knn_dist,
+                          uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w, uint64_t conn_capacity,
+                          uint64_t* conn_nnz, sc_graph** graph_out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(X != nullptr || n == 0, "X is NULL");
+        sc_knn_opts o;
+        if (opts) o = *opts;
+        else sc_knn_opts_default(&o);
+        sc::DevGraph* g = nullptr;
+        sc::knn_gaussian(c, X, n, d, k, o, knn_index, knn_dist, conn_ptrs, conn_nbrs, conn_w, conn_capacity,
+                         conn_nnz, graph_out ? &g : nullptr);
+        if (graph_out) *graph_out = new sc_graph{g};
+    });
+}
+
+}  // extern "C"

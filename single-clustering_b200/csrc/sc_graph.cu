@@ -1,0 +1,1011 @@
+// sc_graph.cu — device construction of CSRNetwork (csr_network.rs) on sm_100a.
+//
+// Parity rule: every f64 sum is taken in the reference's order. Per-row sums
+// (duplicate merge, strengths) run one thread per row in ascending neighbour
+// order. Cross-row sums (total_weight, Σ strength, aggregate's per-pair
+// accumulators) are either provably order-independent — every term is a
+// multiple of 2^e0 and the grand total is below 2^(52+e0), so every partial
+// sum is exact in f64 (the "exact regime") — or are taken by an ordered chain.
+#include "sc_prims.cuh"
+
+namespace sc {
+
+namespace {
+
+constexpr unsigned TB = 256;
+
+void galloc(DevGraph& g, uint64_t n, uint64_t E) {
+    SC_CUDA(cudaGetDevice(&g.device));
+    g.n = n;
+    g.E = E;
+    SC_CUDA(cudaMalloc(&g.ptr, (n + 1) * sizeof(uint64_t)));
+    if (E) {
+        SC_CUDA(cudaMalloc(&g.nbr, E * sizeof(uint32_t)));
+        SC_CUDA(cudaMalloc(&g.w, E * sizeof(float)));
+        SC_CUDA(cudaMalloc(&g.erow, E * sizeof(uint32_t)));
+    }
+    if (n) {
+        SC_CUDA(cudaMalloc(&g.node_w, n * sizeof(double)));
+        SC_CUDA(cudaMalloc(&g.strength, n * sizeof(double)));
+        SC_CUDA(cudaMalloc(&g.self_loop, n * sizeof(double)));
+    }
+}
+
+// ------------------------------------------------------------ validation
+__global__ void k_first_bad_ptr(const uint64_t* __restrict__ ptr, uint64_t n,
+                                unsigned long long* first) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        if (ptr[v] > ptr[v + 1]) atomicMin(first, (unsigned long long)v);
+}
+
+__global__ void k_first_bad_entry(const uint32_t* __restrict__ nbr, const float* __restrict__ w,
+                                  uint64_t E, uint64_t n, unsigned long long* first) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        float x = w[e];
+        if ((uint64_t)nbr[e] >= n || !isfinite(x) || x < 0.0f) atomicMin(first, (unsigned long long)e);
+    }
+}
+
+__global__ void k_first_bad_nodew(const double* __restrict__ nw, uint64_t n,
+                                  unsigned long long* first) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        double x = nw[v];
+        if (!isfinite(x) || x < 0.0) atomicMin(first, (unsigned long long)v);
+    }
+}
+
+__global__ void k_first_bad_edge(const uint64_t* __restrict__ from, const uint64_t* __restrict__ to,
+                                 const double* __restrict__ w, uint64_t m, uint64_t n,
+                                 unsigned long long* first) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        double x = w[i];
+        if (from[i] >= n || to[i] >= n || !isfinite(x) || x < 0.0)
+            atomicMin(first, (unsigned long long)i);
+    }
+}
+
+__global__ void k_fill_double(double* p, uint64_t n, double v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+__global__ void k_lowbit_f64(const double* __restrict__ x, uint64_t n, int* min_low) {
+    int best = 0x7FFFFFFF;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        best = min(best, lowbit_exp_f64(x[i]));
+    for (int o = 16; o; o >>= 1) best = min(best, __shfl_xor_sync(0xFFFFFFFFu, best, o));
+    if ((threadIdx.x & 31) == 0 && best != 0x7FFFFFFF) atomicMin(min_low, best);
+}
+
+// ------------------------------------------------------------ row kernels
+// One warp per row writes the row id over its entries (coalesced).
+__global__ void k_fill_erow(const uint64_t* __restrict__ ptr, uint64_t n, uint32_t* erow) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < n; v += nwarps) {
+        uint64_t b = ptr[v], e = ptr[v + 1];
+        for (uint64_t i = b + lane; i < e; i += 32) erow[i] = (uint32_t)v;
+    }
+}
+
+// dirty = 1 if some row is not strictly increasing or holds a zero weight.
+__global__ void k_rows_clean(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                             const float* __restrict__ w, const uint32_t* __restrict__ erow,
+                             uint64_t E, int* dirty) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        bool bad = (w[e] == 0.0f);
+        if (e > 0 && erow[e - 1] == erow[e] && nbr[e - 1] >= nbr[e]) bad = true;
+        if (bad) *dirty = 1;
+    }
+}
+
+__global__ void k_make_row_keys(const uint32_t* __restrict__ erow, const uint32_t* __restrict__ nbr,
+                                uint64_t E, uint64_t* keys) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x)
+        keys[e] = ((uint64_t)erow[e] << 32) | nbr[e];
+}
+
+// Rows sorted by neighbour id (duplicates in input order): per row, count the
+// distinct ids whose f64 sum is non-zero (finish, csr_network.rs:295-306).
+__global__ void k_merge_count(const uint64_t* __restrict__ ptr, const uint64_t* __restrict__ keys,
+                              const float* __restrict__ w, uint64_t n, uint64_t* cnt) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = ptr[v], e = ptr[v + 1], c = 0;
+        while (i < e) {
+            uint32_t u = (uint32_t)keys[i];
+            double acc = 0.0;
+            while (i < e && (uint32_t)keys[i] == u) {
+                acc = __dadd_rn(acc, (double)w[i]);
+                ++i;
+            }
+            if (acc != 0.0) ++c;
+        }
+        cnt[v] = c;
+    }
+}
+
+__global__ void k_merge_write(const uint64_t* __restrict__ ptr_in, const uint64_t* __restrict__ keys,
+                              const float* __restrict__ w_in, uint64_t n,
+                              const uint64_t* __restrict__ ptr_out, uint32_t* nbr_out, float* w_out) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t i = ptr_in[v], e = ptr_in[v + 1], o = ptr_out[v];
+        while (i < e) {
+            uint32_t u = (uint32_t)keys[i];
+            double acc = 0.0;
+            while (i < e && (uint32_t)keys[i] == u) {
+                acc = __dadd_rn(acc, (double)w_in[i]);
+                ++i;
+            }
+            if (acc == 0.0) continue;
+            nbr_out[o] = u;
+            w_out[o] = __double2float_rn(acc);
+            ++o;
+        }
+    }
+}
+
+// Per row of a clean CSR: strength in ascending-neighbour order (self-loop
+// twice, csr_network.rs:313-320), self-loop weight, lowest set bit of the
+// stored weights, any self-loop, max degree.
+__global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                            const float* __restrict__ w, uint64_t n, double* strength,
+                            double* self_loop, int* min_low, unsigned* any_loop, unsigned* max_deg) {
+    int low = 0x7FFFFFFF;
+    unsigned loop = 0, mdeg = 0;
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t b = ptr[v], e = ptr[v + 1];
+        double s = 0.0, sl = 0.0;
+        for (uint64_t i = b; i < e; ++i) {
+            float x = w[i];
+            double st = (double)x;
+            low = min(low, lowbit_exp_f32(x));
+            if (nbr[i] == (uint32_t)v) {
+                loop = 1;
+                sl = st;
+                s = __dadd_rn(s, __dmul_rn(2.0, st));
+            } else {
+                s = __dadd_rn(s, st);
+            }
+        }
+        strength[v] = s;
+        self_loop[v] = sl;
+        mdeg = max(mdeg, (unsigned)(e - b));
+    }
+    for (int o = 16; o; o >>= 1) {
+        low = min(low, __shfl_xor_sync(0xFFFFFFFFu, low, o));
+        loop |= __shfl_xor_sync(0xFFFFFFFFu, loop, o);
+        mdeg = max(mdeg, __shfl_xor_sync(0xFFFFFFFFu, mdeg, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (low != 0x7FFFFFFF) atomicMin(min_low, low);
+        if (loop) atomicOr(any_loop, 1u);
+        atomicMax(max_deg, mdeg);
+    }
+}
+
+// total_weight terms: stored weight of entries with row <= neighbour, else 0.
+__global__ void k_upper_terms(const uint32_t* __restrict__ erow, const uint32_t* __restrict__ nbr,
+                              const float* __restrict__ w, uint64_t E, double* terms,
+                              uint8_t* flags) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        bool up = erow[e] <= nbr[e];
+        terms[e] = up ? (double)w[e] : 0.0;
+        flags[e] = up ? 1 : 0;
+    }
+}
+
+__global__ void k_u8_to_u64(const uint8_t* f, uint64_t n, uint64_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = f[i];
+}
+
+// CSR offsets from keys sorted by row: start[r] = first index with row >= r.
+__global__ void k_starts_from_sorted(const uint32_t* __restrict__ rows, uint64_t N, uint64_t R,
+                                     uint64_t* start) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = i < N ? rows[i] : R;
+        uint64_t prev = i == 0 ? 0 : (uint64_t)rows[i - 1] + 1;
+        if (i == 0) prev = 0;
+        for (uint64_t q = prev; q <= r && q <= R; ++q) start[q] = i;
+    }
+}
+
+// ------------------------------------------------------------ totals
+struct Totals {
+    double total_weight;
+    uint64_t edge_count;
+};
+
+// total_weight (csr_network.rs:321-324) and edge_count of a clean CSR.
+Totals ordered_total(Ctx& c, const DevGraph& g, bool exact) {
+    Totals t{0.0, 0};
+    if (g.E == 0) return t;
+    DBuf<double> terms(c, g.E);
+    DBuf<uint8_t> flags(c, g.E);
+    k_upper_terms<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.erow, g.nbr, g.w, g.E, terms.get(),
+                                                          flags.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    DBuf<uint64_t> f64s(c, g.E);
+    k_u8_to_u64<<<grid_for(g.E, TB), TB, 0, c.stream>>>(flags.get(), g.E, f64s.get());
+    c.launches++;
+    DBuf<uint64_t> cnt(c, 1);
+    device_sum(c, f64s.get(), cnt.get(), g.E);
+    t.edge_count = to_host(c, cnt.get());
+    if (exact) {
+        DBuf<double> s(c, 1);
+        device_sum(c, terms.get(), s.get(), g.E);
+        t.total_weight = to_host(c, s.get());
+    } else {
+        DBuf<double> up(c, g.E);
+        DBuf<uint64_t> nup(c, 1);
+        select_flagged(c, terms.get(), flags.get(), up.get(), nup.get(), g.E);
+        uint64_t k = to_host(c, nup.get());
+        t.total_weight = ordered_sum_from(c, up.get(), k, 0.0);
+    }
+    return t;
+}
+
+// Rust-order Σ of an f64 array (fold from -0.0), exact or chained.
+double rust_sum_dev(Ctx& c, const double* d, uint64_t n, bool exact) {
+    if (n == 0) return -0.0;
+    if (exact) {
+        DBuf<double> s(c, 1);
+        device_sum(c, d, s.get(), n);
+        double x = to_host(c, s.get());
+        return x;  // n > 0 terms, each >= +0.0: the -0.0 start never shows
+    }
+    return ordered_sum(c, d, n);
+}
+
+// Stats, regime, totals and check_degree_sum of a graph whose rows are clean.
+void finalize(Ctx& c, DevGraph& g, bool check_sum) {
+    const uint64_t n = g.n;
+    DBuf<int> d_low(c, 2);
+    DBuf<unsigned> d_flags(c, 2);
+    int init_low[2] = {0x7FFFFFFF, 0x7FFFFFFF};
+    h2d(c, d_low.get(), init_low, 2);
+    zero(c, d_flags.get(), 2);
+    if (n) {
+        k_row_stats<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength,
+                                                          g.self_loop, d_low.get(), d_flags.get(),
+                                                          d_flags.get() + 1);
+        SC_LAUNCH_CHECK();
+        k_lowbit_f64<<<grid_for(n, TB), TB, 0, c.stream>>>(g.node_w, n, d_low.get() + 1);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    int low[2];
+    unsigned flags[2];
+    d2h(c, low, d_low.get(), 2);
+    d2h(c, flags, d_flags.get(), 2);
+    sync(c);
+    g.any_self_loops = flags[0] != 0;
+    g.max_degree = flags[1];
+    g.e0_w = low[0];
+    g.e0_nw = low[1];
+
+    // approximate Σ strength (= 2m) decides the regime; exact inside it
+    double approx2m = 0.0;
+    if (n) {
+        DBuf<double> s(c, 1);
+        device_sum(c, g.strength, s.get(), n);
+        approx2m = to_host(c, s.get());
+    }
+    g.exact_w = (g.e0_w == 0x7FFFFFFF) || (approx2m < std::ldexp(1.0, 52 + g.e0_w));
+    double approx_nw = 0.0;
+    if (n) {
+        DBuf<double> s(c, 1);
+        device_sum(c, g.node_w, s.get(), n);
+        approx_nw = to_host(c, s.get());
+    }
+    g.exact_nw = (g.e0_nw == 0x7FFFFFFF) || (approx_nw < std::ldexp(1.0, 52 + g.e0_nw));
+    g.total_node_weight = rust_sum_dev(c, g.node_w, n, g.exact_nw);
+
+    Totals t = ordered_total(c, g, g.exact_w);
+    g.total_weight = t.total_weight;
+    g.edge_count = t.edge_count;
+
+    if (check_sum) {
+        // check_degree_sum (csr_network.rs:712-723)
+        double expected = 2.0 * g.total_weight;
+        double tol = 1e-6 * std::max(std::fabs(expected), 1.0);
+        double sum = g.exact_w ? (n ? approx2m : -0.0) : approx2m;
+        if (!g.exact_w && std::fabs(sum - expected) > 0.25 * tol) sum = rust_sum_dev(c, g.strength, n, false);
+        if (std::fabs(sum - expected) > tol) {
+            sc_error_info i{};
+            i.code = SC_E_ASYMMETRIC_GRAPH;
+            i.degree_sum = sum;
+            i.expected = expected;
+            fail_info(i);
+        }
+    }
+}
+
+// finish (csr_network.rs:262-351) on validated device arrays the graph owns.
+void finish(Ctx& c, DevGraph& g) {
+    const uint64_t n = g.n;
+    if (g.E) {
+        k_fill_erow<<<grid_for(n * 32, TB), TB, 0, c.stream>>>(g.ptr, n, g.erow);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        DBuf<int> dirty(c, 1);
+        zero(c, dirty.get(), 1);
+        k_rows_clean<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E,
+                                                             dirty.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        if (to_host(c, dirty.get())) {
+            // stable sort of every entry by (row, neighbour): duplicates keep input order
+            DBuf<uint64_t> keys(c, g.E), keys_s(c, g.E);
+            DBuf<float> w_s(c, g.E);
+            k_make_row_keys<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.erow, g.nbr, g.E, keys.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+            sort_pairs(c, keys.get(), keys_s.get(), g.w, w_s.get(), g.E, 32 + bits_for(n));
+            DBuf<uint64_t> cnt(c, n + 1), nptr(c, n + 1);
+            k_merge_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, keys_s.get(), w_s.get(), n,
+                                                                cnt.get());
+            SC_LAUNCH_CHECK();
+            zero(c, cnt.get() + n, 1);
+            exclusive_sum(c, cnt.get(), nptr.get(), n + 1);
+            uint64_t E2 = to_host(c, nptr.get() + n);
+            uint32_t* nbr2 = nullptr;
+            float* w2 = nullptr;
+            uint32_t* erow2 = nullptr;
+            if (E2) {
+                SC_CUDA(cudaMalloc(&nbr2, E2 * sizeof(uint32_t)));
+                SC_CUDA(cudaMalloc(&w2, E2 * sizeof(float)));
+                SC_CUDA(cudaMalloc(&erow2, E2 * sizeof(uint32_t)));
+            }
+            k_merge_write<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, keys_s.get(), w_s.get(), n,
+                                                                nptr.get(), nbr2, w2);
+            SC_LAUNCH_CHECK();
+            c.launches += 2;
+            d2d(c, g.ptr, nptr.get(), n + 1);
+            sync(c);
+            cudaFree(g.nbr);
+            cudaFree(g.w);
+            cudaFree(g.erow);
+            g.nbr = nbr2;
+            g.w = w2;
+            g.erow = erow2;
+            g.E = E2;
+            if (E2) {
+                k_fill_erow<<<grid_for(n * 32, TB), TB, 0, c.stream>>>(g.ptr, n, g.erow);
+                SC_LAUNCH_CHECK();
+                c.launches++;
+            }
+        }
+    }
+    finalize(c, g, true);
+}
+
+uint64_t first_bad(Ctx& c, DBuf<unsigned long long>& d) {
+    unsigned long long v = to_host(c, d.get());
+    return (uint64_t)v;
+}
+
+}  // namespace
+
+// from_csr_parts (csr_network.rs:185-256)
+DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint32_t* nbr,
+                         uint64_t n_nbr, const float* w, uint64_t n_w, const double* node_w,
+                         uint64_t n_node_w, bool device_inputs) {
+    if (n_ptr == 0)
+        fail(SC_E_INVALID_CSR, "malformed CSR input: node_ptrs must have at least one element");
+    const uint64_t n = n_ptr - 1;
+    if (n > MAX_NODES) {
+        sc_error_info i{};
+        i.code = SC_E_TOO_MANY_NODES;
+        i.n_nodes = n;
+        fail_info(i);
+    }
+    if (n_nbr != n_w)
+        fail(SC_E_INVALID_CSR, "malformed CSR input: neighbors has %llu entries but weights has %llu",
+             (unsigned long long)n_nbr, (unsigned long long)n_w);
+    const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    std::unique_ptr<DevGraph> g(new DevGraph());
+    galloc(*g, n, n_nbr);
+    SC_CUDA(cudaMemcpyAsync(g->ptr, ptr, n_ptr * sizeof(uint64_t), kind, c.stream));
+    if (n_nbr) {
+        SC_CUDA(cudaMemcpyAsync(g->nbr, nbr, n_nbr * sizeof(uint32_t), kind, c.stream));
+        SC_CUDA(cudaMemcpyAsync(g->w, w, n_nbr * sizeof(float), kind, c.stream));
+    }
+    uint64_t last = to_host(c, g->ptr + n);
+    if (last != n_nbr)
+        fail(SC_E_INVALID_CSR, "malformed CSR input: node_ptrs ends at %llu but there are %llu entries",
+             (unsigned long long)last, (unsigned long long)n_nbr);
+    DBuf<unsigned long long> first(c, 1);
+    const unsigned long long NOBAD = ~0ull;
+    if (n) {
+        h2d(c, first.get(), &NOBAD, 1);
+        k_first_bad_ptr<<<grid_for(n, TB), TB, 0, c.stream>>>(g->ptr, n, first.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        uint64_t v = first_bad(c, first);
+        if (v != NOBAD)
+            fail(SC_E_INVALID_CSR, "malformed CSR input: node_ptrs is not non-decreasing at %llu",
+                 (unsigned long long)v);
+    }
+    if (n_nbr) {
+        h2d(c, first.get(), &NOBAD, 1);
+        k_first_bad_entry<<<grid_for(n_nbr, TB), TB, 0, c.stream>>>(g->nbr, g->w, n_nbr, n,
+                                                                    first.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        uint64_t e = first_bad(c, first);
+        if (e != NOBAD) {
+            uint32_t u;
+            float x;
+            d2h(c, &u, g->nbr + e, 1);
+            d2h(c, &x, g->w + e, 1);
+            sync(c);
+            sc_error_info i{};
+            if ((uint64_t)u >= n) {
+                i.code = SC_E_NODE_INDEX_OUT_OF_RANGE;
+                i.node = u;
+                i.n_nodes = n;
+            } else if (!std::isfinite(x)) {
+                i.code = SC_E_NON_FINITE_WEIGHT;
+                i.edge_from = 0;
+                i.edge_to = u;
+            } else {
+                i.code = SC_E_NEGATIVE_WEIGHT;
+                i.edge_from = 0;
+                i.edge_to = u;
+                i.weight = (double)x;
+            }
+            fail_info(i);
+        }
+    }
+    if (node_w) {
+        if (n_node_w != n) {
+            sc_error_info i{};
+            i.code = SC_E_NODE_WEIGHT_LENGTH_MISMATCH;
+            i.got = n_node_w;
+            i.expected_len = n;
+            fail_info(i);
+        }
+        SC_CUDA(cudaMemcpyAsync(g->node_w, node_w, n * sizeof(double), kind, c.stream));
+        if (n) {
+            h2d(c, first.get(), &NOBAD, 1);
+            k_first_bad_nodew<<<grid_for(n, TB), TB, 0, c.stream>>>(g->node_w, n, first.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+            uint64_t v = first_bad(c, first);
+            if (v != NOBAD) {
+                sc_error_info i{};
+                i.code = SC_E_INVALID_NODE_WEIGHT;
+                i.node = v;
+                d2h(c, &i.weight, g->node_w + v, 1);
+                sync(c);
+                fail_info(i);
+            }
+        }
+    } else if (n) {
+        k_fill_double<<<grid_for(n, TB), TB, 0, c.stream>>>(g->node_w, n, 1.0);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    finish(c, *g);
+    sync(c);
+    return g.release();
+}
+
+namespace {
+// Expands edge i into slots 2i (from,to) and 2i+1 (to,from); loops use one slot.
+__global__ void k_expand_edges(const uint64_t* __restrict__ from, const uint64_t* __restrict__ to,
+                               const double* __restrict__ w, uint64_t m, uint64_t* keys, float* ws) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t a = from[i], b = to[i];
+        float x = __double2float_rn(w[i]);
+        keys[2 * i] = (a << 32) | b;
+        ws[2 * i] = x;
+        keys[2 * i + 1] = a == b ? ~0ull : ((b << 32) | a);
+        ws[2 * i + 1] = x;
+    }
+}
+
+__global__ void k_split_keys(const uint64_t* __restrict__ keys, uint64_t N, uint32_t* rows,
+                             uint32_t* cols) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        rows[i] = (uint32_t)(keys[i] >> 32);
+        cols[i] = (uint32_t)keys[i];
+    }
+}
+}  // namespace
+
+// from_edges_with_node_weights (csr_network.rs:120-167)
+DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint64_t* to,
+                           const double* w, uint64_t m, const double* node_w) {
+    std::unique_ptr<DevGraph> g(new DevGraph());
+    DBuf<unsigned long long> first(c, 1);
+    const unsigned long long NOBAD = ~0ull;
+    if (n > MAX_NODES) {
+        // validate_node_weights runs first (csr_network.rs:128-131)
+        for (uint64_t v = 0; node_w && v < n; ++v) {
+            if (!std::isfinite(node_w[v]) || node_w[v] < 0.0) {
+                sc_error_info i{};
+                i.code = SC_E_INVALID_NODE_WEIGHT;
+                i.node = v;
+                i.weight = node_w[v];
+                fail_info(i);
+            }
+        }
+        sc_error_info i{};
+        i.code = SC_E_TOO_MANY_NODES;
+        i.n_nodes = n;
+        fail_info(i);
+    }
+    DBuf<double> nw(c, n);
+    if (node_w) {
+        h2d(c, nw.get(), node_w, n);
+        if (n) {
+            h2d(c, first.get(), &NOBAD, 1);
+            k_first_bad_nodew<<<grid_for(n, TB), TB, 0, c.stream>>>(nw.get(), n, first.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+            uint64_t v = first_bad(c, first);
+            if (v != NOBAD) {
+                sc_error_info i{};
+                i.code = SC_E_INVALID_NODE_WEIGHT;
+                i.node = v;
+                i.weight = node_w[v];
+                fail_info(i);
+            }
+        }
+    } else if (n) {
+        k_fill_double<<<grid_for(n, TB), TB, 0, c.stream>>>(nw.get(), n, 1.0);
+        c.launches++;
+    }
+    DBuf<uint64_t> df(c, m), dt(c, m);
+    DBuf<double> dw(c, m);
+    h2d(c, df.get(), from, m);
+    h2d(c, dt.get(), to, m);
+    h2d(c, dw.get(), w, m);
+    if (m) {
+        h2d(c, first.get(), &NOBAD, 1);
+        k_first_bad_edge<<<grid_for(m, TB), TB, 0, c.stream>>>(df.get(), dt.get(), dw.get(), m, n,
+                                                               first.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        uint64_t i0 = first_bad(c, first);
+        if (i0 != NOBAD) {
+            sc_error_info i{};
+            uint64_t a = from[i0], b = to[i0];
+            double x = w[i0];
+            if (a >= n) {
+                i.code = SC_E_NODE_INDEX_OUT_OF_RANGE;
+                i.node = a;
+                i.n_nodes = n;
+            } else if (b >= n) {
+                i.code = SC_E_NODE_INDEX_OUT_OF_RANGE;
+                i.node = b;
+                i.n_nodes = n;
+            } else if (!std::isfinite(x)) {
+                i.code = SC_E_NON_FINITE_WEIGHT;
+                i.edge_from = a;
+                i.edge_to = b;
+            } else {
+                i.code = SC_E_NEGATIVE_WEIGHT;
+                i.edge_from = a;
+                i.edge_to = b;
+                i.weight = x;
+            }
+            fail_info(i);
+        }
+    }
+    // scatter into both rows in edge order, then a stable sort by (row, neighbour)
+    DBuf<uint64_t> keys(c, 2 * m), keys_s(c, 2 * m);
+    DBuf<float> ws(c, 2 * m), ws_s(c, 2 * m);
+    if (m) {
+        k_expand_edges<<<grid_for(m, TB), TB, 0, c.stream>>>(df.get(), dt.get(), dw.get(), m,
+                                                             keys.get(), ws.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        sort_pairs(c, keys.get(), keys_s.get(), ws.get(), ws_s.get(), 2 * m, 64);
+    }
+    // entries with key ~0 (the unused slots of self-loops) sort to the end
+    uint64_t loops_slots = 0;
+    for (uint64_t i = 0; i < m; ++i) loops_slots += from[i] == to[i];
+    const uint64_t E = 2 * m - loops_slots;
+    galloc(*g, n, E);
+    d2d(c, g->node_w, nw.get(), n);
+    if (E) {
+        k_split_keys<<<grid_for(E, TB), TB, 0, c.stream>>>(keys_s.get(), E, g->erow, g->nbr);
+        SC_LAUNCH_CHECK();
+        d2d(c, g->w, ws_s.get(), E);
+        k_starts_from_sorted<<<grid_for(E + 1, TB), TB, 0, c.stream>>>(g->erow, E, n, g->ptr);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    } else {
+        zero(c, g->ptr, n + 1);
+    }
+    finish(c, *g);
+    sync(c);
+    return g.release();
+}
+
+// ------------------------------------------------------------ aggregate
+namespace {
+
+__global__ void k_iota(uint32_t* p, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = (uint32_t)i;
+}
+
+// Per group, in ascending member order: Σ node weight (csr_network.rs:520-523)
+// and Σ self-loop weight (the `self_loop_weight` accumulator of :549-554).
+__global__ void k_group_sums(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
+                             uint64_t G, const double* __restrict__ node_w,
+                             const double* __restrict__ self_loop, double* nw_out, double* loops_out) {
+    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < G;
+         gi += (uint64_t)gridDim.x * blockDim.x) {
+        double a = 0.0, l = 0.0;
+        for (uint64_t i = gstart[gi]; i < gstart[gi + 1]; ++i) {
+            uint32_t v = members[i];
+            a = __dadd_rn(a, node_w[v]);
+            l = __dadd_rn(l, self_loop[v]);
+        }
+        nw_out[gi] = a;
+        loops_out[gi] = l;
+    }
+}
+
+// Entries whose neighbour's group is >= the row's group, keyed by (g, h).
+__global__ void k_group_keys(const uint32_t* __restrict__ erow, const uint32_t* __restrict__ nbr,
+                             const uint32_t* __restrict__ grp, uint64_t E, uint64_t G,
+                             uint64_t* keys, uint8_t* flags) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t g = grp[erow[e]], h = grp[nbr[e]];
+        keys[e] = g * G + h;
+        flags[e] = h >= g;
+    }
+}
+
+__global__ void k_seg_heads(const uint64_t* __restrict__ keys, uint64_t N, uint8_t* head) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        head[i] = (i == 0 || keys[i] != keys[i - 1]);
+}
+
+__global__ void k_iota64(uint64_t* p, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = i;
+}
+
+// One thread per (g, h) segment: acc in (member asc, neighbour asc) order; the
+// pair rule of csr_network.rs:566-581 then finish's zero drop (:304).
+__global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
+                             const uint64_t* __restrict__ keys, const float* __restrict__ w,
+                             uint64_t G, const double* __restrict__ loops, uint32_t* prow,
+                             uint32_t* pcol, float* pw, uint8_t* keep) {
+    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < P;
+         s += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
+        double acc = 0.0;
+        for (uint64_t i = b; i < e; ++i) acc = __dadd_rn(acc, (double)w[i]);
+        uint64_t key = keys[b];
+        uint32_t g = (uint32_t)(key / G), h = (uint32_t)(key % G);
+        float val;
+        if (h == g) val = __double2float_rn(__dmul_rn(0.5, __dadd_rn(acc, loops[g])));
+        else val = __double2float_rn(acc);
+        prow[s] = g;
+        pcol[s] = h;
+        pw[s] = val;
+        keep[s] = (acc > 0.0) && ((double)val != 0.0);
+    }
+}
+
+// Mirror keys (h, g) of the kept off-diagonal pairs.
+__global__ void k_mirror(const uint32_t* __restrict__ prow, const uint32_t* __restrict__ pcol,
+                         const float* __restrict__ pw, uint64_t P, uint64_t G, uint64_t* mkeys,
+                         float* mw, uint8_t* mflag) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < P;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t g = prow[i], h = pcol[i];
+        mkeys[i] = h * G + g;
+        mw[i] = pw[i];
+        mflag[i] = h != g;
+    }
+}
+
+__global__ void k_key_rows(const uint64_t* __restrict__ keys, uint64_t N, uint64_t G, uint32_t* rows,
+                           uint32_t* cols) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        rows[i] = (uint32_t)(keys[i] / G);
+        cols[i] = (uint32_t)(keys[i] % G);
+    }
+}
+
+__global__ void k_row_counts(const uint64_t* __restrict__ ls, const uint64_t* __restrict__ us,
+                             uint64_t G, uint64_t* cnt) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < G;
+         r += (uint64_t)gridDim.x * blockDim.x)
+        cnt[r] = (ls[r + 1] - ls[r]) + (us[r + 1] - us[r]);
+}
+
+// Row r of the coarse CSR: its lower pairs (ascending g < r) then its diagonal
+// and upper pairs (ascending h >= r) — already the order finish sorts to.
+__global__ void k_row_assemble(const uint64_t* __restrict__ ptr, const uint64_t* __restrict__ ls,
+                               const uint32_t* __restrict__ lcol, const float* __restrict__ lw,
+                               const uint64_t* __restrict__ us, const uint32_t* __restrict__ ucol,
+                               const float* __restrict__ uw, uint64_t G, uint32_t* nbr, float* w) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = warp; r < G; r += nw) {
+        uint64_t o = ptr[r];
+        uint64_t l0 = ls[r], l1 = ls[r + 1], u0 = us[r], u1 = us[r + 1];
+        for (uint64_t i = l0 + lane; i < l1; i += 32) {
+            nbr[o + (i - l0)] = lcol[i];
+            w[o + (i - l0)] = lw[i];
+        }
+        o += l1 - l0;
+        for (uint64_t i = u0 + lane; i < u1; i += 32) {
+            nbr[o + (i - u0)] = ucol[i];
+            w[o + (i - u0)] = uw[i];
+        }
+    }
+}
+
+}  // namespace
+
+// aggregate (csr_network.rs:516-608): d_grp holds ids already normalised to [0, G).
+DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t G) {
+    const uint64_t n = g.n, E = g.E;
+    std::unique_ptr<DevGraph> out(new DevGraph());
+    // members of each group in ascending node order
+    DBuf<uint32_t> idx(c, n), grp_s(c, n), members(c, n);
+    DBuf<uint64_t> gstart(c, (uint64_t)G + 1);
+    DBuf<double> nw_new(c, G), loops(c, G);
+    if (n) {
+        k_iota<<<grid_for(n, TB), TB, 0, c.stream>>>(idx.get(), n);
+        c.launches++;
+        sort_pairs(c, d_grp, grp_s.get(), idx.get(), members.get(), n, bits_for(G));
+        k_starts_from_sorted<<<grid_for(n + 1, TB), TB, 0, c.stream>>>(grp_s.get(), n, G, gstart.get());
+        k_group_sums<<<grid_for(G, TB), TB, 0, c.stream>>>(gstart.get(), members.get(), G, g.node_w,
+                                                           g.self_loop, nw_new.get(), loops.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    idx.release();
+    grp_s.release();
+    members.release();
+    gstart.release();
+
+    // (g, h >= g) entries in CSR order, stably sorted by (g, h)
+    uint64_t N = 0;
+    DBuf<uint64_t> ukeys, ukeys_s;
+    DBuf<float> uw, uw_s;
+    if (E) {
+        DBuf<uint64_t> keys(c, E);
+        DBuf<uint8_t> flags(c, E);
+        k_group_keys<<<grid_for(E, TB), TB, 0, c.stream>>>(g.erow, g.nbr, d_grp, E, G, keys.get(),
+                                                           flags.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        ukeys.alloc(c, E);
+        uw.alloc(c, E);
+        DBuf<uint64_t> cnt(c, 1);
+        select_flagged(c, keys.get(), flags.get(), ukeys.get(), cnt.get(), E);
+        select_flagged(c, g.w, flags.get(), uw.get(), cnt.get(), E);
+        N = to_host(c, cnt.get());
+        ukeys_s.alloc(c, N);
+        uw_s.alloc(c, N);
+        sort_pairs(c, ukeys.get(), ukeys_s.get(), uw.get(), uw_s.get(), N,
+                   bits_for((uint64_t)G * G - 1));
+        ukeys.release();
+        uw.release();
+    }
+    // segments = distinct (g, h)
+    uint64_t P = 0;
+    DBuf<uint32_t> prow, pcol;
+    DBuf<float> pw;
+    DBuf<uint8_t> keep;
+    if (N) {
+        DBuf<uint8_t> head(c, N);
+        k_seg_heads<<<grid_for(N, TB), TB, 0, c.stream>>>(ukeys_s.get(), N, head.get());
+        c.launches++;
+        DBuf<uint64_t> iota(c, N), seg(c, N), cnt(c, 1);
+        k_iota64<<<grid_for(N, TB), TB, 0, c.stream>>>(iota.get(), N);
+        c.launches++;
+        select_flagged(c, iota.get(), head.get(), seg.get(), cnt.get(), N);
+        P = to_host(c, cnt.get());
+        prow.alloc(c, P);
+        pcol.alloc(c, P);
+        pw.alloc(c, P);
+        keep.alloc(c, P);
+        k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
+                                                           uw_s.get(), G, loops.get(), prow.get(),
+                                                           pcol.get(), pw.get(), keep.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    ukeys_s.release();
+    uw_s.release();
+    // kept pairs, still in (g, h) order: the upper triangle incl. diagonal
+    uint64_t K = 0;
+    DBuf<uint32_t> krow, kcol;
+    DBuf<float> kw;
+    if (P) {
+        krow.alloc(c, P);
+        kcol.alloc(c, P);
+        kw.alloc(c, P);
+        DBuf<uint64_t> cnt(c, 1);
+        select_flagged(c, prow.get(), keep.get(), krow.get(), cnt.get(), P);
+        select_flagged(c, pcol.get(), keep.get(), kcol.get(), cnt.get(), P);
+        select_flagged(c, pw.get(), keep.get(), kw.get(), cnt.get(), P);
+        K = to_host(c, cnt.get());
+    }
+    prow.release();
+    pcol.release();
+    pw.release();
+    keep.release();
+    // lower triangle: mirrored off-diagonal pairs sorted by (h, g)
+    uint64_t L = 0;
+    DBuf<uint32_t> lrow, lcol;
+    DBuf<float> lw;
+    if (K) {
+        DBuf<uint64_t> mk(c, K), mk_c(c, K), mk_s(c, K);
+        DBuf<float> mw(c, K), mw_c(c, K);
+        DBuf<uint8_t> mf(c, K);
+        k_mirror<<<grid_for(K, TB), TB, 0, c.stream>>>(krow.get(), kcol.get(), kw.get(), K, G,
+                                                       mk.get(), mw.get(), mf.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        DBuf<uint64_t> cnt(c, 1);
+        select_flagged(c, mk.get(), mf.get(), mk_c.get(), cnt.get(), K);
+        select_flagged(c, mw.get(), mf.get(), mw_c.get(), cnt.get(), K);
+        L = to_host(c, cnt.get());
+        lw.alloc(c, L);
+        sort_pairs(c, mk_c.get(), mk_s.get(), mw_c.get(), lw.get(), L,
+                   bits_for((uint64_t)G * G - 1));
+        lrow.alloc(c, L);
+        lcol.alloc(c, L);
+        if (L) {
+            k_key_rows<<<grid_for(L, TB), TB, 0, c.stream>>>(mk_s.get(), L, G, lrow.get(), lcol.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+        }
+    }
+    // assemble
+    const uint64_t E2 = K + L;
+    galloc(*out, G, E2);
+    d2d(c, out->node_w, nw_new.get(), G);
+    {
+        DBuf<uint64_t> us(c, (uint64_t)G + 1), ls(c, (uint64_t)G + 1), cnt(c, (uint64_t)G + 1);
+        k_starts_from_sorted<<<grid_for(K + 1, TB), TB, 0, c.stream>>>(krow.get(), K, G, us.get());
+        k_starts_from_sorted<<<grid_for(L + 1, TB), TB, 0, c.stream>>>(lrow.get(), L, G, ls.get());
+        SC_LAUNCH_CHECK();
+        k_row_counts<<<grid_for(G, TB), TB, 0, c.stream>>>(ls.get(), us.get(), G, cnt.get());
+        zero(c, cnt.get() + G, 1);
+        exclusive_sum(c, cnt.get(), out->ptr, (uint64_t)G + 1);
+        if (E2) {
+            k_row_assemble<<<grid_for((uint64_t)G * 32, TB), TB, 0, c.stream>>>(
+                out->ptr, ls.get(), lcol.get(), lw.get(), us.get(), kcol.get(), kw.get(), G,
+                out->nbr, out->w);
+            SC_LAUNCH_CHECK();
+            k_fill_erow<<<grid_for((uint64_t)G * 32, TB), TB, 0, c.stream>>>(out->ptr, G, out->erow);
+            SC_LAUNCH_CHECK();
+            c.launches += 2;
+        }
+        c.launches += 3;
+    }
+    // aggregate cannot fail in the reference (csr_network.rs:605-607)
+    try {
+        finalize(c, *out, true);
+    } catch (Failure& f) {
+        if (f.info.code == SC_E_ASYMMETRIC_GRAPH) {
+            f.info.code = SC_E_INTERNAL;
+            std::snprintf(f.info.message, sizeof f.info.message,
+                          "aggregate produced a graph failing the degree-sum check");
+        }
+        throw;
+    }
+    sync(c);
+    return out.release();
+}
+
+// ------------------------------------------------------------ symmetry
+namespace {
+// validate_symmetry (csr_network.rs:627-646) with edge_weight's shorter-row
+// search (:465-478): first failing stored entry, as its index.
+__global__ void k_symmetry(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                           const float* __restrict__ w, const uint32_t* __restrict__ erow,
+                           uint64_t E, unsigned long long* first) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t v = erow[e], u = nbr[e];
+        double x = (double)w[e];
+        // edge_weight(u, v)
+        uint64_t du = ptr[u + 1] - ptr[u], dv = ptr[v + 1] - ptr[v];
+        uint32_t s = du <= dv ? u : v, t = du <= dv ? v : u;
+        uint64_t lo = ptr[s], hi = ptr[s + 1];
+        while (lo < hi) {
+            uint64_t mid = (lo + hi) >> 1;
+            if (nbr[mid] < t) lo = mid + 1;
+            else hi = mid;
+        }
+        bool found = lo < ptr[s + 1] && nbr[lo] == t;
+        bool ok = found && fabs((double)w[lo] - x) <= 1e-6 * fmax(fabs(x), 1.0);
+        if (!ok) atomicMin(first, (unsigned long long)e);
+    }
+}
+}  // namespace
+
+void graph_validate_symmetry(Ctx& c, const DevGraph& g) {
+    if (g.E == 0) return;
+    DBuf<unsigned long long> first(c, 1);
+    const unsigned long long NOBAD = ~0ull;
+    h2d(c, first.get(), &NOBAD, 1);
+    k_symmetry<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, first.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    uint64_t e = first_bad(c, first);
+    if (e == NOBAD) return;
+    // re-derive the message on the host from the few values involved
+    uint32_t v, u;
+    float x;
+    d2h(c, &v, g.erow + e, 1);
+    d2h(c, &u, g.nbr + e, 1);
+    d2h(c, &x, g.w + e, 1);
+    uint64_t pu[2], pv[2];
+    sync(c);
+    d2h(c, pu, g.ptr + u, 2);
+    d2h(c, pv, g.ptr + v, 2);
+    sync(c);
+    uint64_t du = pu[1] - pu[0], dv = pv[1] - pv[0];
+    uint32_t s = du <= dv ? u : v, t = du <= dv ? v : u;
+    uint64_t lo = du <= dv ? pu[0] : pv[0], hi = du <= dv ? pu[1] : pv[1];
+    std::vector<uint32_t> row(hi - lo);
+    std::vector<float> rw(hi - lo);
+    d2h(c, row.data(), g.nbr + lo, hi - lo);
+    d2h(c, rw.data(), g.w + lo, hi - lo);
+    sync(c);
+    (void)s;
+    auto it = std::lower_bound(row.begin(), row.end(), t);
+    if (it == row.end() || *it != t)
+        fail(SC_E_INVALID_CSR,
+             "malformed CSR input: edge (%u, %u) is present but (%u, %u) is missing", v, u, u, v);
+    double back = (double)rw[it - row.begin()];
+    fail(SC_E_INVALID_CSR, "malformed CSR input: edge (%u, %u) has weight %s but (%u, %u) has %s", v,
+         u, fmt_f64((double)x).c_str(), u, v, fmt_f64(back).c_str());
+}
+
+void graph_copy_csr(Ctx& c, const DevGraph& g, uint64_t* ptr, uint32_t* nbr, float* w) {
+    if (ptr) d2h(c, ptr, g.ptr, g.n + 1);
+    if (nbr) d2h(c, nbr, g.nbr, g.E);
+    if (w) d2h(c, w, g.w, g.E);
+    sync(c);
+}
+
+void graph_copy_node_data(Ctx& c, const DevGraph& g, double* node_w, double* strength) {
+    if (node_w) d2h(c, node_w, g.node_w, g.n);
+    if (strength) d2h(c, strength, g.strength, g.n);
+    sync(c);
+}
+
+}  // namespace sc

@@ -1,0 +1,252 @@
+// sc_internal.cuh — shared definitions of the sm_100a Leiden / kNN library.
+//
+// The whole library is compiled with -fmad=false: Rust never contracts a*b+c
+// into an FMA, and the parity functions (finish, aggregate, partition
+// aggregates, quality, modularity) must reproduce its f64 results bit for bit.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <memory>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/sc_gpu.h"
+
+namespace sc {
+
+constexpr uint32_t UNASSIGNED = 0xFFFFFFFFu;
+constexpr uint32_t NONE32 = 0xFFFFFFFFu;
+constexpr uint64_t MAX_NODES = 0xFFFFFFFFull;  // csr_network.rs:36
+
+// Device status word bits (written by guarded kernels, read by the host).
+enum DevStatus : uint32_t {
+    DEV_OK = 0,
+    DEV_BOUNDS = 1u << 0,    // an index check failed; the access was skipped
+    DEV_TIMEOUT = 1u << 1,   // a bounded wait gave up
+    DEV_OVERFLOW = 1u << 2,  // a capacity was exceeded
+};
+
+// ------------------------------------------------------------------ errors
+struct Error {
+    sc_status code = SC_OK;
+    sc_error_info info{};
+};
+
+// Thrown inside the library, caught at the C ABI boundary. `info.code` is the
+// status and `info.message` the Display text of the matching ClusteringError.
+struct Failure {
+    sc_error_info info;
+};
+
+[[noreturn]] void throw_cuda(cudaError_t e, const char* what, const char* file, int line);
+[[noreturn]] void fail(sc_status code, const char* fmt, ...);
+[[noreturn]] void fail_info(sc_error_info info);  // formats info.message from the payload
+
+#define SC_CUDA(call)                                                      \
+    do {                                                                   \
+        cudaError_t _e = (call);                                           \
+        if (_e != cudaSuccess) ::sc::throw_cuda(_e, #call, __FILE__, __LINE__); \
+    } while (0)
+
+#define SC_LAUNCH_CHECK() SC_CUDA(cudaGetLastError())
+
+// ------------------------------------------------------------------ context
+struct Ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    uint32_t* d_status = nullptr;      // device status word
+    Error last;
+    sc_run_stats stats{};
+    uint64_t launches = 0;             // kernels launched by the current call
+    int sm_count = 148;
+    size_t smem_optin = 0;
+};
+
+// Stream-ordered device buffer of T (cudaMallocAsync on the context stream).
+template <class T>
+struct DBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    cudaStream_t s = nullptr;
+    DBuf() = default;
+    DBuf(Ctx& c, size_t count) { alloc(c, count); }
+    void alloc(Ctx& c, size_t count) {
+        release();
+        s = c.stream;
+        n = count;
+        if (count) {
+            cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), s);
+            if (e == cudaErrorMemoryAllocation) {
+                cudaGetLastError();
+                fail(SC_E_OUT_OF_MEMORY, "device allocation of %zu bytes failed", count * sizeof(T));
+            }
+            if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
+        }
+    }
+    void release() {
+        if (p) cudaFreeAsync(p, s);
+        p = nullptr;
+        n = 0;
+    }
+    ~DBuf() { release(); }
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    DBuf(DBuf&& o) noexcept : p(o.p), n(o.n), s(o.s) { o.p = nullptr; o.n = 0; }
+    DBuf& operator=(DBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            s = o.s;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    T* get() const { return p; }
+    size_t bytes() const { return n * sizeof(T); }
+};
+
+// ------------------------------------------------------------------ graph
+// Device-resident CSRNetworkData (csr_network.rs:38-60) plus cached per-node
+// self-loop weights and the row id of every stored entry.
+struct DevGraph {
+    int device = 0;
+    uint64_t n = 0;           // node_count
+    uint64_t E = 0;           // stored entries
+    uint64_t* ptr = nullptr;  // n+1
+    uint32_t* nbr = nullptr;  // E, strictly increasing per row
+    float* w = nullptr;       // E
+    uint32_t* erow = nullptr; // E, row of each entry
+    double* node_w = nullptr; // n
+    double* strength = nullptr;   // n
+    double* self_loop = nullptr;  // n (0.0 where there is none)
+    double total_weight = 0.0;
+    uint64_t edge_count = 0;
+    bool any_self_loops = false;
+    uint32_t max_degree = 0;
+    // exact-summation regime (every subset sum of edge weights is exact in f64)
+    int e0_w = 0;             // exponent of the lowest set bit over stored weights
+    bool exact_w = true;
+    int e0_nw = 0;            // same over node weights
+    bool exact_nw = true;
+    double total_node_weight = 0.0;  // Σ node_w, Rust `sum()` order
+    void free_all();
+    ~DevGraph() { free_all(); }
+};
+
+// ------------------------------------------------------------------ helpers
+inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 148u * 16u) {
+    uint64_t g = (work + block - 1) / block;
+    if (g < 1) g = 1;
+    if (g > cap) g = cap;
+    return (unsigned)g;
+}
+
+__host__ __device__ inline uint64_t splitmix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+__host__ __device__ inline uint64_t hash3(uint64_t seed, uint64_t a, uint64_t b) {
+    return splitmix(splitmix(splitmix(seed) ^ a) ^ b);
+}
+
+// Exponent of the lowest set bit of a finite non-zero value (INT32_MAX for 0).
+__host__ __device__ inline int lowbit_exp_f32(float x) {
+    uint32_t b;
+    memcpy(&b, &x, 4);
+    b &= 0x7FFFFFFFu;
+    if (b == 0) return 0x7FFFFFFF;
+    int e = (int)(b >> 23);
+    uint32_t m = b & 0x7FFFFFu;
+#ifdef __CUDA_ARCH__
+    if (e == 0) return -149 + (__ffs((int)m) - 1);
+    m |= 0x800000u;
+    return (e - 150) + (__ffs((int)m) - 1);
+#else
+    if (e == 0) return -149 + __builtin_ctz(m);
+    m |= 0x800000u;
+    return (e - 150) + __builtin_ctz(m);
+#endif
+}
+__host__ __device__ inline int lowbit_exp_f64(double x) {
+    uint64_t b;
+    memcpy(&b, &x, 8);
+    b &= 0x7FFFFFFFFFFFFFFFull;
+    if (b == 0) return 0x7FFFFFFF;
+    int e = (int)(b >> 52);
+    uint64_t m = b & 0xFFFFFFFFFFFFFull;
+#ifdef __CUDA_ARCH__
+    if (e == 0) return -1074 + (__ffsll((long long)m) - 1);
+    m |= 0x10000000000000ull;
+    return (e - 1075) + (__ffsll((long long)m) - 1);
+#else
+    if (e == 0) return -1074 + __builtin_ctzll(m);
+    m |= 0x10000000000000ull;
+    return (e - 1075) + __builtin_ctzll(m);
+#endif
+}
+
+// ------------------------------------------------------------------ API of the .cu files
+// graph.cu
+DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint32_t* nbr,
+                         uint64_t n_nbr, const float* w, uint64_t n_w, const double* node_w,
+                         uint64_t n_node_w, bool device_inputs);
+DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint64_t* to,
+                           const double* w, uint64_t m, const double* node_w);
+DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t n_groups);
+void graph_validate_symmetry(Ctx& c, const DevGraph& g);
+void graph_copy_csr(Ctx& c, const DevGraph& g, uint64_t* ptr, uint32_t* nbr, float* w);
+void graph_copy_node_data(Ctx& c, const DevGraph& g, double* node_w, double* strength);
+
+// partition.cu
+// Normalises arbitrary u64 labels (host) to ascending-rank ids on the device.
+uint32_t renumber_u64_labels(Ctx& c, const uint64_t* d_labels, uint64_t n, uint32_t* d_out,
+                             uint64_t* max_label_out);
+// ascending-rank renumber of u32 ids < id_space; returns the number of distinct ids.
+uint32_t renumber_ids(Ctx& c, const uint32_t* d_ids, uint64_t n, uint64_t id_space, uint32_t* d_out);
+struct PartStats {
+    uint64_t slots = 0;
+    DBuf<uint32_t> size;
+    DBuf<double> weight, strength, internal;
+};
+void partition_stats(Ctx& c, const DevGraph& g, const uint32_t* d_memb, uint64_t slots,
+                     PartStats& out, bool need_internal);
+// Σ terms in index order, as Rust's `Iterator::sum` (fold from -0.0).
+double ordered_sum(Ctx& c, const double* d_terms, uint64_t n);
+// ((init + t0) + t1) + ... in index order.
+double ordered_sum_from(Ctx& c, const double* d_terms, uint64_t n, double init);
+double quality(Ctx& c, const DevGraph& g, const uint32_t* d_memb, uint64_t slots, int objective,
+               double gamma);
+double modularity(Ctx& c, const DevGraph& g, const uint32_t* d_labels, uint64_t n_comms,
+                  double gamma);
+
+// leiden.cu
+struct LeidenOut {
+    std::vector<uint32_t> labels;
+    uint64_t n_clusters = 0;
+};
+void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64_t* initial_host,
+            uint32_t* d_labels_out, uint64_t* n_clusters);
+
+// knn.cu
+void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k,
+                  const sc_knn_opts& opts, uint32_t* knn_index, float* knn_dist,
+                  uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w, uint64_t conn_cap,
+                  uint64_t* conn_nnz, DevGraph** graph_out);
+
+// common.cu
+void check_device_status(Ctx& c);
+// Rust-style shortest round-trip text of an f64 (Display of f64).
+std::string fmt_f64(double x);
+
+}  // namespace sc

@@ -1,0 +1,1213 @@
+// sc_leiden.cu — parallel Leiden on sm_100a: local moving, refinement and the
+// level / pass driver of src/community_search/leiden/mod.rs:168-289.
+//
+// Local moving (local_move.rs:39-122) becomes synchronous sweeps over the
+// active nodes, split into B hash batches. Inside a batch every node scores
+// its candidates against a snapshot (decide kernels), then one kernel commits
+// the moves (apply). A move into a singleton community whose sole member is
+// moving in the same batch is cancelled — for a mutual pair the lower seeded
+// priority yields — so two singletons never swap past each other.
+//
+// Community aggregates (K_c, node weight n_c, size) are int64 fixed point:
+// integer atomics are associative, so a fixed seed gives bit-identical runs.
+// In the exact regime the fixed-point values are the f64 values themselves.
+//
+// Degree buckets: a group of G = 8 / 16 / 32 lanes per node for degree <= G
+// (neighbour communities merged with __match_any_sync, no shared memory);
+// one 256-thread block per node above that, with an open-addressing hash in
+// shared memory (global memory past its capacity).
+#include <random>
+
+#include "sc_prims.cuh"
+
+namespace sc {
+
+namespace {
+
+constexpr unsigned TB = 256;
+constexpr int NBUCKET = 4;          // G8, G16, G32, block
+constexpr int HCAP_SMEM = 4096;     // shared hash entries per block (u32 key + i64 val)
+constexpr int LM_BATCHES = 8;
+constexpr int RF_BATCHES = 8;
+constexpr int MAX_SWEEPS = 100;
+constexpr uint32_t EMPTYK = 0xFFFFFFFFu;
+constexpr int REF_CAND_SMEM = 2048;  // candidates sorted in shared memory per block
+
+struct Params {
+    // graph
+    const uint64_t* ptr;
+    const uint32_t* nbr;
+    const float* w;
+    const double* strength;
+    const double* node_w;
+    const double* self_loop;
+    // partition being changed (working partition or refined partition)
+    uint32_t* memb;
+    long long* Kf;
+    long long* Wf;
+    uint32_t* csize;
+    // refinement only: the constraint (working membership)
+    const uint32_t* constraint;
+    // decisions
+    uint32_t* tgt;
+    uint32_t* hint;
+    uint32_t* from;
+    long long* dgain;
+    uint32_t* epoch;
+    uint32_t cur;
+    uint64_t S0;           // fresh-community id base (local moving)
+    // objective
+    int objective;
+    double gamma, four_m, thr;
+    double scale, inv_scale;    // 2^F, 2^-F for edge-weight quantities
+    double nscale, inv_nscale;  // same for node weights
+    int has_limit;
+    double limit;
+    double theta;               // refinement randomness (<= 0: argmax)
+    uint64_t seed;
+    uint32_t* status;
+    unsigned long long* counters;  // [0] moves, [1] Σdeg, [2] Σcand, [3] nodes
+    long long* gain_acc;
+};
+
+__device__ __forceinline__ long long to_fix(double x, double inv) { return __double2ll_rn(__dmul_rn(x, inv)); }
+__device__ __forceinline__ double from_fix(long long q, double s) { return __dmul_rn(__ll2double_rn(q), s); }
+
+// Rb::delta_insert (objective.rs:91-106) / Cpm::delta_insert (:158-169)
+__device__ __forceinline__ double gain_of(const Params& p, double wto, double sl, double k, double kc,
+                                          double a, double nc) {
+    if (p.objective == SC_OBJECTIVE_RB) {
+        if (p.four_m == 0.0) return 0.0;
+        return __dsub_rn(__dadd_rn(wto, sl),
+                         __ddiv_rn(__dmul_rn(__dmul_rn(p.gamma, k), __dadd_rn(__dmul_rn(2.0, kc), k)),
+                                   p.four_m));
+    }
+    return __dsub_rn(__dadd_rn(wto, sl),
+                     __ddiv_rn(__dmul_rn(__dmul_rn(p.gamma, a),
+                                         __dsub_rn(__dadd_rn(__dmul_rn(2.0, nc), a), 1.0)),
+                               2.0));
+}
+
+__device__ __forceinline__ bool better(double g, uint32_t c, double bg, uint32_t bc) {
+    return g > bg || (g == bg && c < bc);
+}
+
+__device__ __forceinline__ uint64_t prio(uint64_t seed, uint32_t ep, uint32_t v) {
+    return hash3(seed ^ 0xA5A5A5A5DEADBEEFull, ep, v);
+}
+
+// Whether node x's move (decided in epoch p.cur) is cancelled.
+__device__ __forceinline__ bool cancelled(const Params& p, uint32_t x) {
+    uint32_t h = p.hint[x];
+    if (h == NONE32) return false;
+    if (p.epoch[h] != p.cur) return false;  // the target's member is not moving
+    if (p.hint[h] == x) {                   // mutual: the lower priority yields
+        uint64_t px = prio(p.seed, p.cur, x), ph = prio(p.seed, p.cur, h);
+        return px < ph || (px == ph && x < h);
+    }
+    return true;
+}
+
+__device__ __forceinline__ double uniform01(uint64_t seed, uint64_t a, uint64_t b) {
+    return (double)(hash3(seed ^ 0x5151515151515151ull, a, b) >> 11) * 0x1.0p-53;
+}
+
+// Warp-aggregated counter add.
+__device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long long x) {
+    for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+    if ((threadIdx.x & 31) == 0 && x) atomicAdd(ctr, x);
+}
+
+// ------------------------------------------------------------ small-degree decide
+// REFINE=false: local moving. REFINE=true: refinement (singletons only, inside
+// the constraint, randomised choice among non-negative candidates).
+template <int G, bool REFINE>
+__global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* __restrict__ list,
+                                                     uint32_t count) {
+    __shared__ uint32_t s_c[TB];
+    __shared__ double s_r[TB];
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & (G - 1);
+    const int gw = lane / G;  // group within warp
+    const int gbase = gw * G;
+    const unsigned gmask = (G == 32) ? FULL : (((1u << G) - 1u) << gbase);
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const int per_warp = 32 / G;
+    unsigned long long sdeg = 0, scand = 0, snodes = 0;
+
+    for (uint64_t wb = warp * per_warp; wb < count; wb += nwarps * per_warp) {
+        const uint64_t i = wb + gw;
+        const bool have = i < count;
+        const uint32_t v = have ? list[i] : 0;
+        uint64_t b = 0, e = 0;
+        if (have) {
+            b = p.ptr[v];
+            e = p.ptr[v + 1];
+        }
+        const int deg = (int)(e - b);
+        const uint32_t own = have ? p.memb[v] : 0;
+        bool eligible = have;
+        if (REFINE && have) eligible = p.csize[own] == 1;  // refine.rs:60-62
+        bool valid = eligible && sub < deg;
+        uint32_t u = 0;
+        float wt = 0.0f;
+        if (valid) {
+            u = p.nbr[b + sub];
+            wt = p.w[b + sub];
+        }
+        valid = valid && u != v;
+        if (REFINE && valid) valid = p.constraint[u] == p.constraint[v];
+        const uint32_t cu = valid ? p.memb[u] : NONE32;
+        const long long wf = valid ? to_fix((double)wt, p.inv_scale) : 0;
+        const uint64_t key = valid ? (((uint64_t)gw << 32) | cu) : (0xFFFFFFFF00000000ull | (uint64_t)lane);
+        const unsigned mm = __match_any_sync(FULL, key);
+        const bool leader = valid && (__ffs(mm) - 1 == lane);
+        long long acc = 0;
+#pragma unroll
+        for (int t = 0; t < G; ++t) {
+            long long x = __shfl_sync(FULL, wf, gbase + t);
+            if ((mm >> (gbase + t)) & 1u) acc += x;
+        }
+        // node quantities (identical in all lanes of the group)
+        long long kf = 0, af = 0;
+        double sl = 0.0;
+        if (eligible) {
+            kf = to_fix(p.strength[v], p.inv_scale);
+            af = to_fix(p.node_w[v], p.inv_nscale);
+            sl = p.self_loop[v];
+        }
+        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale);
+        // weight to the own community
+        unsigned ob = __ballot_sync(FULL, leader && cu == own) & gmask;
+        long long wof = __shfl_sync(FULL, acc, ob ? (__ffs(ob) - 1) : lane);
+        if (!ob) wof = 0;
+        double base = 0.0;
+        if (eligible) {
+            base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale), a,
+                           from_fix(p.Wf[own] - af, p.nscale));
+        }
+        // candidates held by leader lanes
+        double g = -INFINITY;
+        uint32_t c = NONE32, cu_member = NONE32;
+        bool cand = false;
+        if (leader && cu != own) {
+            double nc = from_fix(p.Wf[cu], p.nscale);
+            if (!p.has_limit || __dadd_rn(nc, a) <= p.limit) {
+                g = gain_of(p, from_fix(acc, p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+                if (REFINE) {
+                    double rel = __dsub_rn(g, base);
+                    if (rel >= 0.0) {
+                        cand = true;
+                        g = rel;
+                    } else {
+                        g = -INFINITY;
+                    }
+                } else {
+                    cand = true;
+                }
+                if (cand) {
+                    c = cu;
+                    cu_member = u;
+                }
+            }
+        }
+        if (sub == 0 && eligible) {
+            snodes += 1;
+            sdeg += (unsigned long long)deg;
+        }
+        scand += (leader && cu != own) ? 1ull : 0ull;
+        if (!REFINE) {
+            // argmax over the group: higher gain, then lower id
+#pragma unroll
+            for (int o = G / 2; o; o >>= 1) {
+                double og = __shfl_xor_sync(FULL, g, o);
+                uint32_t oc = __shfl_xor_sync(FULL, c, o);
+                uint32_t om = __shfl_xor_sync(FULL, cu_member, o);
+                if (better(og, oc, g, c)) {
+                    g = og;
+                    c = oc;
+                    cu_member = om;
+                }
+            }
+            if (sub == 0 && eligible) {
+                uint32_t best = own;
+                double bg = base;
+                if (c != NONE32 && better(g, c, bg, best)) {
+                    best = c;
+                    bg = g;
+                }
+                // one empty community per node (local_move.rs:92-100)
+                const uint32_t fresh = (uint32_t)(p.S0 + v);
+                if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 &&
+                    (!p.has_limit || a <= p.limit)) {
+                    double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                    if (better(ge, fresh, bg, best)) {
+                        best = fresh;
+                        bg = ge;
+                    }
+                }
+                double d = __dsub_rn(bg, base);
+                if (best != own && d > p.thr) {
+                    p.tgt[v] = best;
+                    p.from[v] = own;
+                    p.dgain[v] = to_fix(d, p.inv_scale);
+                    p.hint[v] = (best != fresh && p.csize[best] == 1) ? cu_member : NONE32;
+                    p.epoch[v] = p.cur;
+                }
+            }
+        } else {
+            // candidates in ascending community id: each candidate lane finds its rank
+            int rank = 0, ncand = 0;
+#pragma unroll
+            for (int t = 0; t < G; ++t) {
+                uint32_t oc = __shfl_sync(FULL, c, gbase + t);
+                int ocand = __shfl_sync(FULL, (int)cand, gbase + t);
+                if (ocand) {
+                    ncand++;
+                    if (oc < c) rank++;
+                }
+            }
+            double best_rel = 0.0;
+            {
+                double x = cand ? g : 0.0;
+#pragma unroll
+                for (int o = G / 2; o; o >>= 1) x = fmax(x, __shfl_xor_sync(FULL, x, o));
+                best_rel = x;
+            }
+            if (cand) {
+                s_c[threadIdx.x - lane + gbase + rank] = c;
+                s_r[threadIdx.x - lane + gbase + rank] = g;
+            }
+            __syncwarp();
+            // hint member of each candidate: lane order equals candidate rank order
+            if (sub == 0 && eligible && ncand > 0) {
+                const uint32_t* cc = s_c + (threadIdx.x - lane + gbase);
+                const double* cr = s_r + (threadIdx.x - lane + gbase);
+                uint32_t target = NONE32;
+                if (p.theta <= 0.0) {
+                    for (int j = 0; j < ncand; ++j)
+                        if (cr[j] >= best_rel && (target == NONE32 || cc[j] < target)) target = cc[j];
+                } else {
+                    double tot = -0.0;
+                    for (int j = 0; j < ncand; ++j)
+                        tot = __dadd_rn(tot, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
+                    if (!isfinite(tot) || tot <= 0.0) {
+                        for (int j = 0; j < ncand; ++j)
+                            if (cr[j] >= best_rel && (target == NONE32 || cc[j] < target)) target = cc[j];
+                    } else {
+                        double thr = __dmul_rn(uniform01(p.seed, p.cur, v), tot);
+                        target = cc[ncand - 1];
+                        for (int j = 0; j < ncand; ++j) {
+                            thr = __dsub_rn(thr, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
+                            if (thr <= 0.0) {
+                                target = cc[j];
+                                break;
+                            }
+                        }
+                    }
+                }
+                s_c[threadIdx.x] = target;  // broadcast slot (lane sub==0 of the group)
+            }
+            __syncwarp();
+            uint32_t target = __shfl_sync(FULL, (sub == 0 && eligible && ncand > 0) ? s_c[threadIdx.x] : NONE32,
+                                          gbase);
+            // member of the target if it is a singleton: the lane holding it
+            unsigned hb = __ballot_sync(FULL, cand && c == target) & gmask;
+            uint32_t member = __shfl_sync(FULL, cu_member, hb ? (__ffs(hb) - 1) : lane);
+            if (sub == 0 && eligible && target != NONE32) {
+                p.tgt[v] = target;
+                p.from[v] = own;
+                p.dgain[v] = 0;
+                p.hint[v] = (p.csize[target] == 1) ? member : NONE32;
+                p.epoch[v] = p.cur;
+            }
+            __syncwarp();
+        }
+    }
+    warp_add(p.counters + 1, sdeg);
+    warp_add(p.counters + 2, scand);
+    warp_add(p.counters + 3, snodes);
+}
+
+// ------------------------------------------------------------ large-degree decide
+__device__ __forceinline__ uint32_t hslot(uint32_t c, uint32_t mask) {
+    return (c * 0x9E3779B1u) & mask;
+}
+
+__device__ bool hinsert(uint32_t* keys, long long* vals, uint32_t mask, uint32_t c, long long x,
+                        uint32_t* status) {
+    uint32_t h = hslot(c, mask);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+        uint32_t k = keys[h];
+        if (k == c) {
+            atomicAdd((unsigned long long*)(vals + h), (unsigned long long)x);
+            return true;
+        }
+        if (k == EMPTYK) {
+            uint32_t prev = atomicCAS(keys + h, EMPTYK, c);
+            if (prev == EMPTYK || prev == c) {
+                atomicAdd((unsigned long long*)(vals + h), (unsigned long long)x);
+                return true;
+            }
+        }
+        h = (h + 1) & mask;
+    }
+    atomicOr(status, DEV_OVERFLOW);
+    return false;
+}
+
+__device__ long long hlookup(const uint32_t* keys, const long long* vals, uint32_t mask, uint32_t c) {
+    uint32_t h = hslot(c, mask);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+        uint32_t k = keys[h];
+        if (k == c) return vals[h];
+        if (k == EMPTYK) return 0;
+        h = (h + 1) & mask;
+    }
+    return 0;
+}
+
+// Block-wide argmax of (g, c) with ties to the lower id.
+__device__ void block_argmax(double& g, uint32_t& c, double* sg, uint32_t* sc) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int o = 16; o; o >>= 1) {
+        double og = __shfl_xor_sync(0xFFFFFFFFu, g, o);
+        uint32_t oc = __shfl_xor_sync(0xFFFFFFFFu, c, o);
+        if (better(og, oc, g, c)) {
+            g = og;
+            c = oc;
+        }
+    }
+    if (lane == 0) {
+        sg[wid] = g;
+        sc[wid] = c;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        int nw = blockDim.x >> 5;
+        g = lane < nw ? sg[lane] : -INFINITY;
+        c = lane < nw ? sc[lane] : NONE32;
+        for (int o = 16; o; o >>= 1) {
+            double og = __shfl_xor_sync(0xFFFFFFFFu, g, o);
+            uint32_t oc = __shfl_xor_sync(0xFFFFFFFFu, c, o);
+            if (better(og, oc, g, c)) {
+                g = og;
+                c = oc;
+            }
+        }
+        if (lane == 0) {
+            sg[0] = g;
+            sc[0] = c;
+        }
+    }
+    __syncthreads();
+    g = sg[0];
+    c = sc[0];
+    __syncthreads();
+}
+
+// In-place bitonic sort of (key, val) pairs, n a power of two, by the block.
+__device__ void block_bitonic(uint32_t* key, double* val, uint32_t n) {
+    for (uint32_t size = 2; size <= n; size <<= 1) {
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t t = threadIdx.x; t < n / 2; t += blockDim.x) {
+                uint32_t lo = 2 * stride * (t / stride) + (t % stride);
+                uint32_t hi = lo + stride;
+                bool up = ((lo & size) == 0);
+                if ((key[lo] > key[hi]) == up) {
+                    uint32_t tk = key[lo];
+                    key[lo] = key[hi];
+                    key[hi] = tk;
+                    double tv = val[lo];
+                    val[lo] = val[hi];
+                    val[hi] = tv;
+                }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <bool REFINE>
+__global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* __restrict__ list,
+                                                     uint32_t count, uint32_t* gkeys, long long* gvals,
+                                                     uint32_t* gck, double* gcr, uint64_t gcap) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    long long* s_vals = (long long*)smem;
+    uint32_t* s_keys = (uint32_t*)(smem + HCAP_SMEM * sizeof(long long));
+    __shared__ double red_g[32];
+    __shared__ uint32_t red_c[32];
+    __shared__ uint32_t s_member, s_ncand, s_target;
+    __shared__ double s_bestrel;
+
+    unsigned long long sdeg = 0, scand = 0, snodes = 0;
+    for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
+        const uint32_t v = list[i];
+        const uint64_t b = p.ptr[v], e = p.ptr[v + 1];
+        const uint32_t deg = (uint32_t)(e - b);
+        const uint32_t own = p.memb[v];
+        if (REFINE && p.csize[own] != 1) continue;  // uniform over the block
+        uint32_t cap = 64;
+        while (cap < 2 * deg) cap <<= 1;
+        uint32_t* keys;
+        long long* vals;
+        if (cap <= (uint32_t)HCAP_SMEM) {
+            keys = s_keys;
+            vals = s_vals;
+        } else {
+            if (cap > gcap) {
+                if (threadIdx.x == 0) atomicOr(p.status, DEV_OVERFLOW);
+                continue;
+            }
+            keys = gkeys + (uint64_t)blockIdx.x * gcap;
+            vals = gvals + (uint64_t)blockIdx.x * gcap;
+        }
+        const uint32_t mask = cap - 1;
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
+            keys[s] = EMPTYK;
+            vals[s] = 0;
+        }
+        __syncthreads();
+        const uint32_t cv = REFINE ? p.constraint[v] : 0;
+        for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+            uint32_t u = p.nbr[j];
+            if (u == v) continue;
+            if (REFINE && p.constraint[u] != cv) continue;
+            hinsert(keys, vals, mask, p.memb[u], to_fix((double)p.w[j], p.inv_scale), p.status);
+        }
+        __syncthreads();
+        const long long kf = to_fix(p.strength[v], p.inv_scale);
+        const long long af = to_fix(p.node_w[v], p.inv_nscale);
+        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = p.self_loop[v];
+        const long long wof = hlookup(keys, vals, mask, own);
+        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale),
+                                    a, from_fix(p.Wf[own] - af, p.nscale));
+        double g = -INFINITY;
+        uint32_t c = NONE32;
+        if (threadIdx.x == 0) s_ncand = 0;
+        __syncthreads();
+        uint32_t lc = 0;
+        for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
+            uint32_t cu = keys[s];
+            if (cu == EMPTYK || cu == own) continue;
+            lc++;
+            double nc = from_fix(p.Wf[cu], p.nscale);
+            if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
+            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+            if (REFINE) {
+                double rel = __dsub_rn(gg, base);
+                if (rel >= 0.0) {
+                    uint32_t slot = atomicAdd(&s_ncand, 1u);
+                    if (slot < gcap) {
+                        gck[(uint64_t)blockIdx.x * gcap + slot] = cu;
+                        gcr[(uint64_t)blockIdx.x * gcap + slot] = rel;
+                    }
+                    if (rel > g) g = rel;
+                }
+            } else if (better(gg, cu, g, c)) {
+                g = gg;
+                c = cu;
+            }
+        }
+        scand += lc;
+        if (threadIdx.x == 0) {
+            snodes += 1;
+            sdeg += deg;
+        }
+        if (!REFINE) {
+            block_argmax(g, c, red_g, red_c);
+            if (threadIdx.x == 0) {
+                uint32_t best = own;
+                double bg = base;
+                if (c != NONE32 && better(g, c, bg, best)) {
+                    best = c;
+                    bg = g;
+                }
+                const uint32_t fresh = (uint32_t)(p.S0 + v);
+                if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 &&
+                    (!p.has_limit || a <= p.limit)) {
+                    double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                    if (better(ge, fresh, bg, best)) {
+                        best = fresh;
+                        bg = ge;
+                    }
+                }
+                double d = __dsub_rn(bg, base);
+                s_target = (best != own && d > p.thr) ? best : NONE32;
+                if (s_target != NONE32) {
+                    p.tgt[v] = best;
+                    p.from[v] = own;
+                    p.dgain[v] = to_fix(d, p.inv_scale);
+                    p.epoch[v] = p.cur;
+                }
+                s_member = NONE32;
+            }
+            __syncthreads();
+        } else {
+            // best_rel: block max of the non-negative rels (0.0 floor)
+            double x = g > 0.0 ? g : 0.0;
+            uint32_t dummy = 0;
+            block_argmax(x, dummy, red_g, red_c);
+            if (threadIdx.x == 0) s_bestrel = x;
+            __syncthreads();
+            uint32_t nc = min(s_ncand, (uint32_t)gcap);
+            if (threadIdx.x == 0 && s_ncand > gcap) atomicOr(p.status, DEV_OVERFLOW);
+            uint32_t n2 = 1;
+            while (n2 < nc) n2 <<= 1;
+            uint32_t* ck = gck + (uint64_t)blockIdx.x * gcap;
+            double* cr = gcr + (uint64_t)blockIdx.x * gcap;
+            if (n2 <= gcap) {
+                for (uint32_t s = nc + threadIdx.x; s < n2; s += blockDim.x) {
+                    ck[s] = 0xFFFFFFFFu;
+                    cr[s] = 0.0;
+                }
+            }
+            __syncthreads();
+            if (nc > 1 && n2 <= gcap) block_bitonic(ck, cr, n2);
+            if (threadIdx.x == 0) {
+                uint32_t target = NONE32;
+                double best_rel = s_bestrel;
+                if (nc > 0) {
+                    if (p.theta <= 0.0) {
+                        for (uint32_t j = 0; j < nc; ++j)
+                            if (cr[j] >= best_rel && (target == NONE32 || ck[j] < target)) target = ck[j];
+                    } else {
+                        double tot = -0.0;
+                        for (uint32_t j = 0; j < nc; ++j)
+                            tot = __dadd_rn(tot, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
+                        if (!isfinite(tot) || tot <= 0.0) {
+                            for (uint32_t j = 0; j < nc; ++j)
+                                if (cr[j] >= best_rel && (target == NONE32 || ck[j] < target))
+                                    target = ck[j];
+                        } else {
+                            double thr = __dmul_rn(uniform01(p.seed, p.cur, v), tot);
+                            target = ck[nc - 1];
+                            for (uint32_t j = 0; j < nc; ++j) {
+                                thr = __dsub_rn(thr, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
+                                if (thr <= 0.0) {
+                                    target = ck[j];
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                }
+                s_target = target;
+                if (target != NONE32) {
+                    p.tgt[v] = target;
+                    p.from[v] = own;
+                    p.dgain[v] = 0;
+                    p.epoch[v] = p.cur;
+                }
+                s_member = NONE32;
+            }
+            __syncthreads();
+        }
+        // the member of a singleton target, for conflict detection
+        const uint32_t target = s_target;
+        if (target != NONE32) {
+            if (p.csize[target] == 1) {
+                for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) {
+                    uint32_t u = p.nbr[j];
+                    if (u != v && p.memb[u] == target) s_member = u;
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) p.hint[v] = s_member;
+        }
+        __syncthreads();
+    }
+    // block-level counter flush (thread 0 holds the node and degree counts)
+    atomicAdd(p.counters + 2, scand);
+    if (threadIdx.x == 0) {
+        atomicAdd(p.counters + 1, sdeg);
+        atomicAdd(p.counters + 3, snodes);
+    }
+}
+
+// ------------------------------------------------------------ commit
+template <bool REFINE>
+__global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t count,
+                        uint8_t* next_active) {
+    unsigned long long nmoves = 0;
+    long long gsum = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = list[i];
+        if (p.epoch[v] != p.cur) continue;
+        if (cancelled(p, v)) continue;
+        const uint32_t t = p.tgt[v], old = p.from[v];
+        const long long kf = to_fix(p.strength[v], p.inv_scale);
+        const long long af = to_fix(p.node_w[v], p.inv_nscale);
+        p.memb[v] = t;
+        atomicAdd((unsigned long long*)(p.Kf + old), (unsigned long long)(-kf));
+        atomicAdd((unsigned long long*)(p.Kf + t), (unsigned long long)kf);
+        atomicAdd((unsigned long long*)(p.Wf + old), (unsigned long long)(-af));
+        atomicAdd((unsigned long long*)(p.Wf + t), (unsigned long long)af);
+        atomicSub(p.csize + old, 1u);
+        atomicAdd(p.csize + t, 1u);
+        nmoves++;
+        gsum += p.dgain[v];
+        if (!REFINE) {
+            // re-queue neighbours outside the new community (local_move.rs:113-118)
+            for (uint64_t j = p.ptr[v]; j < p.ptr[v + 1]; ++j) {
+                uint32_t u = p.nbr[j];
+                if (u == v) continue;
+                uint32_t cu;
+                if (p.epoch[u] == p.cur) cu = cancelled(p, u) ? p.from[u] : p.tgt[u];
+                else cu = p.memb[u];
+                if (cu != t) next_active[u] = 1;
+            }
+        }
+    }
+    warp_add(p.counters + 0, nmoves);
+    for (int o = 16; o; o >>= 1) gsum += __shfl_xor_sync(0xFFFFFFFFu, gsum, o);
+    if ((threadIdx.x & 31) == 0 && gsum) atomicAdd((unsigned long long*)p.gain_acc, (unsigned long long)gsum);
+}
+
+// ------------------------------------------------------------ bucketing
+__device__ __forceinline__ int bucket_of(uint32_t deg) {
+    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : 3;
+}
+
+__global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
+                               uint64_t n, uint64_t seed, uint32_t sweep, int B, uint32_t* counts) {
+    __shared__ uint32_t sc[64];
+    for (int t = threadIdx.x; t < B * NBUCKET; t += blockDim.x) sc[t] = 0;
+    __syncthreads();
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        if (active && !active[v]) continue;
+        int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
+        int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
+        atomicAdd(&sc[b * NBUCKET + k], 1u);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < B * NBUCKET; t += blockDim.x)
+        if (sc[t]) atomicAdd(counts + t, sc[t]);
+}
+
+__global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
+                                 uint64_t n, uint64_t seed, uint32_t sweep, int B, uint32_t* cursor,
+                                 uint32_t* list) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        if (active && !active[v]) continue;
+        int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
+        int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
+        uint32_t pos = atomicAdd(cursor + b * NBUCKET + k, 1u);
+        list[pos] = (uint32_t)v;
+    }
+}
+
+// ------------------------------------------------------------ partition state
+__global__ void k_init_comm(const uint32_t* __restrict__ memb, uint64_t n, const double* __restrict__ strength,
+                            const double* __restrict__ node_w, double inv_scale, double inv_nscale,
+                            long long* Kf, long long* Wf, uint32_t* csize) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t c = memb[v];
+        atomicAdd((unsigned long long*)(Kf + c), (unsigned long long)to_fix(strength[v], inv_scale));
+        atomicAdd((unsigned long long*)(Wf + c), (unsigned long long)to_fix(node_w[v], inv_nscale));
+        atomicAdd(csize + c, 1u);
+    }
+}
+
+__global__ void k_identity(uint32_t* p, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = (uint32_t)i;
+}
+
+__global__ void k_scatter_coarse(const uint32_t* __restrict__ grp, const uint32_t* __restrict__ memb,
+                                 uint64_t n, uint32_t* cmemb) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        cmemb[grp[v]] = memb[v];
+}
+
+__global__ void k_gather(const uint32_t* __restrict__ map, uint32_t* x, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        x[i] = map[x[i]];
+}
+
+__global__ void k_fill_u8(uint8_t* p, uint64_t n, uint8_t v) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = v;
+}
+
+// ------------------------------------------------------------ host side
+struct Scales {
+    double scale, inv, nscale, ninv;
+};
+
+Scales scales_for(const DevGraph& g) {
+    Scales s;
+    int F;
+    if (g.exact_w) F = (g.e0_w == 0x7FFFFFFF) ? 0 : g.e0_w;
+    else F = (int)std::ceil(std::log2(std::max(2.0 * g.total_weight, 1e-300))) + 1 - 61;
+    int Fn;
+    if (g.exact_nw) Fn = (g.e0_nw == 0x7FFFFFFF) ? 0 : g.e0_nw;
+    else Fn = (int)std::ceil(std::log2(std::max(g.total_node_weight, 1e-300))) + 1 - 61;
+    s.scale = std::ldexp(1.0, F);
+    s.inv = std::ldexp(1.0, -F);
+    s.nscale = std::ldexp(1.0, Fn);
+    s.ninv = std::ldexp(1.0, -Fn);
+    return s;
+}
+
+struct Workspace {
+    DBuf<uint32_t> tgt, hint, from, epoch, list;
+    DBuf<long long> dgain;
+    DBuf<uint8_t> active, next_active;
+    DBuf<uint32_t> counts;
+    DBuf<unsigned long long> counters;
+    DBuf<long long> gain_acc;
+    DBuf<uint32_t> gkeys, gck;
+    DBuf<long long> gvals;
+    DBuf<double> gcr;
+    uint64_t gcap = 0;
+    int nblk_large = 0;
+};
+
+class Timer {
+   public:
+    explicit Timer(Ctx& c) : c_(c) {
+        cudaEventCreate(&a_);
+        cudaEventCreate(&b_);
+        cudaEventRecord(a_, c.stream);
+    }
+    double stop() {
+        cudaEventRecord(b_, c_.stream);
+        cudaEventSynchronize(b_);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a_, b_);
+        return ms;
+    }
+    ~Timer() {
+        cudaEventDestroy(a_);
+        cudaEventDestroy(b_);
+    }
+
+   private:
+    Ctx& c_;
+    cudaEvent_t a_, b_;
+};
+
+void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
+    const uint64_t n = g.n;
+    ws.tgt.alloc(c, n);
+    ws.hint.alloc(c, n);
+    ws.from.alloc(c, n);
+    ws.epoch.alloc(c, n);
+    ws.list.alloc(c, n);
+    ws.dgain.alloc(c, n);
+    ws.active.alloc(c, n);
+    ws.next_active.alloc(c, n);
+    ws.counts.alloc(c, 64);
+    ws.counters.alloc(c, 4);
+    ws.gain_acc.alloc(c, 1);
+    zero(c, ws.epoch.get(), n);
+    zero(c, ws.hint.get(), n);
+    // global hash / candidate scratch for nodes past the shared-memory table
+    uint64_t cap = 64;
+    while (cap < 2ull * g.max_degree) cap <<= 1;
+    int nblk = c.sm_count * 2;
+    uint64_t budget = 1ull << 31;  // bytes for the large-degree scratch
+    while (nblk > 1 && (uint64_t)nblk * cap * 24 > budget) nblk >>= 1;
+    ws.nblk_large = nblk;
+    ws.gcap = cap;
+    ws.gkeys.alloc(c, (uint64_t)nblk * cap);
+    ws.gvals.alloc(c, (uint64_t)nblk * cap);
+    ws.gck.alloc(c, (uint64_t)nblk * cap);
+    ws.gcr.alloc(c, (uint64_t)nblk * cap);
+}
+
+template <bool REFINE>
+void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list, uint32_t cnt) {
+    if (!cnt) return;
+    if (k == 0) {
+        unsigned warps = (cnt + 3) / 4;
+        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+    } else if (k == 1) {
+        unsigned warps = (cnt + 1) / 2;
+        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+    } else if (k == 2) {
+        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+    } else {
+        size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
+        unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
+        k_decide_block<REFINE><<<grid, TB, sm, c.stream>>>(p, list, cnt, ws.gkeys.get(), ws.gvals.get(),
+                                                          ws.gck.get(), ws.gcr.get(), ws.gcap);
+    }
+    SC_LAUNCH_CHECK();
+    c.launches++;
+}
+
+struct MoveResult {
+    double improvement = 0.0;
+    uint64_t sweeps = 0, moves = 0;
+    double alg_bytes = 0.0;
+};
+
+// Parallel local moving over communities `memb` (ids < S0), extra ids
+// [S0, S0+n) are the fresh empty communities.
+MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, uint64_t S0,
+                      const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
+    MoveResult r;
+    const uint64_t n = g.n;
+    if (n == 0) return r;
+    const uint64_t S = S0 + n;
+    DBuf<long long> Kf(c, S), Wf(c, S);
+    DBuf<uint32_t> csize(c, S);
+    zero(c, Kf.get(), S);
+    zero(c, Wf.get(), S);
+    zero(c, csize.get(), S);
+    k_init_comm<<<grid_for(n, TB), TB, 0, c.stream>>>(memb, n, g.strength, g.node_w, sc.inv, sc.ninv,
+                                                      Kf.get(), Wf.get(), csize.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    Params p{};
+    p.ptr = g.ptr;
+    p.nbr = g.nbr;
+    p.w = g.w;
+    p.strength = g.strength;
+    p.node_w = g.node_w;
+    p.self_loop = g.self_loop;
+    p.memb = memb;
+    p.Kf = Kf.get();
+    p.Wf = Wf.get();
+    p.csize = csize.get();
+    p.constraint = nullptr;
+    p.tgt = ws.tgt.get();
+    p.hint = ws.hint.get();
+    p.from = ws.from.get();
+    p.dgain = ws.dgain.get();
+    p.epoch = ws.epoch.get();
+    p.S0 = S0;
+    p.objective = cfg.objective;
+    p.gamma = gamma;
+    p.four_m = 4.0 * g.total_weight;
+    p.thr = 1e-12 * std::max(std::fabs(g.total_weight), 1.0);  // local_move.rs:26-28
+    p.scale = sc.scale;
+    p.inv_scale = sc.inv;
+    p.nscale = sc.nscale;
+    p.inv_nscale = sc.ninv;
+    p.has_limit = cfg.has_max_community_weight;
+    p.limit = cfg.max_community_weight;
+    p.theta = 0.0;
+    p.seed = seed;
+    p.status = c.d_status;
+    p.counters = ws.counters.get();
+    p.gain_acc = ws.gain_acc.get();
+    zero(c, ws.counters.get(), 4);
+    zero(c, ws.gain_acc.get(), 1);
+    zero(c, ws.epoch.get(), n);
+    k_fill_u8<<<grid_for(n, TB), TB, 0, c.stream>>>(ws.active.get(), n, 1);
+    c.launches++;
+    const int B = LM_BATCHES;
+    uint32_t epoch = 0;
+    uint64_t moves_before = 0;
+    const uint64_t budget = n * 100;  // MAX_MOVES_PER_NODE, local_move.rs:32
+    for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
+        zero(c, ws.counts.get(), B * NBUCKET);
+        zero(c, ws.next_active.get(), n);
+        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B,
+                                                             ws.counts.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        uint32_t counts[64];
+        unsigned long long ctr[4];
+        d2h(c, counts, ws.counts.get(), B * NBUCKET);
+        d2h(c, ctr, ws.counters.get(), 4);
+        sync(c);
+        if (sweep > 0 && ctr[0] == moves_before) break;  // last sweep moved nothing
+        if (ctr[0] >= budget) break;
+        moves_before = ctr[0];
+        uint32_t offs[65];
+        offs[0] = 0;
+        for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
+        if (offs[B * NBUCKET] == 0) break;
+        DBuf<uint32_t> cursor(c, 64);
+        h2d(c, cursor.get(), offs, B * NBUCKET);
+        k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B,
+                                                               cursor.get(), ws.list.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        for (int b = 0; b < B; ++b) {
+            ++epoch;
+            p.cur = epoch;
+            p.seed = seed;
+            uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
+            if (lo == hi) continue;
+            for (int k = 0; k < NBUCKET; ++k) {
+                uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
+                launch_decide<false>(c, p, ws, k, ws.list.get() + s, e - s);
+            }
+            k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
+                                                                       ws.next_active.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+        }
+        std::swap(ws.active, ws.next_active);
+        r.sweeps++;
+    }
+    unsigned long long ctr[4];
+    long long gacc = 0;
+    d2h(c, ctr, ws.counters.get(), 4);
+    d2h(c, &gacc, ws.gain_acc.get(), 1);
+    sync(c);
+    r.moves = ctr[0];
+    r.improvement = (double)gacc * sc.scale;
+    // algorithmic bytes: 16 per node visit + 12 per scanned entry + 8 per candidate
+    r.alg_bytes = 16.0 * (double)ctr[3] + 12.0 * (double)ctr[1] + 8.0 * (double)ctr[2];
+    return r;
+}
+
+// refine (refine.rs:29-103): refined ids < n; constraint = working membership.
+double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint, uint32_t* refined,
+              const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
+    const uint64_t n = g.n;
+    if (n == 0) return 0.0;
+    DBuf<long long> Kf(c, n), Wf(c, n);
+    DBuf<uint32_t> csize(c, n);
+    zero(c, Kf.get(), n);
+    zero(c, Wf.get(), n);
+    zero(c, csize.get(), n);
+    k_identity<<<grid_for(n, TB), TB, 0, c.stream>>>(refined, n);
+    k_init_comm<<<grid_for(n, TB), TB, 0, c.stream>>>(refined, n, g.strength, g.node_w, sc.inv, sc.ninv,
+                                                      Kf.get(), Wf.get(), csize.get());
+    SC_LAUNCH_CHECK();
+    c.launches += 2;
+    Params p{};
+    p.ptr = g.ptr;
+    p.nbr = g.nbr;
+    p.w = g.w;
+    p.strength = g.strength;
+    p.node_w = g.node_w;
+    p.self_loop = g.self_loop;
+    p.memb = refined;
+    p.Kf = Kf.get();
+    p.Wf = Wf.get();
+    p.csize = csize.get();
+    p.constraint = constraint;
+    p.tgt = ws.tgt.get();
+    p.hint = ws.hint.get();
+    p.from = ws.from.get();
+    p.dgain = ws.dgain.get();
+    p.epoch = ws.epoch.get();
+    p.S0 = n;
+    p.objective = cfg.objective;
+    p.gamma = gamma;
+    p.four_m = 4.0 * g.total_weight;
+    p.thr = 0.0;
+    p.scale = sc.scale;
+    p.inv_scale = sc.inv;
+    p.nscale = sc.nscale;
+    p.inv_nscale = sc.ninv;
+    p.has_limit = cfg.has_max_community_weight;
+    p.limit = cfg.max_community_weight;
+    double mean_edge = g.edge_count > 0 ? g.total_weight / (double)g.edge_count : 1.0;
+    p.theta = cfg.refine_randomness * mean_edge;  // refine.rs:44-50
+    p.seed = seed;
+    p.status = c.d_status;
+    p.counters = ws.counters.get();
+    p.gain_acc = ws.gain_acc.get();
+    zero(c, ws.counters.get(), 4);
+    zero(c, ws.epoch.get(), n);
+    const int B = RF_BATCHES;
+    zero(c, ws.counts.get(), B * NBUCKET);
+    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B,
+                                                         ws.counts.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    uint32_t counts[64];
+    d2h(c, counts, ws.counts.get(), B * NBUCKET);
+    sync(c);
+    uint32_t offs[65];
+    offs[0] = 0;
+    for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
+    DBuf<uint32_t> cursor(c, 64);
+    h2d(c, cursor.get(), offs, B * NBUCKET);
+    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B,
+                                                           cursor.get(), ws.list.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    for (int b = 0; b < B; ++b) {
+        p.cur = (uint32_t)(b + 1);
+        uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
+        if (lo == hi) continue;
+        for (int k = 0; k < NBUCKET; ++k) {
+            uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
+            launch_decide<true>(c, p, ws, k, ws.list.get() + s, e - s);
+        }
+        k_apply<true><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo, nullptr);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    unsigned long long ctr[4];
+    d2h(c, ctr, ws.counters.get(), 4);
+    sync(c);
+    return 16.0 * (double)ctr[3] + 16.0 * (double)ctr[1] + 8.0 * (double)ctr[2];
+}
+
+struct PassOut {
+    DBuf<uint32_t> labels;  // compact, n
+    uint64_t n_clusters = 0;
+    double improvement = 0.0;
+};
+
+// run_once (mod.rs:214-289) from compact initial ids `init` (< C0).
+void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, const sc_leiden_config& cfg,
+              uint64_t pass_seed, PassOut& out, sc_run_stats& st) {
+    const uint64_t n0 = g0.n;
+    const double gamma = cfg.resolution;
+    std::unique_ptr<DevGraph> owned;
+    const DevGraph* gl = &g0;
+    DBuf<uint32_t> memb(c, n0), node_at(c, n0);
+    d2d(c, memb.get(), init, n0);
+    k_identity<<<grid_for(n0, TB), TB, 0, c.stream>>>(node_at.get(), n0);
+    c.launches++;
+    uint64_t C = C0;
+    double improvement = 0.0;
+    for (uint64_t level = 0; level < cfg.max_levels; ++level) {
+        const uint64_t nl = gl->n;
+        const uint64_t lvl_seed = hash3(pass_seed, level, 0x1eafull);
+        Scales sc = scales_for(*gl);
+        Workspace ws;
+        prepare_workspace(c, ws, *gl);
+        // ids of memb are < C; fresh ids live in [C, C + nl)
+        {
+            Timer t(c);
+            MoveResult mr = local_move(c, *gl, ws, memb.get(), C, cfg, lvl_seed, sc, gamma);
+            st.ms_local_move += t.stop();
+            improvement += mr.improvement;
+            st.local_move_sweeps += mr.sweeps;
+            st.moves += mr.moves;
+            st.alg_bytes_local_move += mr.alg_bytes;
+        }
+        DBuf<uint32_t> collapse(c, nl);
+        uint64_t id_space;
+        if (cfg.refine) {
+            Timer t(c);
+            st.alg_bytes_refine += refine(c, *gl, ws, memb.get(), collapse.get(), cfg,
+                                          hash3(lvl_seed, 0x7e71eull, 1), sc, gamma);
+            st.ms_refine += t.stop();
+            id_space = nl;
+        } else {
+            d2d(c, collapse.get(), memb.get(), nl);
+            id_space = C + nl;
+        }
+        Timer t_agg(c);
+        DBuf<uint32_t> grp(c, nl);
+        uint32_t G = renumber_ids(c, collapse.get(), nl, id_space, grp.get());
+        st.levels++;
+        if (G >= nl) {
+            st.ms_aggregate += t_agg.stop();
+            break;
+        }
+        std::unique_ptr<DevGraph> coarse(graph_aggregate(c, *gl, grp.get(), G));
+        st.alg_bytes_aggregate += 12.0 * (double)gl->E + 12.0 * (double)nl + 8.0 * (double)coarse->E +
+                                  24.0 * (double)coarse->n;
+        // coarse membership from the working partition (mod.rs:269-272), compacted
+        DBuf<uint32_t> cm(c, G), cm2(c, G);
+        k_scatter_coarse<<<grid_for(nl, TB), TB, 0, c.stream>>>(grp.get(), memb.get(), nl, cm.get());
+        k_gather<<<grid_for(n0, TB), TB, 0, c.stream>>>(grp.get(), node_at.get(), n0);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+        C = renumber_ids(c, cm.get(), G, C + nl, cm2.get());
+        memb = std::move(cm2);
+        owned = std::move(coarse);
+        gl = owned.get();
+        st.ms_aggregate += t_agg.stop();
+    }
+    // final ascending renumber (mod.rs:282-286)
+    const uint64_t nl = gl->n;
+    DBuf<uint32_t> fin(c, nl);
+    uint32_t K = renumber_ids(c, memb.get(), nl, C + nl, fin.get());
+    out.labels.alloc(c, n0);
+    d2d(c, out.labels.get(), node_at.get(), n0);
+    k_gather<<<grid_for(n0, TB), TB, 0, c.stream>>>(fin.get(), out.labels.get(), n0);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    out.n_clusters = K;
+    out.improvement = improvement;
+}
+
+// LeidenConfig::validate (mod.rs:117-153)
+void validate_config(const sc_leiden_config& cfg) {
+    double r = cfg.resolution;
+    if (cfg.objective != SC_OBJECTIVE_RB && cfg.objective != SC_OBJECTIVE_CPM)
+        fail(SC_E_INVALID_CONFIG, "invalid configuration: unknown objective %d", cfg.objective);
+    if (!std::isfinite(r) || r < 0.0)
+        fail(SC_E_INVALID_CONFIG, "invalid configuration: resolution must be finite and non-negative, got %s",
+             fmt_f64(r).c_str());
+    if (cfg.n_iterations == 0) fail(SC_E_INVALID_CONFIG, "invalid configuration: n_iterations must be at least 1");
+    if (cfg.max_levels == 0) fail(SC_E_INVALID_CONFIG, "invalid configuration: max_levels must be at least 1");
+    if (cfg.patience == 0) fail(SC_E_INVALID_CONFIG, "invalid configuration: patience must be at least 1");
+    if (!std::isfinite(cfg.refine_randomness) || cfg.refine_randomness < 0.0)
+        fail(SC_E_INVALID_CONFIG,
+             "invalid configuration: refine_randomness must be finite and non-negative, got %s",
+             fmt_f64(cfg.refine_randomness).c_str());
+    if (cfg.has_max_community_weight &&
+        (!std::isfinite(cfg.max_community_weight) || cfg.max_community_weight <= 0.0))
+        fail(SC_E_INVALID_CONFIG,
+             "invalid configuration: max_community_weight must be finite and positive, got %s",
+             fmt_f64(cfg.max_community_weight).c_str());
+}
+
+}  // namespace
+
+// leiden (mod.rs:168-204). initial_host: optional warm-start labels (n entries).
+void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64_t* initial_host,
+            uint32_t* d_labels_out, uint64_t* n_clusters) {
+    validate_config(cfg);
+    std::memset(&c.stats, 0, sizeof c.stats);
+    Timer total(c);
+    const uint64_t n = g.n;
+    if (n == 0) {
+        *n_clusters = 0;
+        return;
+    }
+    uint64_t seed = cfg.has_seed ? cfg.seed : (uint64_t)std::random_device{}() << 32 ^ std::random_device{}();
+    DBuf<uint32_t> labels(c, n);
+    uint64_t C;
+    if (initial_host) {
+        DBuf<uint64_t> ini(c, n);
+        h2d(c, ini.get(), initial_host, n);
+        C = renumber_u64_labels(c, ini.get(), n, labels.get(), nullptr);
+    } else {
+        k_identity<<<grid_for(n, TB), TB, 0, c.stream>>>(labels.get(), n);
+        c.launches++;
+        C = n;
+    }
+    uint64_t clusters = C;
+    uint64_t stagnant = 0;
+    for (uint64_t it = 0; it < cfg.n_iterations; ++it) {
+        PassOut po;
+        run_pass(c, g, labels.get(), C, cfg, hash3(seed, it, 0x9a55ull), po, c.stats);
+        labels = std::move(po.labels);
+        C = po.n_clusters;
+        clusters = C;
+        c.stats.passes++;
+        double scale = std::max(std::fabs(g.total_weight), 1.0);
+        if (po.improvement <= cfg.tolerance * scale) {
+            stagnant++;
+            if (stagnant >= cfg.patience) break;
+        } else {
+            stagnant = 0;
+        }
+    }
+    d2d(c, d_labels_out, labels.get(), n);
+    check_device_status(c);
+    c.stats.ms_total = total.stop();
+    c.stats.ms_other = c.stats.ms_total - c.stats.ms_local_move - c.stats.ms_refine - c.stats.ms_aggregate;
+    c.stats.kernel_launches = c.launches;
+    *n_clusters = clusters;
+}
+
+}  // namespace sc

@@ -1,0 +1,115 @@
+// sc_prims.cuh — device-wide primitives (stable radix sort, scans, reductions)
+// on the context stream. Temporary storage comes from the stream-ordered pool.
+#pragma once
+
+#include <cub/cub.cuh>
+
+#include "sc_internal.cuh"
+
+namespace sc {
+
+inline int bits_for(uint64_t max_value) {
+    int b = 0;
+    while (b < 64 && (max_value >> b) != 0) ++b;
+    return b < 1 ? 1 : b;
+}
+
+// Stable LSD radix sort of (key, value) pairs on bits [0, end_bit).
+template <class K, class V>
+void sort_pairs(Ctx& c, const K* kin, K* kout, const V* vin, V* vout, size_t n, int end_bit) {
+    if (n == 0) return;
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceRadixSort::SortPairs(nullptr, bytes, kin, kout, vin, vout, n, 0, end_bit,
+                                            c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceRadixSort::SortPairs(tmp.get(), bytes, kin, kout, vin, vout, n, 0, end_bit,
+                                            c.stream));
+    c.launches += 4;
+}
+
+template <class T>
+void exclusive_sum(Ctx& c, const T* in, T* out, size_t n) {
+    if (n == 0) return;
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceScan::ExclusiveSum(tmp.get(), bytes, in, out, n, c.stream));
+    c.launches += 2;
+}
+
+template <class T>
+void inclusive_sum(Ctx& c, const T* in, T* out, size_t n) {
+    if (n == 0) return;
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceScan::InclusiveSum(nullptr, bytes, in, out, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceScan::InclusiveSum(tmp.get(), bytes, in, out, n, c.stream));
+    c.launches += 2;
+}
+
+// out[0] = Σ in (device scalar)
+template <class T>
+void device_sum(Ctx& c, const T* in, T* out, size_t n) {
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceReduce::Sum(nullptr, bytes, in, out, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceReduce::Sum(tmp.get(), bytes, in, out, n, c.stream));
+    c.launches += 1;
+}
+
+template <class T>
+void device_max(Ctx& c, const T* in, T* out, size_t n) {
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceReduce::Max(nullptr, bytes, in, out, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceReduce::Max(tmp.get(), bytes, in, out, n, c.stream));
+    c.launches += 1;
+}
+
+template <class T>
+void device_min(Ctx& c, const T* in, T* out, size_t n) {
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceReduce::Min(nullptr, bytes, in, out, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceReduce::Min(tmp.get(), bytes, in, out, n, c.stream));
+    c.launches += 1;
+}
+
+// Stable compaction of `in` where flags != 0; *d_count receives the kept count.
+template <class T, class F>
+void select_flagged(Ctx& c, const T* in, const F* flags, T* out, uint64_t* d_count, size_t n) {
+    size_t bytes = 0;
+    SC_CUDA(cub::DeviceSelect::Flagged(nullptr, bytes, in, flags, out, d_count, n, c.stream));
+    DBuf<uint8_t> tmp(c, bytes);
+    SC_CUDA(cub::DeviceSelect::Flagged(tmp.get(), bytes, in, flags, out, d_count, n, c.stream));
+    c.launches += 2;
+}
+
+template <class T>
+T to_host(Ctx& c, const T* d) {
+    T h;
+    SC_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+    SC_CUDA(cudaStreamSynchronize(c.stream));
+    return h;
+}
+
+template <class T>
+void h2d(Ctx& c, T* d, const T* h, size_t n) {
+    if (n) SC_CUDA(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, c.stream));
+}
+template <class T>
+void d2h(Ctx& c, T* h, const T* d, size_t n) {
+    if (n) SC_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+}
+template <class T>
+void d2d(Ctx& c, T* dst, const T* src, size_t n) {
+    if (n) SC_CUDA(cudaMemcpyAsync(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice, c.stream));
+}
+template <class T>
+void zero(Ctx& c, T* d, size_t n) {
+    if (n) SC_CUDA(cudaMemsetAsync(d, 0, n * sizeof(T), c.stream));
+}
+inline void sync(Ctx& c) { SC_CUDA(cudaStreamSynchronize(c.stream)); }
+
+
+}  // namespace sc

@@ -1,0 +1,499 @@
+"""sc_gpu — single-clustering's Leiden hot path on B200, behind the reference API.
+
+Mirrors single-clustering v0.7.0 (names, argument meaning and error
+behaviour) over the C ABI of include/sc_gpu.h:
+
+    CSRNetwork.from_edges / from_csr_parts / from_csr_matrix  (src/network/csr_network.rs)
+    leiden(graph, LeidenConfig) -> Clustering                 (src/community_search/leiden/mod.rs)
+    modularity(graph, labels, resolution)                     (.../leiden/objective.rs:221)
+    Rb / Cpm objectives                                       (.../leiden/objective.rs:188-199)
+    knn_gaussian(X, k, ...)                                   (src/neighborhood/mod.rs)
+
+All computation runs in libsc_gpu.so on the GPU; nothing here computes.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Iterable, Optional, Sequence, Union
+
+import numpy as np
+
+from . import _lib
+from ._lib import context, lib
+
+MAX_NODES = 0xFFFFFFFF  # csr_network.rs:36
+NOISE = (1 << 64) - 1   # clustering.rs:8
+
+
+# ---------------------------------------------------------------- errors
+class ClusteringError(Exception):
+    """ClusteringError (src/error.rs:7-68); `code` is the sc_status value."""
+
+    code = 0
+
+    def __init__(self, info: "_lib.ErrorInfo"):
+        self.info = info
+        super().__init__(info.message.decode("utf-8", errors="replace"))
+
+
+class NodeIndexOutOfRange(ClusteringError):
+    code = 1
+
+    @property
+    def node(self):
+        return self.info.node
+
+    @property
+    def n_nodes(self):
+        return self.info.n_nodes
+
+
+class NonFiniteWeight(ClusteringError):
+    code = 2
+
+    @property
+    def edge(self):
+        return (self.info.edge_from, self.info.edge_to)
+
+
+class NegativeWeight(ClusteringError):
+    code = 3
+
+    @property
+    def edge(self):
+        return (self.info.edge_from, self.info.edge_to)
+
+    @property
+    def weight(self):
+        return self.info.weight
+
+
+class InvalidNodeWeight(ClusteringError):
+    code = 4
+
+    @property
+    def node(self):
+        return self.info.node
+
+    @property
+    def weight(self):
+        return self.info.weight
+
+
+class NodeWeightLengthMismatch(ClusteringError):
+    code = 5
+
+
+class MembershipLengthMismatch(ClusteringError):
+    code = 6
+
+
+class InvalidConfig(ClusteringError):
+    code = 7
+
+
+class TooManyNodes(ClusteringError):
+    code = 8
+
+
+class InvalidCsr(ClusteringError):
+    code = 9
+
+
+class AsymmetricGraph(ClusteringError):
+    code = 10
+
+    @property
+    def degree_sum(self):
+        return self.info.degree_sum
+
+    @property
+    def expected(self):
+        return self.info.expected
+
+
+class DeviceError(ClusteringError):
+    """Failures the Rust API has no variant for (CUDA, allocation, timeout, ...)."""
+
+
+_BY_CODE = {cls.code: cls for cls in (NodeIndexOutOfRange, NonFiniteWeight, NegativeWeight,
+                                      InvalidNodeWeight, NodeWeightLengthMismatch,
+                                      MembershipLengthMismatch, InvalidConfig, TooManyNodes,
+                                      InvalidCsr, AsymmetricGraph)}
+
+
+def _check(rc: int, ctx):
+    if rc != 0:
+        info = ctx.error_info()
+        cls = _BY_CODE.get(rc, DeviceError)
+        err = cls(info)
+        err.status = rc
+        raise err
+
+
+def _ptr(a, t):
+    return None if a is None else a.ctypes.data_as(t)
+
+
+# ---------------------------------------------------------------- config
+@dataclass(frozen=True)
+class Rb:
+    """Reichardt-Bornholdt configuration model (objective.rs:66-125)."""
+    resolution: float = 1.0
+
+
+@dataclass(frozen=True)
+class Cpm:
+    """Constant Potts Model (objective.rs:127-184)."""
+    resolution: float = 0.05
+
+
+ObjectiveKind = Union[Rb, Cpm]
+
+
+@dataclass
+class LeidenConfig:
+    """LeidenConfig (src/community_search/leiden/mod.rs:49-106)."""
+    objective: ObjectiveKind = field(default_factory=Rb)
+    seed: Optional[int] = 42
+    n_iterations: int = 2
+    max_levels: int = 64
+    tolerance: float = 1e-9
+    refine: bool = True
+    refine_randomness: float = 0.01
+    patience: int = 2
+    max_community_weight: Optional[float] = None
+
+    @classmethod
+    def with_resolution(cls, resolution: float) -> "LeidenConfig":
+        return cls(objective=Rb(resolution))
+
+    def to_c(self) -> _lib.LeidenConfigC:
+        c = _lib.LeidenConfigC()
+        c.objective = 0 if isinstance(self.objective, Rb) else 1
+        c.resolution = float(self.objective.resolution)
+        c.has_seed = 0 if self.seed is None else 1
+        c.seed = 0 if self.seed is None else int(self.seed) & ((1 << 64) - 1)
+        c.n_iterations = int(self.n_iterations)
+        c.max_levels = int(self.max_levels)
+        c.tolerance = float(self.tolerance)
+        c.refine = 1 if self.refine else 0
+        c.refine_randomness = float(self.refine_randomness)
+        c.patience = int(self.patience)
+        c.has_max_community_weight = 0 if self.max_community_weight is None else 1
+        c.max_community_weight = 0.0 if self.max_community_weight is None else float(
+            self.max_community_weight)
+        return c
+
+
+# ---------------------------------------------------------------- result
+class Clustering:
+    """Clustering (src/clustering.rs:11-108)."""
+
+    def __init__(self, labels: np.ndarray, n_clusters: int):
+        self._labels = labels
+        self._n = int(n_clusters)
+
+    def labels(self) -> np.ndarray:
+        return self._labels
+
+    def n_clusters(self) -> int:
+        return self._n
+
+    def __len__(self):
+        return len(self._labels)
+
+    def is_empty(self) -> bool:
+        return len(self._labels) == 0
+
+    def cluster_sizes(self) -> list:
+        return np.bincount(self._labels.astype(np.int64), minlength=self._n).tolist()
+
+    def into_labels(self) -> np.ndarray:
+        return self._labels
+
+    def __eq__(self, other):
+        return isinstance(other, Clustering) and self._n == other._n and np.array_equal(
+            self._labels, other._labels)
+
+
+# ---------------------------------------------------------------- graph
+class CSRNetwork:
+    """A device-resident CSRNetwork (src/network/csr_network.rs:62-69)."""
+
+    def __init__(self, handle: C.c_void_p, ctx):
+        self._h = handle
+        self._ctx = ctx
+
+    def __del__(self):
+        try:
+            if self._h:
+                lib().sc_graph_destroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    # constructors -------------------------------------------------------
+    @classmethod
+    def from_edges(cls, n_nodes: int, edges: Iterable, *, device: int | None = None):
+        """from_edges (csr_network.rs:104-109); edges are (u, v, w) tuples or an (m, 3) array."""
+        return cls._from_edges(n_nodes, edges, None, device)
+
+    @classmethod
+    def from_edges_with_node_weights(cls, edges: Iterable, node_weights: Sequence[float], *,
+                                     device: int | None = None):
+        nw = np.ascontiguousarray(node_weights, dtype=np.float64)
+        return cls._from_edges(len(nw), edges, nw, device)
+
+    @classmethod
+    def from_edge_arrays(cls, n_nodes: int, src, dst, w, node_weights=None, *, device=None):
+        src = np.ascontiguousarray(src, dtype=np.uint64)
+        dst = np.ascontiguousarray(dst, dtype=np.uint64)
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        nw = None if node_weights is None else np.ascontiguousarray(node_weights, np.float64)
+        ctx = context(device)
+        h = C.c_void_p()
+        _check(lib().sc_graph_from_edges(ctx.h, int(n_nodes), _ptr(src, _lib.u64p), _ptr(dst, _lib.u64p),
+                                         _ptr(w, _lib.f64p), len(src), _ptr(nw, _lib.f64p),
+                                         C.byref(h)), ctx)
+        return cls(h, ctx)
+
+    @classmethod
+    def _from_edges(cls, n_nodes, edges, nw, device):
+        if isinstance(edges, np.ndarray) and edges.ndim == 2:
+            src, dst, w = edges[:, 0], edges[:, 1], edges[:, 2]
+        else:
+            edges = list(edges)
+            src = [int(e[0]) for e in edges]
+            dst = [int(e[1]) for e in edges]
+            w = [float(e[2]) for e in edges]
+        return cls.from_edge_arrays(n_nodes, np.array(src, dtype=np.uint64),
+                                    np.array(dst, dtype=np.uint64), np.array(w, dtype=np.float64),
+                                    nw, device=device)
+
+    @classmethod
+    def from_csr_parts(cls, node_ptrs, neighbors, weights, node_weights=None, *, device=None):
+        """from_csr_parts (csr_network.rs:185-256)."""
+        ptrs = np.ascontiguousarray(node_ptrs, dtype=np.uint64)
+        nbrs = np.ascontiguousarray(neighbors, dtype=np.uint32)
+        w = np.ascontiguousarray(weights, dtype=np.float32)
+        nw = None if node_weights is None else np.ascontiguousarray(node_weights, np.float64)
+        ctx = context(device)
+        h = C.c_void_p()
+        _check(lib().sc_graph_from_csr(ctx.h, _ptr(ptrs, _lib.u64p), len(ptrs), _ptr(nbrs, _lib.u32p),
+                                       len(nbrs), _ptr(w, _lib.f32p), len(w), _ptr(nw, _lib.f64p),
+                                       0 if nw is None else len(nw), C.byref(h)), ctx)
+        return cls(h, ctx)
+
+    @classmethod
+    def from_csr_parts_device(cls, node_ptrs, neighbors, weights, node_weights=None, *, device=None):
+        """from_csr_parts on torch CUDA tensors already on the device (no host round trip)."""
+        ctx = context(device)
+        h = C.c_void_p()
+        nwp = None if node_weights is None else node_weights.data_ptr()
+        _check(lib().sc_graph_from_csr_device(ctx.h, node_ptrs.data_ptr(), node_ptrs.numel(),
+                                              neighbors.data_ptr(), neighbors.numel(),
+                                              weights.data_ptr(), weights.numel(), nwp,
+                                              0 if node_weights is None else node_weights.numel(),
+                                              C.byref(h)), ctx)
+        return cls(h, ctx)
+
+    @classmethod
+    def from_csr_matrix(cls, indptr, indices, data, node_weights=None, *, device=None):
+        """from_csr_matrix (csr_network.rs:360-391): reads the upper triangle only."""
+        indptr = np.ascontiguousarray(indptr, dtype=np.uint64)
+        indices = np.ascontiguousarray(indices, dtype=np.uint64)
+        data = np.ascontiguousarray(data, dtype=np.float64)
+        n = len(indptr) - 1
+        nw = None if node_weights is None else np.ascontiguousarray(node_weights, np.float64)
+        if nw is not None and len(nw) != n:
+            raise NodeWeightLengthMismatch(_mismatch_info(5, len(nw), n,
+                                                          "node weight vector has length {got}, expected {exp}"))
+        ctx = context(device)
+        h = C.c_void_p()
+        _check(lib().sc_graph_from_csr_matrix(ctx.h, _ptr(indptr, _lib.u64p), n, _ptr(indices, _lib.u64p),
+                                              _ptr(data, _lib.f64p), len(data), _ptr(nw, _lib.f64p),
+                                              C.byref(h)), ctx)
+        return cls(h, ctx)
+
+    # accessors ----------------------------------------------------------
+    def _info(self):
+        n, e, ec = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        tw, loops = C.c_double(), C.c_int32()
+        lib().sc_graph_info(self._h, C.byref(n), C.byref(e), C.byref(ec), C.byref(tw), C.byref(loops))
+        return n.value, e.value, ec.value, tw.value, bool(loops.value)
+
+    def node_count(self) -> int:
+        return self._info()[0]
+
+    def entry_count(self) -> int:
+        return self._info()[1]
+
+    def edge_count(self) -> int:
+        return self._info()[2]
+
+    def total_weight(self) -> float:
+        return self._info()[3]
+
+    def has_self_loops(self) -> bool:
+        return self._info()[4]
+
+    def to_csr_parts(self):
+        n, e, *_ = self._info()
+        ptr = np.zeros(n + 1, np.uint64)
+        nbr = np.zeros(e, np.uint32)
+        w = np.zeros(e, np.float32)
+        _check(lib().sc_graph_copy_csr(self._ctx.h, self._h, _ptr(ptr, _lib.u64p), _ptr(nbr, _lib.u32p),
+                                       _ptr(w, _lib.f32p)), self._ctx)
+        return ptr, nbr, w
+
+    def node_weights(self) -> np.ndarray:
+        n = self.node_count()
+        nw = np.zeros(n, np.float64)
+        _check(lib().sc_graph_copy_node_data(self._ctx.h, self._h, _ptr(nw, _lib.f64p), None), self._ctx)
+        return nw
+
+    def strengths(self) -> np.ndarray:
+        n = self.node_count()
+        st = np.zeros(n, np.float64)
+        _check(lib().sc_graph_copy_node_data(self._ctx.h, self._h, None, _ptr(st, _lib.f64p)), self._ctx)
+        return st
+
+    def strength(self, node: int) -> float:
+        return float(self.strengths()[node])
+
+    def node_weight(self, node: int) -> float:
+        return float(self.node_weights()[node])
+
+    def degree(self, node: int) -> int:
+        ptr, _, _ = self.to_csr_parts()
+        return int(ptr[node + 1] - ptr[node])
+
+    def neighbors(self, node: int):
+        ptr, nbr, w = self.to_csr_parts()
+        s, e = int(ptr[node]), int(ptr[node + 1])
+        return [(int(u), float(x)) for u, x in zip(nbr[s:e], w[s:e])]
+
+    def self_loop_weight(self, node: int) -> float:
+        for u, x in self.neighbors(node):
+            if u == node:
+                return x
+        return 0.0
+
+    def edge_weight(self, a: int, b: int):
+        for u, x in self.neighbors(a):
+            if u == b:
+                return x
+        return None
+
+    def validate_symmetry(self):
+        _check(lib().sc_graph_validate_symmetry(self._ctx.h, self._h), self._ctx)
+
+    def aggregate(self, groups) -> "CSRNetwork":
+        """aggregate(&VectorGrouping::from_assignments(groups)) (csr_network.rs:516-608)."""
+        g = np.ascontiguousarray(groups, dtype=np.uint64)
+        h = C.c_void_p()
+        _check(lib().sc_aggregate(self._ctx.h, self._h, _ptr(g, _lib.u64p), len(g), C.byref(h)), self._ctx)
+        return CSRNetwork(h, self._ctx)
+
+    def partition_stats(self, membership):
+        """Partition::from_membership aggregates (partition.rs:75-112) per slot."""
+        m = np.ascontiguousarray(membership, dtype=np.uint64)
+        cap = int(m.max()) + 1 if len(m) else 0
+        slots = C.c_uint64()
+        size = np.zeros(cap, np.uint32)
+        wt = np.zeros(cap, np.float64)
+        st = np.zeros(cap, np.float64)
+        inn = np.zeros(cap, np.float64)
+        _check(lib().sc_partition_stats(self._ctx.h, self._h, _ptr(m, _lib.u64p), len(m), C.byref(slots),
+                                        _ptr(size, _lib.u32p), _ptr(wt, _lib.f64p), _ptr(st, _lib.f64p),
+                                        _ptr(inn, _lib.f64p), cap), self._ctx)
+        return dict(size=size, weight=wt, strength=st, internal=inn)
+
+    def __str__(self):
+        n, _, ec, tw, _ = self._info()
+        dens = ec / (n * (n - 1) / 2) if n > 1 else 0.0
+        return f"CSRNetwork({n} nodes, {ec} edges, total_weight: {tw}, density: {dens:.4f})"
+
+
+def _mismatch_info(code, got, exp, fmt):
+    i = _lib.ErrorInfo()
+    i.code = code
+    i.got = got
+    i.expected_len = exp
+    i.message = fmt.format(got=got, exp=exp).encode()
+    return i
+
+
+# ---------------------------------------------------------------- algorithms
+def leiden(graph: CSRNetwork, config: LeidenConfig | None = None) -> Clustering:
+    """leiden(&graph, &config) (src/community_search/leiden/mod.rs:168-204)."""
+    return leiden_from(graph, config, None)
+
+
+def leiden_from(graph: CSRNetwork, config: LeidenConfig | None, initial) -> Clustering:
+    """leiden starting from `initial` labels (the `initial` of run_once, mod.rs:214-220)."""
+    cfg = (config or LeidenConfig()).to_c()
+    n = graph.node_count()
+    labels = np.zeros(n, np.uint64)
+    ncl = C.c_uint64()
+    ini = None if initial is None else np.ascontiguousarray(initial, dtype=np.uint64)
+    ctx = graph._ctx
+    _check(lib().sc_leiden_from(ctx.h, graph._h, C.byref(cfg), _ptr(ini, _lib.u64p),
+                                0 if ini is None else len(ini), _ptr(labels, _lib.u64p), C.byref(ncl)), ctx)
+    return Clustering(labels, ncl.value)
+
+
+def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig]) -> list:
+    """Many leiden() runs in one call (resolution x seed sweeps, many graphs)."""
+    count = len(graphs)
+    if count == 0:
+        return []
+    ctx = graphs[0]._ctx
+    sizes = [g.node_count() for g in graphs]
+    offs = np.zeros(count, np.uint64)
+    offs[1:] = np.cumsum(sizes)[:-1]
+    labels = np.zeros(int(sum(sizes)), np.uint64)
+    ncl = np.zeros(count, np.uint64)
+    harr = (C.c_void_p * count)(*[g._h for g in graphs])
+    carr = (_lib.LeidenConfigC * count)(*[c.to_c() for c in configs])
+    _check(lib().sc_leiden_batch(ctx.h, harr, carr, count, _ptr(offs, _lib.u64p), _ptr(labels, _lib.u64p),
+                                 _ptr(ncl, _lib.u64p)), ctx)
+    out = []
+    for i in range(count):
+        s = int(offs[i])
+        out.append(Clustering(labels[s:s + sizes[i]].copy(), int(ncl[i])))
+    return out
+
+
+def modularity(graph: CSRNetwork, labels, resolution: float = 1.0) -> float:
+    """modularity (src/community_search/leiden/objective.rs:221-244)."""
+    lab = np.ascontiguousarray(labels, dtype=np.uint64)
+    out = C.c_double()
+    _check(lib().sc_modularity(graph._ctx.h, graph._h, _ptr(lab, _lib.u64p), len(lab), float(resolution),
+                               C.byref(out)), graph._ctx)
+    return out.value
+
+
+def quality(graph: CSRNetwork, membership, objective: ObjectiveKind = Rb()) -> float:
+    """Rb::quality / Cpm::quality of Partition::from_membership (objective.rs:108-178)."""
+    m = np.ascontiguousarray(membership, dtype=np.uint64)
+    out = C.c_double()
+    kind = 0 if isinstance(objective, Rb) else 1
+    _check(lib().sc_quality(graph._ctx.h, graph._h, _ptr(m, _lib.u64p), len(m), kind,
+                            float(objective.resolution), C.byref(out)), graph._ctx)
+    return out.value
+
+
+def last_run_stats(device: int | None = None) -> dict:
+    return context(device).run_stats()
+
+
+__all__ = [
+    "CSRNetwork", "LeidenConfig", "Rb", "Cpm", "ObjectiveKind", "Clustering", "leiden", "leiden_from",
+    "leiden_batch", "modularity", "quality", "ClusteringError", "NodeIndexOutOfRange", "NonFiniteWeight",
+    "NegativeWeight", "InvalidNodeWeight", "NodeWeightLengthMismatch", "MembershipLengthMismatch",
+    "InvalidConfig", "TooManyNodes", "InvalidCsr", "AsymmetricGraph", "DeviceError", "MAX_NODES", "NOISE",
+    "last_run_stats", "context",
+]

@@ -1,0 +1,94 @@
+"""Seeded synthetic inputs with the shapes of the benchmark configurations.
+
+No public dataset is used anywhere: every workload is drawn from numpy's
+PCG64 with a recorded seed, so the CPU oracle and the GPU path see identical
+bytes.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def planted_partition(n: int = 20_000, blocks: int = 40, intra: int = 12, inter: int = 3,
+                      seed: int = 1, w_lo: float = 0.5, w_hi: float = 1.5):
+    """Planted-partition edge list: each node draws `intra` partners inside its
+    block and `inter` partners outside it, uniformly; weights f32 U[w_lo, w_hi].
+
+    Returns (src u64, dst u64, w f64 holding f32 values, truth labels). Duplicate
+    pairs are left in: `from_edges` merges them by summing (csr_network.rs:104-109).
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    per = n // blocks
+    node = np.arange(n, dtype=np.int64)
+    block = np.minimum(node // per, blocks - 1)
+    base = block * per
+    size = np.where(block == blocks - 1, n - base, per)
+    src_a = np.repeat(node, intra)
+    off = rng.integers(1, np.repeat(size, intra), dtype=np.int64)
+    dst_a = base[src_a] + ((src_a - base[src_a]) + off) % size[src_a]
+    src_b = np.repeat(node, inter)
+    outside = n - size[src_b]
+    r = rng.integers(0, outside, dtype=np.int64)
+    dst_b = np.where(r < base[src_b], r, r + size[src_b])
+    src = np.concatenate([src_a, src_b]).astype(np.uint64)
+    dst = np.concatenate([dst_a, dst_b]).astype(np.uint64)
+    w = rng.uniform(w_lo, w_hi, size=src.shape[0]).astype(np.float32).astype(np.float64)
+    return src, dst, w, block.astype(np.uint64)
+
+
+def gaussian_mixture(n: int, d: int, components: int, seed: int, sigma=(1.0, 1.0),
+                     centre_scale: float = 2.0):
+    """Isotropic Gaussian mixture, f32 row-major [n, d]: centres ~ N(0, centre_scale^2 I),
+    per-component sigma ~ U[sigma], mixture weights ~ Dirichlet(1)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    centres = rng.normal(0.0, centre_scale, size=(components, d))
+    sig = rng.uniform(sigma[0], sigma[1], size=components)
+    pi = rng.dirichlet(np.ones(components))
+    comp = rng.choice(components, size=n, p=pi)
+    x = np.empty((n, d), dtype=np.float32)
+    chunk = 1 << 20
+    for s in range(0, n, chunk):
+        e = min(n, s + chunk)
+        c = comp[s:e]
+        x[s:e] = (centres[c] + rng.standard_normal((e - s, d)) * sig[c, None]).astype(np.float32)
+    return x, comp.astype(np.uint64)
+
+
+def knn_like_graph(n: int, k: int = 10, blocks: int = 100, seed: int = 7):
+    """A symmetrised kNN-shaped CSR without a full kNN search: points on a 2-D
+    jittered lattice per block, each linked to k lattice neighbours; Gaussian
+    weights of the lattice distance. Returns (ptrs u64, nbrs u32, w f32)."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    side = int(np.ceil(np.sqrt(n)))
+    idx = np.arange(n, dtype=np.int64)
+    gx, gy = idx % side, idx // side
+    offs = [(1, 0), (0, 1), (1, 1), (1, -1), (2, 0), (0, 2), (2, 1), (1, 2), (2, -1), (1, -2)]
+    offs = offs[: max(1, k // 2 + k % 2)]
+    src_l, dst_l = [], []
+    for dx, dy in offs:
+        nx, ny = gx + dx, gy + dy
+        ok = (nx >= 0) & (nx < side) & (ny >= 0)
+        j = ny * side + nx
+        ok &= j < n
+        src_l.append(idx[ok])
+        dst_l.append(j[ok])
+    src = np.concatenate(src_l)
+    dst = np.concatenate(dst_l)
+    # random long-range rewiring keeps it from being a pure lattice
+    rew = rng.random(src.shape[0]) < 0.02
+    dst[rew] = rng.integers(0, n, size=int(rew.sum()))
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    lo, hi = np.minimum(src, dst), np.maximum(src, dst)
+    key = np.unique(lo * n + hi)
+    lo, hi = key // n, key % n
+    d2 = ((gx[lo] - gx[hi]) ** 2 + (gy[lo] - gy[hi]) ** 2).astype(np.float64)
+    w = np.exp(-d2 / 4.0) * rng.uniform(0.6, 1.0, size=lo.shape[0])
+    rows = np.concatenate([lo, hi])
+    cols = np.concatenate([hi, lo])
+    ww = np.concatenate([w, w]).astype(np.float32)
+    order = np.lexsort((cols, rows))
+    rows, cols, ww = rows[order], cols[order], ww[order]
+    ptrs = np.zeros(n + 1, dtype=np.uint64)
+    np.cumsum(np.bincount(rows, minlength=n), out=ptrs[1:])
+    return ptrs, cols.astype(np.uint32), ww
