@@ -137,7 +137,10 @@ void DevGraph::free_all() {
         cudaGetDevice(&prev);
         if (prev != device) cudaSetDevice(device);
         for (void* p : ps)
-            if (p) cudaFree(p);
+            if (p) {
+                if (stream) cudaFreeAsync(p, stream);
+                else cudaFree(p);
+            }
         if (prev != device) cudaSetDevice(prev);
     }
     ptr = nullptr;

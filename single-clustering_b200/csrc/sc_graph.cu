@@ -14,20 +14,31 @@ namespace {
 
 constexpr unsigned TB = 256;
 
-void galloc(DevGraph& g, uint64_t n, uint64_t E) {
+template <class T>
+void palloc(Ctx& c, T** p, uint64_t count) {
+    cudaError_t e = cudaMallocAsync((void**)p, count * sizeof(T), c.stream);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(SC_E_OUT_OF_MEMORY, "device allocation of %llu bytes failed",
+             (unsigned long long)(count * sizeof(T)));
+    }
+    if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
+}
+
+void galloc(Ctx& c, DevGraph& g, uint64_t n, uint64_t E) {
     SC_CUDA(cudaGetDevice(&g.device));
     g.n = n;
     g.E = E;
-    SC_CUDA(cudaMalloc(&g.ptr, (n + 1) * sizeof(uint64_t)));
+    palloc(c, &g.ptr, n + 1);
     if (E) {
-        SC_CUDA(cudaMalloc(&g.nbr, E * sizeof(uint32_t)));
-        SC_CUDA(cudaMalloc(&g.w, E * sizeof(float)));
-        SC_CUDA(cudaMalloc(&g.erow, E * sizeof(uint32_t)));
+        palloc(c, &g.nbr, E);
+        palloc(c, &g.w, E);
+        palloc(c, &g.erow, E);
     }
     if (n) {
-        SC_CUDA(cudaMalloc(&g.node_w, n * sizeof(double)));
-        SC_CUDA(cudaMalloc(&g.strength, n * sizeof(double)));
-        SC_CUDA(cudaMalloc(&g.self_loop, n * sizeof(double)));
+        palloc(c, &g.node_w, n);
+        palloc(c, &g.strength, n);
+        palloc(c, &g.self_loop, n);
     }
 }
 
@@ -162,7 +173,7 @@ __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __
                             const float* __restrict__ w, uint64_t n, double* strength,
                             double* self_loop, int* min_low, unsigned* any_loop, unsigned* max_deg) {
     int low = 0x7FFFFFFF;
-    unsigned loop = 0, mdeg = 0;
+    unsigned loop = 0, mdeg = 0, hubs = 0;
     for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
          v += (uint64_t)gridDim.x * blockDim.x) {
         uint64_t b = ptr[v], e = ptr[v + 1];
@@ -182,16 +193,19 @@ __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __
         strength[v] = s;
         self_loop[v] = sl;
         mdeg = max(mdeg, (unsigned)(e - b));
+        hubs += (e - b) > HUB_DEGREE;
     }
     for (int o = 16; o; o >>= 1) {
         low = min(low, __shfl_xor_sync(0xFFFFFFFFu, low, o));
         loop |= __shfl_xor_sync(0xFFFFFFFFu, loop, o);
         mdeg = max(mdeg, __shfl_xor_sync(0xFFFFFFFFu, mdeg, o));
+        hubs += __shfl_xor_sync(0xFFFFFFFFu, hubs, o);
     }
     if ((threadIdx.x & 31) == 0) {
         if (low != 0x7FFFFFFF) atomicMin(min_low, low);
         if (loop) atomicOr(any_loop, 1u);
         atomicMax(max_deg, mdeg);
+        if (hubs) atomicAdd(any_loop + 2, hubs);
     }
 }
 
@@ -277,10 +291,10 @@ double rust_sum_dev(Ctx& c, const double* d, uint64_t n, bool exact) {
 void finalize(Ctx& c, DevGraph& g, bool check_sum) {
     const uint64_t n = g.n;
     DBuf<int> d_low(c, 2);
-    DBuf<unsigned> d_flags(c, 2);
+    DBuf<unsigned> d_flags(c, 3);
     int init_low[2] = {0x7FFFFFFF, 0x7FFFFFFF};
     h2d(c, d_low.get(), init_low, 2);
-    zero(c, d_flags.get(), 2);
+    zero(c, d_flags.get(), 3);
     if (n) {
         k_row_stats<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength,
                                                           g.self_loop, d_low.get(), d_flags.get(),
@@ -291,12 +305,13 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
         c.launches += 2;
     }
     int low[2];
-    unsigned flags[2];
+    unsigned flags[3];
     d2h(c, low, d_low.get(), 2);
-    d2h(c, flags, d_flags.get(), 2);
+    d2h(c, flags, d_flags.get(), 3);
     sync(c);
     g.any_self_loops = flags[0] != 0;
     g.max_degree = flags[1];
+    g.n_hubs = flags[2];
     g.e0_w = low[0];
     g.e0_nw = low[1];
 
@@ -369,19 +384,18 @@ void finish(Ctx& c, DevGraph& g) {
             float* w2 = nullptr;
             uint32_t* erow2 = nullptr;
             if (E2) {
-                SC_CUDA(cudaMalloc(&nbr2, E2 * sizeof(uint32_t)));
-                SC_CUDA(cudaMalloc(&w2, E2 * sizeof(float)));
-                SC_CUDA(cudaMalloc(&erow2, E2 * sizeof(uint32_t)));
+                palloc(c, &nbr2, E2);
+                palloc(c, &w2, E2);
+                palloc(c, &erow2, E2);
             }
             k_merge_write<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, keys_s.get(), w_s.get(), n,
                                                                 nptr.get(), nbr2, w2);
             SC_LAUNCH_CHECK();
             c.launches += 2;
             d2d(c, g.ptr, nptr.get(), n + 1);
-            sync(c);
-            cudaFree(g.nbr);
-            cudaFree(g.w);
-            cudaFree(g.erow);
+            cudaFreeAsync(g.nbr, c.stream);
+            cudaFreeAsync(g.w, c.stream);
+            cudaFreeAsync(g.erow, c.stream);
             g.nbr = nbr2;
             g.w = w2;
             g.erow = erow2;
@@ -421,7 +435,7 @@ DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint
              (unsigned long long)n_nbr, (unsigned long long)n_w);
     const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     std::unique_ptr<DevGraph> g(new DevGraph());
-    galloc(*g, n, n_nbr);
+    galloc(c, *g, n, n_nbr);
     SC_CUDA(cudaMemcpyAsync(g->ptr, ptr, n_ptr * sizeof(uint64_t), kind, c.stream));
     if (n_nbr) {
         SC_CUDA(cudaMemcpyAsync(g->nbr, nbr, n_nbr * sizeof(uint32_t), kind, c.stream));
@@ -627,7 +641,7 @@ DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint6
     uint64_t loops_slots = 0;
     for (uint64_t i = 0; i < m; ++i) loops_slots += from[i] == to[i];
     const uint64_t E = 2 * m - loops_slots;
-    galloc(*g, n, E);
+    galloc(c, *g, n, E);
     d2d(c, g->node_w, nw.get(), n);
     if (E) {
         k_split_keys<<<grid_for(E, TB), TB, 0, c.stream>>>(keys_s.get(), E, g->erow, g->nbr);
@@ -893,7 +907,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
     }
     // assemble
     const uint64_t E2 = K + L;
-    galloc(*out, G, E2);
+    galloc(c, *out, G, E2);
     d2d(c, out->node_w, nw_new.get(), G);
     {
         DBuf<uint64_t> us(c, (uint64_t)G + 1), ls(c, (uint64_t)G + 1), cnt(c, (uint64_t)G + 1);

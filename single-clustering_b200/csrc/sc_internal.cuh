@@ -57,6 +57,8 @@ struct Failure {
 #define SC_LAUNCH_CHECK() SC_CUDA(cudaGetLastError())
 
 // ------------------------------------------------------------------ context
+constexpr uint32_t HUB_DEGREE = 1024;  // degree above which a node's hash lives in global memory
+
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -138,6 +140,11 @@ struct DevGraph {
     int e0_nw = 0;            // same over node weights
     bool exact_nw = true;
     double total_node_weight = 0.0;  // Σ node_w, Rust `sum()` order
+    uint64_t n_hubs = 0;      // nodes whose degree exceeds the shared-memory hash
+    // Arrays come from the stream-ordered pool. A graph owned by a running call
+    // (a coarse level) returns them on that stream; a graph handed to the user
+    // (stream == nullptr) frees them with cudaFree.
+    cudaStream_t stream = nullptr;
     void free_all();
     ~DevGraph() { free_all(); }
 };

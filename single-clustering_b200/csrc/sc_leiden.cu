@@ -25,13 +25,13 @@ namespace sc {
 namespace {
 
 constexpr unsigned TB = 256;
-constexpr int NBUCKET = 4;          // G8, G16, G32, block
-constexpr int HCAP_SMEM = 4096;     // shared hash entries per block (u32 key + i64 val)
+constexpr int NBUCKET = 5;          // G8, G16, G32, block (shared hash), hub (global hash)
+constexpr int HCAP_SMEM = 2 * HUB_DEGREE;  // shared hash entries per block (u32 key + i64 val): 24 KB
 constexpr int LM_BATCHES = 8;
 constexpr int RF_BATCHES = 8;
 constexpr int MAX_SWEEPS = 100;
 constexpr uint32_t EMPTYK = 0xFFFFFFFFu;
-constexpr int REF_CAND_SMEM = 2048;  // candidates sorted in shared memory per block
+constexpr int CAND_SMEM = HUB_DEGREE;  // refinement candidates held in shared memory per block
 
 struct Params {
     // graph
@@ -68,6 +68,9 @@ struct Params {
     uint32_t* status;
     unsigned long long* counters;  // [0] moves, [1] Σdeg, [2] Σcand, [3] nodes
     long long* gain_acc;
+    // max_community_weight: one joiner per target community per batch (the
+    // highest claim key wins), so a community never passes the cap
+    unsigned long long* claim;
 };
 
 __device__ __forceinline__ long long to_fix(double x, double inv) { return __double2ll_rn(__dmul_rn(x, inv)); }
@@ -106,6 +109,16 @@ __device__ __forceinline__ bool cancelled(const Params& p, uint32_t x) {
         return px < ph || (px == ph && x < h);
     }
     return true;
+}
+
+__device__ __forceinline__ unsigned long long claim_key(const Params& p, uint32_t v) {
+    return ((unsigned long long)p.cur << 40) | ((prio(p.seed ^ 0x77ull, p.cur, v) & 0xFFull) << 32) | v;
+}
+
+// Whether node x's move is dropped: cancelled, or beaten to a capped community.
+__device__ __forceinline__ bool lost(const Params& p, uint32_t x) {
+    if (cancelled(p, x)) return true;
+    return p.has_limit && p.claim[p.tgt[x]] != claim_key(p, x);
 }
 
 __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t a, uint64_t b) {
@@ -430,13 +443,22 @@ __device__ void block_bitonic(uint32_t* key, double* val, uint32_t n) {
     }
 }
 
-template <bool REFINE>
+// One block per node. HUB = false: degree <= HUB_DEGREE, hash table and
+// candidate list in shared memory. HUB = true: both in this block's slice of
+// the global scratch (gcap entries each), which the host sized for the
+// largest degree; the grid never exceeds the number of slices.
+template <bool REFINE, bool HUB>
 __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* __restrict__ list,
                                                      uint32_t count, uint32_t* gkeys, long long* gvals,
                                                      uint32_t* gck, double* gcr, uint64_t gcap) {
     extern __shared__ __align__(16) unsigned char smem[];
     long long* s_vals = (long long*)smem;
-    uint32_t* s_keys = (uint32_t*)(smem + HCAP_SMEM * sizeof(long long));
+    double* s_cr = (double*)(smem + HCAP_SMEM * sizeof(long long));
+    uint32_t* s_keys = (uint32_t*)(smem + (HCAP_SMEM + CAND_SMEM) * sizeof(long long));
+    uint32_t* s_ck = s_keys + HCAP_SMEM;
+    const uint64_t ccap = HUB ? gcap : (uint64_t)CAND_SMEM;
+    uint32_t* ck = HUB ? gck + (uint64_t)blockIdx.x * gcap : s_ck;
+    double* cr = HUB ? gcr + (uint64_t)blockIdx.x * gcap : s_cr;
     __shared__ double red_g[32];
     __shared__ uint32_t red_c[32];
     __shared__ uint32_t s_member, s_ncand, s_target;
@@ -453,7 +475,11 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
         while (cap < 2 * deg) cap <<= 1;
         uint32_t* keys;
         long long* vals;
-        if (cap <= (uint32_t)HCAP_SMEM) {
+        if (!HUB) {
+            if (cap > (uint32_t)HCAP_SMEM) {  // not this bucket's node: skip it, flag it
+                if (threadIdx.x == 0) atomicOr(p.status, DEV_OVERFLOW);
+                continue;
+            }
             keys = s_keys;
             vals = s_vals;
         } else {
@@ -500,9 +526,9 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
                 double rel = __dsub_rn(gg, base);
                 if (rel >= 0.0) {
                     uint32_t slot = atomicAdd(&s_ncand, 1u);
-                    if (slot < gcap) {
-                        gck[(uint64_t)blockIdx.x * gcap + slot] = cu;
-                        gcr[(uint64_t)blockIdx.x * gcap + slot] = rel;
+                    if (slot < ccap) {
+                        ck[slot] = cu;
+                        cr[slot] = rel;
                     }
                     if (rel > g) g = rel;
                 }
@@ -552,20 +578,18 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             block_argmax(x, dummy, red_g, red_c);
             if (threadIdx.x == 0) s_bestrel = x;
             __syncthreads();
-            uint32_t nc = min(s_ncand, (uint32_t)gcap);
-            if (threadIdx.x == 0 && s_ncand > gcap) atomicOr(p.status, DEV_OVERFLOW);
+            uint32_t nc = min(s_ncand, (uint32_t)ccap);
+            if (threadIdx.x == 0 && s_ncand > ccap) atomicOr(p.status, DEV_OVERFLOW);
             uint32_t n2 = 1;
             while (n2 < nc) n2 <<= 1;
-            uint32_t* ck = gck + (uint64_t)blockIdx.x * gcap;
-            double* cr = gcr + (uint64_t)blockIdx.x * gcap;
-            if (n2 <= gcap) {
+            if (n2 <= ccap) {
                 for (uint32_t s = nc + threadIdx.x; s < n2; s += blockDim.x) {
                     ck[s] = 0xFFFFFFFFu;
                     cr[s] = 0.0;
                 }
             }
             __syncthreads();
-            if (nc > 1 && n2 <= gcap) block_bitonic(ck, cr, n2);
+            if (nc > 1 && n2 <= ccap) block_bitonic(ck, cr, n2);
             if (threadIdx.x == 0) {
                 uint32_t target = NONE32;
                 double best_rel = s_bestrel;
@@ -637,7 +661,7 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = list[i];
         if (p.epoch[v] != p.cur) continue;
-        if (cancelled(p, v)) continue;
+        if (lost(p, v)) continue;
         const uint32_t t = p.tgt[v], old = p.from[v];
         const long long kf = to_fix(p.strength[v], p.inv_scale);
         const long long af = to_fix(p.node_w[v], p.inv_nscale);
@@ -656,7 +680,7 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
                 uint32_t u = p.nbr[j];
                 if (u == v) continue;
                 uint32_t cu;
-                if (p.epoch[u] == p.cur) cu = cancelled(p, u) ? p.from[u] : p.tgt[u];
+                if (p.epoch[u] == p.cur) cu = lost(p, u) ? p.from[u] : p.tgt[u];
                 else cu = p.memb[u];
                 if (cu != t) next_active[u] = 1;
             }
@@ -667,9 +691,18 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
     if ((threadIdx.x & 31) == 0 && gsum) atomicAdd((unsigned long long*)p.gain_acc, (unsigned long long)gsum);
 }
 
+__global__ void k_claim(Params p, const uint32_t* __restrict__ list, uint32_t count) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = list[i];
+        if (p.epoch[v] != p.cur || cancelled(p, v)) continue;
+        atomicMax(p.claim + p.tgt[v], claim_key(p, v));
+    }
+}
+
 // ------------------------------------------------------------ bucketing
 __device__ __forceinline__ int bucket_of(uint32_t deg) {
-    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : 3;
+    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= HUB_DEGREE ? 3 : 4;
 }
 
 __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
@@ -813,18 +846,22 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.gain_acc.alloc(c, 1);
     zero(c, ws.epoch.get(), n);
     zero(c, ws.hint.get(), n);
-    // global hash / candidate scratch for nodes past the shared-memory table
-    uint64_t cap = 64;
-    while (cap < 2ull * g.max_degree) cap <<= 1;
-    int nblk = c.sm_count * 2;
-    uint64_t budget = 1ull << 31;  // bytes for the large-degree scratch
-    while (nblk > 1 && (uint64_t)nblk * cap * 24 > budget) nblk >>= 1;
-    ws.nblk_large = nblk;
-    ws.gcap = cap;
-    ws.gkeys.alloc(c, (uint64_t)nblk * cap);
-    ws.gvals.alloc(c, (uint64_t)nblk * cap);
-    ws.gck.alloc(c, (uint64_t)nblk * cap);
-    ws.gcr.alloc(c, (uint64_t)nblk * cap);
+    // global hash / candidate scratch, one slice per block, for the hubs only
+    ws.nblk_large = 0;
+    ws.gcap = 0;
+    if (g.n_hubs) {
+        uint64_t cap = 64;
+        while (cap < 2ull * g.max_degree) cap <<= 1;
+        int nblk = (int)std::min<uint64_t>((uint64_t)c.sm_count * 2, g.n_hubs);
+        const uint64_t budget = 1ull << 31;  // bytes of hub scratch at most
+        while (nblk > 1 && (uint64_t)nblk * cap * 24 > budget) nblk >>= 1;
+        ws.nblk_large = nblk;
+        ws.gcap = cap;
+        ws.gkeys.alloc(c, (uint64_t)nblk * cap);
+        ws.gvals.alloc(c, (uint64_t)nblk * cap);
+        ws.gck.alloc(c, (uint64_t)nblk * cap);
+        ws.gcr.alloc(c, (uint64_t)nblk * cap);
+    }
 }
 
 template <bool REFINE>
@@ -838,11 +875,16 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list
         k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
     } else if (k == 2) {
         k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+    } else if (k == 3) {
+        size_t sm = (HCAP_SMEM + CAND_SMEM) * (sizeof(long long) + sizeof(uint32_t));
+        unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
+        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, cnt, nullptr, nullptr, nullptr,
+                                                                  nullptr, 0);
     } else {
-        size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
+        if (ws.nblk_large < 1 || ws.gcap == 0) fail(SC_E_INTERNAL, "hub scratch missing");
         unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
-        k_decide_block<REFINE><<<grid, TB, sm, c.stream>>>(p, list, cnt, ws.gkeys.get(), ws.gvals.get(),
-                                                          ws.gck.get(), ws.gcr.get(), ws.gcap);
+        k_decide_block<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, cnt, ws.gkeys.get(), ws.gvals.get(),
+                                                               ws.gck.get(), ws.gcr.get(), ws.gcap);
     }
     SC_LAUNCH_CHECK();
     c.launches++;
@@ -864,6 +906,8 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     const uint64_t S = S0 + n;
     DBuf<long long> Kf(c, S), Wf(c, S);
     DBuf<uint32_t> csize(c, S);
+    DBuf<unsigned long long> claim(c, cfg.has_max_community_weight ? S : 0);
+    zero(c, claim.get(), claim.n);
     zero(c, Kf.get(), S);
     zero(c, Wf.get(), S);
     zero(c, csize.get(), S);
@@ -904,6 +948,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     p.status = c.d_status;
     p.counters = ws.counters.get();
     p.gain_acc = ws.gain_acc.get();
+    p.claim = claim.get();
     zero(c, ws.counters.get(), 4);
     zero(c, ws.gain_acc.get(), 1);
     zero(c, ws.epoch.get(), n);
@@ -948,6 +993,10 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
                 uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
                 launch_decide<false>(c, p, ws, k, ws.list.get() + s, e - s);
             }
+            if (p.has_limit) {
+                k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
+                c.launches++;
+            }
             k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
                                                                        ws.next_active.get());
             SC_LAUNCH_CHECK();
@@ -975,6 +1024,8 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     if (n == 0) return 0.0;
     DBuf<long long> Kf(c, n), Wf(c, n);
     DBuf<uint32_t> csize(c, n);
+    DBuf<unsigned long long> claim(c, cfg.has_max_community_weight ? n : 0);
+    zero(c, claim.get(), claim.n);
     zero(c, Kf.get(), n);
     zero(c, Wf.get(), n);
     zero(c, csize.get(), n);
@@ -1017,6 +1068,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     p.status = c.d_status;
     p.counters = ws.counters.get();
     p.gain_acc = ws.gain_acc.get();
+    p.claim = claim.get();
     zero(c, ws.counters.get(), 4);
     zero(c, ws.epoch.get(), n);
     const int B = RF_BATCHES;
@@ -1044,6 +1096,10 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
         for (int k = 0; k < NBUCKET; ++k) {
             uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
             launch_decide<true>(c, p, ws, k, ws.list.get() + s, e - s);
+        }
+        if (p.has_limit) {
+            k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
+            c.launches++;
         }
         k_apply<true><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo, nullptr);
         SC_LAUNCH_CHECK();
@@ -1074,8 +1130,10 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
     c.launches++;
     uint64_t C = C0;
     double improvement = 0.0;
+    static const bool trace = std::getenv("SC_TRACE") != nullptr;
     for (uint64_t level = 0; level < cfg.max_levels; ++level) {
         const uint64_t nl = gl->n;
+        const sc_run_stats before = st;
         const uint64_t lvl_seed = hash3(pass_seed, level, 0x1eafull);
         Scales sc = scales_for(*gl);
         Workspace ws;
@@ -1106,11 +1164,24 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         DBuf<uint32_t> grp(c, nl);
         uint32_t G = renumber_ids(c, collapse.get(), nl, id_space, grp.get());
         st.levels++;
+        auto trace_level = [&](uint64_t ng) {
+            if (!trace) return;
+            std::fprintf(stderr,
+                         "[sc] level %llu n=%llu E=%llu groups=%llu sweeps=%llu moves=%llu lm=%.3fms "
+                         "ref=%.3fms agg=%.3fms\n",
+                         (unsigned long long)level, (unsigned long long)nl, (unsigned long long)gl->E,
+                         (unsigned long long)ng,
+                         (unsigned long long)(st.local_move_sweeps - before.local_move_sweeps),
+                         (unsigned long long)(st.moves - before.moves), st.ms_local_move - before.ms_local_move,
+                         st.ms_refine - before.ms_refine, st.ms_aggregate - before.ms_aggregate);
+        };
         if (G >= nl) {
             st.ms_aggregate += t_agg.stop();
+            trace_level(G);
             break;
         }
         std::unique_ptr<DevGraph> coarse(graph_aggregate(c, *gl, grp.get(), G));
+        coarse->stream = c.stream;
         st.alg_bytes_aggregate += 12.0 * (double)gl->E + 12.0 * (double)nl + 8.0 * (double)coarse->E +
                                   24.0 * (double)coarse->n;
         // coarse membership from the working partition (mod.rs:269-272), compacted
@@ -1124,6 +1195,7 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         owned = std::move(coarse);
         gl = owned.get();
         st.ms_aggregate += t_agg.stop();
+        trace_level(G);
     }
     // final ascending renumber (mod.rs:282-286)
     const uint64_t nl = gl->n;
