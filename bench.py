@@ -95,11 +95,29 @@ def knn_graph_torch(n, d, comps, seed, k, device):
     return out
 
 
+def knn_graph_sc(n, d, comps, seed, k, device_index):
+    """The library's own kNN builder: exact search (BF16 tcgen05 candidates +
+    FP32 re-rank), sigma = k-th distance, union symmetrisation."""
+    import sc_gpu
+    from sc_gpu import synth
+    X, _ = synth.gaussian_mixture(n, d, comps, seed, sigma=(0.7, 1.5))
+    t = time.perf_counter()
+    r = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    KNN_INFO["seconds"] = time.perf_counter() - t
+    KNN_INFO["stats"] = sc_gpu.last_run_stats(device_index)
+    return r.conn_ptrs, r.conn_nbrs, r.conn_w
+
+
+KNN_INFO = {}
+
+
 def make_graph(args, device):
     if args.graph == "lattice":
         from sc_gpu import synth
         return synth.knn_like_graph(args.n, k=K, seed=GRAPH_SEED)
-    return knn_graph_torch(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device)
+    if args.graph == "gmm-torch":
+        return knn_graph_torch(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device)
+    return knn_graph_sc(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device.index or 0)
 
 
 # ---------------------------------------------------------------- clocks
@@ -182,7 +200,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
-    ap.add_argument("--graph", default="gmm", choices=["gmm", "lattice"])
+    ap.add_argument("--graph", default="gmm", choices=["gmm", "gmm-torch", "lattice"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
@@ -293,6 +311,8 @@ def main():
             "clocks": clk,
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
+    if KNN_INFO:
+        line["knn_graph_build_s"] = KNN_INFO["seconds"]
     if not args.no_cpu_baseline:
         og, lab_o, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
         q_o = og.modularity(lab_o)

@@ -166,34 +166,40 @@ __global__ void k_merge_write(const uint64_t* __restrict__ ptr_in, const uint64_
     }
 }
 
-// Per row of a clean CSR: strength in ascending-neighbour order (self-loop
-// twice, csr_network.rs:313-320), self-loop weight, lowest set bit of the
-// stored weights, any self-loop, max degree.
+// Per row of a clean CSR, one warp per row: strength in ascending-neighbour
+// order (self-loop twice, csr_network.rs:313-320), self-loop weight, lowest set
+// bit of the stored weights, any self-loop, max degree, hub count.
 __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                             const float* __restrict__ w, uint64_t n, double* strength,
                             double* self_loop, int* min_low, unsigned* any_loop, unsigned* max_deg) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     int low = 0x7FFFFFFF;
     unsigned loop = 0, mdeg = 0, hubs = 0;
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t b = ptr[v], e = ptr[v + 1];
-        double s = 0.0, sl = 0.0;
-        for (uint64_t i = b; i < e; ++i) {
+    for (uint64_t v = warp; v < n; v += nwarps) {
+        const uint64_t b = ptr[v], e = ptr[v + 1];
+        double sl = 0.0;
+        for (uint64_t i = b + lane; i < e; i += 32) {
             float x = w[i];
-            double st = (double)x;
             low = min(low, lowbit_exp_f32(x));
             if (nbr[i] == (uint32_t)v) {
                 loop = 1;
-                sl = st;
-                s = __dadd_rn(s, __dmul_rn(2.0, st));
-            } else {
-                s = __dadd_rn(s, st);
+                sl = (double)x;
             }
         }
-        strength[v] = s;
-        self_loop[v] = sl;
-        mdeg = max(mdeg, (unsigned)(e - b));
-        hubs += (e - b) > HUB_DEGREE;
+        const double s = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) {
+            const double st = (double)w[i];
+            return nbr[i] == (uint32_t)v ? __dmul_rn(2.0, st) : st;
+        });
+        // at most one lane saw the self-loop
+        for (int o = 16; o; o >>= 1) sl = fmax(sl, __shfl_xor_sync(0xFFFFFFFFu, sl, o));
+        if (lane == 0) {
+            strength[v] = s;
+            self_loop[v] = sl;
+            mdeg = max(mdeg, (unsigned)(e - b));
+            hubs += (e - b) > HUB_DEGREE;
+        }
     }
     for (int o = 16; o; o >>= 1) {
         low = min(low, __shfl_xor_sync(0xFFFFFFFFu, low, o));
@@ -201,7 +207,7 @@ __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __
         mdeg = max(mdeg, __shfl_xor_sync(0xFFFFFFFFu, mdeg, o));
         hubs += __shfl_xor_sync(0xFFFFFFFFu, hubs, o);
     }
-    if ((threadIdx.x & 31) == 0) {
+    if (lane == 0) {
         if (low != 0x7FFFFFFF) atomicMin(min_low, low);
         if (loop) atomicOr(any_loop, 1u);
         atomicMax(max_deg, mdeg);
@@ -296,7 +302,7 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
     h2d(c, d_low.get(), init_low, 2);
     zero(c, d_flags.get(), 3);
     if (n) {
-        k_row_stats<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength,
+        k_row_stats<<<grid_for(n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength,
                                                           g.self_loop, d_low.get(), d_flags.get(),
                                                           d_flags.get() + 1);
         SC_LAUNCH_CHECK();
@@ -667,21 +673,22 @@ __global__ void k_iota(uint32_t* p, uint64_t n) {
         p[i] = (uint32_t)i;
 }
 
-// Per group, in ascending member order: Σ node weight (csr_network.rs:520-523)
-// and Σ self-loop weight (the `self_loop_weight` accumulator of :549-554).
+// Per group, in ascending member order, one warp per group: Σ node weight
+// (csr_network.rs:520-523) and Σ self-loop weight (the `self_loop_weight`
+// accumulator of :549-554; members without a loop add +0.0, a no-op).
 __global__ void k_group_sums(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
                              uint64_t G, const double* __restrict__ node_w,
                              const double* __restrict__ self_loop, double* nw_out, double* loops_out) {
-    for (uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; gi < G;
-         gi += (uint64_t)gridDim.x * blockDim.x) {
-        double a = 0.0, l = 0.0;
-        for (uint64_t i = gstart[gi]; i < gstart[gi + 1]; ++i) {
-            uint32_t v = members[i];
-            a = __dadd_rn(a, node_w[v]);
-            l = __dadd_rn(l, self_loop[v]);
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t gi = warp; gi < G; gi += nwarps) {
+        const uint64_t b = gstart[gi], e = gstart[gi + 1];
+        const double a = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return node_w[members[i]]; });
+        const double l = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return self_loop[members[i]]; });
+        if ((threadIdx.x & 31) == 0) {
+            nw_out[gi] = a;
+            loops_out[gi] = l;
         }
-        nw_out[gi] = a;
-        loops_out[gi] = l;
     }
 }
 
@@ -709,17 +716,19 @@ __global__ void k_iota64(uint64_t* p, uint64_t n) {
         p[i] = i;
 }
 
-// One thread per (g, h) segment: acc in (member asc, neighbour asc) order; the
-// pair rule of csr_network.rs:566-581 then finish's zero drop (:304).
+// One warp per (g, h) segment: acc in (member asc, neighbour asc) order, the
+// reference's left fold; then the pair rule of csr_network.rs:566-581 and
+// finish's zero drop (:304).
 __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
                              const uint64_t* __restrict__ keys, const float* __restrict__ w,
                              uint64_t G, const double* __restrict__ loops, uint32_t* prow,
                              uint32_t* pcol, float* pw, uint8_t* keep) {
-    for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < P;
-         s += (uint64_t)gridDim.x * blockDim.x) {
-        uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
-        double acc = 0.0;
-        for (uint64_t i = b; i < e; ++i) acc = __dadd_rn(acc, (double)w[i]);
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t s = warp; s < P; s += nwarps) {
+        const uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
+        const double acc = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return (double)w[i]; });
+        if ((threadIdx.x & 31) != 0) continue;
         uint64_t key = keys[b];
         uint32_t g = (uint32_t)(key / G), h = (uint32_t)(key % G);
         float val;
@@ -800,7 +809,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         c.launches++;
         sort_pairs(c, d_grp, grp_s.get(), idx.get(), members.get(), n, bits_for(G));
         k_starts_from_sorted<<<grid_for(n + 1, TB), TB, 0, c.stream>>>(grp_s.get(), n, G, gstart.get());
-        k_group_sums<<<grid_for(G, TB), TB, 0, c.stream>>>(gstart.get(), members.get(), G, g.node_w,
+        k_group_sums<<<grid_for((uint64_t)G * 32, TB), TB, 0, c.stream>>>(gstart.get(), members.get(), G, g.node_w,
                                                            g.self_loop, nw_new.get(), loops.get());
         SC_LAUNCH_CHECK();
         c.launches += 2;
@@ -852,7 +861,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         pcol.alloc(c, P);
         pw.alloc(c, P);
         keep.alloc(c, P);
-        k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
+        k_seg_values<<<grid_for(P * 32, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
                                                            uw_s.get(), G, loops.get(), prow.get(),
                                                            pcol.get(), pw.get(), keep.get());
         SC_LAUNCH_CHECK();

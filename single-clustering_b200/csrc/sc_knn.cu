@@ -1,10 +1,650 @@
-// sc_knn.cu — Gaussian kNN graph builder (neighborhood/mod.rs). Placeholder
-// until the tcgen05 distance kernel lands: reports SC_E_UNSUPPORTED.
+// sc_knn.cu — Gaussian kNN graph builder (src/neighborhood/mod.rs) on sm_100a.
+//
+// 1. k_knn_prep       X (f32) -> A = [-2x, 1, 1, 0..] and B = [x, |x|^2 hi, |x|^2 lo, 0..]
+//                     in BF16, KA = 32 (D <= 30) or 64 (D <= 62) columns.
+//                     A . B = |c|^2 - 2 q.c = |q - c|^2 - |q|^2: the row-constant
+//                     |q|^2 does not change a row's ranking, so the contraction
+//                     yields ranking scores directly.
+// 2. k_knn_tc         persistent tcgen05 kernel, one CTA per SM. A group of 256
+//                     queries (two M = 128 tiles) stays in shared memory; every
+//                     128-candidate tile of B streams in by TMA (no multicast)
+//                     through a STAGES-deep ring; one thread issues
+//                     tcgen05.mma (M=128, N=128, K=16, BF16 -> FP32) into a
+//                     double-buffered TMEM accumulator (2 x 2 x 128 columns);
+//                     8 epilogue warps read it with tcgen05.ld and keep, per
+//                     query, the R best scores in shared memory (a candidate is
+//                     rejected with one compare against the row's worst kept).
+// 3. k_knn_rerank     exact FP32 distances sum (q_d - c_d)^2 of the R candidates
+//                     (no norm expansion, so no cancellation), sorted by
+//                     (distance, self first, index); the first k+1 are kept.
+// 4. k_knn_sigma / k_knn_pairs / CSR: sigma (median of the positive distances,
+//                     neighborhood/mod.rs:105-124, or the k-th distance), the
+//                     Gaussian weight of :139-163, lower-id or union emission,
+//                     sorted into a CSR that from_csr_parts then finishes.
+//
+// Every wait on an mbarrier is bounded: on timeout the CTA records
+// DEV_TIMEOUT, drains the copies it issued (again bounded), frees its TMEM and
+// returns; the host turns the status into SC_E_TIMEOUT.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
 #include "sc_prims.cuh"
 
 namespace sc {
-void knn_gaussian(Ctx&, const float*, uint64_t, uint64_t, uint64_t, const sc_knn_opts&, uint32_t*, float*,
-                  uint64_t*, uint32_t*, float*, uint64_t, uint64_t*, DevGraph**) {
-    fail(SC_E_UNSUPPORTED, "kNN graph builder not built yet");
+
+namespace {
+
+constexpr int QT = 2;              // query tiles of 128 per CTA group
+constexpr int TILE = 128;          // rows per tile (M and N of the MMA)
+constexpr int STAGES = 6;          // B ring depth
+constexpr int RCAND = 32;          // candidates kept per query before the exact re-rank
+constexpr int NUM_EPI_WARPS = 8;
+constexpr int KNN_THREADS = 32 * (2 + NUM_EPI_WARPS);
+constexpr uint32_t WAIT_LIMIT = 1u << 26;
+constexpr uint32_t TMEM_COLS = 512;
+
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
 }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bounded wait for the phase with the given parity to complete.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    const uint32_t addr = smem_u32(bar);
+    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(addr), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+            smem_u32(dst)),
+        "l"((uint64_t)map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major, swizzled rows of KA * 2 bytes:
+// start >> 4 at [0,14), stride between 8-row groups >> 4 at [32,46),
+// version 1 at [46,48), layout at [61,64) (4 = 64B swizzle, 2 = 128B swizzle).
+template <int KA>
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
+    constexpr uint64_t row_bytes = KA * 2;
+    constexpr uint64_t sbo = 8 * row_bytes;
+    constexpr uint64_t layout = (KA == 32) ? 4ull : 2ull;
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= 1ull << 46;
+    d |= layout << 61;
+    return d;
+}
+
+// Instruction descriptor, kind::f16: D f32, A/B bf16, both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16_128x128() {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ------------------------------------------------------------ prep
+template <int KA>
+__global__ void k_knn_prep(const float* __restrict__ X, uint64_t n, uint32_t d, __nv_bfloat16* A,
+                           __nv_bfloat16* B) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* x = X + i * d;
+        float nrm = 0.0f;
+        for (uint32_t j = 0; j < d; ++j) nrm = __fmaf_rn(x[j], x[j], nrm);
+        __nv_bfloat16* a = A + i * KA;
+        __nv_bfloat16* b = B + i * KA;
+        for (uint32_t j = 0; j < d; ++j) {
+            __nv_bfloat16 xb = __float2bfloat16_rn(x[j]);
+            a[j] = __float2bfloat16_rn(-2.0f * __bfloat162float(xb));
+            b[j] = xb;
+        }
+        __nv_bfloat16 hi = __float2bfloat16_rn(nrm);
+        __nv_bfloat16 lo = __float2bfloat16_rn(nrm - __bfloat162float(hi));
+        a[d] = __float2bfloat16_rn(1.0f);
+        a[d + 1] = __float2bfloat16_rn(1.0f);
+        b[d] = hi;
+        b[d + 1] = lo;
+        for (uint32_t j = d + 2; j < (uint32_t)KA; ++j) {
+            a[j] = __float2bfloat16_rn(0.0f);
+            b[j] = __float2bfloat16_rn(0.0f);
+        }
+    }
+}
+
+// ------------------------------------------------------------ tensor-core candidate search
+template <int KA>
+struct KnnSmem {
+    static constexpr uint32_t TILE_BYTES = TILE * KA * 2;
+    static constexpr uint32_t A_OFF = 0;
+    static constexpr uint32_t B_OFF = A_OFF + QT * TILE_BYTES;
+    static constexpr uint32_t C_OFF = B_OFF + STAGES * TILE_BYTES;               // candidate scores
+    static constexpr uint32_t I_OFF = C_OFF + RCAND * QT * TILE * 4;              // candidate ids
+    static constexpr uint32_t BAR_OFF = I_OFF + RCAND * QT * TILE * 4;
+    static constexpr uint32_t NBAR = 2 * STAGES + 4 + 2;
+    static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR * 8;
+    static constexpr uint32_t BYTES = MISC_OFF + 64 + 1024;  // + alignment slack
+};
+
+template <int KA>
+__global__ void __launch_bounds__(KNN_THREADS, 1)
+    k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
+             float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status) {
+    using L = KnnSmem<KA>;
+    extern __shared__ __align__(1024) unsigned char raw[];
+    unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
+    unsigned char* sA = smem + L::A_OFF;
+    unsigned char* sB = smem + L::B_OFF;
+    float* cs = (float*)(smem + L::C_OFF);
+    uint32_t* ci = (uint32_t*)(smem + L::I_OFF);
+    uint64_t* bars = (uint64_t*)(smem + L::BAR_OFF);
+    uint64_t* full = bars;                 // [STAGES] B tile landed
+    uint64_t* empty = bars + STAGES;       // [STAGES] B tile consumed by the MMAs
+    uint64_t* accfull = bars + 2 * STAGES;       // [2] accumulator ready
+    uint64_t* accempty = bars + 2 * STAGES + 2;  // [2] accumulator drained
+    uint64_t* afull = bars + 2 * STAGES + 4;     // query tiles landed
+    uint64_t* aempty = bars + 2 * STAGES + 5;    // query tiles no longer read
+    uint32_t* misc = (uint32_t*)(smem + L::MISC_OFF);
+    volatile uint32_t* abort_flag = misc + 1;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t ntiles = (n + TILE - 1) / TILE;
+    const uint32_t ngroups = (n + QT * TILE - 1) / (QT * TILE);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(full + s, 1);
+            mbar_init(empty + s, 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(accfull + b, 1);
+            mbar_init(accempty + b, NUM_EPI_WARPS);
+        }
+        mbar_init(afull, 1);
+        mbar_init(aempty, 1);
+        misc[1] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(misc)),
+                     "r"(TMEM_COLS)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    const uint32_t tmem = misc[0];
+
+    if (warp == 0) {
+        // ---------------- TMA producer
+        if (lane == 0) {
+            uint64_t it = 0;  // global B tile counter (all groups)
+            uint32_t gi = 0;
+            bool a_in_flight = false;
+            for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x, ++gi) {
+                if (gi > 0 && !mbar_wait(aempty, (gi - 1) & 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                mbar_expect_tx(afull, QT * L::TILE_BYTES);
+                a_in_flight = true;
+                for (int q = 0; q < QT; ++q)
+                    tma_load_2d(sA + q * L::TILE_BYTES, &tmA, afull, 0, (int)(g * QT * TILE + q * TILE));
+                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                    const uint32_t s = (uint32_t)(it % STAGES);
+                    const uint64_t use = it / STAGES;
+                    if (use > 0 && !mbar_wait(empty + s, (uint32_t)((use - 1) & 1))) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    if (*abort_flag) break;
+                    mbar_expect_tx(full + s, L::TILE_BYTES);
+                    tma_load_2d(sB + s * L::TILE_BYTES, &tmB, full + s, 0, (int)(t * TILE));
+                }
+            }
+            // drain: the copies issued last (one per stage, and the query tiles)
+            // must land before the CTA exits
+            if (*abort_flag) {
+                for (uint64_t x = it > STAGES ? it - STAGES : 0; x < it; ++x)
+                    mbar_wait(full + (x % STAGES), (uint32_t)((x / STAGES) & 1));
+                if (a_in_flight && gi > 0) mbar_wait(afull, (gi - 1) & 1);
+            }
+        }
+    } else if (warp == 1) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            constexpr uint32_t idesc = idesc_bf16_128x128();
+            uint64_t it = 0;
+            uint32_t gi = 0;
+            for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x, ++gi) {
+                if (!mbar_wait(afull, gi & 1)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                fence_after();
+                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                    const uint32_t s = (uint32_t)(it % STAGES);
+                    const uint32_t b = (uint32_t)(it & 1);
+                    const uint64_t use_b = it >> 1;
+                    if (!mbar_wait(full + s, (uint32_t)((it / STAGES) & 1))) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    if (use_b > 0 && !mbar_wait(accempty + b, (uint32_t)((use_b - 1) & 1))) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    fence_after();
+                    const uint32_t bbase = smem_u32(sB + s * L::TILE_BYTES);
+#pragma unroll
+                    for (int q = 0; q < QT; ++q) {
+                        const uint32_t abase = smem_u32(sA + q * L::TILE_BYTES);
+                        const uint32_t d = tmem + b * (QT * TILE) + q * TILE;
+#pragma unroll
+                        for (int kk = 0; kk < KA / 16; ++kk)
+                            mma_bf16(d, smem_desc<KA>(abase + kk * 32), smem_desc<KA>(bbase + kk * 32), idesc,
+                                     kk > 0 ? 1u : 0u);
+                    }
+                    mma_commit(empty + s);
+                    mma_commit(accfull + b);
+                }
+                mma_commit(aempty);
+            }
+        }
+    } else {
+        // ---------------- epilogue: 8 warps, warp % 4 selects the TMEM lane quarter
+        const int ew = warp - 2;
+        const int q = ew >> 2;                  // query tile
+        const int lq = warp & 3;                // lane quarter (hardware rule)
+        const int row = lq * 32 + lane;         // row within the query tile
+        const int qrow = q * TILE + row;        // 0..255 within the group
+        uint64_t it = 0;
+        for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x) {
+            float thr = INFINITY;
+            int thr_slot = 0;
+            for (int s = 0; s < RCAND; ++s) {
+                cs[s * (QT * TILE) + qrow] = INFINITY;
+                ci[s * (QT * TILE) + qrow] = 0xFFFFFFFFu;
+            }
+            for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                const uint32_t b = (uint32_t)(it & 1);
+                if (!mbar_wait(accfull + b, (uint32_t)((it >> 1) & 1))) {
+                    *abort_flag = 1;
+                    break;
+                }
+                fence_after();
+                const uint32_t taddr = tmem + ((uint32_t)(lq * 32) << 16) + b * (QT * TILE) + q * TILE;
+#pragma unroll 1
+                for (int c0 = 0; c0 < TILE; c0 += 32) {
+                    float v[32];
+                    tmem_ld32(taddr + c0, v);
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (v[j] < thr) {
+                            const uint32_t idx = t * TILE + c0 + j;
+                            if (idx < n) {
+                                cs[thr_slot * (QT * TILE) + qrow] = v[j];
+                                ci[thr_slot * (QT * TILE) + qrow] = idx;
+                                thr = -INFINITY;
+                                for (int s = 0; s < RCAND; ++s) {
+                                    float x = cs[s * (QT * TILE) + qrow];
+                                    if (x > thr) {
+                                        thr = x;
+                                        thr_slot = s;
+                                    }
+                                }
+                            }
+                        }
+                    }
+                }
+                fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(accempty + b);
+            }
+            if (*abort_flag) break;
+            const uint64_t qg = (uint64_t)g * QT * TILE + qrow;
+            if (qg < n) {
+                for (int s = 0; s < RCAND; ++s) {
+                    cand_score[qg * RCAND + s] = cs[s * (QT * TILE) + qrow];
+                    cand_idx[qg * RCAND + s] = ci[s * (QT * TILE) + qrow];
+                }
+            }
+        }
+    }
+    fence_before();
+    __syncthreads();
+    fence_after();
+    if (threadIdx.x == 0 && *abort_flag) atomicOr(status, DEV_TIMEOUT);
+    if (warp == 1) {
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
+                     : "memory");
+    }
+}
+
+// ------------------------------------------------------------ exact re-rank
+// One warp per query: lane j owns candidate j (RCAND == 32).
+__global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d, uint32_t k,
+                             const uint32_t* __restrict__ cand_idx, uint32_t* __restrict__ out_idx,
+                             float* __restrict__ out_d2) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = warp; q < n; q += nwarps) {
+        uint32_t j = cand_idx[q * RCAND + lane];
+        uint64_t key = ~0ull;
+        float d2 = INFINITY;
+        if (j < n) {
+            const float* a = X + q * d;
+            const float* b = X + (uint64_t)j * d;
+            float acc = 0.0f;
+            for (uint32_t t = 0; t < d; ++t) {
+                float diff = __fsub_rn(a[t], b[t]);
+                acc = __fmaf_rn(diff, diff, acc);
+            }
+            d2 = acc;
+            // (distance, self first, index); d2 >= 0 so its bits order like the value
+            key = ((uint64_t)__float_as_uint(d2) << 32) | (j == (uint32_t)q ? 0u : j + 1u);
+        }
+        // bitonic sort of 32 keys across the warp, ascending
+        for (int size = 2; size <= 32; size <<= 1) {
+            for (int stride = size >> 1; stride > 0; stride >>= 1) {
+                uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, stride);
+                bool up = ((lane & size) == 0);
+                bool lower = (lane & stride) == 0;
+                uint64_t mn = key < other ? key : other, mx = key < other ? other : key;
+                key = (lower == up) ? mn : mx;
+            }
+        }
+        if (lane <= k) {
+            uint32_t tag = (uint32_t)key;
+            uint32_t idx = (key == ~0ull) ? 0xFFFFFFFFu : (tag == 0 ? (uint32_t)q : tag - 1u);
+            out_idx[q * (k + 1) + lane] = idx;
+            out_d2[q * (k + 1) + lane] = key == ~0ull ? INFINITY : __uint_as_float((uint32_t)(key >> 32));
+        }
+    }
+}
+
+// ------------------------------------------------------------ sigma and connectivities
+// sigma_i: median of the positive distances among the k+1 (neighborhood/mod.rs:480-499;
+// the kd-tree path's sqrt(median(d^2)), :105-124, is the same element), 1 if none;
+// or the k-th neighbour's distance.
+__global__ void k_knn_sigma(const float* __restrict__ d2, uint64_t n, uint32_t k, int kth, float* sigma) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* r = d2 + i * (k + 1);
+        if (kth) {
+            sigma[i] = sqrtf(r[k]);
+            continue;
+        }
+        uint32_t pos = 0;
+        for (uint32_t t = 0; t <= k; ++t) pos += r[t] > 0.0f;
+        if (pos == 0) {
+            sigma[i] = 1.0f;
+            continue;
+        }
+        // rows are sorted ascending, positive entries are the last `pos`
+        uint32_t first = (k + 1) - pos;
+        sigma[i] = sqrtf(r[first + pos / 2]);
+    }
+}
+
+// Connectivity weight of :139-163 in f32, operation for operation.
+__device__ __forceinline__ float gauss_w(float dist_sq, float si, float sj, bool* ok) {
+    float si2 = __fmul_rn(si, si), sj2 = __fmul_rn(sj, sj);
+    float den = __fadd_rn(si2, sj2);
+    *ok = den > 0.0f;
+    if (!*ok) return 0.0f;
+    float num = __fmul_rn(__fmul_rn(2.0f, si), sj);
+    float norm = sqrtf(__fdiv_rn(num, den));
+    float ex = expf(__fdiv_rn(-dist_sq, den));
+    return __fmul_rn(norm, ex);
+}
+
+// Emit (row << 32 | col) keys and weights. lower_id: only from the row i <= j,
+// both directions (the reference's rule). union: every listed pair, both
+// directions; duplicates are removed after the sort.
+__global__ void k_knn_pairs(const uint32_t* __restrict__ idx, const float* __restrict__ d2, uint64_t n,
+                            uint32_t k, const float* __restrict__ sigma, int sym_union, int squared,
+                            unsigned long long* keys, float* w, unsigned long long* count) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        for (uint32_t t = 1; t <= k; ++t) {
+            uint32_t j = idx[i * (k + 1) + t];
+            if (j >= n) continue;
+            if (!sym_union && !(i <= j)) continue;
+            if (sym_union && j == i) continue;
+            // HNSW path: squares the returned distance; kd-tree path: already squared
+            float dist_sq = squared ? d2[i * (k + 1) + t] : __fmul_rn(sqrtf(d2[i * (k + 1) + t]),
+                                                                       sqrtf(d2[i * (k + 1) + t]));
+            bool ok;
+            float wt = gauss_w(dist_sq, sigma[i], sigma[j], &ok);
+            if (!ok || !(wt > 1e-14f)) continue;
+            unsigned long long pos = atomicAdd(count, i == j ? 1ull : 2ull);
+            keys[pos] = ((unsigned long long)i << 32) | j;
+            w[pos] = wt;
+            if (i != j) {
+                keys[pos + 1] = ((unsigned long long)j << 32) | i;
+                w[pos + 1] = wt;
+            }
+        }
+    }
+}
+
+__global__ void k_dedupe_flags(const unsigned long long* __restrict__ keys, uint64_t N, uint8_t* keep) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        keep[i] = (i == 0 || keys[i] != keys[i - 1]);
+}
+
+__global__ void k_split_rowcol(const unsigned long long* __restrict__ keys, uint64_t N, uint32_t* rows,
+                               uint32_t* cols) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        rows[i] = (uint32_t)(keys[i] >> 32);
+        cols[i] = (uint32_t)keys[i];
+    }
+}
+
+__global__ void k_ptr_from_rows(const uint32_t* __restrict__ rows, uint64_t N, uint64_t R, uint64_t* start) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= N;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        uint64_t r = i < N ? rows[i] : R;
+        uint64_t prev = i == 0 ? 0 : (uint64_t)rows[i - 1] + 1;
+        for (uint64_t q = prev; q <= r && q <= R; ++q) start[q] = i;
+    }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    if (!fn) {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        SC_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q));
+        if (q != cudaDriverEntryPointSuccess || !p) fail(SC_E_CUDA, "cuTensorMapEncodeTiled is unavailable");
+        fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+    }
+    return fn;
+}
+
+template <int KA>
+CUtensorMap make_map(const __nv_bfloat16* base, uint64_t n) {
+    CUtensorMap m;
+    cuuint64_t dims[2] = {(cuuint64_t)KA, (cuuint64_t)n};
+    cuuint64_t strides[1] = {(cuuint64_t)KA * 2};
+    cuuint32_t box[2] = {(cuuint32_t)KA, (cuuint32_t)TILE};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
+                             CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             KA == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                             CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) fail(SC_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return m;
+}
+
+template <int KA>
+void candidates(Ctx& c, const float* dX, uint64_t n, uint32_t d, float* cand_score, uint32_t* cand_idx) {
+    DBuf<__nv_bfloat16> A(c, n * KA), B(c, n * KA);
+    k_knn_prep<KA><<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, A.get(), B.get());
+    SC_LAUNCH_CHECK();
+    CUtensorMap ta = make_map<KA>(A.get(), n), tb = make_map<KA>(B.get(), n);
+    using L = KnnSmem<KA>;
+    SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
+    const uint32_t ngroups = (uint32_t)((n + QT * TILE - 1) / (QT * TILE));
+    const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
+    k_knn_tc<KA><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, cand_score, cand_idx,
+                                                             c.d_status);
+    SC_LAUNCH_CHECK();
+    c.launches += 2;
+}
+
+}  // namespace
+
+// knn_arrayd_* (neighborhood/mod.rs:51-202, :359-578) with exact (brute-force)
+// search. The search keeps RCAND = 32 candidates per query from the BF16
+// tensor-core scores, then ranks them exactly in FP32.
+void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
+                  uint32_t* knn_index, float* knn_dist, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                  uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
+    if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
+    if (k + 1 > (uint64_t)RCAND) fail(SC_E_UNSUPPORTED, "kNN supports k <= %d", RCAND - 1);
+    if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
+    if (opts.precision != SC_KNN_BF16) fail(SC_E_UNSUPPORTED, "only the BF16 contraction is built");
+    DBuf<float> dX(c, n * d);
+    h2d(c, dX.get(), X, n * d);
+    DBuf<float> cscore(c, n * RCAND);
+    DBuf<uint32_t> cidx(c, n * RCAND);
+    if (n) {
+        if (d <= 30) candidates<32>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());
+        else candidates<64>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());
+    }
+    DBuf<uint32_t> idx(c, n * (k + 1));
+    DBuf<float> d2(c, n * (k + 1));
+    if (n) {
+        k_knn_rerank<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(dX.get(), n, (uint32_t)d, (uint32_t)k, cidx.get(),
+                                                                   idx.get(), d2.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    check_device_status(c);
+    if (knn_index) d2h(c, knn_index, idx.get(), n * (k + 1));
+    if (knn_dist) {
+        std::vector<float> h(n * (k + 1));
+        d2h(c, h.data(), d2.get(), n * (k + 1));
+        sync(c);
+        for (uint64_t i = 0; i < h.size(); ++i) knn_dist[i] = opts.squared_kiddo ? h[i] : std::sqrt(h[i]);
+    }
+    if (!conn_ptrs && !graph_out) {
+        sync(c);
+        return;
+    }
+    DBuf<float> sigma(c, n);
+    DBuf<unsigned long long> keys(c, 2 * n * k + 1), keys_s(c, 2 * n * k + 1);
+    DBuf<float> w(c, 2 * n * k + 1), w_s(c, 2 * n * k + 1);
+    DBuf<unsigned long long> cnt(c, 1);
+    zero(c, cnt.get(), 1);
+    if (n) {
+        k_knn_sigma<<<grid_for(n, 256), 256, 0, c.stream>>>(d2.get(), n, (uint32_t)k, opts.sigma == SC_SIGMA_KTH,
+                                                            sigma.get());
+        k_knn_pairs<<<grid_for(n, 256), 256, 0, c.stream>>>(idx.get(), d2.get(), n, (uint32_t)k, sigma.get(),
+                                                            opts.sym == SC_SYM_UNION, opts.squared_kiddo,
+                                                            keys.get(), w.get(), cnt.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    uint64_t N = to_host(c, cnt.get());
+    sort_pairs(c, keys.get(), keys_s.get(), w.get(), w_s.get(), N, 64);
+    DBuf<uint8_t> keep(c, N);
+    DBuf<unsigned long long> ukeys(c, N);
+    DBuf<float> uw(c, N);
+    uint64_t M = N;
+    if (N) {
+        k_dedupe_flags<<<grid_for(N, 256), 256, 0, c.stream>>>(keys_s.get(), N, keep.get());
+        c.launches++;
+        DBuf<uint64_t> m(c, 1);
+        select_flagged(c, keys_s.get(), keep.get(), ukeys.get(), m.get(), N);
+        select_flagged(c, w_s.get(), keep.get(), uw.get(), m.get(), N);
+        M = to_host(c, m.get());
+    }
+    DBuf<uint32_t> rows(c, M), cols(c, M);
+    DBuf<uint64_t> ptr(c, n + 1);
+    if (M) {
+        k_split_rowcol<<<grid_for(M, 256), 256, 0, c.stream>>>(ukeys.get(), M, rows.get(), cols.get());
+        c.launches++;
+    }
+    k_ptr_from_rows<<<grid_for(M + 1, 256), 256, 0, c.stream>>>(rows.get(), M, n, ptr.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    if (conn_nnz) *conn_nnz = M;
+    if (conn_ptrs) {
+        if (M > conn_cap) fail(SC_E_INVALID_ARGUMENT, "conn_capacity %llu < %llu entries",
+                               (unsigned long long)conn_cap, (unsigned long long)M);
+        d2h(c, conn_ptrs, ptr.get(), n + 1);
+        if (conn_nbrs) d2h(c, conn_nbrs, cols.get(), M);
+        if (conn_w) d2h(c, conn_w, uw.get(), M);
+    }
+    if (graph_out) *graph_out = graph_from_csr(c, ptr.get(), n + 1, cols.get(), M, uw.get(), M, nullptr, 0, true);
+    sync(c);
+}
+
 }  // namespace sc

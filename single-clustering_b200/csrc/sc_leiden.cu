@@ -31,7 +31,6 @@ constexpr int LM_BATCHES = 8;
 constexpr int RF_BATCHES = 8;
 constexpr int MAX_SWEEPS = 100;
 constexpr uint32_t EMPTYK = 0xFFFFFFFFu;
-constexpr int CAND_SMEM = HUB_DEGREE;  // refinement candidates held in shared memory per block
 
 struct Params {
     // graph
@@ -125,6 +124,19 @@ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t a, uint64_t 
     return (double)(hash3(seed ^ 0x5151515151515151ull, a, b) >> 11) * 0x1.0p-53;
 }
 
+// Refinement's randomised choice (refine.rs:110-153) draws candidate c with
+// probability exp(rel_c / theta) / sum. Gumbel-max draws from the same
+// distribution: argmax_c rel_c / theta + G_c with G_c = -log(-log U_c), U_c
+// uniform in (0, 1) from a hash of (seed, epoch, node, c). The result does not
+// depend on the order candidates are visited in, so no candidate list or sort
+// is needed. theta <= 0 is the deterministic argmax (ties to the lower id).
+__device__ __forceinline__ double refine_key(const Params& p, double rel, uint32_t v, uint32_t c) {
+    if (p.theta <= 0.0) return rel;
+    uint64_t h = hash3(p.seed ^ 0x5151515151515151ull, ((uint64_t)p.cur << 32) | v, c);
+    double u = ((double)(h >> 11) + 0.5) * 0x1.0p-53;
+    return __dadd_rn(__ddiv_rn(rel, p.theta), -log(-log(u)));
+}
+
 // Warp-aggregated counter add.
 __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long long x) {
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
@@ -137,8 +149,6 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 template <int G, bool REFINE>
 __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* __restrict__ list,
                                                      uint32_t count) {
-    __shared__ uint32_t s_c[TB];
-    __shared__ double s_r[TB];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (G - 1);
@@ -211,9 +221,9 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
                 g = gain_of(p, from_fix(acc, p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
                 if (REFINE) {
                     double rel = __dsub_rn(g, base);
-                    if (rel >= 0.0) {
+                    if (rel >= 0.0) {  // `>=` takes ties (refine.rs:91-95)
                         cand = true;
-                        g = rel;
+                        g = refine_key(p, rel, v, cu);
                     } else {
                         g = -INFINITY;
                     }
@@ -231,19 +241,19 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
             sdeg += (unsigned long long)deg;
         }
         scand += (leader && cu != own) ? 1ull : 0ull;
-        if (!REFINE) {
-            // argmax over the group: higher gain, then lower id
+        // argmax over the group: higher key, then lower id
 #pragma unroll
-            for (int o = G / 2; o; o >>= 1) {
-                double og = __shfl_xor_sync(FULL, g, o);
-                uint32_t oc = __shfl_xor_sync(FULL, c, o);
-                uint32_t om = __shfl_xor_sync(FULL, cu_member, o);
-                if (better(og, oc, g, c)) {
-                    g = og;
-                    c = oc;
-                    cu_member = om;
-                }
+        for (int o = G / 2; o; o >>= 1) {
+            double og = __shfl_xor_sync(FULL, g, o);
+            uint32_t oc = __shfl_xor_sync(FULL, c, o);
+            uint32_t om = __shfl_xor_sync(FULL, cu_member, o);
+            if (better(og, oc, g, c)) {
+                g = og;
+                c = oc;
+                cu_member = om;
             }
+        }
+        if (!REFINE) {
             if (sub == 0 && eligible) {
                 uint32_t best = own;
                 double bg = base;
@@ -270,73 +280,12 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
                     p.epoch[v] = p.cur;
                 }
             }
-        } else {
-            // candidates in ascending community id: each candidate lane finds its rank
-            int rank = 0, ncand = 0;
-#pragma unroll
-            for (int t = 0; t < G; ++t) {
-                uint32_t oc = __shfl_sync(FULL, c, gbase + t);
-                int ocand = __shfl_sync(FULL, (int)cand, gbase + t);
-                if (ocand) {
-                    ncand++;
-                    if (oc < c) rank++;
-                }
-            }
-            double best_rel = 0.0;
-            {
-                double x = cand ? g : 0.0;
-#pragma unroll
-                for (int o = G / 2; o; o >>= 1) x = fmax(x, __shfl_xor_sync(FULL, x, o));
-                best_rel = x;
-            }
-            if (cand) {
-                s_c[threadIdx.x - lane + gbase + rank] = c;
-                s_r[threadIdx.x - lane + gbase + rank] = g;
-            }
-            __syncwarp();
-            // hint member of each candidate: lane order equals candidate rank order
-            if (sub == 0 && eligible && ncand > 0) {
-                const uint32_t* cc = s_c + (threadIdx.x - lane + gbase);
-                const double* cr = s_r + (threadIdx.x - lane + gbase);
-                uint32_t target = NONE32;
-                if (p.theta <= 0.0) {
-                    for (int j = 0; j < ncand; ++j)
-                        if (cr[j] >= best_rel && (target == NONE32 || cc[j] < target)) target = cc[j];
-                } else {
-                    double tot = -0.0;
-                    for (int j = 0; j < ncand; ++j)
-                        tot = __dadd_rn(tot, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
-                    if (!isfinite(tot) || tot <= 0.0) {
-                        for (int j = 0; j < ncand; ++j)
-                            if (cr[j] >= best_rel && (target == NONE32 || cc[j] < target)) target = cc[j];
-                    } else {
-                        double thr = __dmul_rn(uniform01(p.seed, p.cur, v), tot);
-                        target = cc[ncand - 1];
-                        for (int j = 0; j < ncand; ++j) {
-                            thr = __dsub_rn(thr, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
-                            if (thr <= 0.0) {
-                                target = cc[j];
-                                break;
-                            }
-                        }
-                    }
-                }
-                s_c[threadIdx.x] = target;  // broadcast slot (lane sub==0 of the group)
-            }
-            __syncwarp();
-            uint32_t target = __shfl_sync(FULL, (sub == 0 && eligible && ncand > 0) ? s_c[threadIdx.x] : NONE32,
-                                          gbase);
-            // member of the target if it is a singleton: the lane holding it
-            unsigned hb = __ballot_sync(FULL, cand && c == target) & gmask;
-            uint32_t member = __shfl_sync(FULL, cu_member, hb ? (__ffs(hb) - 1) : lane);
-            if (sub == 0 && eligible && target != NONE32) {
-                p.tgt[v] = target;
-                p.from[v] = own;
-                p.dgain[v] = 0;
-                p.hint[v] = (p.csize[target] == 1) ? member : NONE32;
-                p.epoch[v] = p.cur;
-            }
-            __syncwarp();
+        } else if (sub == 0 && eligible && c != NONE32) {
+            p.tgt[v] = c;
+            p.from[v] = own;
+            p.dgain[v] = 0;
+            p.hint[v] = (p.csize[c] == 1) ? cu_member : NONE32;
+            p.epoch[v] = p.cur;
         }
     }
     warp_add(p.counters + 1, sdeg);
@@ -421,48 +370,20 @@ __device__ void block_argmax(double& g, uint32_t& c, double* sg, uint32_t* sc) {
     __syncthreads();
 }
 
-// In-place bitonic sort of (key, val) pairs, n a power of two, by the block.
-__device__ void block_bitonic(uint32_t* key, double* val, uint32_t n) {
-    for (uint32_t size = 2; size <= n; size <<= 1) {
-        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
-            for (uint32_t t = threadIdx.x; t < n / 2; t += blockDim.x) {
-                uint32_t lo = 2 * stride * (t / stride) + (t % stride);
-                uint32_t hi = lo + stride;
-                bool up = ((lo & size) == 0);
-                if ((key[lo] > key[hi]) == up) {
-                    uint32_t tk = key[lo];
-                    key[lo] = key[hi];
-                    key[hi] = tk;
-                    double tv = val[lo];
-                    val[lo] = val[hi];
-                    val[hi] = tv;
-                }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-// One block per node. HUB = false: degree <= HUB_DEGREE, hash table and
-// candidate list in shared memory. HUB = true: both in this block's slice of
-// the global scratch (gcap entries each), which the host sized for the
-// largest degree; the grid never exceeds the number of slices.
+// One block per node. HUB = false: degree <= HUB_DEGREE, hash table in shared
+// memory. HUB = true: the table lives in this block's slice of the global
+// scratch (gcap entries), which the host sized for the largest degree; the
+// grid never exceeds the number of slices.
 template <bool REFINE, bool HUB>
 __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* __restrict__ list,
                                                      uint32_t count, uint32_t* gkeys, long long* gvals,
-                                                     uint32_t* gck, double* gcr, uint64_t gcap) {
+                                                     uint64_t gcap) {
     extern __shared__ __align__(16) unsigned char smem[];
     long long* s_vals = (long long*)smem;
-    double* s_cr = (double*)(smem + HCAP_SMEM * sizeof(long long));
-    uint32_t* s_keys = (uint32_t*)(smem + (HCAP_SMEM + CAND_SMEM) * sizeof(long long));
-    uint32_t* s_ck = s_keys + HCAP_SMEM;
-    const uint64_t ccap = HUB ? gcap : (uint64_t)CAND_SMEM;
-    uint32_t* ck = HUB ? gck + (uint64_t)blockIdx.x * gcap : s_ck;
-    double* cr = HUB ? gcr + (uint64_t)blockIdx.x * gcap : s_cr;
+    uint32_t* s_keys = (uint32_t*)(smem + HCAP_SMEM * sizeof(long long));
     __shared__ double red_g[32];
     __shared__ uint32_t red_c[32];
-    __shared__ uint32_t s_member, s_ncand, s_target;
-    __shared__ double s_bestrel;
+    __shared__ uint32_t s_member, s_target;
 
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
@@ -512,8 +433,6 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
                                     a, from_fix(p.Wf[own] - af, p.nscale));
         double g = -INFINITY;
         uint32_t c = NONE32;
-        if (threadIdx.x == 0) s_ncand = 0;
-        __syncthreads();
         uint32_t lc = 0;
         for (uint32_t s = threadIdx.x; s < cap; s += blockDim.x) {
             uint32_t cu = keys[s];
@@ -524,15 +443,10 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
             if (REFINE) {
                 double rel = __dsub_rn(gg, base);
-                if (rel >= 0.0) {
-                    uint32_t slot = atomicAdd(&s_ncand, 1u);
-                    if (slot < ccap) {
-                        ck[slot] = cu;
-                        cr[slot] = rel;
-                    }
-                    if (rel > g) g = rel;
-                }
-            } else if (better(gg, cu, g, c)) {
+                if (!(rel >= 0.0)) continue;
+                gg = refine_key(p, rel, v, cu);
+            }
+            if (better(gg, cu, g, c)) {
                 g = gg;
                 c = cu;
             }
@@ -542,11 +456,11 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             snodes += 1;
             sdeg += deg;
         }
-        if (!REFINE) {
-            block_argmax(g, c, red_g, red_c);
-            if (threadIdx.x == 0) {
-                uint32_t best = own;
-                double bg = base;
+        block_argmax(g, c, red_g, red_c);
+        if (threadIdx.x == 0) {
+            uint32_t best = own;
+            double bg = base;
+            if (!REFINE) {
                 if (c != NONE32 && better(g, c, bg, best)) {
                     best = c;
                     bg = g;
@@ -562,73 +476,19 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
                 }
                 double d = __dsub_rn(bg, base);
                 s_target = (best != own && d > p.thr) ? best : NONE32;
-                if (s_target != NONE32) {
-                    p.tgt[v] = best;
-                    p.from[v] = own;
-                    p.dgain[v] = to_fix(d, p.inv_scale);
-                    p.epoch[v] = p.cur;
-                }
-                s_member = NONE32;
+                if (s_target != NONE32) p.dgain[v] = to_fix(d, p.inv_scale);
+            } else {
+                s_target = c;  // NONE32 when no candidate has rel >= 0
+                p.dgain[v] = 0;
             }
-            __syncthreads();
-        } else {
-            // best_rel: block max of the non-negative rels (0.0 floor)
-            double x = g > 0.0 ? g : 0.0;
-            uint32_t dummy = 0;
-            block_argmax(x, dummy, red_g, red_c);
-            if (threadIdx.x == 0) s_bestrel = x;
-            __syncthreads();
-            uint32_t nc = min(s_ncand, (uint32_t)ccap);
-            if (threadIdx.x == 0 && s_ncand > ccap) atomicOr(p.status, DEV_OVERFLOW);
-            uint32_t n2 = 1;
-            while (n2 < nc) n2 <<= 1;
-            if (n2 <= ccap) {
-                for (uint32_t s = nc + threadIdx.x; s < n2; s += blockDim.x) {
-                    ck[s] = 0xFFFFFFFFu;
-                    cr[s] = 0.0;
-                }
+            if (s_target != NONE32) {
+                p.tgt[v] = s_target;
+                p.from[v] = own;
+                p.epoch[v] = p.cur;
             }
-            __syncthreads();
-            if (nc > 1 && n2 <= ccap) block_bitonic(ck, cr, n2);
-            if (threadIdx.x == 0) {
-                uint32_t target = NONE32;
-                double best_rel = s_bestrel;
-                if (nc > 0) {
-                    if (p.theta <= 0.0) {
-                        for (uint32_t j = 0; j < nc; ++j)
-                            if (cr[j] >= best_rel && (target == NONE32 || ck[j] < target)) target = ck[j];
-                    } else {
-                        double tot = -0.0;
-                        for (uint32_t j = 0; j < nc; ++j)
-                            tot = __dadd_rn(tot, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
-                        if (!isfinite(tot) || tot <= 0.0) {
-                            for (uint32_t j = 0; j < nc; ++j)
-                                if (cr[j] >= best_rel && (target == NONE32 || ck[j] < target))
-                                    target = ck[j];
-                        } else {
-                            double thr = __dmul_rn(uniform01(p.seed, p.cur, v), tot);
-                            target = ck[nc - 1];
-                            for (uint32_t j = 0; j < nc; ++j) {
-                                thr = __dsub_rn(thr, exp(__ddiv_rn(__dsub_rn(cr[j], best_rel), p.theta)));
-                                if (thr <= 0.0) {
-                                    target = ck[j];
-                                    break;
-                                }
-                            }
-                        }
-                    }
-                }
-                s_target = target;
-                if (target != NONE32) {
-                    p.tgt[v] = target;
-                    p.from[v] = own;
-                    p.dgain[v] = 0;
-                    p.epoch[v] = p.cur;
-                }
-                s_member = NONE32;
-            }
-            __syncthreads();
+            s_member = NONE32;
         }
+        __syncthreads();
         // the member of a singleton target, for conflict detection
         const uint32_t target = s_target;
         if (target != NONE32) {
@@ -800,9 +660,8 @@ struct Workspace {
     DBuf<uint32_t> counts;
     DBuf<unsigned long long> counters;
     DBuf<long long> gain_acc;
-    DBuf<uint32_t> gkeys, gck;
+    DBuf<uint32_t> gkeys;
     DBuf<long long> gvals;
-    DBuf<double> gcr;
     uint64_t gcap = 0;
     int nblk_large = 0;
 };
@@ -854,13 +713,11 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
         while (cap < 2ull * g.max_degree) cap <<= 1;
         int nblk = (int)std::min<uint64_t>((uint64_t)c.sm_count * 2, g.n_hubs);
         const uint64_t budget = 1ull << 31;  // bytes of hub scratch at most
-        while (nblk > 1 && (uint64_t)nblk * cap * 24 > budget) nblk >>= 1;
+        while (nblk > 1 && (uint64_t)nblk * cap * 12 > budget) nblk >>= 1;
         ws.nblk_large = nblk;
         ws.gcap = cap;
         ws.gkeys.alloc(c, (uint64_t)nblk * cap);
         ws.gvals.alloc(c, (uint64_t)nblk * cap);
-        ws.gck.alloc(c, (uint64_t)nblk * cap);
-        ws.gcr.alloc(c, (uint64_t)nblk * cap);
     }
 }
 
@@ -876,15 +733,14 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list
     } else if (k == 2) {
         k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
     } else if (k == 3) {
-        size_t sm = (HCAP_SMEM + CAND_SMEM) * (sizeof(long long) + sizeof(uint32_t));
+        size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
         unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
-        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, cnt, nullptr, nullptr, nullptr,
-                                                                  nullptr, 0);
+        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, cnt, nullptr, nullptr, 0);
     } else {
         if (ws.nblk_large < 1 || ws.gcap == 0) fail(SC_E_INTERNAL, "hub scratch missing");
         unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
         k_decide_block<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, cnt, ws.gkeys.get(), ws.gvals.get(),
-                                                               ws.gck.get(), ws.gcr.get(), ws.gcap);
+                                                               ws.gcap);
     }
     SC_LAUNCH_CHECK();
     c.launches++;
@@ -958,6 +814,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     uint32_t epoch = 0;
     uint64_t moves_before = 0;
     const uint64_t budget = n * 100;  // MAX_MOVES_PER_NODE, local_move.rs:32
+    static const int trace = std::getenv("SC_TRACE") ? std::atoi(std::getenv("SC_TRACE")) : 0;
     for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
         zero(c, ws.counts.get(), B * NBUCKET);
         zero(c, ws.next_active.get(), n);
@@ -970,12 +827,15 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         d2h(c, counts, ws.counts.get(), B * NBUCKET);
         d2h(c, ctr, ws.counters.get(), 4);
         sync(c);
-        if (sweep > 0 && ctr[0] == moves_before) break;  // last sweep moved nothing
-        if (ctr[0] >= budget) break;
-        moves_before = ctr[0];
         uint32_t offs[65];
         offs[0] = 0;
         for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
+        if (trace >= 2 && sweep > 0)
+            std::fprintf(stderr, "[sc]   sweep %u moves=%llu next_active=%u\n", sweep - 1,
+                         (unsigned long long)(ctr[0] - moves_before), offs[B * NBUCKET]);
+        if (sweep > 0 && ctr[0] == moves_before) break;  // last sweep moved nothing
+        if (ctr[0] >= budget) break;
+        moves_before = ctr[0];
         if (offs[B * NBUCKET] == 0) break;
         DBuf<uint32_t> cursor(c, 64);
         h2d(c, cursor.get(), offs, B * NBUCKET);
@@ -1167,9 +1027,10 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         auto trace_level = [&](uint64_t ng) {
             if (!trace) return;
             std::fprintf(stderr,
-                         "[sc] level %llu n=%llu E=%llu groups=%llu sweeps=%llu moves=%llu lm=%.3fms "
-                         "ref=%.3fms agg=%.3fms\n",
+                         "[sc] level %llu n=%llu E=%llu exact=%d/%d groups=%llu sweeps=%llu moves=%llu "
+                         "lm=%.3fms ref=%.3fms agg=%.3fms\n",
                          (unsigned long long)level, (unsigned long long)nl, (unsigned long long)gl->E,
+                         (int)gl->exact_w, (int)gl->exact_nw,
                          (unsigned long long)ng,
                          (unsigned long long)(st.local_move_sweeps - before.local_move_sweeps),
                          (unsigned long long)(st.moves - before.moves), st.ms_local_move - before.ms_local_move,

@@ -57,36 +57,37 @@ __global__ void k_starts_u32(const uint32_t* __restrict__ rows, uint64_t N, uint
     }
 }
 
-// Ordered per-community aggregates: one thread per community walks its members
-// in ascending order (partition.rs:90-105).
+// Ordered per-community aggregates, one warp per community walking its members
+// in ascending order (partition.rs:90-105); internal sums each member's row in
+// ascending neighbour order, entries outside the rule adding +0.0 (a no-op).
 __global__ void k_stats_ordered(const uint64_t* __restrict__ cstart, const uint32_t* __restrict__ members,
                                 uint64_t C, const uint32_t* __restrict__ memb,
                                 const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                                 const float* __restrict__ w, const double* __restrict__ node_w,
                                 const double* __restrict__ strength, uint32_t* size, double* weight,
                                 double* stren, double* internal, int need_internal) {
-    for (uint64_t c = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; c < C;
-         c += (uint64_t)gridDim.x * blockDim.x) {
-        double a = 0.0, s = 0.0, in = 0.0;
-        for (uint64_t i = cstart[c]; i < cstart[c + 1]; ++i) {
-            uint32_t v = members[i];
-            a = __dadd_rn(a, node_w[v]);
-            s = __dadd_rn(s, strength[v]);
-        }
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t c = warp; c < C; c += nwarps) {
+        const uint64_t b = cstart[c], e = cstart[c + 1];
+        const double a = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return node_w[members[i]]; });
+        const double s = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return strength[members[i]]; });
+        double in = 0.0;
         if (need_internal) {
-            for (uint64_t i = cstart[c]; i < cstart[c + 1]; ++i) {
-                uint32_t v = members[i];
-                for (uint64_t e = ptr[v]; e < ptr[v + 1]; ++e) {
-                    uint32_t u = nbr[e];
-                    if (memb[u] != (uint32_t)c) continue;
-                    if (u == v || v < u) in = __dadd_rn(in, (double)w[e]);
-                }
+            for (uint64_t i = b; i < e; ++i) {
+                const uint32_t v = members[i];
+                in = warp_ordered_sum(ptr[v], ptr[v + 1], in, [&](uint64_t j) {
+                    const uint32_t u = nbr[j];
+                    return (memb[u] == (uint32_t)c && (u == v || v < u)) ? (double)w[j] : 0.0;
+                });
             }
         }
-        size[c] = (uint32_t)(cstart[c + 1] - cstart[c]);
-        weight[c] = a;
-        stren[c] = s;
-        internal[c] = in;
+        if ((threadIdx.x & 31) == 0) {
+            size[c] = (uint32_t)(e - b);
+            weight[c] = a;
+            stren[c] = s;
+            internal[c] = in;
+        }
     }
 }
 
@@ -219,7 +220,7 @@ void partition_stats(Ctx& c, const DevGraph& g, const uint32_t* d_memb, uint64_t
     sort_pairs(c, d_memb, ms.get(), idx.get(), members.get(), n, bits_for(C));
     k_starts_u32<<<grid_for(n + 1, TB), TB, 0, c.stream>>>(ms.get(), n, C, cstart.get());
     SC_LAUNCH_CHECK();
-    k_stats_ordered<<<grid_for(C, 128), 128, 0, c.stream>>>(
+    k_stats_ordered<<<grid_for(C * 32, 256), 256, 0, c.stream>>>(
         cstart.get(), members.get(), C, d_memb, g.ptr, g.nbr, g.w, g.node_w, g.strength,
         out.size.get(), out.weight.get(), out.strength.get(), out.internal.get(),
         need_internal ? 1 : 0);

@@ -112,4 +112,21 @@ void zero(Ctx& c, T* d, size_t n) {
 inline void sync(Ctx& c) { SC_CUDA(cudaStreamSynchronize(c.stream)); }
 
 
+// Σ_{i in [b, e)} f(i) in index order, by one warp: lanes load 32 terms at a
+// time (coalesced), then every lane folds them in order through shuffles, so
+// the result is the sequential left fold of the reference, bit for bit, while
+// the loads stay memory-parallel. Every lane returns the same value.
+template <class F>
+__device__ __forceinline__ double warp_ordered_sum(uint64_t b, uint64_t e, double init, F f) {
+    const unsigned lane = threadIdx.x & 31u;
+    double acc = init;
+    for (uint64_t base = b; base < e; base += 32) {
+        const uint64_t i = base + lane;
+        const double x = i < e ? f(i) : 0.0;
+        const unsigned cnt = (unsigned)((e - base) < 32 ? (e - base) : 32);
+        for (unsigned j = 0; j < cnt; ++j) acc = __dadd_rn(acc, __shfl_sync(0xFFFFFFFFu, x, (int)j));
+    }
+    return acc;
+}
+
 }  // namespace sc

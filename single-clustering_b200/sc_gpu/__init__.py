@@ -497,3 +497,57 @@ __all__ = [
     "InvalidConfig", "TooManyNodes", "InvalidCsr", "AsymmetricGraph", "DeviceError", "MAX_NODES", "NOISE",
     "last_run_stats", "context",
 ]
+
+
+# ---------------------------------------------------------------- kNN graph builder
+SIGMA_MEDIAN, SIGMA_KTH = 0, 1
+SYM_LOWER_ID, SYM_UNION = 0, 1
+KNN_FP32, KNN_BF16, KNN_FP8 = 0, 1, 2
+
+
+class NeighborResult:
+    """NeighborResult (src/neighborhood/mod.rs:29-34): k+1 neighbours per row
+    (self first) with their distances, and the connectivities CSR."""
+
+    def __init__(self, index, distances, conn_ptrs, conn_nbrs, conn_w, graph=None):
+        self.index = index
+        self.distances = distances
+        self.conn_ptrs = conn_ptrs
+        self.conn_nbrs = conn_nbrs
+        self.conn_w = conn_w
+        self.graph = graph
+
+
+def knn_gaussian(X, k: int, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_ID,
+                 precision: int = KNN_BF16, squared: bool = False, build_graph: bool = False,
+                 device: int | None = None) -> NeighborResult:
+    """knn_arrayd_* (neighborhood/mod.rs:51-202, :359-578) with an exact search.
+
+    Defaults follow the reference: sigma = median neighbour distance, pairs
+    emitted from the lower id only. `squared=True` mirrors the kd-tree path
+    (squared distances returned, sigma = sqrt(median d^2))."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n, d = X.shape
+    ctx = context(device)
+    opts = _lib.KnnOpts()
+    lib().sc_knn_opts_default(C.byref(opts))
+    opts.sigma, opts.sym, opts.precision, opts.squared_kiddo = sigma, sym, precision, int(squared)
+    idx = np.zeros((n, k + 1), np.uint32)
+    dist = np.zeros((n, k + 1), np.float32)
+    cap = 2 * n * k
+    ptrs = np.zeros(n + 1, np.uint64)
+    nbrs = np.zeros(cap, np.uint32)
+    w = np.zeros(cap, np.float32)
+    nnz = C.c_uint64()
+    gh = C.c_void_p()
+    _check(lib().sc_knn_gaussian(ctx.h, _ptr(X, _lib.f32p), n, d, k, C.byref(opts), _ptr(idx, _lib.u32p),
+                                 _ptr(dist, _lib.f32p), _ptr(ptrs, _lib.u64p), _ptr(nbrs, _lib.u32p),
+                                 _ptr(w, _lib.f32p), cap, C.byref(nnz),
+                                 C.byref(gh) if build_graph else None), ctx)
+    m = nnz.value
+    graph = CSRNetwork(gh, ctx) if build_graph else None
+    return NeighborResult(idx, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), graph)
+
+
+__all__ += ["knn_gaussian", "NeighborResult", "SIGMA_MEDIAN", "SIGMA_KTH", "SYM_LOWER_ID", "SYM_UNION",
+            "KNN_FP32", "KNN_BF16", "KNN_FP8"]

@@ -1,0 +1,76 @@
+"""GPU kNN + Gaussian connectivities against the FP64 exact oracle.
+
+Bar: neighbour sets equal the FP64 exact search's except for distance ties
+within 1e-6 relative; connectivity weights within 1e-5 relative of the FP64
+formula evaluated on the GPU's own neighbour lists.
+"""
+import numpy as np
+import pytest
+
+import knn_oracle as K
+import sc_gpu
+from sc_gpu import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def check_sets(idx_gpu, idx_true, dist_true, X):
+    """Every mismatch must be a tie with the true k-th distance (1e-6 relative)."""
+    bad = 0
+    for q in range(idx_true.shape[0]):
+        a, b = set(idx_gpu[q].tolist()), set(idx_true[q].tolist())
+        if a == b:
+            continue
+        kth = dist_true[q, -1]
+        for j in a - b:
+            dj = float(np.sqrt(((X[q].astype(np.float64) - X[j]) ** 2).sum()))
+            if abs(dj - kth) > 1e-6 * max(kth, 1e-30):
+                bad += 1
+    return bad
+
+
+@pytest.mark.parametrize("n,d,k", [(1000, 30, 10), (3000, 50, 15), (777, 7, 5), (300, 62, 10)])
+def test_neighbour_sets_match_exact_fp64(n, d, k):
+    X, _ = synth.gaussian_mixture(n, d, 8, seed=n + d, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, k)
+    idx_t, dist_t = K.knn_exact(X, k)
+    assert np.all(r.index[:, 0] == np.arange(n)), "self first"
+    assert check_sets(r.index, idx_t, dist_t, X) == 0
+    # distances: FP32 exact differences vs FP64
+    d64 = K.exact_dist_matrix_rows(X, np.arange(n)[:, None], r.index.astype(np.int64))
+    assert np.allclose(r.distances, d64, rtol=1e-5, atol=1e-6)
+
+
+@pytest.mark.parametrize("sigma,sym", [(sc_gpu.SIGMA_MEDIAN, sc_gpu.SYM_LOWER_ID), (sc_gpu.SIGMA_KTH, sc_gpu.SYM_UNION)])
+def test_connectivities_match_reference_formula(sigma, sym):
+    n, d, k = 2000, 30, 10
+    X, _ = synth.gaussian_mixture(n, d, 10, seed=5, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, k, sigma=sigma, sym=sym, build_graph=True)
+    dist64 = K.exact_dist_matrix_rows(X, np.arange(n)[:, None], r.index.astype(np.int64))
+    sig = K.sigmas(dist64, kth=sigma == sc_gpu.SIGMA_KTH)
+    rows, cols, w = K.connectivities(r.index.astype(np.int64), dist64, sig, union=sym == sc_gpu.SYM_UNION)
+    ptr = r.conn_ptrs.astype(np.int64)
+    grow = np.repeat(np.arange(n), np.diff(ptr))
+    assert np.array_equal(grow, rows) and np.array_equal(r.conn_nbrs.astype(np.int64), cols)
+    assert np.max(np.abs(r.conn_w - w) / np.maximum(w, 1e-30)) < 1e-5
+    g = r.graph
+    assert g.node_count() == n and g.entry_count() == len(w)
+    g.validate_symmetry()
+
+
+def test_recall_at_k_on_larger_mixture():
+    n, d, k = 20000, 30, 10
+    X, _ = synth.gaussian_mixture(n, d, 30, seed=11, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, k)
+    sample = np.random.Generator(np.random.PCG64(0)).choice(n, 500, replace=False)
+    idx_t, dist_t = K.knn_exact(X, k)
+    rec = K.recall(r.index[sample], idx_t[sample])
+    assert rec >= 0.999, rec
+
+
+def test_squared_kiddo_semantics():
+    X, _ = synth.gaussian_mixture(500, 20, 4, seed=3)
+    a = sc_gpu.knn_gaussian(X, 8)
+    b = sc_gpu.knn_gaussian(X, 8, squared=True)
+    assert np.array_equal(a.index, b.index)
+    assert np.allclose(b.distances, a.distances.astype(np.float64) ** 2, rtol=1e-5)
