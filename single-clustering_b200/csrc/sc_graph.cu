@@ -678,13 +678,14 @@ __global__ void k_iota(uint32_t* p, uint64_t n) {
 // accumulator of :549-554; members without a loop add +0.0, a no-op).
 __global__ void k_group_sums(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
                              uint64_t G, const double* __restrict__ node_w,
-                             const double* __restrict__ self_loop, double* nw_out, double* loops_out) {
+                             const double* __restrict__ self_loop, double* nw_out, double* loops_out,
+                             int exact_nw, int exact_w) {
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t gi = warp; gi < G; gi += nwarps) {
         const uint64_t b = gstart[gi], e = gstart[gi + 1];
-        const double a = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return node_w[members[i]]; });
-        const double l = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return self_loop[members[i]]; });
+        const double a = warp_fold(b, e, 0.0, exact_nw, [&](uint64_t i) { return node_w[members[i]]; });
+        const double l = warp_fold(b, e, 0.0, exact_w, [&](uint64_t i) { return self_loop[members[i]]; });
         if ((threadIdx.x & 31) == 0) {
             nw_out[gi] = a;
             loops_out[gi] = l;
@@ -722,12 +723,12 @@ __global__ void k_iota64(uint64_t* p, uint64_t n) {
 __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
                              const uint64_t* __restrict__ keys, const float* __restrict__ w,
                              uint64_t G, const double* __restrict__ loops, uint32_t* prow,
-                             uint32_t* pcol, float* pw, uint8_t* keep) {
+                             uint32_t* pcol, float* pw, uint8_t* keep, int exact) {
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t s = warp; s < P; s += nwarps) {
         const uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
-        const double acc = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) { return (double)w[i]; });
+        const double acc = warp_fold(b, e, 0.0, exact, [&](uint64_t i) { return (double)w[i]; });
         if ((threadIdx.x & 31) != 0) continue;
         uint64_t key = keys[b];
         uint32_t g = (uint32_t)(key / G), h = (uint32_t)(key % G);
@@ -810,7 +811,8 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         sort_pairs(c, d_grp, grp_s.get(), idx.get(), members.get(), n, bits_for(G));
         k_starts_from_sorted<<<grid_for(n + 1, TB), TB, 0, c.stream>>>(grp_s.get(), n, G, gstart.get());
         k_group_sums<<<grid_for((uint64_t)G * 32, TB), TB, 0, c.stream>>>(gstart.get(), members.get(), G, g.node_w,
-                                                           g.self_loop, nw_new.get(), loops.get());
+                                                           g.self_loop, nw_new.get(), loops.get(),
+                                                           (int)g.exact_nw, (int)g.exact_w);
         SC_LAUNCH_CHECK();
         c.launches += 2;
     }
@@ -863,7 +865,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         keep.alloc(c, P);
         k_seg_values<<<grid_for(P * 32, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
                                                            uw_s.get(), G, loops.get(), prow.get(),
-                                                           pcol.get(), pw.get(), keep.get());
+                                                           pcol.get(), pw.get(), keep.get(), (int)g.exact_w);
         SC_LAUNCH_CHECK();
         c.launches++;
     }

@@ -25,7 +25,10 @@ namespace sc {
 namespace {
 
 constexpr unsigned TB = 256;
-constexpr int NBUCKET = 5;          // G8, G16, G32, block (shared hash), hub (global hash)
+constexpr int NBUCKET = 6;          // G8, G16, G32, warp (shared hash), block (shared hash), hub (global hash)
+constexpr uint32_t WARP_DEGREE = 256;  // largest degree of the warp-per-node bucket
+constexpr int WCAP = 2 * WARP_DEGREE;  // per-warp shared hash entries
+constexpr int WARPS_PER_BLOCK = 4;
 constexpr int HCAP_SMEM = 2 * HUB_DEGREE;  // shared hash entries per block (u32 key + i64 val): 24 KB
 constexpr int LM_BATCHES = 8;
 constexpr int RF_BATCHES = 8;
@@ -70,6 +73,7 @@ struct Params {
     // max_community_weight: one joiner per target community per batch (the
     // highest claim key wins), so a community never passes the cap
     unsigned long long* claim;
+    uint32_t* moved;  // epoch in which the node last committed a move
 };
 
 __device__ __forceinline__ long long to_fix(double x, double inv) { return __double2ll_rn(__dmul_rn(x, inv)); }
@@ -370,6 +374,137 @@ __device__ void block_argmax(double& g, uint32_t& c, double* sg, uint32_t* sc) {
     __syncthreads();
 }
 
+// One warp per node of degree 33..WARP_DEGREE: an open-addressing hash of
+// neighbour communities in this warp's slice of shared memory, gains scored
+// by every lane over its slots, warp argmax.
+template <bool REFINE>
+__global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, const uint32_t* __restrict__ list,
+                                                                      uint32_t count) {
+    __shared__ uint32_t s_keys[WARPS_PER_BLOCK][WCAP];
+    __shared__ long long s_vals[WARPS_PER_BLOCK][WCAP];
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* keys = s_keys[wib];
+    long long* vals = s_vals[wib];
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    unsigned long long sdeg = 0, scand = 0, snodes = 0;
+    for (uint64_t i = warp; i < count; i += nwarps) {
+        const uint32_t v = list[i];
+        const uint64_t b = p.ptr[v], e = p.ptr[v + 1];
+        const uint32_t deg = (uint32_t)(e - b);
+        const uint32_t own = p.memb[v];
+        if (REFINE && p.csize[own] != 1) continue;  // warp-uniform
+        uint32_t cap = 64;
+        while (cap < 2 * deg) cap <<= 1;
+        if (cap > (uint32_t)WCAP) {  // not this bucket's node
+            if (lane == 0) atomicOr(p.status, DEV_OVERFLOW);
+            continue;
+        }
+        const uint32_t mask = cap - 1;
+        for (uint32_t s = lane; s < cap; s += 32) {
+            keys[s] = EMPTYK;
+            vals[s] = 0;
+        }
+        __syncwarp();
+        const uint32_t cv = REFINE ? p.constraint[v] : 0;
+        for (uint64_t j = b + lane; j < e; j += 32) {
+            const uint32_t u = p.nbr[j];
+            if (u == v) continue;
+            if (REFINE && p.constraint[u] != cv) continue;
+            hinsert(keys, vals, mask, p.memb[u], to_fix((double)p.w[j], p.inv_scale), p.status);
+        }
+        __syncwarp();
+        const long long kf = to_fix(p.strength[v], p.inv_scale);
+        const long long af = to_fix(p.node_w[v], p.inv_nscale);
+        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = p.self_loop[v];
+        const long long wof = hlookup(keys, vals, mask, own);
+        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale), a,
+                                    from_fix(p.Wf[own] - af, p.nscale));
+        double g = -INFINITY;
+        uint32_t c = NONE32;
+        uint32_t lc = 0;
+        for (uint32_t s = lane; s < cap; s += 32) {
+            const uint32_t cu = keys[s];
+            if (cu == EMPTYK || cu == own) continue;
+            lc++;
+            const double nc = from_fix(p.Wf[cu], p.nscale);
+            if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
+            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+            if (REFINE) {
+                const double rel = __dsub_rn(gg, base);
+                if (!(rel >= 0.0)) continue;
+                gg = refine_key(p, rel, v, cu);
+            }
+            if (better(gg, cu, g, c)) {
+                g = gg;
+                c = cu;
+            }
+        }
+        for (int o = 16; o; o >>= 1) {
+            const double og = __shfl_xor_sync(FULL, g, o);
+            const uint32_t oc = __shfl_xor_sync(FULL, c, o);
+            if (better(og, oc, g, c)) {
+                g = og;
+                c = oc;
+            }
+        }
+        scand += lc;
+        uint32_t target = NONE32;
+        long long dg = 0;
+        if (!REFINE) {
+            uint32_t best = own;
+            double bg = base;
+            if (c != NONE32 && better(g, c, bg, best)) {
+                best = c;
+                bg = g;
+            }
+            const uint32_t fresh = (uint32_t)(p.S0 + v);
+            if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 && (!p.has_limit || a <= p.limit)) {
+                const double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                if (better(ge, fresh, bg, best)) {
+                    best = fresh;
+                    bg = ge;
+                }
+            }
+            const double d = __dsub_rn(bg, base);
+            if (best != own && d > p.thr) {
+                target = best;
+                dg = to_fix(d, p.inv_scale);
+            }
+        } else {
+            target = c;
+        }
+        // the member of a singleton target, for conflict detection
+        uint32_t member = NONE32;
+        if (target != NONE32 && p.csize[target] == 1) {
+            for (uint64_t base0 = b; base0 < e; base0 += 32) {
+                const uint64_t j = base0 + lane;
+                const uint32_t u = j < e ? p.nbr[j] : v;
+                const bool hit = u != v && p.memb[u] == target;
+                if (hit) member = u;
+                if (__ballot_sync(FULL, hit)) break;
+            }
+            for (int o = 16; o; o >>= 1) member = min(member, __shfl_xor_sync(FULL, member, o));
+        }
+        if (lane == 0) {
+            snodes += 1;
+            sdeg += deg;
+            if (target != NONE32) {
+                p.tgt[v] = target;
+                p.from[v] = own;
+                p.dgain[v] = dg;
+                p.hint[v] = member;
+                p.epoch[v] = p.cur;
+            }
+        }
+        __syncwarp();
+    }
+    warp_add(p.counters + 1, sdeg);
+    warp_add(p.counters + 2, scand);
+    warp_add(p.counters + 3, snodes);
+}
+
 // One block per node. HUB = false: degree <= HUB_DEGREE, hash table in shared
 // memory. HUB = true: the table lives in this block's slice of the global
 // scratch (gcap entries), which the host sized for the largest degree; the
@@ -534,21 +669,27 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
         atomicAdd(p.csize + t, 1u);
         nmoves++;
         gsum += p.dgain[v];
-        if (!REFINE) {
-            // re-queue neighbours outside the new community (local_move.rs:113-118)
-            for (uint64_t j = p.ptr[v]; j < p.ptr[v + 1]; ++j) {
-                uint32_t u = p.nbr[j];
-                if (u == v) continue;
-                uint32_t cu;
-                if (p.epoch[u] == p.cur) cu = lost(p, u) ? p.from[u] : p.tgt[u];
-                else cu = p.memb[u];
-                if (cu != t) next_active[u] = 1;
-            }
-        }
+        if (!REFINE) p.moved[v] = p.cur;
     }
     warp_add(p.counters + 0, nmoves);
     for (int o = 16; o; o >>= 1) gsum += __shfl_xor_sync(0xFFFFFFFFu, gsum, o);
     if ((threadIdx.x & 31) == 0 && gsum) atomicAdd((unsigned long long*)p.gain_acc, (unsigned long long)gsum);
+}
+
+// Re-queue the neighbours of every node that moved in this batch and now sits
+// in a different community from them (local_move.rs:113-118). Runs after the
+// commit, so every membership it reads is final.
+__global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t count, uint8_t* next_active) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = list[i];
+        if (p.moved[v] != p.cur) continue;
+        const uint32_t t = p.memb[v];
+        for (uint64_t j = p.ptr[v]; j < p.ptr[v + 1]; ++j) {
+            const uint32_t u = p.nbr[j];
+            if (u != v && p.memb[u] != t) next_active[u] = 1;
+        }
+    }
 }
 
 __global__ void k_claim(Params p, const uint32_t* __restrict__ list, uint32_t count) {
@@ -562,7 +703,7 @@ __global__ void k_claim(Params p, const uint32_t* __restrict__ list, uint32_t co
 
 // ------------------------------------------------------------ bucketing
 __device__ __forceinline__ int bucket_of(uint32_t deg) {
-    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= HUB_DEGREE ? 3 : 4;
+    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= WARP_DEGREE ? 3 : deg <= HUB_DEGREE ? 4 : 5;
 }
 
 __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
@@ -582,16 +723,26 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* 
         if (sc[t]) atomicAdd(counts + t, sc[t]);
 }
 
+// One warp-aggregated atomic per distinct (batch, bucket) per warp.
 __global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
                                  uint64_t n, uint64_t seed, uint32_t sweep, int B, uint32_t* cursor,
                                  uint32_t* list) {
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        if (active && !active[v]) continue;
-        int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
-        int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
-        uint32_t pos = atomicAdd(cursor + b * NBUCKET + k, 1u);
-        list[pos] = (uint32_t)v;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
+        const uint64_t v = base + lane;
+        int slot = -1;
+        if (v < n && (!active || active[v])) {
+            int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
+            int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
+            slot = b * NBUCKET + k;
+        }
+        const unsigned mm = __match_any_sync(0xFFFFFFFFu, slot < 0 ? 1000 + (int)lane : slot);
+        const int leader = __ffs(mm) - 1;
+        uint32_t pos0 = 0;
+        if (slot >= 0 && (int)lane == leader) pos0 = atomicAdd(cursor + slot, (uint32_t)__popc(mm));
+        pos0 = __shfl_sync(0xFFFFFFFFu, pos0, leader);
+        if (slot >= 0) list[pos0 + __popc(mm & ((1u << lane) - 1u))] = (uint32_t)v;
     }
 }
 
@@ -654,7 +805,7 @@ Scales scales_for(const DevGraph& g) {
 }
 
 struct Workspace {
-    DBuf<uint32_t> tgt, hint, from, epoch, list;
+    DBuf<uint32_t> tgt, hint, from, epoch, list, moved;
     DBuf<long long> dgain;
     DBuf<uint8_t> active, next_active;
     DBuf<uint32_t> counts;
@@ -696,6 +847,7 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.hint.alloc(c, n);
     ws.from.alloc(c, n);
     ws.epoch.alloc(c, n);
+    ws.moved.alloc(c, n);
     ws.list.alloc(c, n);
     ws.dgain.alloc(c, n);
     ws.active.alloc(c, n);
@@ -704,6 +856,7 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.counters.alloc(c, 4);
     ws.gain_acc.alloc(c, 1);
     zero(c, ws.epoch.get(), n);
+    zero(c, ws.moved.get(), n);
     zero(c, ws.hint.get(), n);
     // global hash / candidate scratch, one slice per block, for the hubs only
     ws.nblk_large = 0;
@@ -733,6 +886,10 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list
     } else if (k == 2) {
         k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
     } else if (k == 3) {
+        const uint64_t warps = cnt;
+        k_decide_warp<REFINE><<<grid_for(warps * 32, 32 * WARPS_PER_BLOCK, 148u * 64u), 32 * WARPS_PER_BLOCK, 0,
+                                c.stream>>>(p, list, cnt);
+    } else if (k == 4) {
         size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
         unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
         k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, cnt, nullptr, nullptr, 0);
@@ -805,9 +962,11 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     p.counters = ws.counters.get();
     p.gain_acc = ws.gain_acc.get();
     p.claim = claim.get();
+    p.moved = ws.moved.get();
     zero(c, ws.counters.get(), 4);
     zero(c, ws.gain_acc.get(), 1);
     zero(c, ws.epoch.get(), n);
+    zero(c, ws.moved.get(), n);
     k_fill_u8<<<grid_for(n, TB), TB, 0, c.stream>>>(ws.active.get(), n, 1);
     c.launches++;
     const int B = LM_BATCHES;
@@ -815,6 +974,8 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     uint64_t moves_before = 0;
     const uint64_t budget = n * 100;  // MAX_MOVES_PER_NODE, local_move.rs:32
     static const int trace = std::getenv("SC_TRACE") ? std::atoi(std::getenv("SC_TRACE")) : 0;
+    // experimental: stop once a sweep moves fewer than tail * n nodes (0 = run to a local optimum)
+    const double tail = std::getenv("SC_LM_TAIL") ? std::atof(std::getenv("SC_LM_TAIL")) : 0.0;
     for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
         zero(c, ws.counts.get(), B * NBUCKET);
         zero(c, ws.next_active.get(), n);
@@ -834,6 +995,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             std::fprintf(stderr, "[sc]   sweep %u moves=%llu next_active=%u\n", sweep - 1,
                          (unsigned long long)(ctr[0] - moves_before), offs[B * NBUCKET]);
         if (sweep > 0 && ctr[0] == moves_before) break;  // last sweep moved nothing
+        if (sweep > 1 && tail > 0.0 && (double)(ctr[0] - moves_before) < tail * (double)n) break;
         if (ctr[0] >= budget) break;
         moves_before = ctr[0];
         if (offs[B * NBUCKET] == 0) break;
@@ -859,8 +1021,10 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             }
             k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
                                                                        ws.next_active.get());
+            k_activate<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
+                                                                   ws.next_active.get());
             SC_LAUNCH_CHECK();
-            c.launches++;
+            c.launches += 2;
         }
         std::swap(ws.active, ws.next_active);
         r.sweeps++;
@@ -929,6 +1093,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     p.counters = ws.counters.get();
     p.gain_acc = ws.gain_acc.get();
     p.claim = claim.get();
+    p.moved = ws.moved.get();
     zero(c, ws.counters.get(), 4);
     zero(c, ws.epoch.get(), n);
     const int B = RF_BATCHES;

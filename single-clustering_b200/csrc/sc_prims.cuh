@@ -129,4 +129,17 @@ __device__ __forceinline__ double warp_ordered_sum(uint64_t b, uint64_t e, doubl
     return acc;
 }
 
+// init + Σ f(i) when every partial sum is exact (the exact regime): any order
+// gives the same bits, so lanes accumulate strided and reduce by butterfly.
+// Falls back to the ordered fold otherwise. Every lane returns the same value.
+template <class F>
+__device__ __forceinline__ double warp_fold(uint64_t b, uint64_t e, double init, bool exact, F f) {
+    if (!exact) return warp_ordered_sum(b, e, init, f);
+    const unsigned lane = threadIdx.x & 31u;
+    double acc = 0.0;
+    for (uint64_t i = b + lane; i < e; i += 32) acc = __dadd_rn(acc, f(i));
+    for (int o = 16; o; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, o));
+    return e > b ? __dadd_rn(init, acc) : init;
+}
+
 }  // namespace sc
