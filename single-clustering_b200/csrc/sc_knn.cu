@@ -143,6 +143,53 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Insert (v, idx) into a query's candidate slots over its current worst slot and
+// return the new worst (value, slot). Kept out of line: it is the rare path,
+// and inlining it into the unrolled filter loop overflows the instruction cache.
+struct Worst {
+    float thr;
+    int slot;
+};
+
+__device__ __noinline__ Worst cand_insert(float* cs, uint32_t* ci, int qrow, int slot, float v, uint32_t idx) {
+    constexpr int S = QT * TILE;
+    cs[slot * S + qrow] = v;
+    ci[slot * S + qrow] = idx;
+    Worst w{-INFINITY, 0};
+    for (int s = 0; s < RCAND; ++s) {
+        const float x = cs[s * S + qrow];
+        if (x > w.thr) {
+            w.thr = x;
+            w.slot = s;
+        }
+    }
+    return w;
+}
+
+__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
+          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+          "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]),
+          "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]),
+          "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]),
+          "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]),
+          "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+        : "r"(taddr + 32));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
 // ------------------------------------------------------------ prep
 template <int KA>
 __global__ void k_knn_prep(const float* __restrict__ X, uint64_t n, uint32_t d, __nv_bfloat16* A,
@@ -336,25 +383,17 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 fence_after();
                 const uint32_t taddr = tmem + ((uint32_t)(lq * 32) << 16) + b * (QT * TILE) + q * TILE;
 #pragma unroll 1
-                for (int c0 = 0; c0 < TILE; c0 += 32) {
-                    float v[32];
-                    tmem_ld32(taddr + c0, v);
+                for (int c0 = 0; c0 < TILE; c0 += 64) {
+                    uint32_t r[64];
+                    tmem_ld64(taddr + c0, r);
+                    const uint32_t base_idx = t * TILE + c0;
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (v[j] < thr) {
-                            const uint32_t idx = t * TILE + c0 + j;
-                            if (idx < n) {
-                                cs[thr_slot * (QT * TILE) + qrow] = v[j];
-                                ci[thr_slot * (QT * TILE) + qrow] = idx;
-                                thr = -INFINITY;
-                                for (int s = 0; s < RCAND; ++s) {
-                                    float x = cs[s * (QT * TILE) + qrow];
-                                    if (x > thr) {
-                                        thr = x;
-                                        thr_slot = s;
-                                    }
-                                }
-                            }
+                    for (int j = 0; j < 64; ++j) {
+                        const float v = __uint_as_float(r[j]);
+                        if (v < thr && base_idx + j < n) {
+                            const Worst w = cand_insert(cs, ci, qrow, thr_slot, v, base_idx + j);
+                            thr = w.thr;
+                            thr_slot = w.slot;
                         }
                     }
                 }
