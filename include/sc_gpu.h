@@ -202,6 +202,24 @@ sc_status sc_aggregate(sc_ctx* ctx, const sc_graph* g, const uint64_t* groups,
 sc_status sc_modularity(sc_ctx* ctx, const sc_graph* g, const uint64_t* labels,
                         uint64_t n_labels, double resolution, double* out);
 
+/*
+ * Modularity for callers that cannot allocate device memory (a host framework
+ * that owns the device memory pool, a fixed device-memory budget, a section
+ * where cudaMalloc's implicit synchronisation is not allowed). No counterpart
+ * in the reference: it is sc_modularity with the labels already on the device
+ * as compact uint32 ids (< 65,536, so at most 65,536 communities; larger ids
+ * return SC_E_UNSUPPORTED) and no device allocation. Its scratch is a fixed
+ * 1 MiB array in the library, held by every GPU that loads the library until
+ * the process exits; the first call on a device looks up that array's address,
+ * so make that first call before any stream capture. Every call shares the
+ * array: calls whose work overlaps on the GPU race and must be serialised.
+ * Bit-exact with sc_modularity when every sum of the graph's edge weights is
+ * exact in f64 (all unit or f32-valued weights below 2^(52+e0) in total);
+ * otherwise it may differ in the last bits.
+ */
+sc_status sc_modularity_static(sc_ctx* ctx, const sc_graph* g, const uint32_t* labels_device,
+                               uint64_t n_labels, double resolution, double* out);
+
 /* Partition::from_membership (partition.rs:75-112) then Rb::quality (objective.rs:108-119)
  * or Cpm::quality (:171-178). */
 sc_status sc_quality(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership,

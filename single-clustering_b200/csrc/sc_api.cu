@@ -291,6 +291,20 @@ sc_status sc_modularity(sc_ctx* ctx, const sc_graph* g, const uint64_t* labels, 
     });
 }
 
+// No device allocation: scratch is the fixed array of sc_static.cu. The first
+// call on a device also looks up that array's device address.
+sc_status sc_modularity_static(sc_ctx* ctx, const sc_graph* g, const uint32_t* labels_device, uint64_t n_labels,
+                               double resolution, double* out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && out, "graph or out is NULL");
+        require_same_device(c, *g->g);
+        const sc::DevGraph& G = *g->g;
+        check_membership_len(n_labels, G.n);
+        require(G.n == 0 || labels_device, "labels_device is NULL");
+        *out = sc::modularity_static(c, G, labels_device, G.n, resolution);
+    });
+}
+
 sc_status sc_quality(sc_ctx* ctx, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
                      int32_t objective, double resolution, double* out) {
     return guarded(ctx, [&](sc::Ctx& c) {

@@ -237,6 +237,9 @@ double quality(Ctx& c, const DevGraph& g, const uint32_t* d_memb, uint64_t slots
 double modularity(Ctx& c, const DevGraph& g, const uint32_t* d_labels, uint64_t n_comms,
                   double gamma);
 
+// static.cu: modularity from compact device labels, no device allocation
+double modularity_static(Ctx& c, const DevGraph& g, const uint32_t* d_labels, uint64_t n, double gamma);
+
 // leiden.cu
 struct LeidenOut {
     std::vector<uint32_t> labels;

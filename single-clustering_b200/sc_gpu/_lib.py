@@ -106,6 +106,7 @@ SIGNATURES = [
     ("sc_aggregate", C.c_int, [vp, vp, u64p, C.c_uint64, vpp]),
     ("sc_modularity", C.c_int, [vp, vp, u64p, C.c_uint64, C.c_double, f64p]),
     ("sc_quality", C.c_int, [vp, vp, u64p, C.c_uint64, C.c_int32, C.c_double, f64p]),
+    ("sc_modularity_static", C.c_int, [vp, vp, vp, C.c_uint64, C.c_double, f64p]),
     ("sc_partition_stats", C.c_int, [vp, vp, u64p, C.c_uint64, u64p, u32p, f64p, f64p, f64p, C.c_uint64]),
     ("sc_leiden", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), u64p, u64p]),
     ("sc_leiden_from", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), u64p, C.c_uint64, u64p, u64p]),
