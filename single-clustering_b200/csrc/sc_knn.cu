@@ -386,14 +386,24 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 for (int c0 = 0; c0 < TILE; c0 += 64) {
                     uint32_t r[64];
                     tmem_ld64(taddr + c0, r);
-                    const uint32_t base_idx = t * TILE + c0;
+                    // branch-free prefilter: the chunk's minimum against the row's worst kept
+                    float m[32];
 #pragma unroll
-                    for (int j = 0; j < 64; ++j) {
-                        const float v = __uint_as_float(r[j]);
-                        if (v < thr && base_idx + j < n) {
-                            const Worst w = cand_insert(cs, ci, qrow, thr_slot, v, base_idx + j);
-                            thr = w.thr;
-                            thr_slot = w.slot;
+                    for (int j = 0; j < 32; ++j) m[j] = fminf(__uint_as_float(r[j]), __uint_as_float(r[j + 32]));
+#pragma unroll
+                    for (int w2 = 16; w2 >= 1; w2 >>= 1)
+#pragma unroll
+                        for (int j = 0; j < w2; ++j) m[j] = fminf(m[j], m[j + w2]);
+                    if (m[0] < thr) {
+                        const uint32_t base_idx = t * TILE + c0;
+#pragma unroll
+                        for (int j = 0; j < 64; ++j) {
+                            const float v = __uint_as_float(r[j]);
+                            if (v < thr && base_idx + j < n) {
+                                const Worst w = cand_insert(cs, ci, qrow, thr_slot, v, base_idx + j);
+                                thr = w.thr;
+                                thr_slot = w.slot;
+                            }
                         }
                     }
                 }
