@@ -259,6 +259,22 @@ sc_status sc_leiden_batch(sc_ctx* ctx, const sc_graph* const* graphs,
                           const uint64_t* label_offsets, uint64_t* labels_out,
                           uint64_t* n_clusters_out);
 
+/*
+ * sc_leiden_batch with its scheduling exposed. Instances run concurrently on
+ * n_streams worker streams (0 = 8), each with its own stream and state, so the
+ * small kernels of coarse levels from different instances overlap. When
+ * warm_from is non-NULL, instance i with warm_from[i] = j >= 0 (j < i, same
+ * node count) starts from instance j's final labels — leiden with `initial`
+ * (run_once, src/community_search/leiden/mod.rs:207-220) — and waits for j;
+ * -1 starts from singletons. A resolution sweep chains each resolution to its
+ * neighbour this way.
+ */
+sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs,
+                             const sc_leiden_config* cfgs, uint64_t count,
+                             const int64_t* warm_from, const uint64_t* label_offsets,
+                             uint64_t* labels_out, uint64_t* n_clusters_out,
+                             uint32_t n_streams);
+
 /* ---- kNN graph builder --------------------------------------------------- */
 typedef enum sc_knn_sigma { SC_SIGMA_MEDIAN = 0, SC_SIGMA_KTH = 1 } sc_knn_sigma;
 typedef enum sc_knn_sym { SC_SYM_LOWER_ID = 0, SC_SYM_UNION = 1 } sc_knn_sym;

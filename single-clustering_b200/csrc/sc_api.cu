@@ -1,7 +1,11 @@
 // sc_api.cu — the extern "C" boundary (include/sc_gpu.h). Every entry point
 // catches library failures and turns them into an sc_status plus the context's
 // last-error record; nothing escapes as a C++ exception or an abort.
+#include <atomic>
+#include <condition_variable>
+#include <mutex>
 #include <random>
+#include <thread>
 
 #include "sc_prims.cuh"
 
@@ -66,6 +70,47 @@ void require_same_device(sc::Ctx& c, const sc::DevGraph& g) {
     if (c.device != g.device) bad_arg("graph lives on another device than the context");
 }
 
+// Stream, pool and status word of a context on `device` (SC_OK or the failure).
+sc_status init_ctx(sc::Ctx& c, int device) {
+    c.device = device;
+    if (cudaSetDevice(device) != cudaSuccess) return SC_E_CUDA;
+    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
+    if (cudaDeviceGetDefaultMemPool(&c.pool, device) != cudaSuccess) return SC_E_CUDA;
+    uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
+    cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+    if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
+    cudaMemset(c.d_status, 0, sizeof(uint32_t));
+    cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
+    int optin = 0;
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    c.smem_optin = (size_t)optin;
+    return SC_OK;
+}
+
+void release_ctx(sc::Ctx& c) {
+    cudaSetDevice(c.device);
+    if (c.stream) {
+        cudaStreamSynchronize(c.stream);
+        cudaStreamDestroy(c.stream);
+        c.stream = nullptr;
+    }
+    if (c.d_status) cudaFree(c.d_status);
+    c.d_status = nullptr;
+}
+
+// Runs instance i of a batch on worker context w (labels copied to the host).
+void run_instance(sc::Ctx& w, const sc::DevGraph& G, const sc_leiden_config& cfg, const uint64_t* initial,
+                  uint64_t* labels_out, uint64_t* n_clusters) {
+    sc::DBuf<uint32_t> lab(w, G.n);
+    uint64_t ncl = 0;
+    sc::leiden(w, G, cfg, initial, lab.get(), &ncl);
+    std::vector<uint32_t> h(G.n);
+    sc::d2h(w, h.data(), lab.get(), G.n);
+    sc::sync(w);
+    for (uint64_t j = 0; j < G.n; ++j) labels_out[j] = h[j];
+    *n_clusters = ncl;
+}
+
 }  // namespace
 
 extern "C" {
@@ -82,31 +127,18 @@ sc_status sc_ctx_create(int32_t device, sc_ctx** out) {
     }
     if (device < 0 || device >= count) return SC_E_INVALID_ARGUMENT;
     std::unique_ptr<sc_ctx> ctx(new sc_ctx());
-    sc::Ctx& c = ctx->c;
-    c.device = device;
-    if (cudaSetDevice(device) != cudaSuccess) return SC_E_CUDA;
-    if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
-    if (cudaDeviceGetDefaultMemPool(&c.pool, device) != cudaSuccess) return SC_E_CUDA;
-    uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
-    cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh);
-    if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
-    cudaMemset(c.d_status, 0, sizeof(uint32_t));
-    cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
-    int optin = 0;
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
-    c.smem_optin = (size_t)optin;
+    sc_status st = init_ctx(ctx->c, device);
+    if (st != SC_OK) {
+        release_ctx(ctx->c);
+        return st;
+    }
     *out = ctx.release();
     return SC_OK;
 }
 
 void sc_ctx_destroy(sc_ctx* ctx) {
     if (!ctx) return;
-    cudaSetDevice(ctx->c.device);
-    if (ctx->c.stream) {
-        cudaStreamSynchronize(ctx->c.stream);
-        cudaStreamDestroy(ctx->c.stream);
-    }
-    if (ctx->c.d_status) cudaFree(ctx->c.d_status);
+    release_ctx(ctx->c);
     delete ctx;
 }
 
@@ -394,22 +426,96 @@ sc_status sc_leiden_from(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config*
 sc_status sc_leiden_batch(sc_ctx* ctx, const sc_graph* const* graphs, const sc_leiden_config* cfgs,
                           uint64_t count, const uint64_t* label_offsets, uint64_t* labels_out,
                           uint64_t* n_clusters_out) {
+    return sc_leiden_batch_ex(ctx, graphs, cfgs, count, nullptr, label_offsets, labels_out, n_clusters_out, 0);
+}
+
+sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs, const sc_leiden_config* cfgs,
+                             uint64_t count, const int64_t* warm_from, const uint64_t* label_offsets,
+                             uint64_t* labels_out, uint64_t* n_clusters_out, uint32_t n_streams) {
     return guarded(ctx, [&](sc::Ctx& c) {
         require(count == 0 || (graphs && cfgs && label_offsets && labels_out && n_clusters_out),
                 "batch arrays are NULL");
         for (uint64_t i = 0; i < count; ++i) {
             require(graphs[i] && graphs[i]->g, "a graph of the batch is NULL");
             require_same_device(c, *graphs[i]->g);
-            const sc::DevGraph& G = *graphs[i]->g;
-            sc::DBuf<uint32_t> lab(c, G.n);
-            uint64_t ncl = 0;
-            sc::leiden(c, G, cfgs[i], nullptr, lab.get(), &ncl);
-            std::vector<uint32_t> h(G.n);
-            sc::d2h(c, h.data(), lab.get(), G.n);
-            sc::sync(c);
-            for (uint64_t j = 0; j < G.n; ++j) labels_out[label_offsets[i] + j] = h[j];
-            n_clusters_out[i] = ncl;
+            if (warm_from) {
+                require(warm_from[i] < (int64_t)i, "warm_from must name an earlier instance or -1");
+                if (warm_from[i] >= 0)
+                    require(graphs[warm_from[i]]->g->n == graphs[i]->g->n,
+                            "a warm start needs an instance on a graph with the same node count");
+            }
         }
+        if (count == 0) return;
+        uint32_t W = n_streams ? n_streams : 8u;
+        if (W > count) W = (uint32_t)count;
+        // dependency-ordered work list: instance i is ready once warm_from[i] is done
+        std::mutex mu;
+        std::condition_variable cv;
+        std::vector<char> done(count, 0), taken(count, 0);
+        uint64_t remaining = count;
+        bool failed = false;
+        sc_error_info first_err{};
+        auto worker = [&]() {
+            sc::Ctx w;
+            sc_status st = init_ctx(w, c.device);
+            if (st != SC_OK) {
+                std::lock_guard<std::mutex> lk(mu);
+                if (!failed) {
+                    failed = true;
+                    first_err.code = st;
+                    std::snprintf(first_err.message, sizeof first_err.message, "worker context creation failed");
+                }
+                cv.notify_all();
+                release_ctx(w);
+                return;
+            }
+            for (;;) {
+                uint64_t pick = count;
+                {
+                    std::unique_lock<std::mutex> lk(mu);
+                    for (;;) {
+                        if (failed || remaining == 0) break;
+                        for (uint64_t i = 0; i < count; ++i)
+                            if (!taken[i] && (!warm_from || warm_from[i] < 0 || done[warm_from[i]])) {
+                                pick = i;
+                                break;
+                            }
+                        if (pick < count) {
+                            taken[pick] = 1;
+                            break;
+                        }
+                        bool any_untaken = false;
+                        for (uint64_t i = 0; i < count; ++i) any_untaken |= !taken[i];
+                        if (!any_untaken) break;
+                        cv.wait(lk);
+                    }
+                }
+                if (pick == count) break;
+                try {
+                    const sc::DevGraph& G = *graphs[pick]->g;
+                    const uint64_t* initial = nullptr;
+                    if (warm_from && warm_from[pick] >= 0) initial = labels_out + label_offsets[warm_from[pick]];
+                    run_instance(w, G, cfgs[pick], initial, labels_out + label_offsets[pick], n_clusters_out + pick);
+                } catch (sc::Failure& f) {
+                    std::lock_guard<std::mutex> lk(mu);
+                    if (!failed) {
+                        failed = true;
+                        first_err = f.info;
+                    }
+                }
+                {
+                    std::lock_guard<std::mutex> lk(mu);
+                    done[pick] = 1;
+                    remaining--;
+                }
+                cv.notify_all();
+            }
+            release_ctx(w);
+        };
+        std::vector<std::thread> pool;
+        for (uint32_t t = 0; t < W; ++t) pool.emplace_back(worker);
+        for (auto& th : pool) th.join();
+        if (failed) throw sc::Failure{first_err};
     });
 }
 

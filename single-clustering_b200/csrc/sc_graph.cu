@@ -717,28 +717,53 @@ __global__ void k_iota64(uint64_t* p, uint64_t n) {
         p[i] = i;
 }
 
-// One warp per (g, h) segment: acc in (member asc, neighbour asc) order, the
-// reference's left fold; then the pair rule of csr_network.rs:566-581 and
-// finish's zero drop (:304).
+// The (g, h) segments, 32 per warp: acc in (member asc, neighbour asc) order,
+// the reference's left fold — a lane folds a short segment alone, the warp
+// folds a long one together (warp_fold); then the pair rule of
+// csr_network.rs:566-581 and finish's zero drop (:304).
+__device__ __forceinline__ void seg_emit(uint64_t s, uint64_t b, double acc, const uint64_t* __restrict__ keys,
+                                         uint64_t G, const double* __restrict__ loops, uint32_t* prow,
+                                         uint32_t* pcol, float* pw, uint8_t* keep) {
+    const uint64_t key = keys[b];
+    const uint32_t g = (uint32_t)(key / G), h = (uint32_t)(key % G);
+    float val;
+    if (h == g) val = __double2float_rn(__dmul_rn(0.5, __dadd_rn(acc, loops[g])));
+    else val = __double2float_rn(acc);
+    prow[s] = g;
+    pcol[s] = h;
+    pw[s] = val;
+    keep[s] = (acc > 0.0) && ((double)val != 0.0);
+}
+
 __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
                              const uint64_t* __restrict__ keys, const float* __restrict__ w,
                              uint64_t G, const double* __restrict__ loops, uint32_t* prow,
                              uint32_t* pcol, float* pw, uint8_t* keep, int exact) {
+    constexpr uint64_t SHORT = 64;
+    const unsigned lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t s = warp; s < P; s += nwarps) {
-        const uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
-        const double acc = warp_fold(b, e, 0.0, exact, [&](uint64_t i) { return (double)w[i]; });
-        if ((threadIdx.x & 31) != 0) continue;
-        uint64_t key = keys[b];
-        uint32_t g = (uint32_t)(key / G), h = (uint32_t)(key % G);
-        float val;
-        if (h == g) val = __double2float_rn(__dmul_rn(0.5, __dadd_rn(acc, loops[g])));
-        else val = __double2float_rn(acc);
-        prow[s] = g;
-        pcol[s] = h;
-        pw[s] = val;
-        keep[s] = (acc > 0.0) && ((double)val != 0.0);
+    for (uint64_t base = warp * 32; base < P; base += nwarps * 32) {
+        const uint64_t s = base + lane;
+        uint64_t b = 0, e = 0;
+        if (s < P) {
+            b = seg_start[s];
+            e = s + 1 < P ? seg_start[s + 1] : N;
+        }
+        const bool mine = s < P && e - b <= SHORT;
+        if (mine) {
+            double acc = 0.0;
+            for (uint64_t i = b; i < e; ++i) acc = __dadd_rn(acc, (double)w[i]);
+            seg_emit(s, b, acc, keys, G, loops, prow, pcol, pw, keep);
+        }
+        unsigned long_mask = __ballot_sync(0xFFFFFFFFu, s < P && !mine);
+        while (long_mask) {
+            const int src = __ffs(long_mask) - 1;
+            long_mask &= long_mask - 1;
+            const uint64_t bb = __shfl_sync(0xFFFFFFFFu, b, src), ee = __shfl_sync(0xFFFFFFFFu, e, src);
+            const double acc = warp_fold(bb, ee, 0.0, exact, [&](uint64_t i) { return (double)w[i]; });
+            if ((int)lane == src) seg_emit(s, b, acc, keys, G, loops, prow, pcol, pw, keep);
+        }
     }
 }
 
@@ -863,7 +888,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         pcol.alloc(c, P);
         pw.alloc(c, P);
         keep.alloc(c, P);
-        k_seg_values<<<grid_for(P * 32, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
+        k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
                                                            uw_s.get(), G, loops.get(), prow.get(),
                                                            pcol.get(), pw.get(), keep.get(), (int)g.exact_w);
         SC_LAUNCH_CHECK();

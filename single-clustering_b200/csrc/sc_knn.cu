@@ -37,10 +37,13 @@ namespace {
 
 constexpr int QT = 2;              // query tiles of 128 per CTA group
 constexpr int TILE = 128;          // rows per tile (M and N of the MMA)
-constexpr int STAGES = 6;          // B ring depth
-constexpr int RCAND = 32;          // candidates kept per query before the exact re-rank
-constexpr int NUM_EPI_WARPS = 8;
+constexpr int HALVES = 2;          // each accumulator row is read as two 64-column halves
+constexpr int RCAND = 32;          // candidates kept per (query, half) before the exact re-rank
+constexpr int RTOTAL = RCAND * HALVES;  // candidates per query handed to the re-rank
+constexpr int NUM_EPI_WARPS = 4 * QT * HALVES;  // a full set of 4 TMEM lane quarters per (tile, half)
 constexpr int KNN_THREADS = 32 * (2 + NUM_EPI_WARPS);
+template <int KA>
+constexpr int stages_for() { return KA == 32 ? 6 : 3; }  // B ring depth within 227 KB
 constexpr uint32_t WAIT_LIMIT = 1u << 26;
 constexpr uint32_t TMEM_COLS = 512;
 
@@ -152,7 +155,7 @@ struct Worst {
 };
 
 __device__ __noinline__ Worst cand_insert(float* cs, uint32_t* ci, int qrow, int slot, float v, uint32_t idx) {
-    constexpr int S = QT * TILE;
+    constexpr int S = QT * HALVES * TILE;
     cs[slot * S + qrow] = v;
     ci[slot * S + qrow] = idx;
     Worst w{-INFINITY, 0};
@@ -222,12 +225,14 @@ __global__ void k_knn_prep(const float* __restrict__ X, uint64_t n, uint32_t d, 
 // ------------------------------------------------------------ tensor-core candidate search
 template <int KA>
 struct KnnSmem {
+    static constexpr int STAGES = stages_for<KA>();
     static constexpr uint32_t TILE_BYTES = TILE * KA * 2;
+    static constexpr uint32_t SLOTS = QT * HALVES * TILE;                       // (tile, half, row) owners
     static constexpr uint32_t A_OFF = 0;
     static constexpr uint32_t B_OFF = A_OFF + QT * TILE_BYTES;
     static constexpr uint32_t C_OFF = B_OFF + STAGES * TILE_BYTES;               // candidate scores
-    static constexpr uint32_t I_OFF = C_OFF + RCAND * QT * TILE * 4;              // candidate ids
-    static constexpr uint32_t BAR_OFF = I_OFF + RCAND * QT * TILE * 4;
+    static constexpr uint32_t I_OFF = C_OFF + RCAND * SLOTS * 4;                 // candidate ids
+    static constexpr uint32_t BAR_OFF = I_OFF + RCAND * SLOTS * 4;
     static constexpr uint32_t NBAR = 2 * STAGES + 4 + 2;
     static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR * 8;
     static constexpr uint32_t BYTES = MISC_OFF + 64 + 1024;  // + alignment slack
@@ -244,13 +249,14 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
     unsigned char* sB = smem + L::B_OFF;
     float* cs = (float*)(smem + L::C_OFF);
     uint32_t* ci = (uint32_t*)(smem + L::I_OFF);
+    constexpr int STG = L::STAGES;
     uint64_t* bars = (uint64_t*)(smem + L::BAR_OFF);
-    uint64_t* full = bars;                 // [STAGES] B tile landed
-    uint64_t* empty = bars + STAGES;       // [STAGES] B tile consumed by the MMAs
-    uint64_t* accfull = bars + 2 * STAGES;       // [2] accumulator ready
-    uint64_t* accempty = bars + 2 * STAGES + 2;  // [2] accumulator drained
-    uint64_t* afull = bars + 2 * STAGES + 4;     // query tiles landed
-    uint64_t* aempty = bars + 2 * STAGES + 5;    // query tiles no longer read
+    uint64_t* full = bars;                 // [STG] B tile landed
+    uint64_t* empty = bars + L::STAGES;       // [L::STAGES] B tile consumed by the MMAs
+    uint64_t* accfull = bars + 2 * L::STAGES;       // [2] accumulator ready
+    uint64_t* accempty = bars + 2 * L::STAGES + 2;  // [2] accumulator drained
+    uint64_t* afull = bars + 2 * L::STAGES + 4;     // query tiles landed
+    uint64_t* aempty = bars + 2 * L::STAGES + 5;    // query tiles no longer read
     uint32_t* misc = (uint32_t*)(smem + L::MISC_OFF);
     volatile uint32_t* abort_flag = misc + 1;
 
@@ -259,7 +265,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
     const uint32_t ngroups = (n + QT * TILE - 1) / (QT * TILE);
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < STAGES; ++s) {
+        for (int s = 0; s < L::STAGES; ++s) {
             mbar_init(full + s, 1);
             mbar_init(empty + s, 1);
         }
@@ -299,8 +305,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 for (int q = 0; q < QT; ++q)
                     tma_load_2d(sA + q * L::TILE_BYTES, &tmA, afull, 0, (int)(g * QT * TILE + q * TILE));
                 for (uint32_t t = 0; t < ntiles; ++t, ++it) {
-                    const uint32_t s = (uint32_t)(it % STAGES);
-                    const uint64_t use = it / STAGES;
+                    const uint32_t s = (uint32_t)(it % L::STAGES);
+                    const uint64_t use = it / L::STAGES;
                     if (use > 0 && !mbar_wait(empty + s, (uint32_t)((use - 1) & 1))) {
                         *abort_flag = 1;
                         break;
@@ -313,8 +319,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             // drain: the copies issued last (one per stage, and the query tiles)
             // must land before the CTA exits
             if (*abort_flag) {
-                for (uint64_t x = it > STAGES ? it - STAGES : 0; x < it; ++x)
-                    mbar_wait(full + (x % STAGES), (uint32_t)((x / STAGES) & 1));
+                for (uint64_t x = it > L::STAGES ? it - L::STAGES : 0; x < it; ++x)
+                    mbar_wait(full + (x % L::STAGES), (uint32_t)((x / L::STAGES) & 1));
                 if (a_in_flight && gi > 0) mbar_wait(afull, (gi - 1) & 1);
             }
         }
@@ -331,10 +337,10 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 }
                 fence_after();
                 for (uint32_t t = 0; t < ntiles; ++t, ++it) {
-                    const uint32_t s = (uint32_t)(it % STAGES);
+                    const uint32_t s = (uint32_t)(it % L::STAGES);
                     const uint32_t b = (uint32_t)(it & 1);
                     const uint64_t use_b = it >> 1;
-                    if (!mbar_wait(full + s, (uint32_t)((it / STAGES) & 1))) {
+                    if (!mbar_wait(full + s, (uint32_t)((it / L::STAGES) & 1))) {
                         *abort_flag = 1;
                         break;
                     }
@@ -360,19 +366,23 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             }
         }
     } else {
-        // ---------------- epilogue: 8 warps, warp % 4 selects the TMEM lane quarter
+        // ---------------- epilogue: 16 warps; warp % 4 selects the TMEM lane quarter
+        // (hardware rule), (warp - 2) / 4 the (query tile, column half) it reads
         const int ew = warp - 2;
-        const int q = ew >> 2;                  // query tile
-        const int lq = warp & 3;                // lane quarter (hardware rule)
+        const int combo = ew >> 2;
+        const int q = combo / HALVES;           // query tile
+        const int h = combo % HALVES;           // column half
+        const int lq = warp & 3;                // lane quarter
         const int row = lq * 32 + lane;         // row within the query tile
-        const int qrow = q * TILE + row;        // 0..255 within the group
+        const int owner = combo * TILE + row;   // candidate-buffer column
+        constexpr int S = L::SLOTS;
         uint64_t it = 0;
         for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x) {
             float thr = INFINITY;
             int thr_slot = 0;
-            for (int s = 0; s < RCAND; ++s) {
-                cs[s * (QT * TILE) + qrow] = INFINITY;
-                ci[s * (QT * TILE) + qrow] = 0xFFFFFFFFu;
+            for (int s2 = 0; s2 < RCAND; ++s2) {
+                cs[s2 * S + owner] = INFINITY;
+                ci[s2 * S + owner] = 0xFFFFFFFFu;
             }
             for (uint32_t t = 0; t < ntiles; ++t, ++it) {
                 const uint32_t b = (uint32_t)(it & 1);
@@ -381,26 +391,26 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     break;
                 }
                 fence_after();
-                const uint32_t taddr = tmem + ((uint32_t)(lq * 32) << 16) + b * (QT * TILE) + q * TILE;
+                const uint32_t taddr =
+                    tmem + ((uint32_t)(lq * 32) << 16) + b * (QT * TILE) + q * TILE + h * (TILE / HALVES);
 #pragma unroll 1
-                for (int c0 = 0; c0 < TILE; c0 += 64) {
-                    uint32_t r[64];
-                    tmem_ld64(taddr + c0, r);
-                    // branch-free prefilter: the chunk's minimum against the row's worst kept
-                    float m[32];
+                for (int c0 = 0; c0 < TILE / HALVES; c0 += 32) {
+                    float r[32];
+                    tmem_ld32(taddr + c0, r);
+                    // branch-free prefilter: the chunk's minimum against the worst kept
+                    float m[16];
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) m[j] = fminf(__uint_as_float(r[j]), __uint_as_float(r[j + 32]));
+                    for (int j = 0; j < 16; ++j) m[j] = fminf(r[j], r[j + 16]);
 #pragma unroll
-                    for (int w2 = 16; w2 >= 1; w2 >>= 1)
+                    for (int w2 = 8; w2 >= 1; w2 >>= 1)
 #pragma unroll
                         for (int j = 0; j < w2; ++j) m[j] = fminf(m[j], m[j + w2]);
                     if (m[0] < thr) {
-                        const uint32_t base_idx = t * TILE + c0;
+                        const uint32_t base_idx = t * TILE + h * (TILE / HALVES) + c0;
 #pragma unroll
-                        for (int j = 0; j < 64; ++j) {
-                            const float v = __uint_as_float(r[j]);
-                            if (v < thr && base_idx + j < n) {
-                                const Worst w = cand_insert(cs, ci, qrow, thr_slot, v, base_idx + j);
+                        for (int j = 0; j < 32; ++j) {
+                            if (r[j] < thr && base_idx + j < n) {
+                                const Worst w = cand_insert(cs, ci, owner, thr_slot, r[j], base_idx + j);
                                 thr = w.thr;
                                 thr_slot = w.slot;
                             }
@@ -412,11 +422,11 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 if (lane == 0) mbar_arrive(accempty + b);
             }
             if (*abort_flag) break;
-            const uint64_t qg = (uint64_t)g * QT * TILE + qrow;
+            const uint64_t qg = (uint64_t)g * QT * TILE + q * TILE + row;
             if (qg < n) {
-                for (int s = 0; s < RCAND; ++s) {
-                    cand_score[qg * RCAND + s] = cs[s * (QT * TILE) + qrow];
-                    cand_idx[qg * RCAND + s] = ci[s * (QT * TILE) + qrow];
+                for (int s2 = 0; s2 < RCAND; ++s2) {
+                    cand_score[qg * RTOTAL + h * RCAND + s2] = cs[s2 * S + owner];
+                    cand_idx[qg * RTOTAL + h * RCAND + s2] = ci[s2 * S + owner];
                 }
             }
         }
@@ -432,7 +442,37 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
 }
 
 // ------------------------------------------------------------ exact re-rank
-// One warp per query: lane j owns candidate j (RCAND == 32).
+__device__ __forceinline__ uint64_t rerank_key(const float* __restrict__ X, uint64_t n, uint32_t d, uint64_t q,
+                                               uint32_t j) {
+    if (j >= n) return ~0ull;
+    const float* a = X + q * d;
+    const float* b = X + (uint64_t)j * d;
+    float acc = 0.0f;
+    for (uint32_t t = 0; t < d; ++t) {
+        const float diff = __fsub_rn(a[t], b[t]);
+        acc = __fmaf_rn(diff, diff, acc);
+    }
+    // (distance, self first, index); acc >= 0 so its bits order like the value
+    return ((uint64_t)__float_as_uint(acc) << 32) | (j == (uint32_t)q ? 0u : j + 1u);
+}
+
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t key) {
+    const unsigned lane = threadIdx.x & 31u;
+    for (int size = 2; size <= 32; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, stride);
+            const bool up = ((lane & size) == 0);
+            const bool lower = (lane & stride) == 0;
+            const uint64_t mn = key < other ? key : other, mx = key < other ? other : key;
+            key = (lower == up) ? mn : mx;
+        }
+    }
+    return key;
+}
+
+// One warp per query: exact FP32 distances of its RTOTAL = 64 candidates (two
+// per lane), the 32 smallest kept by a merge-split of two sorted halves, then
+// the first k+1 written.
 __global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d, uint32_t k,
                              const uint32_t* __restrict__ cand_idx, uint32_t* __restrict__ out_idx,
                              float* __restrict__ out_d2) {
@@ -440,34 +480,17 @@ __global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t q = warp; q < n; q += nwarps) {
-        uint32_t j = cand_idx[q * RCAND + lane];
-        uint64_t key = ~0ull;
-        float d2 = INFINITY;
-        if (j < n) {
-            const float* a = X + q * d;
-            const float* b = X + (uint64_t)j * d;
-            float acc = 0.0f;
-            for (uint32_t t = 0; t < d; ++t) {
-                float diff = __fsub_rn(a[t], b[t]);
-                acc = __fmaf_rn(diff, diff, acc);
-            }
-            d2 = acc;
-            // (distance, self first, index); d2 >= 0 so its bits order like the value
-            key = ((uint64_t)__float_as_uint(d2) << 32) | (j == (uint32_t)q ? 0u : j + 1u);
-        }
-        // bitonic sort of 32 keys across the warp, ascending
-        for (int size = 2; size <= 32; size <<= 1) {
-            for (int stride = size >> 1; stride > 0; stride >>= 1) {
-                uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, stride);
-                bool up = ((lane & size) == 0);
-                bool lower = (lane & stride) == 0;
-                uint64_t mn = key < other ? key : other, mx = key < other ? other : key;
-                key = (lower == up) ? mn : mx;
-            }
+        uint64_t ka = warp_sort32(rerank_key(X, n, d, q, cand_idx[q * RTOTAL + lane]));
+        uint64_t kb = warp_sort32(rerank_key(X, n, d, q, cand_idx[q * RTOTAL + 32 + lane]));
+        const uint64_t kbr = __shfl_sync(0xFFFFFFFFu, kb, 31 - lane);
+        uint64_t key = ka < kbr ? ka : kbr;  // the 32 smallest, as a bitonic sequence
+        for (int stride = 16; stride > 0; stride >>= 1) {
+            const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, key, stride);
+            key = (lane & stride) == 0 ? (key < other ? key : other) : (key < other ? other : key);
         }
         if (lane <= k) {
-            uint32_t tag = (uint32_t)key;
-            uint32_t idx = (key == ~0ull) ? 0xFFFFFFFFu : (tag == 0 ? (uint32_t)q : tag - 1u);
+            const uint32_t tag = (uint32_t)key;
+            const uint32_t idx = (key == ~0ull) ? 0xFFFFFFFFu : (tag == 0 ? (uint32_t)q : tag - 1u);
             out_idx[q * (k + 1) + lane] = idx;
             out_d2[q * (k + 1) + lane] = key == ~0ull ? INFINITY : __uint_as_float((uint32_t)(key >> 32));
         }
@@ -610,19 +633,20 @@ void candidates(Ctx& c, const float* dX, uint64_t n, uint32_t d, float* cand_sco
 }  // namespace
 
 // knn_arrayd_* (neighborhood/mod.rs:51-202, :359-578) with exact (brute-force)
-// search. The search keeps RCAND = 32 candidates per query from the BF16
-// tensor-core scores, then ranks them exactly in FP32.
+// search. The search keeps 64 candidates per query (the 32 best of each half
+// of the candidate columns) from the BF16 tensor-core scores, then ranks them
+// exactly in FP32.
 void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
                   uint32_t* knn_index, float* knn_dist, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
                   uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
     if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
-    if (k + 1 > (uint64_t)RCAND) fail(SC_E_UNSUPPORTED, "kNN supports k <= %d", RCAND - 1);
+    if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
     if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
     if (opts.precision != SC_KNN_BF16) fail(SC_E_UNSUPPORTED, "only the BF16 contraction is built");
     DBuf<float> dX(c, n * d);
     h2d(c, dX.get(), X, n * d);
-    DBuf<float> cscore(c, n * RCAND);
-    DBuf<uint32_t> cidx(c, n * RCAND);
+    DBuf<float> cscore(c, n * RTOTAL);
+    DBuf<uint32_t> cidx(c, n * RTOTAL);
     if (n) {
         if (d <= 30) candidates<32>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());
         else candidates<64>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());

@@ -680,12 +680,16 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
 // in a different community from them (local_move.rs:113-118). Runs after the
 // commit, so every membership it reads is final.
 __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t count, uint8_t* next_active) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
-         i += (uint64_t)gridDim.x * blockDim.x) {
+    // one warp per node of the batch, lanes over its row (coalesced)
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < count; i += nwarps) {
         const uint32_t v = list[i];
         if (p.moved[v] != p.cur) continue;
         const uint32_t t = p.memb[v];
-        for (uint64_t j = p.ptr[v]; j < p.ptr[v + 1]; ++j) {
+        const uint64_t e = p.ptr[v + 1];
+        for (uint64_t j = p.ptr[v] + lane; j < e; j += 32) {
             const uint32_t u = p.nbr[j];
             if (u != v && p.memb[u] != t) next_active[u] = 1;
         }
@@ -1021,8 +1025,8 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             }
             k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
                                                                        ws.next_active.get());
-            k_activate<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
-                                                                   ws.next_active.get());
+            k_activate<<<grid_for((uint64_t)(hi - lo) * 32, TB, 148u * 64u), TB, 0, c.stream>>>(
+                p, ws.list.get() + lo, hi - lo, ws.next_active.get());
             SC_LAUNCH_CHECK();
             c.launches += 2;
         }

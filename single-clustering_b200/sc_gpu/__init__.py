@@ -445,8 +445,12 @@ def leiden_from(graph: CSRNetwork, config: LeidenConfig | None, initial) -> Clus
     return Clustering(labels, ncl.value)
 
 
-def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig]) -> list:
-    """Many leiden() runs in one call (resolution x seed sweeps, many graphs)."""
+def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig], warm_from=None,
+                 n_streams: int = 0) -> list:
+    """Many leiden() runs in one call, concurrently on `n_streams` worker streams.
+
+    warm_from[i] = j (j < i) starts instance i from instance j's labels (leiden
+    with `initial`); -1 starts from singletons."""
     count = len(graphs)
     if count == 0:
         return []
@@ -458,13 +462,45 @@ def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig]) 
     ncl = np.zeros(count, np.uint64)
     harr = (C.c_void_p * count)(*[g._h for g in graphs])
     carr = (_lib.LeidenConfigC * count)(*[c.to_c() for c in configs])
-    _check(lib().sc_leiden_batch(ctx.h, harr, carr, count, _ptr(offs, _lib.u64p), _ptr(labels, _lib.u64p),
-                                 _ptr(ncl, _lib.u64p)), ctx)
+    wf = None
+    if warm_from is not None:
+        wf = np.ascontiguousarray(warm_from, dtype=np.int64)
+    _check(lib().sc_leiden_batch_ex(ctx.h, harr, carr, count,
+                                    None if wf is None else wf.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    _ptr(offs, _lib.u64p), _ptr(labels, _lib.u64p), _ptr(ncl, _lib.u64p),
+                                    int(n_streams)), ctx)
     out = []
     for i in range(count):
-        s = int(offs[i])
-        out.append(Clustering(labels[s:s + sizes[i]].copy(), int(ncl[i])))
+        s0 = int(offs[i])
+        out.append(Clustering(labels[s0:s0 + sizes[i]].copy(), int(ncl[i])))
     return out
+
+
+def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb, warm_start: bool = True,
+               base: LeidenConfig | None = None):
+    """Configs and warm-start links of a resolution x seed sweep.
+
+    Instances are ordered seed-major with resolutions descending; with warm_start
+    each instance starts from the previous (finer) resolution's result of the
+    same seed, so a chain coarsens a partition instead of rebuilding it."""
+    base = base or LeidenConfig()
+    res = sorted(resolutions, reverse=True)
+    configs, warm, keys = [], [], []
+    for s in seeds:
+        for j, r in enumerate(res):
+            cfg = LeidenConfig(**{**base.__dict__, "objective": objective(r), "seed": int(s)})
+            configs.append(cfg)
+            warm.append(len(configs) - 2 if (warm_start and j > 0) else -1)
+            keys.append((float(r), int(s)))
+    return configs, warm, keys
+
+
+def leiden_sweep(graph: CSRNetwork, resolutions, seeds, objective=Rb, warm_start: bool = True,
+                 n_streams: int = 0, base: LeidenConfig | None = None) -> dict:
+    """Resolution x seed sweep on one graph: {(resolution, seed): Clustering}."""
+    configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base)
+    res = leiden_batch([graph] * len(configs), configs, warm if warm_start else None, n_streams)
+    return dict(zip(keys, res))
 
 
 def modularity(graph: CSRNetwork, labels, resolution: float = 1.0) -> float:
@@ -495,7 +531,7 @@ __all__ = [
     "leiden_batch", "modularity", "quality", "ClusteringError", "NodeIndexOutOfRange", "NonFiniteWeight",
     "NegativeWeight", "InvalidNodeWeight", "NodeWeightLengthMismatch", "MembershipLengthMismatch",
     "InvalidConfig", "TooManyNodes", "InvalidCsr", "AsymmetricGraph", "DeviceError", "MAX_NODES", "NOISE",
-    "last_run_stats", "context",
+    "last_run_stats", "context", "sweep_plan", "leiden_sweep",
 ]
 
 

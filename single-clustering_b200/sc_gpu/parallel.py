@@ -1,0 +1,68 @@
+"""Multi-GPU sharding of independent Leiden instances.
+
+A single graph does not shard (every move reads global community statistics),
+so one graph runs as replicas. A resolution x seed sweep or a set of many
+graphs is made of independent units: whole warm-start chains (or single
+instances) are dealt to ranks by estimated cost, each rank runs its share on
+its own GPU with `leiden_batch`, and the labels are gathered with one
+all-gather of Python objects over the process group (NCCL over NVLink between
+GPUs, gloo on CPU). No collective runs inside a Leiden run.
+"""
+from __future__ import annotations
+
+from typing import Callable, Sequence
+
+
+def chains(warm_from: Sequence[int]) -> list:
+    """Instance ids grouped into warm-start chains (a chain never splits)."""
+    owner = {}
+    out = []
+    for i, j in enumerate(warm_from):
+        if j is None or j < 0:
+            owner[i] = len(out)
+            out.append([i])
+        else:
+            owner[i] = owner[j]
+            out[owner[j]].append(i)
+    return out
+
+
+def deal(costs: Sequence[float], world: int) -> list:
+    """Longest-processing-time-first assignment of units to `world` ranks:
+    the costliest unit goes to the least loaded rank, ties to the lower rank."""
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for u in sorted(range(len(costs)), key=lambda u: (-costs[u], u)):
+        r = min(range(world), key=lambda r: (load[r], r))
+        parts[r].append(u)
+        load[r] += costs[u]
+    return [sorted(p) for p in parts]
+
+
+def shard(warm_from: Sequence[int], instance_cost: Sequence[float], world: int) -> list:
+    """Instance ids per rank: chains dealt whole by their summed cost."""
+    ch = chains(warm_from)
+    parts = deal([sum(instance_cost[i] for i in c) for c in ch], world)
+    return [sorted(i for u in p for i in ch[u]) for p in parts]
+
+
+def run_sharded(run_local: Callable, n_instances: int, warm_from: Sequence[int],
+                instance_cost: Sequence[float], rank: int, world: int, group=None) -> list:
+    """Runs this rank's instances with run_local(ids, local_warm_from) -> list of
+    results (in ids order) and gathers every rank's results: returns the results
+    of all n_instances in instance order on every rank."""
+    mine = shard(warm_from, instance_cost, world)[rank]
+    pos = {g: k for k, g in enumerate(mine)}
+    local_warm = [pos[warm_from[g]] if warm_from[g] >= 0 else -1 for g in mine]
+    local = run_local(mine, local_warm)
+    if world == 1:
+        gathered = [(mine, local)]
+    else:
+        import torch.distributed as dist
+        gathered = [None] * world
+        dist.all_gather_object(gathered, (mine, local), group=group)
+    out = [None] * n_instances
+    for ids, res in gathered:
+        for g, r in zip(ids, res):
+            out[g] = r
+    return out
