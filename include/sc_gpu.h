@@ -306,6 +306,52 @@ sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, u
                           uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
                           uint64_t conn_capacity, uint64_t* conn_nnz, sc_graph** graph_out);
 
+/* ---------------------------------------------------------------- learned warm start
+ * No counterpart in single-clustering: its only warm-start hook is the
+ * `initial` membership of run_once (src/community_search/leiden/mod.rs:207-220),
+ * which sc_leiden_from exposes. These functions produce such a membership.
+ *
+ * The model is a 2-layer MLP (sc_mlp_feature_count() inputs, 128 hidden units,
+ * ReLU, one logit) scoring each undirected edge with the probability that its
+ * endpoints share a community, from endpoint degree/strength, the edge weight,
+ * the RB null-model term at the given resolution and the endpoints' common
+ * neighbourhood. Forward passes use BF16 weights with FP32 accumulation; Adam
+ * updates an FP32 master copy. Parameters are laid out W1[f*128+u], b1[u],
+ * w2[u], b2 (sc_mlp_param_count() floats). The feature scaler (means, then
+ * inverse standard deviations, 2 * feature_count floats) is fitted on the first
+ * graph the model trains on or extracts features from.
+ *
+ * The proposal is the connected components of the edges whose probability
+ * exceeds `threshold`, numbered 0..k-1 by smallest member; pass it to
+ * sc_leiden_from as `initial`.
+ */
+typedef struct sc_mlp sc_mlp;
+
+uint32_t sc_mlp_param_count(void);
+uint32_t sc_mlp_feature_count(void);
+sc_status sc_mlp_create(sc_ctx* ctx, uint64_t seed, sc_mlp** out);
+void sc_mlp_destroy(sc_mlp* m);
+/* Copies the parameters and/or the scaler (either may be NULL) to host;
+ * *has_scaler (nullable) says whether a scaler is set. */
+sc_status sc_mlp_get(sc_ctx* ctx, const sc_mlp* m, float* params, float* scaler, int32_t* has_scaler);
+/* Replaces the parameters (resets the Adam state) and/or the scaler. */
+sc_status sc_mlp_set(sc_ctx* ctx, sc_mlp* m, const float* params, const float* scaler);
+/* The scaled edge features the model sees for g at `resolution`, edges (i < j)
+ * in ascending (i, j) order: feat[e * feature_count + f], endpoints ei/ej (each
+ * nullable). `capacity` is the room in edges; *n_edges receives the count. */
+sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, float* feat,
+                          uint32_t* ei, uint32_t* ej, uint64_t capacity, uint64_t* n_edges);
+/* `epochs` full-batch Adam steps (learning rate lr) of the mean binary
+ * cross-entropy against "same community in `membership`". *loss_out receives the
+ * loss before the last step; grad_out (nullable, param_count floats) the last
+ * gradient. epochs == 0 evaluates loss and gradient without a step. */
+sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
+                       double resolution, uint32_t epochs, double lr, double* loss_out, float* grad_out);
+/* Initial membership for sc_leiden_from (see above); prob_out (nullable) gets
+ * the edge probabilities in sc_mlp_features order, prob_capacity entries. */
+sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
+                         uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity);
+
 #ifdef __cplusplus
 }
 #endif

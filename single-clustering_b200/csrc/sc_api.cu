@@ -15,6 +15,10 @@ struct sc_ctx {
 struct sc_graph {
     sc::DevGraph* g = nullptr;
 };
+struct sc_mlp {
+    sc::Mlp* m = nullptr;
+    int device = 0;
+};
 
 namespace {
 
@@ -541,6 +545,100 @@ sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, u
         sc::knn_gaussian(c, X, n, d, k, o, knn_index, knn_dist, conn_ptrs, conn_nbrs, conn_w, conn_capacity,
                          conn_nnz, graph_out ? &g : nullptr);
         if (graph_out) *graph_out = new sc_graph{g};
+    });
+}
+
+// ---------------------------------------------------------------- learned warm start
+uint32_t sc_mlp_param_count(void) { return sc::mlp_param_count(); }
+
+uint32_t sc_mlp_feature_count(void) { return sc::mlp_feature_count(); }
+
+sc_status sc_mlp_create(sc_ctx* ctx, uint64_t seed, sc_mlp** out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(out, "out is NULL");
+        *out = nullptr;
+        sc::Mlp* m = sc::mlp_create(c, seed);
+        *out = new sc_mlp{m, c.device};
+    });
+}
+
+void sc_mlp_destroy(sc_mlp* m) {
+    if (!m) return;
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaSetDevice(m->device);
+    sc::mlp_destroy(m->m);
+    cudaSetDevice(prev);
+    delete m;
+}
+
+sc_status sc_mlp_get(sc_ctx* ctx, const sc_mlp* m, float* params, float* scaler, int32_t* has_scaler) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(m && m->m, "model is NULL");
+        if (m->device != c.device) bad_arg("model lives on another device than the context");
+        const bool has = sc::mlp_get(c, *m->m, params, scaler);
+        if (has_scaler) *has_scaler = has ? 1 : 0;
+    });
+}
+
+sc_status sc_mlp_set(sc_ctx* ctx, sc_mlp* m, const float* params, const float* scaler) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(m && m->m, "model is NULL");
+        if (m->device != c.device) bad_arg("model lives on another device than the context");
+        sc::mlp_set(c, *m->m, params, scaler);
+    });
+}
+
+sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, float* feat,
+                          uint32_t* ei, uint32_t* ej, uint64_t capacity, uint64_t* n_edges) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(m && m->m && g && g->g && n_edges, "model, graph or n_edges is NULL");
+        if (m->device != c.device) bad_arg("model lives on another device than the context");
+        require_same_device(c, *g->g);
+        require(resolution > 0.0 && std::isfinite(resolution), "resolution must be positive and finite");
+        sc::mlp_features(c, *m->m, *g->g, resolution, feat, ei, ej, capacity, n_edges);
+    });
+}
+
+sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
+                       double resolution, uint32_t epochs, double lr, double* loss_out, float* grad_out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(m && m->m && g && g->g, "model or graph is NULL");
+        if (m->device != c.device) bad_arg("model lives on another device than the context");
+        require_same_device(c, *g->g);
+        require(resolution > 0.0 && std::isfinite(resolution), "resolution must be positive and finite");
+        require(lr >= 0.0 && std::isfinite(lr), "learning rate must be non-negative and finite");
+        const sc::DevGraph& G = *g->g;
+        require(membership || G.n == 0, "membership is NULL");
+        check_membership_len(n_membership, G.n);
+        sc::DBuf<uint64_t> dl(c, G.n);
+        sc::DBuf<uint32_t> ids(c, G.n);
+        sc::h2d(c, dl.get(), membership, G.n);
+        if (G.n) sc::renumber_u64_labels(c, dl.get(), G.n, ids.get(), nullptr);
+        const double loss = sc::mlp_train(c, *m->m, G, ids.get(), resolution, epochs, lr, grad_out);
+        if (loss_out) *loss_out = loss;
+    });
+}
+
+sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
+                         uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(m && m->m && g && g->g && n_clusters_out, "model, graph or n_clusters_out is NULL");
+        if (m->device != c.device) bad_arg("model lives on another device than the context");
+        require_same_device(c, *g->g);
+        require(resolution > 0.0 && std::isfinite(resolution), "resolution must be positive and finite");
+        require(std::isfinite(threshold), "threshold must be finite");
+        const sc::DevGraph& G = *g->g;
+        require(labels_out || G.n == 0, "labels_out is NULL");
+        sc::DBuf<uint32_t> lab(c, G.n);
+        const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, threshold, lab.get(), prob_out, prob_capacity);
+        if (G.n) {
+            std::vector<uint32_t> h(G.n);
+            sc::d2h(c, h.data(), lab.get(), G.n);
+            sc::sync(c);
+            for (uint64_t i = 0; i < G.n; ++i) labels_out[i] = h[i];
+        }
+        *n_clusters_out = k;
     });
 }
 

@@ -254,6 +254,21 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k,
                   uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w, uint64_t conn_cap,
                   uint64_t* conn_nnz, DevGraph** graph_out);
 
+// mlp.cu: learned warm start (edge MLP; proposal = components of confident edges)
+struct Mlp;
+Mlp* mlp_create(Ctx& c, uint64_t seed);
+void mlp_destroy(Mlp* m);
+uint32_t mlp_param_count();
+uint32_t mlp_feature_count();
+bool mlp_get(Ctx& c, const Mlp& m, float* params, float* scaler);  // returns whether a scaler is set
+void mlp_set(Ctx& c, Mlp& m, const float* params, const float* scaler);
+void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_host, uint32_t* ei_host,
+                  uint32_t* ej_host, uint64_t cap, uint64_t* M_out);
+double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, uint32_t epochs,
+                 double lr, float* grad_out_host);
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, uint32_t* d_labels,
+                     float* prob_host, uint64_t prob_cap);
+
 // common.cu
 void check_device_status(Ctx& c);
 // Rust-style shortest round-trip text of an f64 (Display of f64).

@@ -1,0 +1,573 @@
+// sc_mlp.cu — learned warm start for Leiden: an edge MLP proposes an initial
+// membership that leiden_from then refines.
+//
+// Community ids are arbitrary (any permutation of a partition is the same
+// partition), so the network does not classify nodes into ids: it scores each
+// undirected edge (i, j) from the features of its two endpoints and their
+// shared neighbourhood, F = 10 of them,
+//   w, log1p(k_i) + log1p(k_j), |log1p(k_i) - log1p(k_j)|, log(d_i) + log(d_j),
+//   |log d_i - log d_j|, w/k_i + w/k_j, log(gamma), gamma k_i k_j / (2 m w),
+//   sum_c min(w_ic, w_jc) / min(k_i, k_j), |N(i) & N(j)| / min(d_i, d_j)
+// (w edge weight, k strength, d degree, gamma the RB resolution; the 8th is the
+// configuration-model null term relative to the edge, the quantity local moving
+// weighs; the last two compare the endpoints' neighbour histograms, c over the
+// common neighbours other than i and j) and outputs the logit that i and j
+// share a community:
+//   h = relu(x W1 + b1) (hidden H), z = h . w2 + b2.
+// Weights are BF16 in the forward pass with FP32 accumulation; an FP32 master
+// copy is updated by Adam. Training labels are partitions plain Leiden found;
+// the proposal is the connected components of the edges with p > threshold.
+//
+// Kernels: one warp per edge stream, lane l owns hidden units l, l+32, ...;
+// gradients accumulate in registers, then per block in shared memory, then in
+// a fixed-order reduction over blocks (deterministic).
+#include <cuda_bf16.h>
+
+#include "sc_prims.cuh"
+
+namespace sc {
+
+constexpr int MLP_F = 10;
+constexpr int MLP_H = 128;
+constexpr int MLP_UPL = MLP_H / 32;  // hidden units per lane
+constexpr int MLP_NPARAM = MLP_F * MLP_H + MLP_H + MLP_H + 1;  // W1, b1, w2, b2
+
+struct Mlp {
+    int device = 0;
+    float* master = nullptr;  // MLP_NPARAM, FP32
+    float* m = nullptr;       // Adam first moment
+    float* v = nullptr;       // Adam second moment
+    float* norm = nullptr;    // 2 MLP_F: feature means, then inverse standard deviations
+    bool has_norm = false;
+    uint64_t step = 0;
+};
+
+namespace {
+
+constexpr unsigned TB = 256;
+constexpr int MLP_BLOCKS = 148 * 4;
+
+// Σ_c min(w_ic, w_jc) and the count over common neighbours c ∉ {i, j}: walk the
+// shorter row and binary-search the longer (rows are strictly increasing), so a
+// hub endpoint costs O(d_small log d_large).
+__device__ void common_neighbours(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                  const float* __restrict__ w, uint32_t i, uint32_t j, double& wsum,
+                                  uint32_t& count) {
+    uint64_t a0 = ptr[i], a1 = ptr[i + 1], b0 = ptr[j], b1 = ptr[j + 1];
+    if (a1 - a0 > b1 - b0) {
+        uint64_t t = a0; a0 = b0; b0 = t;
+        t = a1; a1 = b1; b1 = t;
+    }
+    wsum = 0.0;
+    count = 0;
+    for (uint64_t x = a0; x < a1; ++x) {
+        const uint32_t c = nbr[x];
+        if (c == i || c == j) continue;
+        uint64_t lo = b0, hi = b1;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (nbr[mid] < c) lo = mid + 1;
+            else hi = mid;
+        }
+        if (lo < b1 && nbr[lo] == c) {
+            wsum += (double)fminf(w[x], w[lo]);
+            ++count;
+        }
+    }
+}
+
+// Features of the undirected edges (stored entries with row < neighbour).
+__global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
+                                const double* __restrict__ strength, double two_m, double gamma, float* feat,
+                                uint32_t* ei, uint32_t* ej, unsigned long long* count) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t i = erow[e], j = nbr[e];
+        if (!(i < j)) continue;
+        const unsigned long long pos = atomicAdd(count, 1ull);
+        const double wij = (double)w[e];
+        const double ki = strength[i], kj = strength[j];
+        const double di = (double)(ptr[i + 1] - ptr[i]), dj = (double)(ptr[j + 1] - ptr[j]);
+        const double lki = log1p(ki), lkj = log1p(kj), ldi = log(di), ldj = log(dj);
+        double cw;
+        uint32_t cn;
+        common_neighbours(ptr, nbr, w, i, j, cw, cn);
+        float* f = feat + pos * MLP_F;
+        f[0] = (float)wij;
+        f[1] = (float)(lki + lkj);
+        f[2] = (float)fabs(lki - lkj);
+        f[3] = (float)(ldi + ldj);
+        f[4] = (float)fabs(ldi - ldj);
+        f[5] = (float)(wij / fmax(ki, 1e-300) + wij / fmax(kj, 1e-300));
+        f[6] = (float)log(gamma);
+        f[7] = (float)(two_m > 0.0 ? gamma * ki * kj / (two_m * fmax(wij, 1e-300)) : 0.0);
+        f[8] = (float)(cw / fmax(fmin(ki, kj), 1e-300));
+        f[9] = (float)((double)cn / fmax(fmin(di, dj), 1.0));
+        ei[pos] = i;
+        ej[pos] = j;
+    }
+}
+
+// Edges are written in atomic order above; sort by (i, j) so the edge stream
+// (and with it every fixed-order reduction) is the same on every run.
+__global__ void k_edge_keys(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej, uint64_t M,
+                            uint64_t* keys, uint32_t* idx) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        keys[e] = ((uint64_t)ei[e] << 32) | ej[e];
+        idx[e] = (uint32_t)e;
+    }
+}
+
+__global__ void k_gather_edges(const uint32_t* __restrict__ order, uint64_t M, const float* __restrict__ feat,
+                               const uint64_t* __restrict__ keys_sorted, float* feat_out, uint32_t* ei,
+                               uint32_t* ej) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t src = order[e];
+        for (int f = 0; f < MLP_F; ++f) feat_out[e * MLP_F + f] = feat[(uint64_t)src * MLP_F + f];
+        ei[e] = (uint32_t)(keys_sorted[e] >> 32);
+        ej[e] = (uint32_t)keys_sorted[e];
+    }
+}
+
+// Per-feature mean / inverse std over the edges (fixed-order block partials).
+// The scaler is fitted once, on the first graph a model trains on, and is part
+// of the model from then on: a feature that is constant within one graph (the
+// resolution) keeps its value across graphs instead of standardising to zero.
+constexpr int MLP_GAMMA_FEATURE = 6;
+
+__global__ void k_feat_partials(const float* __restrict__ feat, uint64_t M, double* partial) {
+    __shared__ double s[2 * MLP_F][TB / 32];
+    double acc[2 * MLP_F] = {};
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x)
+        for (int f = 0; f < MLP_F; ++f) {
+            const double x = feat[e * MLP_F + f];
+            acc[f] += x;
+            acc[MLP_F + f] += x * x;
+        }
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int f = 0; f < 2 * MLP_F; ++f) {
+        double x = acc[f];
+        for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
+        if (lane == 0) s[f][wid] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < 2 * MLP_F) {
+        double x = 0.0;
+        for (int k = 0; k < (int)(blockDim.x / 32); ++k) x += s[threadIdx.x][k];
+        partial[blockIdx.x * 2 * MLP_F + threadIdx.x] = x;
+    }
+}
+
+__global__ void k_feat_finalize(const double* __restrict__ partial, int nblocks, uint64_t M, float* norm) {
+    if (threadIdx.x >= MLP_F) return;
+    double s = 0.0, s2 = 0.0;
+    for (int b = 0; b < nblocks; ++b) {
+        s += partial[b * 2 * MLP_F + threadIdx.x];
+        s2 += partial[b * 2 * MLP_F + MLP_F + threadIdx.x];
+    }
+    const double mean = M ? s / (double)M : 0.0;
+    const double var = M ? fmax(s2 / (double)M - mean * mean, 0.0) : 0.0;
+    if (threadIdx.x == MLP_GAMMA_FEATURE) {  // log(gamma): passed through unscaled
+        norm[threadIdx.x] = 0.0f;
+        norm[MLP_F + threadIdx.x] = 1.0f;
+        return;
+    }
+    norm[threadIdx.x] = (float)mean;
+    norm[MLP_F + threadIdx.x] = (float)(var > 1e-12 ? 1.0 / sqrt(var) : 1.0);
+}
+
+__global__ void k_normalize(float* feat, uint64_t M, const float* __restrict__ norm) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < M * MLP_F;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const int f = (int)(i % MLP_F);
+        feat[i] = (feat[i] - norm[f]) * norm[MLP_F + f];
+    }
+}
+
+
+__global__ void k_to_bf16(const float* __restrict__ master, __nv_bfloat16* out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NPARAM; i += gridDim.x * blockDim.x)
+        out[i] = __float2bfloat16_rn(master[i]);
+}
+
+// Forward (and with GRAD, backward) over the edge stream. Parameter layout:
+// W1[f * H + u], b1[u], w2[u], b2. Lane l owns units l + 32 t, t < 4.
+template <bool GRAD>
+__global__ void __launch_bounds__(TB) k_mlp(const float* __restrict__ feat, const uint8_t* __restrict__ label,
+                                            uint64_t M, const __nv_bfloat16* __restrict__ wb, float* __restrict__ out_p,
+                                            float* __restrict__ partial_grad, double* __restrict__ partial_loss) {
+    __shared__ float sW1[MLP_F * MLP_H], sb1[MLP_H], sw2[MLP_H];
+    __shared__ float sb2;
+    for (int i = threadIdx.x; i < MLP_F * MLP_H; i += blockDim.x) sW1[i] = __bfloat162float(wb[i]);
+    for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+        sb1[i] = __bfloat162float(wb[MLP_F * MLP_H + i]);
+        sw2[i] = __bfloat162float(wb[MLP_F * MLP_H + MLP_H + i]);
+    }
+    if (threadIdx.x == 0) sb2 = __bfloat162float(wb[MLP_F * MLP_H + 2 * MLP_H]);
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    float gW1[MLP_F][MLP_UPL] = {}, gb1[MLP_UPL] = {}, gw2[MLP_UPL] = {};
+    float gb2 = 0.0f;
+    double loss = 0.0;
+    for (uint64_t e = warp; e < M; e += nwarps) {
+        float x[MLP_F];
+#pragma unroll
+        for (int f = 0; f < MLP_F; ++f) x[f] = feat[e * MLP_F + f];
+        float h[MLP_UPL];
+        float zpart = 0.0f;
+#pragma unroll
+        for (int t = 0; t < MLP_UPL; ++t) {
+            const int u = lane + 32 * t;
+            float a = sb1[u];
+#pragma unroll
+            for (int f = 0; f < MLP_F; ++f) a = __fmaf_rn(x[f], sW1[f * MLP_H + u], a);
+            h[t] = fmaxf(a, 0.0f);
+            zpart = __fmaf_rn(h[t], sw2[u], zpart);
+        }
+        for (int o = 16; o; o >>= 1) zpart += __shfl_xor_sync(0xFFFFFFFFu, zpart, o);
+        const float z = zpart + sb2;
+        const float p = 1.0f / (1.0f + expf(-z));
+        if (!GRAD) {
+            if (lane == 0) out_p[e] = p;
+            continue;
+        }
+        const float y = label[e] ? 1.0f : 0.0f;
+        // BCE with logits, numerically stable: max(z,0) - z y + log(1 + e^-|z|)
+        if (lane == 0) loss += (double)(fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z))));
+        const float dz = p - y;
+        gb2 += dz;
+#pragma unroll
+        for (int t = 0; t < MLP_UPL; ++t) {
+            const int u = lane + 32 * t;
+            gw2[t] = __fmaf_rn(h[t], dz, gw2[t]);
+            const float dh = h[t] > 0.0f ? dz * sw2[u] : 0.0f;
+            gb1[t] += dh;
+#pragma unroll
+            for (int f = 0; f < MLP_F; ++f) gW1[f][t] = __fmaf_rn(x[f], dh, gW1[f][t]);
+        }
+    }
+    if (!GRAD) return;
+    // block reduction in shared memory: warps add in index order (deterministic)
+    __shared__ float sg[MLP_NPARAM];
+    __shared__ double sl;
+    const int wid = threadIdx.x >> 5;
+    for (int k = 0; k < (int)(blockDim.x / 32); ++k) {
+        if (wid == k) {
+            const bool first = k == 0;
+#pragma unroll
+            for (int t = 0; t < MLP_UPL; ++t) {
+                const int u = lane + 32 * t;
+#pragma unroll
+                for (int f = 0; f < MLP_F; ++f)
+                    sg[f * MLP_H + u] = first ? gW1[f][t] : sg[f * MLP_H + u] + gW1[f][t];
+                sg[MLP_F * MLP_H + u] = first ? gb1[t] : sg[MLP_F * MLP_H + u] + gb1[t];
+                sg[MLP_F * MLP_H + MLP_H + u] = first ? gw2[t] : sg[MLP_F * MLP_H + MLP_H + u] + gw2[t];
+            }
+            if (lane == 0) {
+                sg[MLP_NPARAM - 1] = first ? gb2 : sg[MLP_NPARAM - 1] + gb2;
+                sl = first ? loss : sl + loss;
+            }
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) partial_grad[(uint64_t)blockIdx.x * MLP_NPARAM + i] = sg[i];
+    if (threadIdx.x == 0) partial_loss[blockIdx.x] = sl;
+}
+
+__global__ void k_grad_reduce(const float* __restrict__ partial, const double* __restrict__ partial_loss, int nblocks,
+                              uint64_t M, float* grad, double* loss) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NPARAM; i += gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < nblocks; ++b) acc += partial[(uint64_t)b * MLP_NPARAM + i];
+        grad[i] = M ? (float)(acc / (double)M) : 0.0f;  // mean over edges
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        double acc = 0.0;
+        for (int b = 0; b < nblocks; ++b) acc += partial_loss[b];
+        *loss = M ? acc / (double)M : 0.0;
+    }
+}
+
+__global__ void k_adam(float* master, float* m, float* v, const float* __restrict__ grad, float lr, float b1, float b2,
+                       float eps, float bc1, float bc2) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NPARAM; i += gridDim.x * blockDim.x) {
+        const float g = grad[i];
+        m[i] = b1 * m[i] + (1.0f - b1) * g;
+        v[i] = b2 * v[i] + (1.0f - b2) * g * g;
+        master[i] -= lr * (m[i] / bc1) / (sqrtf(v[i] / bc2) + eps);
+    }
+}
+
+__global__ void k_edge_labels(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej, uint64_t M,
+                              const uint32_t* __restrict__ memb, uint8_t* label) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x)
+        label[e] = memb[ei[e]] == memb[ej[e]];
+}
+
+// Connected components of the confident edges: min-label hooking + pointer jumping.
+__global__ void k_cc_hook(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej,
+                          const float* __restrict__ p, uint64_t M, float thr, uint32_t* lab, int* changed) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        if (!(p[e] > thr)) continue;
+        const uint32_t a = lab[ei[e]], b = lab[ej[e]];
+        if (a == b) continue;
+        const uint32_t lo = min(a, b), hi = max(a, b);
+        if (atomicMin(lab + hi, lo) > lo) *changed = 1;
+    }
+}
+
+__global__ void k_cc_jump(uint32_t* lab, uint64_t n, int* changed) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x) {
+        uint32_t l = lab[v];
+        const uint32_t ll = lab[l];
+        if (ll != l) {
+            lab[v] = ll;
+            *changed = 1;
+        }
+    }
+}
+
+__global__ void k_iota_u32(uint32_t* p, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        p[i] = (uint32_t)i;
+}
+
+__global__ void k_init_params(float* p, uint64_t seed) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < MLP_NPARAM; i += gridDim.x * blockDim.x) {
+        const double u = (double)(hash3(seed, 0x31415ull, (uint64_t)i) >> 11) * 0x1.0p-53;  // [0, 1)
+        float x = 0.0f;
+        if (i < MLP_F * MLP_H) x = (float)((2.0 * u - 1.0) * sqrt(6.0 / (MLP_F + MLP_H)));
+        else if (i >= MLP_F * MLP_H + MLP_H && i < MLP_F * MLP_H + 2 * MLP_H)
+            x = (float)((2.0 * u - 1.0) * sqrt(6.0 / (MLP_H + 1)));
+        p[i] = x;
+    }
+}
+
+struct EdgeSet {
+    uint64_t M = 0;
+    DBuf<float> feat;
+    DBuf<uint32_t> ei, ej;
+};
+
+void build_edges(Ctx& c, const DevGraph& g, double gamma, EdgeSet& es) {
+    const uint64_t cap = g.E;
+    DBuf<float> feat(c, cap * MLP_F);
+    DBuf<uint32_t> ei(c, cap), ej(c, cap);
+    DBuf<unsigned long long> cnt(c, 1);
+    zero(c, cnt.get(), 1);
+    if (g.E) {
+        k_edge_features<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, g.strength,
+                                                                2.0 * g.total_weight, gamma, feat.get(), ei.get(),
+                                                                ej.get(), cnt.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    const uint64_t M = to_host(c, cnt.get());
+    es.M = M;
+    es.feat.alloc(c, M * MLP_F);
+    es.ei.alloc(c, M);
+    es.ej.alloc(c, M);
+    if (!M) return;
+    DBuf<uint64_t> keys(c, M), keys_s(c, M);
+    DBuf<uint32_t> idx(c, M), order(c, M);
+    k_edge_keys<<<grid_for(M, TB), TB, 0, c.stream>>>(ei.get(), ej.get(), M, keys.get(), idx.get());
+    sort_pairs(c, keys.get(), keys_s.get(), idx.get(), order.get(), M, 64);
+    k_gather_edges<<<grid_for(M, TB), TB, 0, c.stream>>>(order.get(), M, feat.get(), keys_s.get(), es.feat.get(),
+                                                         es.ei.get(), es.ej.get());
+    SC_LAUNCH_CHECK();
+    c.launches += 2;
+}
+
+// Standardise es's features with the model's scaler, fitting it first if the
+// model has none (and `fit` allows it).
+void scale_edges(Ctx& c, Mlp& m, EdgeSet& es, bool fit) {
+    if (!m.has_norm) {
+        if (!fit) fail(SC_E_INVALID_ARGUMENT, "the model has no feature scaler yet: train it or set one first");
+        const int nb = 148;
+        DBuf<double> partial(c, (uint64_t)nb * 2 * MLP_F);
+        k_feat_partials<<<nb, TB, 0, c.stream>>>(es.feat.get(), es.M, partial.get());
+        k_feat_finalize<<<1, 32, 0, c.stream>>>(partial.get(), nb, es.M, m.norm);
+        SC_LAUNCH_CHECK();
+        sync(c);
+        m.has_norm = true;
+        c.launches += 2;
+    }
+    if (es.M) {
+        k_normalize<<<grid_for(es.M * MLP_F, TB), TB, 0, c.stream>>>(es.feat.get(), es.M, m.norm);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+}
+
+// Mean BCE loss and its gradient at the current BF16 weights.
+double grad_at(Ctx& c, const Mlp& m, const EdgeSet& es, const uint8_t* labels, float* d_grad) {
+    DBuf<__nv_bfloat16> wb(c, MLP_NPARAM);
+    k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());
+    DBuf<float> partial(c, (uint64_t)MLP_BLOCKS * MLP_NPARAM);
+    DBuf<double> partial_loss(c, MLP_BLOCKS), loss(c, 1);
+    k_mlp<true><<<MLP_BLOCKS, TB, 0, c.stream>>>(es.feat.get(), labels, es.M, wb.get(), nullptr, partial.get(),
+                                                 partial_loss.get());
+    k_grad_reduce<<<8, 256, 0, c.stream>>>(partial.get(), partial_loss.get(), MLP_BLOCKS, es.M, d_grad, loss.get());
+    SC_LAUNCH_CHECK();
+    c.launches += 3;
+    return to_host(c, loss.get());
+}
+
+}  // namespace
+
+Mlp* mlp_create(Ctx& c, uint64_t seed) {
+    std::unique_ptr<Mlp> m(new Mlp());
+    m->device = c.device;
+    struct Guard {
+        Mlp* m;
+        ~Guard() { if (m) mlp_destroy(m); }
+    } guard{m.get()};
+    SC_CUDA(cudaMalloc(&m->master, MLP_NPARAM * sizeof(float)));
+    SC_CUDA(cudaMalloc(&m->m, MLP_NPARAM * sizeof(float)));
+    SC_CUDA(cudaMalloc(&m->v, MLP_NPARAM * sizeof(float)));
+    SC_CUDA(cudaMalloc(&m->norm, 2 * MLP_F * sizeof(float)));
+    k_init_params<<<4, 256, 0, c.stream>>>(m->master, seed);
+    SC_LAUNCH_CHECK();
+    zero(c, m->m, MLP_NPARAM);
+    zero(c, m->v, MLP_NPARAM);
+    zero(c, m->norm, 2 * MLP_F);
+    sync(c);
+    guard.m = nullptr;
+    return m.release();
+}
+
+void mlp_destroy(Mlp* m) {
+    if (!m) return;
+    cudaFree(m->master);
+    cudaFree(m->m);
+    cudaFree(m->v);
+    cudaFree(m->norm);
+    delete m;
+}
+
+uint32_t mlp_param_count() { return MLP_NPARAM; }
+
+uint32_t mlp_feature_count() { return MLP_F; }
+
+bool mlp_get(Ctx& c, const Mlp& m, float* params, float* scaler) {
+    if (params) d2h(c, params, m.master, MLP_NPARAM);
+    if (scaler) d2h(c, scaler, m.norm, 2 * MLP_F);
+    sync(c);
+    return m.has_norm;
+}
+
+// New parameters (and optionally scaler); resets the Adam state.
+void mlp_set(Ctx& c, Mlp& m, const float* params, const float* scaler) {
+    if (params) {
+        h2d(c, m.master, params, MLP_NPARAM);
+        zero(c, m.m, MLP_NPARAM);
+        zero(c, m.v, MLP_NPARAM);
+        m.step = 0;
+    }
+    if (scaler) {
+        h2d(c, m.norm, scaler, 2 * MLP_F);
+        m.has_norm = true;
+    }
+    sync(c);
+}
+
+// Edge features of g at resolution gamma as the model sees them (standardised
+// by its scaler, which this fits if the model has none), sorted by (i, j).
+void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_host, uint32_t* ei_host,
+                  uint32_t* ej_host, uint64_t cap, uint64_t* M_out) {
+    EdgeSet es;
+    build_edges(c, g, gamma, es);
+    *M_out = es.M;
+    if (es.M > cap)
+        fail(SC_E_INVALID_ARGUMENT, "capacity %llu is below the %llu undirected edges", (unsigned long long)cap,
+             (unsigned long long)es.M);
+    scale_edges(c, m, es, true);
+    if (feat_host) d2h(c, feat_host, es.feat.get(), es.M * MLP_F);
+    if (ei_host) d2h(c, ei_host, es.ei.get(), es.M);
+    if (ej_host) d2h(c, ej_host, es.ej.get(), es.M);
+    sync(c);
+}
+
+// `epochs` full-batch Adam steps on (g, membership) at gamma; returns the mean
+// loss at the weights before the last step. epochs == 0 only evaluates the loss
+// and gradient. grad_out_host (nullable) receives the last gradient.
+double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, uint32_t epochs,
+                 double lr, float* grad_out_host) {
+    EdgeSet es;
+    build_edges(c, g, gamma, es);
+    scale_edges(c, m, es, true);
+    DBuf<uint8_t> lab(c, es.M);
+    if (es.M) {
+        k_edge_labels<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), es.M, d_memb, lab.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    DBuf<float> grad(c, MLP_NPARAM);
+    double loss = grad_at(c, m, es, lab.get(), grad.get());
+    const float b1 = 0.9f, b2 = 0.999f;
+    for (uint32_t ep = 0; ep < epochs; ++ep) {
+        if (ep) loss = grad_at(c, m, es, lab.get(), grad.get());
+        m.step++;
+        const float bc1 = 1.0f - powf(b1, (float)m.step), bc2 = 1.0f - powf(b2, (float)m.step);
+        k_adam<<<4, 256, 0, c.stream>>>(m.master, m.m, m.v, grad.get(), (float)lr, b1, b2, 1e-8f, bc1, bc2);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    if (grad_out_host) {
+        d2h(c, grad_out_host, grad.get(), MLP_NPARAM);
+        sync(c);
+    }
+    return loss;
+}
+
+// Proposal: components of the edges whose predicted probability exceeds thr.
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, uint32_t* d_labels,
+                     float* prob_host, uint64_t prob_cap) {
+    EdgeSet es;
+    build_edges(c, g, gamma, es);
+    scale_edges(c, m, es, false);
+    DBuf<__nv_bfloat16> wb(c, MLP_NPARAM);
+    k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());
+    DBuf<float> p(c, es.M);
+    if (es.M)
+        k_mlp<false><<<MLP_BLOCKS, TB, 0, c.stream>>>(es.feat.get(), nullptr, es.M, wb.get(), p.get(), nullptr, nullptr);
+    SC_LAUNCH_CHECK();
+    if (prob_host) {
+        if (es.M > prob_cap) fail(SC_E_INVALID_ARGUMENT, "probability capacity too small");
+        d2h(c, prob_host, p.get(), es.M);
+    }
+    const uint64_t n = g.n;
+    k_iota_u32<<<grid_for(n, TB), TB, 0, c.stream>>>(d_labels, n);
+    DBuf<int> changed(c, 1);
+    bool done = false;
+    // Every round either hooks a root under a smaller label or shortens a path,
+    // and labels only decrease, so the loop ends; the cap turns a bug into an error.
+    for (int round = 0; round < 4096 && !done; ++round) {
+        zero(c, changed.get(), 1);
+        if (es.M)
+            k_cc_hook<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
+                                                               d_labels, changed.get());
+        for (int j = 0; j < 4; ++j) k_cc_jump<<<grid_for(n, TB), TB, 0, c.stream>>>(d_labels, n, changed.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 5;
+        done = !to_host(c, changed.get());
+    }
+    if (!done) fail(SC_E_INTERNAL, "proposal components did not converge");
+    DBuf<uint32_t> compact(c, n);
+    const uint32_t K = renumber_ids(c, d_labels, n, n, compact.get());
+    d2d(c, d_labels, compact.get(), n);
+    sync(c);
+    return K;
+}
+
+}  // namespace sc
