@@ -15,7 +15,16 @@ with from_csr_parts. A "step" is one full leiden() call on that graph.
   cpu_baseline  the CPU oracle (single-threaded restatement of the
              reference's Leiden) on the same graph.
 
+  sweep      (also in the line) the resolution x seed sweep on the 1M x 50
+             Gaussian kNN graph (60 components, k = 15): 32 RB resolutions
+             log-spaced in [0.1, 3] x 4 seeds = 128 instances, timed as 128
+             sequential plain runs and as warm-started chains on concurrent
+             streams; speed-up and per-instance modularity differences.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--n POINTS] [--no-sweep] [--no-cpu-baseline]
+  python bench.py --part knn [--n POINTS] [--steps K] [--warmup W]
+             times the kNN graph builder alone (points/s) on the same data.
 """
 from __future__ import annotations
 
@@ -110,6 +119,57 @@ def knn_graph_sc(n, d, comps, seed, k, device_index):
 
 KNN_INFO = {}
 
+SWEEP_POINTS, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_K, SWEEP_SEED = 1_000_000, 50, 60, 15, 11
+SWEEP_RESOLUTIONS = 32
+SWEEP_SEEDS = (1, 2, 3, 4)
+
+
+def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=4):
+    """128-instance resolution x seed sweep: sequential plain runs vs
+    warm-started chains on concurrent streams (same graph, same configs)."""
+    import sc_gpu
+    from sc_gpu import synth
+    X, _ = synth.gaussian_mixture(n_points, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_SEED, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, SWEEP_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w, device=device_index)
+    del X, r
+    res = np.geomspace(0.1, 3.0, SWEEP_RESOLUTIONS)
+    sc_gpu.leiden(g)  # warm-up
+    out = {}
+    for name, warm, streams in (("plain_sequential", False, 1), ("warm_chains", True, n_streams)):
+        t = time.perf_counter()
+        sw = sc_gpu.leiden_sweep(g, res, SWEEP_SEEDS, warm_start=warm, n_streams=streams)
+        dt = time.perf_counter() - t
+        out[name] = (dt, {k: sc_gpu.modularity(g, v.labels(), k[0]) for k, v in sw.items()})
+    base_s, base_q = out["plain_sequential"]
+    warm_s, warm_q = out["warm_chains"]
+    d = np.array([warm_q[k] - base_q[k] for k in base_q])
+    return {"workload": f"sweep_rb{SWEEP_RESOLUTIONS}x{len(SWEEP_SEEDS)}_knn{SWEEP_K}_gmm{n_points}x{SWEEP_DIMS}",
+            "instances": len(base_q), "edge_count": g.edge_count(), "plain_sequential_s": base_s,
+            "warm_chains_s": warm_s, "streams": n_streams, "speedup": base_s / warm_s,
+            "dQ_min": float(d.min()), "dQ_mean": float(d.mean()), "dQ_max": float(d.max()),
+            "frac_dQ_ge_-1e-4": float(np.mean(d >= -1e-4))}
+
+
+def run_knn_part(args, device_index):
+    """The kNN graph builder alone on the bench's point set."""
+    import sc_gpu
+    from sc_gpu import synth
+    X, _ = synth.gaussian_mixture(args.n, DIMS, COMPONENTS, GRAPH_SEED, sigma=(0.7, 1.5))
+    for _ in range(args.warmup):
+        sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        r = sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    dt = (time.perf_counter() - t) / args.steps
+    line = {"metric": "kNN graph build points/s (exact k=10, BF16 tcgen05 candidates + FP32 re-rank)",
+            "value": args.n / dt, "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": f"knn{K}_gmm{args.n}x{DIMS}", "n_points": args.n, "dims": DIMS, "k": K},
+            "timing": "host wall clock around the C ABI call (host input, host CSR output)",
+            "conn_nnz": int(len(r.conn_w))}
+    print(json.dumps(line), flush=True)
+
 
 def make_graph(args, device):
     if args.graph == "lattice":
@@ -202,6 +262,9 @@ def main():
     ap.add_argument("--n", type=int, default=N_POINTS)
     ap.add_argument("--graph", default="gmm", choices=["gmm", "gmm-torch", "lattice"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--sweep-points", type=int, default=SWEEP_POINTS)
+    ap.add_argument("--part", default="leiden", choices=["leiden", "knn"])
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))
@@ -239,6 +302,11 @@ def main():
                                  "cpu": cpu_model(), "nproc": os.cpu_count()},
                 "e2e": {"value": eps, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        return
+
+    if args.part == "knn":
+        if rank == 0:
+            run_knn_part(args, local_rank)
         return
 
     import sc_gpu
@@ -313,6 +381,9 @@ def main():
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
     if KNN_INFO:
         line["knn_graph_build_s"] = KNN_INFO["seconds"]
+    if not args.no_sweep:
+        del g
+        line["sweep"] = run_sweep(local_rank, args.sweep_points)
     if not args.no_cpu_baseline:
         og, lab_o, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
         q_o = og.modularity(lab_o)

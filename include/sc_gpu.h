@@ -306,6 +306,21 @@ sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, u
                           uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
                           uint64_t conn_capacity, uint64_t* conn_nnz, sc_graph** graph_out);
 
+/* The search of sc_knn_gaussian for the query rows [q_begin, q_end) only,
+ * against all n points: one shard of a build split across GPUs by query rows.
+ * knn_index / knn_d2 receive (q_end - q_begin) x (k+1) entries, self first,
+ * with SQUARED FP32 distances (whatever opts.squared_kiddo says). No
+ * counterpart in single-clustering, whose kNN runs on one host. */
+sc_status sc_knn_search(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q_begin,
+                        uint64_t q_end, const sc_knn_opts* opts, uint32_t* knn_index, float* knn_d2);
+
+/* The connectivity step of sc_knn_gaussian from the gathered k+1 lists of all
+ * n points (squared distances, as sc_knn_search writes them); outputs as in
+ * sc_knn_gaussian. */
+sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const float* knn_d2, uint64_t n, uint64_t k,
+                                const sc_knn_opts* opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                                uint64_t conn_capacity, uint64_t* conn_nnz, sc_graph** graph_out);
+
 /* ---------------------------------------------------------------- learned warm start
  * No counterpart in single-clustering: its only warm-start hook is the
  * `initial` membership of run_once (src/community_search/leiden/mod.rs:207-220),
@@ -322,8 +337,10 @@ sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, u
  * graph the model trains on or extracts features from.
  *
  * The proposal is the connected components of the edges whose probability
- * exceeds `threshold`, numbered 0..k-1 by smallest member; pass it to
- * sc_leiden_from as `initial`.
+ * exceeds `threshold` and whose endpoints are both core nodes (at least
+ * `core_fraction` of their edges exceed the threshold), numbered 0..k-1 by
+ * smallest member; other nodes stay singletons. Pass it to sc_leiden_from as
+ * `initial`.
  */
 typedef struct sc_mlp sc_mlp;
 
@@ -350,7 +367,8 @@ sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t
 /* Initial membership for sc_leiden_from (see above); prob_out (nullable) gets
  * the edge probabilities in sc_mlp_features order, prob_capacity entries. */
 sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
-                         uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity);
+                         double core_fraction, uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out,
+                         uint64_t prob_capacity);
 
 #ifdef __cplusplus
 }

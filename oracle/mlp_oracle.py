@@ -8,8 +8,8 @@ tests compare against this numpy FP64 restatement:
 * forward_backward: mean binary cross-entropy of the 2-layer MLP and its
   gradient, evaluated with BF16-rounded weights (the GPU's forward weights) in
   FP64, so the GPU's FP32-accumulated gradient can be checked against it;
-* components: connected components of the edges above a threshold, numbered
-  by smallest member (the proposal).
+* core_mask, components: the edges the proposal keeps (confident, between
+  core nodes) and their connected components, numbered by smallest member.
 
 single-clustering itself has no learned part; what this pins is the GPU's
 arithmetic, and finite differences pin this oracle's own gradient.
@@ -120,6 +120,18 @@ def forward_backward(params, X, y):
 
 def probabilities(params, X):
     return 1.0 / (1.0 + np.exp(-forward(params, np.asarray(X, np.float64))[2]))
+
+
+def core_mask(n, ei, ej, prob, threshold, core_fraction):
+    """Edges kept by the proposal: confident, both endpoints core nodes
+    (confident share of their undirected non-loop edges >= core_fraction)."""
+    ei = np.asarray(ei, np.int64)
+    ej = np.asarray(ej, np.int64)
+    conf = np.asarray(prob) > threshold
+    deg = np.bincount(ei, minlength=n) + np.bincount(ej, minlength=n)
+    cd = np.bincount(ei, weights=conf, minlength=n) + np.bincount(ej, weights=conf, minlength=n)
+    core = cd >= core_fraction * deg
+    return conf & core[ei] & core[ej]
 
 
 def components(n, ei, ej, mask):

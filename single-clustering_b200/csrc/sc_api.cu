@@ -548,6 +548,32 @@ sc_status sc_knn_gaussian(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, u
     });
 }
 
+sc_status sc_knn_search(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q_begin,
+                        uint64_t q_end, const sc_knn_opts* opts, uint32_t* knn_index, float* knn_d2) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(X != nullptr || n == 0, "X is NULL");
+        sc_knn_opts o;
+        if (opts) o = *opts;
+        else sc_knn_opts_default(&o);
+        sc::knn_search(c, X, n, d, k, q_begin, q_end, o, knn_index, knn_d2);
+    });
+}
+
+sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const float* knn_d2, uint64_t n, uint64_t k,
+                                const sc_knn_opts* opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                                uint64_t conn_capacity, uint64_t* conn_nnz, sc_graph** graph_out) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require((knn_index && knn_d2) || n == 0, "knn_index or knn_d2 is NULL");
+        sc_knn_opts o;
+        if (opts) o = *opts;
+        else sc_knn_opts_default(&o);
+        sc::DevGraph* g = nullptr;
+        sc::knn_connectivities(c, knn_index, knn_d2, n, k, o, conn_ptrs, conn_nbrs, conn_w, conn_capacity, conn_nnz,
+                               graph_out ? &g : nullptr);
+        if (graph_out) *graph_out = new sc_graph{g};
+    });
+}
+
 // ---------------------------------------------------------------- learned warm start
 uint32_t sc_mlp_param_count(void) { return sc::mlp_param_count(); }
 
@@ -621,17 +647,20 @@ sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t
 }
 
 sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
-                         uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity) {
+                         double core_fraction, uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out,
+                         uint64_t prob_capacity) {
     return guarded(ctx, [&](sc::Ctx& c) {
         require(m && m->m && g && g->g && n_clusters_out, "model, graph or n_clusters_out is NULL");
         if (m->device != c.device) bad_arg("model lives on another device than the context");
         require_same_device(c, *g->g);
         require(resolution > 0.0 && std::isfinite(resolution), "resolution must be positive and finite");
         require(std::isfinite(threshold), "threshold must be finite");
+        require(core_fraction >= 0.0 && core_fraction <= 1.0, "core_fraction must lie in [0, 1]");
         const sc::DevGraph& G = *g->g;
         require(labels_out || G.n == 0, "labels_out is NULL");
         sc::DBuf<uint32_t> lab(c, G.n);
-        const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, threshold, lab.get(), prob_out, prob_capacity);
+        const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, threshold, core_fraction, lab.get(), prob_out,
+                                             prob_capacity);
         if (G.n) {
             std::vector<uint32_t> h(G.n);
             sc::d2h(c, h.data(), lab.get(), G.n);

@@ -253,6 +253,11 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k,
                   const sc_knn_opts& opts, uint32_t* knn_index, float* knn_dist,
                   uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w, uint64_t conn_cap,
                   uint64_t* conn_nnz, DevGraph** graph_out);
+void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t q1,
+                const sc_knn_opts& opts, uint32_t* knn_index, float* knn_d2);
+void knn_connectivities(Ctx& c, const uint32_t* knn_index, const float* knn_d2, uint64_t n, uint64_t k,
+                        const sc_knn_opts& opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                        uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out);
 
 // mlp.cu: learned warm start (edge MLP; proposal = components of confident edges)
 struct Mlp;
@@ -266,8 +271,8 @@ void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_h
                   uint32_t* ej_host, uint64_t cap, uint64_t* M_out);
 double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, uint32_t epochs,
                  double lr, float* grad_out_host);
-uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, uint32_t* d_labels,
-                     float* prob_host, uint64_t prob_cap);
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, double core_fraction,
+                     uint32_t* d_labels, float* prob_host, uint64_t prob_cap);
 
 // common.cu
 void check_device_status(Ctx& c);

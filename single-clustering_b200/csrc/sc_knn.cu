@@ -241,7 +241,7 @@ struct KnnSmem {
 template <int KA>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
-             float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status) {
+             uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status) {
     using L = KnnSmem<KA>;
     extern __shared__ __align__(1024) unsigned char raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
@@ -261,8 +261,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
     volatile uint32_t* abort_flag = misc + 1;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t ntiles = (n + TILE - 1) / TILE;
-    const uint32_t ngroups = (n + QT * TILE - 1) / (QT * TILE);
+    const uint32_t ntiles = (n + TILE - 1) / TILE;          // point tiles (B)
+    const uint32_t ngroups = (nq + QT * TILE - 1) / (QT * TILE);  // query tile groups (A)
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < L::STAGES; ++s) {
@@ -423,7 +423,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             }
             if (*abort_flag) break;
             const uint64_t qg = (uint64_t)g * QT * TILE + q * TILE + row;
-            if (qg < n) {
+            if (qg < nq) {
                 for (int s2 = 0; s2 < RCAND; ++s2) {
                     cand_score[qg * RTOTAL + h * RCAND + s2] = cs[s2 * S + owner];
                     cand_idx[qg * RTOTAL + h * RCAND + s2] = ci[s2 * S + owner];
@@ -473,15 +473,17 @@ __device__ __forceinline__ uint64_t warp_sort32(uint64_t key) {
 // One warp per query: exact FP32 distances of its RTOTAL = 64 candidates (two
 // per lane), the 32 smallest kept by a merge-split of two sorted halves, then
 // the first k+1 written.
-__global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d, uint32_t k,
-                             const uint32_t* __restrict__ cand_idx, uint32_t* __restrict__ out_idx,
+// Queries are points q0 .. q0 + nq - 1; rows of cand_idx / out_* are local.
+__global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d, uint32_t k, uint64_t q0,
+                             uint64_t nq, const uint32_t* __restrict__ cand_idx, uint32_t* __restrict__ out_idx,
                              float* __restrict__ out_d2) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t q = warp; q < n; q += nwarps) {
-        uint64_t ka = warp_sort32(rerank_key(X, n, d, q, cand_idx[q * RTOTAL + lane]));
-        uint64_t kb = warp_sort32(rerank_key(X, n, d, q, cand_idx[q * RTOTAL + 32 + lane]));
+    for (uint64_t lq = warp; lq < nq; lq += nwarps) {
+        const uint64_t q = q0 + lq;
+        uint64_t ka = warp_sort32(rerank_key(X, n, d, q, cand_idx[lq * RTOTAL + lane]));
+        uint64_t kb = warp_sort32(rerank_key(X, n, d, q, cand_idx[lq * RTOTAL + 32 + lane]));
         const uint64_t kbr = __shfl_sync(0xFFFFFFFFu, kb, 31 - lane);
         uint64_t key = ka < kbr ? ka : kbr;  // the 32 smallest, as a bitonic sequence
         for (int stride = 16; stride > 0; stride >>= 1) {
@@ -491,8 +493,8 @@ __global__ void k_knn_rerank(const float* __restrict__ X, uint64_t n, uint32_t d
         if (lane <= k) {
             const uint32_t tag = (uint32_t)key;
             const uint32_t idx = (key == ~0ull) ? 0xFFFFFFFFu : (tag == 0 ? (uint32_t)q : tag - 1u);
-            out_idx[q * (k + 1) + lane] = idx;
-            out_d2[q * (k + 1) + lane] = key == ~0ull ? INFINITY : __uint_as_float((uint32_t)(key >> 32));
+            out_idx[lq * (k + 1) + lane] = idx;
+            out_d2[lq * (k + 1) + lane] = key == ~0ull ? INFINITY : __uint_as_float((uint32_t)(key >> 32));
         }
     }
 }
@@ -614,72 +616,67 @@ CUtensorMap make_map(const __nv_bfloat16* base, uint64_t n) {
     return m;
 }
 
+// Candidates of the queries q0 .. q0 + nq - 1 against all n points. A is the
+// query operand: its tensor map starts at row q0 (KA * 2 bytes per row, a
+// multiple of 16, so every row start is a legal TMA base).
 template <int KA>
-void candidates(Ctx& c, const float* dX, uint64_t n, uint32_t d, float* cand_score, uint32_t* cand_idx) {
+void candidates(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0, uint64_t nq, float* cand_score,
+                uint32_t* cand_idx) {
     DBuf<__nv_bfloat16> A(c, n * KA), B(c, n * KA);
     k_knn_prep<KA><<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, A.get(), B.get());
     SC_LAUNCH_CHECK();
-    CUtensorMap ta = make_map<KA>(A.get(), n), tb = make_map<KA>(B.get(), n);
+    CUtensorMap ta = make_map<KA>(A.get() + q0 * KA, nq), tb = make_map<KA>(B.get(), n);
     using L = KnnSmem<KA>;
     SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
-    const uint32_t ngroups = (uint32_t)((n + QT * TILE - 1) / (QT * TILE));
+    const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
     const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
-    k_knn_tc<KA><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, cand_score, cand_idx,
-                                                             c.d_status);
+    k_knn_tc<KA><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
+                                                             cand_idx, c.d_status);
     SC_LAUNCH_CHECK();
     c.launches += 2;
 }
 
-}  // namespace
-
-// knn_arrayd_* (neighborhood/mod.rs:51-202, :359-578) with exact (brute-force)
-// search. The search keeps 64 candidates per query (the 32 best of each half
-// of the candidate columns) from the BF16 tensor-core scores, then ranks them
-// exactly in FP32.
-void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
-                  uint32_t* knn_index, float* knn_dist, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
-                  uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
+void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
     if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
     if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
     if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
     if (opts.precision != SC_KNN_BF16) fail(SC_E_UNSUPPORTED, "only the BF16 contraction is built");
-    DBuf<float> dX(c, n * d);
-    h2d(c, dX.get(), X, n * d);
-    DBuf<float> cscore(c, n * RTOTAL);
-    DBuf<uint32_t> cidx(c, n * RTOTAL);
-    if (n) {
-        if (d <= 30) candidates<32>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());
-        else candidates<64>(c, dX.get(), n, (uint32_t)d, cscore.get(), cidx.get());
-    }
-    DBuf<uint32_t> idx(c, n * (k + 1));
-    DBuf<float> d2(c, n * (k + 1));
-    if (n) {
-        k_knn_rerank<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(dX.get(), n, (uint32_t)d, (uint32_t)k, cidx.get(),
-                                                                   idx.get(), d2.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
-    }
+}
+
+// Exact (brute-force) k+1 nearest points of the queries q0 .. q0 + nq - 1
+// among all n points of the device array dX: 64 candidates per query (the 32
+// best of each half of the candidate columns) from the BF16 tensor-core
+// scores, ranked exactly in FP32. idx/d2 are nq x (k+1), self first, then
+// ascending squared distance, ties by lower index.
+void knn_search_device(Ctx& c, const float* dX, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t nq,
+                       uint32_t* idx, float* d2) {
+    if (!nq) return;
+    DBuf<float> cscore(c, nq * RTOTAL);
+    DBuf<uint32_t> cidx(c, nq * RTOTAL);
+    if (d <= 30) candidates<32>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    else candidates<64>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    k_knn_rerank<<<grid_for(nq * 32, 256), 256, 0, c.stream>>>(dX, n, (uint32_t)d, (uint32_t)k, q0, nq,
+                                                                cidx.get(), idx, d2);
+    SC_LAUNCH_CHECK();
+    c.launches++;
     check_device_status(c);
-    if (knn_index) d2h(c, knn_index, idx.get(), n * (k + 1));
-    if (knn_dist) {
-        std::vector<float> h(n * (k + 1));
-        d2h(c, h.data(), d2.get(), n * (k + 1));
-        sync(c);
-        for (uint64_t i = 0; i < h.size(); ++i) knn_dist[i] = opts.squared_kiddo ? h[i] : std::sqrt(h[i]);
-    }
-    if (!conn_ptrs && !graph_out) {
-        sync(c);
-        return;
-    }
+}
+
+// Gaussian connectivities (neighborhood/mod.rs:105-163, :480-544) from the
+// device k+1 lists of all n points (squared distances): sigma per point,
+// weights, symmetrisation, duplicate removal, CSR.
+void knn_connectivities_device(Ctx& c, const uint32_t* idx, const float* d2, uint64_t n, uint64_t k,
+                               const sc_knn_opts& opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                               uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
     DBuf<float> sigma(c, n);
     DBuf<unsigned long long> keys(c, 2 * n * k + 1), keys_s(c, 2 * n * k + 1);
     DBuf<float> w(c, 2 * n * k + 1), w_s(c, 2 * n * k + 1);
     DBuf<unsigned long long> cnt(c, 1);
     zero(c, cnt.get(), 1);
     if (n) {
-        k_knn_sigma<<<grid_for(n, 256), 256, 0, c.stream>>>(d2.get(), n, (uint32_t)k, opts.sigma == SC_SIGMA_KTH,
+        k_knn_sigma<<<grid_for(n, 256), 256, 0, c.stream>>>(d2, n, (uint32_t)k, opts.sigma == SC_SIGMA_KTH,
                                                             sigma.get());
-        k_knn_pairs<<<grid_for(n, 256), 256, 0, c.stream>>>(idx.get(), d2.get(), n, (uint32_t)k, sigma.get(),
+        k_knn_pairs<<<grid_for(n, 256), 256, 0, c.stream>>>(idx, d2, n, (uint32_t)k, sigma.get(),
                                                             opts.sym == SC_SYM_UNION, opts.squared_kiddo,
                                                             keys.get(), w.get(), cnt.get());
         SC_LAUNCH_CHECK();
@@ -718,6 +715,66 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, co
     }
     if (graph_out) *graph_out = graph_from_csr(c, ptr.get(), n + 1, cols.get(), M, uw.get(), M, nullptr, 0, true);
     sync(c);
+}
+
+void copy_lists_out(Ctx& c, const uint32_t* idx, const float* d2, uint64_t rows, uint64_t k, int squared,
+                    uint32_t* knn_index, float* knn_dist) {
+    if (knn_index) d2h(c, knn_index, idx, rows * (k + 1));
+    if (knn_dist) {
+        std::vector<float> h(rows * (k + 1));
+        d2h(c, h.data(), d2, rows * (k + 1));
+        sync(c);
+        for (uint64_t i = 0; i < h.size(); ++i) knn_dist[i] = squared ? h[i] : std::sqrt(h[i]);
+    }
+    sync(c);
+}
+
+}  // namespace
+
+// knn_arrayd_* (neighborhood/mod.rs:51-202, :359-578) with exact search.
+void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
+                  uint32_t* knn_index, float* knn_dist, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                  uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
+    knn_check(n, d, k, opts);
+    DBuf<float> dX(c, n * d);
+    h2d(c, dX.get(), X, n * d);
+    DBuf<uint32_t> idx(c, n * (k + 1));
+    DBuf<float> d2(c, n * (k + 1));
+    knn_search_device(c, dX.get(), n, d, k, 0, n, idx.get(), d2.get());
+    copy_lists_out(c, idx.get(), d2.get(), n, k, opts.squared_kiddo, knn_index, knn_dist);
+    if (!conn_ptrs && !graph_out) return;
+    knn_connectivities_device(c, idx.get(), d2.get(), n, k, opts, conn_ptrs, conn_nbrs, conn_w, conn_cap, conn_nnz,
+                              graph_out);
+}
+
+// The k+1 lists of the query rows [q0, q1) only (one shard of a multi-GPU
+// build); squared FP32 distances.
+void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t q1,
+                const sc_knn_opts& opts, uint32_t* knn_index, float* knn_d2) {
+    knn_check(n, d, k, opts);
+    if (q0 > q1 || q1 > n) fail(SC_E_INVALID_ARGUMENT, "query rows [%llu, %llu) are not inside [0, %llu)",
+                                (unsigned long long)q0, (unsigned long long)q1, (unsigned long long)n);
+    const uint64_t nq = q1 - q0;
+    DBuf<float> dX(c, n * d);
+    h2d(c, dX.get(), X, n * d);
+    DBuf<uint32_t> idx(c, nq * (k + 1));
+    DBuf<float> d2(c, nq * (k + 1));
+    knn_search_device(c, dX.get(), n, d, k, q0, nq, idx.get(), d2.get());
+    copy_lists_out(c, idx.get(), d2.get(), nq, k, 1, knn_index, knn_d2);
+}
+
+// Connectivities from gathered host lists (all n rows, squared distances).
+void knn_connectivities(Ctx& c, const uint32_t* knn_index, const float* knn_d2, uint64_t n, uint64_t k,
+                        const sc_knn_opts& opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
+                        uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
+    if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
+    if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
+    DBuf<uint32_t> idx(c, n * (k + 1));
+    DBuf<float> d2(c, n * (k + 1));
+    h2d(c, idx.get(), knn_index, n * (k + 1));
+    h2d(c, d2.get(), knn_d2, n * (k + 1));
+    knn_connectivities_device(c, idx.get(), d2.get(), n, k, opts, conn_ptrs, conn_nbrs, conn_w, conn_cap, conn_nnz,
+                              graph_out);
 }
 
 }  // namespace sc

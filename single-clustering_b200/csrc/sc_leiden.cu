@@ -65,6 +65,7 @@ struct Params {
     double nscale, inv_nscale;  // same for node weights
     int has_limit;
     double limit;
+    int need_nc;                // community node weights are read (CPM, or a weight cap)
     double theta;               // refinement randomness (<= 0: argmax)
     uint64_t seed;
     uint32_t* status;
@@ -141,6 +142,13 @@ __device__ __forceinline__ double refine_key(const Params& p, double rel, uint32
     return __dadd_rn(__ddiv_rn(rel, p.theta), -log(-log(u)));
 }
 
+// Read-only load (ld.global.nc): the decide kernels never write the graph, the
+// membership or the community aggregates they read; only the commit kernels do.
+template <class T>
+__device__ __forceinline__ T ro(const T* a) {
+    return __ldg(a);
+}
+
 // Warp-aggregated counter add.
 __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long long x) {
     for (int o = 16; o; o >>= 1) x += __shfl_xor_sync(0xFFFFFFFFu, x, o);
@@ -151,7 +159,7 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 // REFINE=false: local moving. REFINE=true: refinement (singletons only, inside
 // the constraint, randomised choice among non-negative candidates).
 template <int G, bool REFINE>
-__global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t* __restrict__ list,
                                                      uint32_t count) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
@@ -167,26 +175,26 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
     for (uint64_t wb = warp * per_warp; wb < count; wb += nwarps * per_warp) {
         const uint64_t i = wb + gw;
         const bool have = i < count;
-        const uint32_t v = have ? list[i] : 0;
+        const uint32_t v = have ? ro(list + (i)) : 0;
         uint64_t b = 0, e = 0;
         if (have) {
-            b = p.ptr[v];
-            e = p.ptr[v + 1];
+            b = ro(p.ptr + (v));
+            e = ro(p.ptr + (v + 1));
         }
         const int deg = (int)(e - b);
-        const uint32_t own = have ? p.memb[v] : 0;
+        const uint32_t own = have ? ro(p.memb + (v)) : 0;
         bool eligible = have;
-        if (REFINE && have) eligible = p.csize[own] == 1;  // refine.rs:60-62
+        if (REFINE && have) eligible = ro(p.csize + (own)) == 1;  // refine.rs:60-62
         bool valid = eligible && sub < deg;
         uint32_t u = 0;
         float wt = 0.0f;
         if (valid) {
-            u = p.nbr[b + sub];
-            wt = p.w[b + sub];
+            u = ro(p.nbr + (b + sub));
+            wt = ro(p.w + (b + sub));
         }
         valid = valid && u != v;
-        if (REFINE && valid) valid = p.constraint[u] == p.constraint[v];
-        const uint32_t cu = valid ? p.memb[u] : NONE32;
+        if (REFINE && valid) valid = ro(p.constraint + (u)) == ro(p.constraint + (v));
+        const uint32_t cu = valid ? ro(p.memb + (u)) : NONE32;
         const long long wf = valid ? to_fix((double)wt, p.inv_scale) : 0;
         const uint64_t key = valid ? (((uint64_t)gw << 32) | cu) : (0xFFFFFFFF00000000ull | (uint64_t)lane);
         const unsigned mm = __match_any_sync(FULL, key);
@@ -201,9 +209,9 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
         long long kf = 0, af = 0;
         double sl = 0.0;
         if (eligible) {
-            kf = to_fix(p.strength[v], p.inv_scale);
-            af = to_fix(p.node_w[v], p.inv_nscale);
-            sl = p.self_loop[v];
+            kf = to_fix(ro(p.strength + (v)), p.inv_scale);
+            af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
+            sl = ro(p.self_loop + (v));
         }
         const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale);
         // weight to the own community
@@ -212,17 +220,17 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
         if (!ob) wof = 0;
         double base = 0.0;
         if (eligible) {
-            base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale), a,
-                           from_fix(p.Wf[own] - af, p.nscale));
+            base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
+                           (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         }
         // candidates held by leader lanes
         double g = -INFINITY;
         uint32_t c = NONE32, cu_member = NONE32;
         bool cand = false;
         if (leader && cu != own) {
-            double nc = from_fix(p.Wf[cu], p.nscale);
+            double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (!p.has_limit || __dadd_rn(nc, a) <= p.limit) {
-                g = gain_of(p, from_fix(acc, p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+                g = gain_of(p, from_fix(acc, p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
                 if (REFINE) {
                     double rel = __dsub_rn(g, base);
                     if (rel >= 0.0) {  // `>=` takes ties (refine.rs:91-95)
@@ -267,7 +275,7 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
                 }
                 // one empty community per node (local_move.rs:92-100)
                 const uint32_t fresh = (uint32_t)(p.S0 + v);
-                if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 &&
+                if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 &&
                     (!p.has_limit || a <= p.limit)) {
                     double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
                     if (better(ge, fresh, bg, best)) {
@@ -280,7 +288,7 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
                     p.tgt[v] = best;
                     p.from[v] = own;
                     p.dgain[v] = to_fix(d, p.inv_scale);
-                    p.hint[v] = (best != fresh && p.csize[best] == 1) ? cu_member : NONE32;
+                    p.hint[v] = (best != fresh && ro(p.csize + (best)) == 1) ? cu_member : NONE32;
                     p.epoch[v] = p.cur;
                 }
             }
@@ -288,7 +296,7 @@ __global__ void __launch_bounds__(TB) k_decide_small(Params p, const uint32_t* _
             p.tgt[v] = c;
             p.from[v] = own;
             p.dgain[v] = 0;
-            p.hint[v] = (p.csize[c] == 1) ? cu_member : NONE32;
+            p.hint[v] = (ro(p.csize + (c)) == 1) ? cu_member : NONE32;
             p.epoch[v] = p.cur;
         }
     }
@@ -390,11 +398,11 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = warp; i < count; i += nwarps) {
-        const uint32_t v = list[i];
-        const uint64_t b = p.ptr[v], e = p.ptr[v + 1];
+        const uint32_t v = ro(list + (i));
+        const uint64_t b = ro(p.ptr + (v)), e = ro(p.ptr + (v + 1));
         const uint32_t deg = (uint32_t)(e - b);
-        const uint32_t own = p.memb[v];
-        if (REFINE && p.csize[own] != 1) continue;  // warp-uniform
+        const uint32_t own = ro(p.memb + (v));
+        if (REFINE && ro(p.csize + (own)) != 1) continue;  // warp-uniform
         uint32_t cap = 64;
         while (cap < 2 * deg) cap <<= 1;
         if (cap > (uint32_t)WCAP) {  // not this bucket's node
@@ -407,20 +415,20 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
             vals[s] = 0;
         }
         __syncwarp();
-        const uint32_t cv = REFINE ? p.constraint[v] : 0;
+        const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
         for (uint64_t j = b + lane; j < e; j += 32) {
-            const uint32_t u = p.nbr[j];
+            const uint32_t u = ro(p.nbr + (j));
             if (u == v) continue;
-            if (REFINE && p.constraint[u] != cv) continue;
-            hinsert(keys, vals, mask, p.memb[u], to_fix((double)p.w[j], p.inv_scale), p.status);
+            if (REFINE && ro(p.constraint + (u)) != cv) continue;
+            hinsert(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status);
         }
         __syncwarp();
-        const long long kf = to_fix(p.strength[v], p.inv_scale);
-        const long long af = to_fix(p.node_w[v], p.inv_nscale);
-        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = p.self_loop[v];
+        const long long kf = to_fix(ro(p.strength + (v)), p.inv_scale);
+        const long long af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
+        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = ro(p.self_loop + (v));
         const long long wof = hlookup(keys, vals, mask, own);
-        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale), a,
-                                    from_fix(p.Wf[own] - af, p.nscale));
+        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
+                                    (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         double g = -INFINITY;
         uint32_t c = NONE32;
         uint32_t lc = 0;
@@ -428,9 +436,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
             const uint32_t cu = keys[s];
             if (cu == EMPTYK || cu == own) continue;
             lc++;
-            const double nc = from_fix(p.Wf[cu], p.nscale);
+            const double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
-            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
             if (REFINE) {
                 const double rel = __dsub_rn(gg, base);
                 if (!(rel >= 0.0)) continue;
@@ -460,7 +468,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
                 bg = g;
             }
             const uint32_t fresh = (uint32_t)(p.S0 + v);
-            if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 && (!p.has_limit || a <= p.limit)) {
+            if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 && (!p.has_limit || a <= p.limit)) {
                 const double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
                 if (better(ge, fresh, bg, best)) {
                     best = fresh;
@@ -477,11 +485,11 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         }
         // the member of a singleton target, for conflict detection
         uint32_t member = NONE32;
-        if (target != NONE32 && p.csize[target] == 1) {
+        if (target != NONE32 && ro(p.csize + (target)) == 1) {
             for (uint64_t base0 = b; base0 < e; base0 += 32) {
                 const uint64_t j = base0 + lane;
-                const uint32_t u = j < e ? p.nbr[j] : v;
-                const bool hit = u != v && p.memb[u] == target;
+                const uint32_t u = j < e ? ro(p.nbr + (j)) : v;
+                const bool hit = u != v && ro(p.memb + (u)) == target;
                 if (hit) member = u;
                 if (__ballot_sync(FULL, hit)) break;
             }
@@ -522,11 +530,11 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
 
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
-        const uint32_t v = list[i];
-        const uint64_t b = p.ptr[v], e = p.ptr[v + 1];
+        const uint32_t v = ro(list + (i));
+        const uint64_t b = ro(p.ptr + (v)), e = ro(p.ptr + (v + 1));
         const uint32_t deg = (uint32_t)(e - b);
-        const uint32_t own = p.memb[v];
-        if (REFINE && p.csize[own] != 1) continue;  // uniform over the block
+        const uint32_t own = ro(p.memb + (v));
+        if (REFINE && ro(p.csize + (own)) != 1) continue;  // uniform over the block
         uint32_t cap = 64;
         while (cap < 2 * deg) cap <<= 1;
         uint32_t* keys;
@@ -552,20 +560,20 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             vals[s] = 0;
         }
         __syncthreads();
-        const uint32_t cv = REFINE ? p.constraint[v] : 0;
+        const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
         for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-            uint32_t u = p.nbr[j];
+            uint32_t u = ro(p.nbr + (j));
             if (u == v) continue;
-            if (REFINE && p.constraint[u] != cv) continue;
-            hinsert(keys, vals, mask, p.memb[u], to_fix((double)p.w[j], p.inv_scale), p.status);
+            if (REFINE && ro(p.constraint + (u)) != cv) continue;
+            hinsert(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status);
         }
         __syncthreads();
-        const long long kf = to_fix(p.strength[v], p.inv_scale);
-        const long long af = to_fix(p.node_w[v], p.inv_nscale);
-        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = p.self_loop[v];
+        const long long kf = to_fix(ro(p.strength + (v)), p.inv_scale);
+        const long long af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
+        const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = ro(p.self_loop + (v));
         const long long wof = hlookup(keys, vals, mask, own);
-        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(p.Kf[own] - kf, p.scale),
-                                    a, from_fix(p.Wf[own] - af, p.nscale));
+        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale),
+                                    a, (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         double g = -INFINITY;
         uint32_t c = NONE32;
         uint32_t lc = 0;
@@ -573,9 +581,9 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             uint32_t cu = keys[s];
             if (cu == EMPTYK || cu == own) continue;
             lc++;
-            double nc = from_fix(p.Wf[cu], p.nscale);
+            double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
-            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(p.Kf[cu], p.scale), a, nc);
+            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
             if (REFINE) {
                 double rel = __dsub_rn(gg, base);
                 if (!(rel >= 0.0)) continue;
@@ -601,7 +609,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
                     bg = g;
                 }
                 const uint32_t fresh = (uint32_t)(p.S0 + v);
-                if (fresh != own && p.csize[own] > 1 && p.csize[fresh] == 0 &&
+                if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 &&
                     (!p.has_limit || a <= p.limit)) {
                     double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
                     if (better(ge, fresh, bg, best)) {
@@ -627,10 +635,10 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
         // the member of a singleton target, for conflict detection
         const uint32_t target = s_target;
         if (target != NONE32) {
-            if (p.csize[target] == 1) {
+            if (ro(p.csize + (target)) == 1) {
                 for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-                    uint32_t u = p.nbr[j];
-                    if (u != v && p.memb[u] == target) s_member = u;
+                    uint32_t u = ro(p.nbr + (j));
+                    if (u != v && ro(p.memb + (u)) == target) s_member = u;
                 }
             }
             __syncthreads();
@@ -907,6 +915,25 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list
     c.launches++;
 }
 
+// The decide launches of batch b (list slices offs[b*NBUCKET + k] ..). A small
+// batch sends its nodes of degree <= WARP_DEGREE (buckets 0-3, contiguous in
+// the list) to the warp-per-node kernel in one launch: it computes the same
+// decision for them as the lane-group kernels (fixed-point sums are exact in
+// any order, ties go to the lower id), and the launches saved are the cost
+// that dominates a batch of a few thousand nodes.
+constexpr uint32_t SMALL_BATCH = 4096;
+
+template <bool REFINE>
+void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs, int b) {
+    const uint32_t* o = offs + b * NBUCKET;
+    if (o[4] - o[0] <= SMALL_BATCH) {
+        launch_decide<REFINE>(c, p, ws, 3, ws.list.get() + o[0], o[4] - o[0]);
+        for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, ws.list.get() + o[k], o[k + 1] - o[k]);
+        return;
+    }
+    for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, ws.list.get() + o[k], o[k + 1] - o[k]);
+}
+
 struct MoveResult {
     double improvement = 0.0;
     uint64_t sweeps = 0, moves = 0;
@@ -960,6 +987,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     p.inv_nscale = sc.ninv;
     p.has_limit = cfg.has_max_community_weight;
     p.limit = cfg.max_community_weight;
+    p.need_nc = cfg.objective == SC_OBJECTIVE_CPM || cfg.has_max_community_weight;
     p.theta = 0.0;
     p.seed = seed;
     p.status = c.d_status;
@@ -1015,10 +1043,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             p.seed = seed;
             uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
             if (lo == hi) continue;
-            for (int k = 0; k < NBUCKET; ++k) {
-                uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
-                launch_decide<false>(c, p, ws, k, ws.list.get() + s, e - s);
-            }
+            launch_batch_decide<false>(c, p, ws, offs, b);
             if (p.has_limit) {
                 k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
                 c.launches++;
@@ -1090,6 +1115,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     p.inv_nscale = sc.ninv;
     p.has_limit = cfg.has_max_community_weight;
     p.limit = cfg.max_community_weight;
+    p.need_nc = cfg.objective == SC_OBJECTIVE_CPM || cfg.has_max_community_weight;
     double mean_edge = g.edge_count > 0 ? g.total_weight / (double)g.edge_count : 1.0;
     p.theta = cfg.refine_randomness * mean_edge;  // refine.rs:44-50
     p.seed = seed;
@@ -1122,10 +1148,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
         p.cur = (uint32_t)(b + 1);
         uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
         if (lo == hi) continue;
-        for (int k = 0; k < NBUCKET; ++k) {
-            uint32_t s = offs[b * NBUCKET + k], e = offs[b * NBUCKET + k + 1];
-            launch_decide<true>(c, p, ws, k, ws.list.get() + s, e - s);
-        }
+        launch_batch_decide<true>(c, p, ws, offs, b);
         if (p.has_limit) {
             k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
             c.launches++;

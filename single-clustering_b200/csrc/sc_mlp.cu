@@ -16,7 +16,12 @@
 //   h = relu(x W1 + b1) (hidden H), z = h . w2 + b2.
 // Weights are BF16 in the forward pass with FP32 accumulation; an FP32 master
 // copy is updated by Adam. Training labels are partitions plain Leiden found;
-// the proposal is the connected components of the edges with p > threshold.
+// the proposal is the connected components of the confident edges (p >
+// threshold) between core nodes, a core node being one whose share of
+// confident edges is at least core_fraction. Edges at a community boundary
+// look like interior edges to local features, so components of all confident
+// edges chain neighbouring communities together; a boundary node has some
+// unconfident edge, stays a singleton, and is placed by local moving.
 //
 // Kernels: one warp per edge stream, lane l owns hidden units l, l+32, ...;
 // gradients accumulate in registers, then per block in shared memory, then in
@@ -312,11 +317,37 @@ __global__ void k_edge_labels(const uint32_t* __restrict__ ei, const uint32_t* _
 }
 
 // Connected components of the confident edges: min-label hooking + pointer jumping.
-__global__ void k_cc_hook(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej,
-                          const float* __restrict__ p, uint64_t M, float thr, uint32_t* lab, int* changed) {
+// Per node: undirected non-loop edges and confident ones among them.
+__global__ void k_conf_degree(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej,
+                              const float* __restrict__ p, uint64_t M, float thr, uint32_t* deg, uint32_t* conf) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
          e += (uint64_t)gridDim.x * blockDim.x) {
-        if (!(p[e] > thr)) continue;
+        const uint32_t a = ei[e], b = ej[e];
+        atomicAdd(deg + a, 1u);
+        atomicAdd(deg + b, 1u);
+        if (p[e] > thr) {
+            atomicAdd(conf + a, 1u);
+            atomicAdd(conf + b, 1u);
+        }
+    }
+}
+
+// Edge mask: confident and both endpoints core (conf >= phi * deg).
+__global__ void k_core_mask(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej,
+                            const float* __restrict__ p, uint64_t M, float thr, double phi,
+                            const uint32_t* __restrict__ deg, const uint32_t* __restrict__ conf, uint8_t* keep) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t a = ei[e], b = ej[e];
+        keep[e] = p[e] > thr && (double)conf[a] >= phi * (double)deg[a] && (double)conf[b] >= phi * (double)deg[b];
+    }
+}
+
+__global__ void k_cc_hook(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej,
+                          const uint8_t* __restrict__ keep, uint64_t M, uint32_t* lab, int* changed) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        if (!keep[e]) continue;
         const uint32_t a = lab[ei[e]], b = lab[ej[e]];
         if (a == b) continue;
         const uint32_t lo = min(a, b), hi = max(a, b);
@@ -531,8 +562,8 @@ double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, doub
 }
 
 // Proposal: components of the edges whose predicted probability exceeds thr.
-uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, uint32_t* d_labels,
-                     float* prob_host, uint64_t prob_cap) {
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, double core_fraction,
+                     uint32_t* d_labels, float* prob_host, uint64_t prob_cap) {
     EdgeSet es;
     build_edges(c, g, gamma, es);
     scale_edges(c, m, es, false);
@@ -547,6 +578,18 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr
         d2h(c, prob_host, p.get(), es.M);
     }
     const uint64_t n = g.n;
+    DBuf<uint32_t> deg(c, n), conf(c, n);
+    DBuf<uint8_t> keep(c, es.M);
+    zero(c, deg.get(), n);
+    zero(c, conf.get(), n);
+    if (es.M) {
+        k_conf_degree<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
+                                                               deg.get(), conf.get());
+        k_core_mask<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
+                                                             core_fraction, deg.get(), conf.get(), keep.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 3;
+    }
     k_iota_u32<<<grid_for(n, TB), TB, 0, c.stream>>>(d_labels, n);
     DBuf<int> changed(c, 1);
     bool done = false;
@@ -555,8 +598,8 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr
     for (int round = 0; round < 4096 && !done; ++round) {
         zero(c, changed.get(), 1);
         if (es.M)
-            k_cc_hook<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
-                                                               d_labels, changed.get());
+            k_cc_hook<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), keep.get(), es.M, d_labels,
+                                                               changed.get());
         for (int j = 0; j < 4; ++j) k_cc_jump<<<grid_for(n, TB), TB, 0, c.stream>>>(d_labels, n, changed.get());
         SC_LAUNCH_CHECK();
         c.launches += 5;

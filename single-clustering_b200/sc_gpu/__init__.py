@@ -585,5 +585,53 @@ def knn_gaussian(X, k: int, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_I
     return NeighborResult(idx, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), graph)
 
 
+def _knn_opts(sigma=SIGMA_MEDIAN, sym=SYM_LOWER_ID, precision=KNN_BF16, squared=False):
+    opts = _lib.KnnOpts()
+    lib().sc_knn_opts_default(C.byref(opts))
+    opts.sigma, opts.sym, opts.precision, opts.squared_kiddo = sigma, sym, precision, int(squared)
+    return opts
+
+
+def knn_search(X, k: int, q_begin: int, q_end: int, *, precision: int = KNN_BF16, device: int | None = None):
+    """The k+1 nearest points (self first) of the query rows [q_begin, q_end) of X
+    among all rows: (index uint32 (q, k+1), squared distances float32 (q, k+1)).
+    One shard of a build split by query rows (sc_knn_search)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n, d = X.shape
+    ctx = context(device)
+    opts = _knn_opts(precision=precision)
+    nq = max(int(q_end) - int(q_begin), 0)
+    idx = np.zeros((nq, k + 1), np.uint32)
+    d2 = np.zeros((nq, k + 1), np.float32)
+    _check(lib().sc_knn_search(ctx.h, _ptr(X, _lib.f32p), n, d, k, int(q_begin), int(q_end), C.byref(opts),
+                               _ptr(idx, _lib.u32p), _ptr(d2, _lib.f32p)), ctx)
+    return idx, d2
+
+
+def knn_connectivities(index, d2, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_ID, squared: bool = False,
+                       build_graph: bool = False, device: int | None = None) -> NeighborResult:
+    """Connectivities from the gathered (n, k+1) lists of knn_search
+    (sc_knn_connectivities); distances in the result follow `squared`."""
+    index = np.ascontiguousarray(index, dtype=np.uint32)
+    d2 = np.ascontiguousarray(d2, dtype=np.float32)
+    n, k1 = index.shape
+    k = k1 - 1
+    ctx = context(device)
+    opts = _knn_opts(sigma, sym, KNN_BF16, squared)
+    cap = 2 * n * k
+    ptrs = np.zeros(n + 1, np.uint64)
+    nbrs = np.zeros(max(cap, 1), np.uint32)
+    w = np.zeros(max(cap, 1), np.float32)
+    nnz = C.c_uint64()
+    gh = C.c_void_p()
+    _check(lib().sc_knn_connectivities(ctx.h, _ptr(index, _lib.u32p), _ptr(d2, _lib.f32p), n, k, C.byref(opts),
+                                       _ptr(ptrs, _lib.u64p), _ptr(nbrs, _lib.u32p), _ptr(w, _lib.f32p), cap,
+                                       C.byref(nnz), C.byref(gh) if build_graph else None), ctx)
+    m = nnz.value
+    dist = d2 if squared else np.sqrt(d2)
+    return NeighborResult(index, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), CSRNetwork(gh, ctx) if build_graph else None)
+
+
+__all__ += ["knn_search", "knn_connectivities"]
 __all__ += ["knn_gaussian", "NeighborResult", "SIGMA_MEDIAN", "SIGMA_KTH", "SYM_LOWER_ID", "SYM_UNION",
             "KNN_FP32", "KNN_BF16", "KNN_FP8"]

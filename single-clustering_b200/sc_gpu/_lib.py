@@ -117,6 +117,10 @@ SIGNATURES = [
     ("sc_knn_opts_default", None, [C.POINTER(KnnOpts)]),
     ("sc_knn_gaussian", C.c_int, [vp, f32p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(KnnOpts), u32p,
                                   f32p, u64p, u32p, f32p, C.c_uint64, u64p, vpp]),
+    ("sc_knn_search", C.c_int, [vp, f32p, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64, C.c_uint64,
+                                C.POINTER(KnnOpts), u32p, f32p]),
+    ("sc_knn_connectivities", C.c_int, [vp, u32p, f32p, C.c_uint64, C.c_uint64, C.POINTER(KnnOpts), u64p, u32p,
+                                        f32p, C.c_uint64, u64p, vpp]),
     ("sc_mlp_param_count", C.c_uint32, []),
     ("sc_mlp_feature_count", C.c_uint32, []),
     ("sc_mlp_create", C.c_int, [vp, C.c_uint64, vpp]),
@@ -125,7 +129,7 @@ SIGNATURES = [
     ("sc_mlp_set", C.c_int, [vp, vp, f32p, f32p]),
     ("sc_mlp_features", C.c_int, [vp, vp, vp, C.c_double, f32p, u32p, u32p, C.c_uint64, u64p]),
     ("sc_mlp_train", C.c_int, [vp, vp, vp, u64p, C.c_uint64, C.c_double, C.c_uint32, C.c_double, f64p, f32p]),
-    ("sc_mlp_propose", C.c_int, [vp, vp, vp, C.c_double, C.c_double, u64p, u64p, f32p, C.c_uint64]),
+    ("sc_mlp_propose", C.c_int, [vp, vp, vp, C.c_double, C.c_double, C.c_double, u64p, u64p, f32p, C.c_uint64]),
 ]
 
 _lib = None

@@ -101,14 +101,16 @@ class EdgeMlp:
                                   None if grad is None else grad.ctypes.data_as(_lib.f32p)), self._ctx)
         return (loss.value, grad) if return_grad else loss.value
 
-    def propose(self, graph, resolution: float, threshold: float = 0.9, return_prob: bool = False):
-        """Initial membership (connected components of edges with p > threshold)."""
+    def propose(self, graph, resolution: float, threshold: float = 0.9, core_fraction: float = 1.0,
+                return_prob: bool = False):
+        """Initial membership: components of the confident edges (p > threshold)
+        between core nodes (>= core_fraction of their edges confident)."""
         n = graph.node_count()
         labels = np.zeros(n, np.uint64)
         k = C.c_uint64()
         prob = np.zeros(max(graph.entry_count(), 1), np.float32) if return_prob else None
         _check(lib().sc_mlp_propose(self._ctx.h, self._h, graph._h, float(resolution), float(threshold),
-                                    labels.ctypes.data_as(_lib.u64p), C.byref(k),
+                                    float(core_fraction), labels.ctypes.data_as(_lib.u64p), C.byref(k),
                                     None if prob is None else prob.ctypes.data_as(_lib.f32p),
                                     0 if prob is None else prob.size), self._ctx)
         if return_prob:
@@ -130,15 +132,15 @@ class WarmStartResult:
     proposal_clusters: int
 
 
-def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, judge: bool = True,
-                      tolerance: float = 1e-4) -> WarmStartResult:
+def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
+                      judge: bool = True, tolerance: float = 1e-4) -> WarmStartResult:
     """leiden_from(model's proposal). With `judge`, the plain singleton start also
     runs and the proposal is kept only if its final modularity is at least the
     plain one minus `tolerance`; otherwise the plain result is returned."""
     from . import leiden, leiden_from, modularity, Rb
     gamma = config.objective.resolution if isinstance(config.objective, Rb) else 1.0
     t0 = time.perf_counter()
-    prop, kprop = model.propose(graph, gamma, threshold)
+    prop, kprop = model.propose(graph, gamma, threshold, core_fraction)
     t_prop = (time.perf_counter() - t0) * 1e3
     warm = leiden_from(graph, config, prop)
     sw = graph._ctx.run_stats()

@@ -1,4 +1,4 @@
-"""Multi-GPU sharding of independent Leiden instances.
+"""Multi-GPU sharding of independent Leiden instances and of the kNN search.
 
 A single graph does not shard (every move reads global community statistics),
 so one graph runs as replicas. A resolution x seed sweep or a set of many
@@ -7,6 +7,10 @@ instances) are dealt to ranks by estimated cost, each rank runs its share on
 its own GPU with `leiden_batch`, and the labels are gathered with one
 all-gather of Python objects over the process group (NCCL over NVLink between
 GPUs, gloo on CPU). No collective runs inside a Leiden run.
+
+The kNN search shards by query rows: every rank holds all points, searches
+its contiguous block of rows (`knn_search`), and one all-gather of the k+1
+lists lets every rank build the connectivities (`knn_connectivities`).
 """
 from __future__ import annotations
 
@@ -66,3 +70,29 @@ def run_sharded(run_local: Callable, n_instances: int, warm_from: Sequence[int],
         for g, r in zip(ids, res):
             out[g] = r
     return out
+
+
+def row_blocks(n: int, world: int) -> list:
+    """Contiguous query-row blocks [begin, end) per rank, sizes differing by at most one."""
+    base, extra = divmod(n, world)
+    out, b = [], 0
+    for r in range(world):
+        e = b + base + (1 if r < extra else 0)
+        out.append((b, e))
+        b = e
+    return out
+
+
+def knn_sharded(search: Callable, n: int, rank: int, world: int, group=None):
+    """search(begin, end) -> (index (end-begin, k+1), squared distances) for this
+    rank's rows; returns the (n, k+1) lists of all rows on every rank."""
+    import numpy as np
+    b, e = row_blocks(n, world)[rank]
+    idx, d2 = search(b, e)
+    if world == 1:
+        return idx, d2
+    import torch.distributed as dist
+    gathered = [None] * world
+    dist.all_gather_object(gathered, (b, idx, d2), group=group)
+    gathered.sort(key=lambda t: t[0])
+    return np.concatenate([g[1] for g in gathered]), np.concatenate([g[2] for g in gathered])

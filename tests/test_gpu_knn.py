@@ -74,3 +74,30 @@ def test_squared_kiddo_semantics():
     b = sc_gpu.knn_gaussian(X, 8, squared=True)
     assert np.array_equal(a.index, b.index)
     assert np.allclose(b.distances, a.distances.astype(np.float64) ** 2, rtol=1e-5)
+
+
+@pytest.mark.parametrize("n,d,world", [(3000, 30, 3), (1000, 50, 2), (257, 7, 4)])
+def test_row_sharded_search_equals_single_build(n, d, world):
+    """The multi-GPU split (each rank searches a block of query rows, the lists
+    are gathered, connectivities built once) gives the single build's bits."""
+    from sc_gpu import parallel
+    X, _ = synth.gaussian_mixture(n, d, 8, seed=13, sigma=(0.7, 1.5))
+    k = 10
+    full = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
+    parts = [sc_gpu.knn_search(X, k, b, e) for b, e in parallel.row_blocks(n, world)]
+    idx = np.concatenate([p[0] for p in parts])
+    d2 = np.concatenate([p[1] for p in parts])
+    assert np.array_equal(idx, full.index)
+    assert np.array_equal(np.sqrt(d2), full.distances)
+    r = sc_gpu.knn_connectivities(idx, d2, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
+    assert np.array_equal(r.conn_ptrs, full.conn_ptrs)
+    assert np.array_equal(r.conn_nbrs, full.conn_nbrs)
+    assert np.array_equal(r.conn_w.view(np.uint32), full.conn_w.view(np.uint32))
+
+
+def test_search_rejects_rows_outside_the_points():
+    X, _ = synth.gaussian_mixture(100, 5, 2, seed=1)
+    with pytest.raises(sc_gpu.ClusteringError):
+        sc_gpu.knn_search(X, 5, 50, 101)
+    idx, d2 = sc_gpu.knn_search(X, 5, 40, 40)
+    assert idx.shape == (0, 6)

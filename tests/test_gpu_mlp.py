@@ -6,8 +6,8 @@
   entry (plus the loss within 1e-5 relative);
 * training: Adam steps on the GPU lower the loss and are bit-for-bit
   deterministic for a fixed seed;
-* proposal: components of the thresholded GPU probabilities equal the oracle's
-  components of the same probabilities;
+* proposal: components of the confident edges between core nodes, from the
+  GPU probabilities, equal the oracle's from the same probabilities;
 * gain: trained on plain-GPU Leiden partitions at RB {0.5, 1, 2}, the proposal
   used as a warm start at RB {0.8, 1.5} needs fewer local-moving sweeps than the
   plain singleton start, with final modularity >= plain - 1e-4 or the judge
@@ -101,10 +101,10 @@ def test_proposal_is_components_of_confident_edges():
     m = EdgeMlp(seed=2)
     m.train(g, labels, 1.0, epochs=60, lr=1e-2)
     feat, ei, ej = m.features(g, 1.0)
-    for thr in (0.5, 0.9, 2.0):
-        lab, k, prob = m.propose(g, 1.0, thr, return_prob=True)
+    for thr, phi in ((0.5, 0.0), (0.9, 0.0), (0.9, 1.0), (0.8, 0.75), (2.0, 1.0)):
+        lab, k, prob = m.propose(g, 1.0, thr, phi, return_prob=True)
         prob = prob[:len(ei)]
-        want = mo.components(g.node_count(), ei, ej, prob > thr)
+        want = mo.components(g.node_count(), ei, ej, mo.core_mask(g.node_count(), ei, ej, prob, thr, phi))
         assert np.array_equal(lab, want)
         assert k == int(want.max()) + 1
     # probabilities agree with the oracle forward at the BF16 weights
@@ -138,7 +138,7 @@ def test_warm_start_gain_over_plain_start():
     saved = []
     for gamma in (0.8, 1.5):
         cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=9)
-        res = warm_start_leiden(m, g, cfg, threshold=0.9)
+        res = warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=1.0)
         assert res.q_warm >= res.q_plain - 1e-4 or not res.used_proposal
         final_q = sc_gpu.modularity(g, res.labels, gamma)
         assert final_q >= res.q_plain - 1e-4

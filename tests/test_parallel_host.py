@@ -1,6 +1,8 @@
-"""Host logic of multi-GPU sweep sharding, on CPU: the dealing rules, and two
-gloo ranks that shard a sweep, run their shares with the CPU oracle standing in
-for the GPU runner, and all-gather the labels."""
+"""Host logic of multi-GPU sharding, on CPU: the dealing rules; two gloo ranks
+that shard a sweep, run their shares with the CPU oracle standing in for the
+GPU runner, and all-gather the labels; two gloo ranks that split a kNN search
+by query rows (FP64 oracle search standing in for sc_knn_search) and gather
+the lists."""
 import os
 import socket
 
@@ -75,3 +77,44 @@ def test_two_gloo_ranks_gather_the_same_sweep():
         assert p.exitcode == 0
     assert out[0] == out[1]
     assert len(out[0]) == 9 and all(k >= 1 for k, _ in out[0])
+
+
+def test_row_blocks_cover_rows_once():
+    for n, world in ((10, 3), (7, 8), (0, 2), (1_000_003, 8)):
+        blocks = parallel.row_blocks(n, world)
+        assert len(blocks) == world and blocks[0][0] == 0 and blocks[-1][1] == n
+        assert all(a[1] == b[0] for a, b in zip(blocks, blocks[1:]))
+        sizes = [e - b for b, e in blocks]
+        assert max(sizes) - min(sizes) <= 1
+
+
+def _knn_rank_main(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    import knn_oracle as K
+    rng = np.random.default_rng(3)
+    X = rng.normal(size=(301, 5)).astype(np.float32)
+    full_idx, full_d = K.knn_exact(X, 6)
+
+    def search(b, e):
+        return full_idx[b:e].astype(np.uint32), (full_d[b:e] ** 2).astype(np.float32)
+
+    idx, d2 = parallel.knn_sharded(search, len(X), rank, world)
+    q.put((rank, idx.tolist(), d2.tolist(), full_idx.tolist()))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_gather_the_knn_lists():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_knn_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = {r: (i, d, f) for r, i, d, f in (q.get(timeout=120) for _ in procs)}
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert out[0][0] == out[1][0] and out[0][1] == out[1][1]
+    assert out[0][0] == out[0][2]
