@@ -111,6 +111,23 @@ typedef struct sc_run_stats {
     double alg_bytes_aggregate;
 } sc_run_stats;
 
+/*
+ * Launch tuning of a context (no counterpart in single-clustering). Nodes of
+ * degree <= lanes8_max_degree are scored by groups of 8 lanes, <= lanes16 by 16,
+ * <= lanes32 by 32, the rest by a warp, a block or (past 1024) a block with a
+ * global-memory table; a batch of at most small_batch nodes of degree <= 256 is
+ * scored by the warp kernel in one launch. Every routing gives the same
+ * decisions (the kernels score the same candidates with the same arithmetic and
+ * tie rule), so tuning changes speed only, never labels.
+ * Limits: lanes8 <= 8, lanes8 <= lanes16 <= 16, lanes16 <= lanes32 <= 32.
+ */
+typedef struct sc_tuning {
+    uint32_t lanes8_max_degree;   /* default 8  */
+    uint32_t lanes16_max_degree;  /* default 16 */
+    uint32_t lanes32_max_degree;  /* default 32 */
+    uint32_t small_batch;         /* default 4096 */
+} sc_tuning;
+
 typedef struct sc_ctx sc_ctx;
 typedef struct sc_graph sc_graph;
 
@@ -126,6 +143,19 @@ sc_status sc_last_run_stats(const sc_ctx* ctx, sc_run_stats* out);
 sc_status sc_ctx_synchronize(sc_ctx* ctx);
 /* LeidenConfig::default() (src/community_search/leiden/mod.rs:92-106). */
 void sc_leiden_config_default(sc_leiden_config* cfg);
+
+void sc_tuning_default(sc_tuning* t);
+sc_status sc_get_tuning(const sc_ctx* ctx, sc_tuning* out);
+/* Validates the limits above (SC_E_INVALID_ARGUMENT otherwise). */
+sc_status sc_set_tuning(sc_ctx* ctx, const sc_tuning* t);
+/*
+ * Autotuner: times the first level of `cfg` (one pass, one level: the level
+ * that dominates a run) on g under each candidate routing, keeps the fastest
+ * on the context and returns it with its time and the default's (device time,
+ * ms). n_candidates (nullable) receives how many were timed.
+ */
+sc_status sc_autotune(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg, sc_tuning* chosen,
+                      double* ms_chosen, double* ms_default, uint32_t* n_candidates);
 
 /* ---- graph construction ------------------------------------------------- */
 /*

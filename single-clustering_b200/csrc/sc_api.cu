@@ -163,6 +163,36 @@ sc_status sc_last_run_stats(const sc_ctx* ctx, sc_run_stats* out) {
     return SC_OK;
 }
 
+void sc_tuning_default(sc_tuning* t) {
+    if (t) *t = sc_tuning{8, 16, 32, 4096};
+}
+
+sc_status sc_get_tuning(const sc_ctx* ctx, sc_tuning* out) {
+    if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
+    *out = ctx->c.tuning;
+    return SC_OK;
+}
+
+sc_status sc_set_tuning(sc_ctx* ctx, const sc_tuning* t) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(t != nullptr, "tuning is NULL");
+        if (!sc::tuning_valid(*t))
+            sc::fail(SC_E_INVALID_ARGUMENT, "tuning limits must satisfy lanes8 <= 8, lanes8 <= lanes16 <= 16, "
+                                            "lanes16 <= lanes32 <= 32");
+        c.tuning = *t;
+    });
+}
+
+sc_status sc_autotune(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg, sc_tuning* chosen,
+                      double* ms_chosen, double* ms_default, uint32_t* n_candidates) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g && cfg, "graph or config is NULL");
+        require_same_device(c, *g->g);
+        const uint32_t k = sc::autotune(c, *g->g, *cfg, chosen, ms_chosen, ms_default);
+        if (n_candidates) *n_candidates = k;
+    });
+}
+
 sc_status sc_ctx_synchronize(sc_ctx* ctx) {
     return guarded(ctx, [&](sc::Ctx& c) { SC_CUDA(cudaStreamSynchronize(c.stream)); });
 }

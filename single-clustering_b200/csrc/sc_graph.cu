@@ -823,6 +823,418 @@ __global__ void k_row_assemble(const uint64_t* __restrict__ ptr, const uint64_t*
 }  // namespace
 
 // aggregate (csr_network.rs:516-608): d_grp holds ids already normalised to [0, G).
+// ------------------------------------------------------------ aggregate, exact regime
+// In the exact regime every (g, h) accumulator of aggregate (csr_network.rs:
+// 516-608) is a subset sum of stored weights and exact in f64 whatever the
+// order. On a graph whose stored weights are bitwise symmetric, the (h, g)
+// value the reference mirrors from row h's upper part equals row g's own sum
+// over its members' entries into h. So each coarse row is built from its own
+// members: a hash of h -> sum per row (a warp per row up to AGG_WARP_CAP
+// member entries, a block per larger row with the table in global memory),
+// then the kept entries in ascending h. Same values, same order, no global
+// sort of the E entries.
+namespace {
+
+constexpr uint64_t AGG_WARP_CAP = 256;
+constexpr int AGG_WARPS = 4;
+constexpr uint32_t AGG_EMPTY = 0xFFFFFFFFu;
+
+// Whether every stored entry (v, u, w) has its mirror (u, v) with the same bits.
+__global__ void k_symmetric_bits(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                 const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
+                                 unsigned* bad) {
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
+         e += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t v = erow[e], u = nbr[e];
+        uint64_t lo = ptr[u], hi = ptr[u + 1];
+        const uint64_t end = hi;
+        while (lo < hi) {
+            const uint64_t mid = (lo + hi) >> 1;
+            if (nbr[mid] < v) lo = mid + 1;
+            else hi = mid;
+        }
+        if (!(lo < end && nbr[lo] == v && __float_as_uint(w[lo]) == __float_as_uint(w[e]))) *bad = 1u;
+    }
+}
+
+// cap[g] = stored entries of g's members (an upper bound on its coarse row).
+__global__ void k_row_caps(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members, uint64_t G,
+                           const uint64_t* __restrict__ ptr, uint64_t* cap) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = warp; g < G; g += nwarps) {
+        uint64_t s = 0;
+        for (uint64_t i = gstart[g] + lane; i < gstart[g + 1]; i += 32) {
+            const uint32_t v = members[i];
+            s += ptr[v + 1] - ptr[v];
+        }
+        for (int o = 16; o; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+        if (lane == 0) cap[g] = s;
+    }
+}
+
+__device__ __forceinline__ uint32_t agg_hash(uint32_t h) { return h * 0x9E3779B1u; }
+
+// Adds x to h's slot of an open-addressing table of `size` slots (size > the
+// number of distinct keys, so a free slot always exists; the probe count is
+// bounded all the same).
+__device__ __forceinline__ void agg_insert(uint32_t* keys, double* vals, uint64_t size, uint32_t h, double x,
+                                           uint32_t* status) {
+    uint64_t s = agg_hash(h) % size;
+    for (uint64_t probe = 0; probe < size; ++probe) {
+        const uint32_t prev = atomicCAS(keys + s, AGG_EMPTY, h);
+        if (prev == AGG_EMPTY || prev == h) {
+            atomicAdd(vals + s, x);
+            return;
+        }
+        s = s + 1 == size ? 0 : s + 1;
+    }
+    atomicOr(status, DEV_OVERFLOW);
+}
+
+// Value and keep flag of the (g, h) entry (seg_emit's rule).
+__device__ __forceinline__ float agg_value(uint32_t g, uint32_t h, double acc, const double* __restrict__ loops,
+                                           bool* keep) {
+    const float val = h == g ? __double2float_rn(__dmul_rn(0.5, __dadd_rn(acc, loops[g]))) : __double2float_rn(acc);
+    *keep = acc > 0.0 && (double)val != 0.0;
+    return val;
+}
+
+// The member entries of one group, flattened across the 32 lanes: calls
+// f(j) for every stored entry j of every member, in no particular order.
+template <class F>
+__device__ __forceinline__ void warp_member_entries(const uint64_t* __restrict__ ptr,
+                                                    const uint32_t* __restrict__ members, uint64_t m0, uint64_t m1,
+                                                    F&& f) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31;
+    for (uint64_t mb = m0; mb < m1; mb += 32) {
+        const uint64_t mi = mb + lane;
+        uint64_t b = 0, d = 0;
+        if (mi < m1) {
+            const uint32_t v = members[mi];
+            b = ptr[v];
+            d = ptr[v + 1] - b;
+        }
+        uint64_t incl = d;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(FULL, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const uint64_t excl = incl - d;
+        const uint64_t total = __shfl_sync(FULL, incl, 31);
+        for (uint64_t base = 0; base < total; base += 32) {
+            const uint64_t t = base + lane;
+            int L = 0;
+            for (int step = 16; step; step >>= 1) {
+                const uint64_t e = __shfl_sync(FULL, excl, L + step);
+                if (e <= t) L += step;
+            }
+            const uint64_t eL = __shfl_sync(FULL, excl, L), bL = __shfl_sync(FULL, b, L);
+            if (t < total) f(bL + (t - eL));
+        }
+    }
+}
+
+__global__ void __launch_bounds__(32 * AGG_WARPS)
+    k_contract_warp(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members, uint64_t G,
+                    const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                    const float* __restrict__ w, const uint32_t* __restrict__ grp, const uint64_t* __restrict__ cap,
+                    const uint64_t* __restrict__ capstart, const double* __restrict__ loops, uint32_t* tnbr,
+                    float* tw, uint32_t* cnt, uint32_t* status) {
+    __shared__ uint32_t s_keys[AGG_WARPS][2 * AGG_WARP_CAP];
+    __shared__ double s_vals[AGG_WARPS][2 * AGG_WARP_CAP];
+    __shared__ uint32_t s_lk[AGG_WARPS][AGG_WARP_CAP];
+    __shared__ float s_lw[AGG_WARPS][AGG_WARP_CAP];
+    const unsigned FULL = 0xFFFFFFFFu;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    uint32_t* keys = s_keys[wib];
+    double* vals = s_vals[wib];
+    uint32_t* lk = s_lk[wib];
+    float* lw = s_lw[wib];
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = warp; g < G; g += nwarps) {
+        const uint64_t cg = cap[g];
+        if (cg > AGG_WARP_CAP) continue;  // warp-uniform: a block-kernel row
+        uint64_t size = 64;
+        while (size < 2 * cg) size <<= 1;
+        for (uint64_t s = lane; s < size; s += 32) {
+            keys[s] = AGG_EMPTY;
+            vals[s] = 0.0;
+        }
+        __syncwarp();
+        warp_member_entries(ptr, members, gstart[g], gstart[g + 1], [&](uint64_t j) {
+            agg_insert(keys, vals, size, grp[nbr[j]], (double)w[j], status);
+        });
+        __syncwarp();
+        uint32_t nk = 0;
+        for (uint64_t s0 = 0; s0 < size; s0 += 32) {
+            const uint64_t s = s0 + lane;
+            const uint32_t h = keys[s];
+            bool keep = false;
+            float val = 0.0f;
+            if (h != AGG_EMPTY) val = agg_value((uint32_t)g, h, vals[s], loops, &keep);
+            const unsigned bal = __ballot_sync(FULL, keep);
+            if (keep) {
+                const uint32_t pos = nk + __popc(bal & ((1u << lane) - 1u));
+                lk[pos] = h;
+                lw[pos] = val;
+            }
+            nk += __popc(bal);
+        }
+        __syncwarp();
+        const uint64_t o = capstart[g];
+        for (uint32_t i = lane; i < nk; i += 32) {
+            const uint32_t h = lk[i];
+            uint32_t r = 0;
+            for (uint32_t j = 0; j < nk; ++j) r += lk[j] < h;
+            tnbr[o + r] = h;
+            tw[o + r] = lw[i];
+        }
+        if (lane == 0) cnt[g] = nk;
+        __syncwarp();
+    }
+}
+
+// One block per large row; its table is `2 cap` slots of the global scratch at
+// hoff[i]. Kept entries are written unsorted; a segmented sort follows.
+__global__ void __launch_bounds__(256)
+    k_contract_block(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ hoff,
+                     const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
+                     const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                     const float* __restrict__ w, const uint32_t* __restrict__ grp, const uint64_t* __restrict__ cap,
+                     const uint64_t* __restrict__ capstart, const double* __restrict__ loops, uint32_t* hkeys,
+                     double* hvals, uint32_t* tnbr, float* tw, uint32_t* cnt, uint32_t* status) {
+    __shared__ unsigned long long s_n;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
+        const uint32_t g = rows[i];
+        const uint64_t size = 2 * cap[g];
+        uint32_t* keys = hkeys + hoff[i];
+        double* vals = hvals + hoff[i];
+        for (uint64_t s = threadIdx.x; s < size; s += blockDim.x) {
+            keys[s] = AGG_EMPTY;
+            vals[s] = 0.0;
+        }
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        // members dealt to the warps in chunks of 32
+        const uint64_t m0 = gstart[g], m1 = gstart[g + 1];
+        for (uint64_t mb = m0 + (uint64_t)wib * 32; mb < m1; mb += (uint64_t)nw * 32) {
+            const uint64_t me = mb + 32 < m1 ? mb + 32 : m1;
+            warp_member_entries(ptr, members, mb, me, [&](uint64_t j) {
+                agg_insert(keys, vals, size, grp[nbr[j]], (double)w[j], status);
+            });
+        }
+        __syncthreads();
+        const uint64_t o = capstart[g];
+        for (uint64_t s = threadIdx.x; s < size; s += blockDim.x) {
+            const uint32_t h = keys[s];
+            if (h == AGG_EMPTY) continue;
+            bool keep;
+            const float val = agg_value(g, h, vals[s], loops, &keep);
+            if (keep) {
+                const unsigned long long pos = atomicAdd(&s_n, 1ull);
+                tnbr[o + pos] = h;
+                tw[o + pos] = val;
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) cnt[g] = (uint32_t)s_n;
+        __syncthreads();
+        (void)lane;
+    }
+}
+
+__global__ void k_flag_large(const uint64_t* __restrict__ cap, uint64_t G, uint8_t* flag, uint64_t* hcap) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const bool large = cap[g] > AGG_WARP_CAP;
+        flag[g] = large;
+        hcap[g] = large ? 2 * cap[g] : 0;
+    }
+}
+
+__global__ void k_gather_u64(const uint32_t* __restrict__ idx, uint64_t n, const uint64_t* __restrict__ src,
+                             uint64_t* dst) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        dst[i] = src[idx[i]];
+}
+
+__global__ void k_segments_of(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ capstart,
+                              const uint32_t* __restrict__ cnt, uint64_t* sb, uint64_t* se) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nrows;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t g = rows[i];
+        sb[i] = capstart[g];
+        se[i] = capstart[g] + cnt[g];
+    }
+}
+
+__global__ void k_copy_segments(const uint64_t* __restrict__ sb, const uint64_t* __restrict__ se, uint64_t nseg,
+                                const uint32_t* __restrict__ kin, const float* __restrict__ vin, uint32_t* kout,
+                                float* vout) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < nseg; i += nwarps)
+        for (uint64_t j = sb[i] + lane; j < se[i]; j += 32) {
+            kout[j] = kin[j];
+            vout[j] = vin[j];
+        }
+}
+
+// Final rows: ptr from the kept counts, entries copied from the row slots.
+__global__ void k_pack_rows(const uint64_t* __restrict__ optr, const uint64_t* __restrict__ capstart, uint64_t G,
+                            const uint32_t* __restrict__ tnbr, const float* __restrict__ tw, uint32_t* nbr,
+                            float* w) {
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t g = warp; g < G; g += nwarps) {
+        const uint64_t o = optr[g], len = optr[g + 1] - o, src = capstart[g];
+        for (uint64_t j = lane; j < len; j += 32) {
+            nbr[o + j] = tnbr[src + j];
+            w[o + j] = tw[src + j];
+        }
+    }
+}
+
+__global__ void k_u32_to_u64(const uint32_t* __restrict__ a, uint64_t n, uint64_t* b) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x)
+        b[i] = i < n ? a[i] : 0;
+}
+
+}  // namespace
+
+// Whether g's stored weights are bitwise symmetric (cached on the graph).
+bool graph_bitwise_symmetric(Ctx& c, const DevGraph& g) {
+    int st = g.sym_state.load(std::memory_order_relaxed);
+    if (st != 0) return st == 1;
+    DBuf<unsigned> bad(c, 1);
+    zero(c, bad.get(), 1);
+    if (g.E) {
+        k_symmetric_bits<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, bad.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    const bool sym = to_host(c, bad.get()) == 0;
+    g.sym_state.store(sym ? 1 : 2, std::memory_order_relaxed);
+    return sym;
+}
+
+namespace {
+
+DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint64_t G, const uint64_t* gstart,
+                         const uint32_t* members, const double* nw_new, const double* loops) {
+    std::unique_ptr<DevGraph> out(new DevGraph());
+    DBuf<uint64_t> cap(c, G + 1), capstart(c, G + 1);
+    zero(c, cap.get() + G, 1);
+    if (G) {
+        k_row_caps<<<grid_for(G * 32, TB), TB, 0, c.stream>>>(gstart, members, G, g.ptr, cap.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    exclusive_sum(c, cap.get(), capstart.get(), G + 1);  // capstart[G] = E
+    DBuf<uint32_t> tnbr(c, g.E), cnt(c, G + 1);
+    DBuf<float> tw(c, g.E);
+    zero(c, cnt.get(), G + 1);
+    // large rows: list, table offsets, table size
+    DBuf<uint8_t> flag(c, G);
+    DBuf<uint64_t> hcap(c, G), nl(c, 1);
+    DBuf<uint32_t> iota(c, G), rows(c, G);
+    uint64_t nlarge = 0;
+    if (G) {
+        k_flag_large<<<grid_for(G, TB), TB, 0, c.stream>>>(cap.get(), G, flag.get(), hcap.get());
+        k_iota<<<grid_for(G, TB), TB, 0, c.stream>>>(iota.get(), G);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+        select_flagged(c, iota.get(), flag.get(), rows.get(), nl.get(), G);
+        nlarge = to_host(c, nl.get());
+    }
+    if (G) {
+        const unsigned grid = grid_for(G * 32, 32 * AGG_WARPS, 148u * 16u);
+        k_contract_warp<<<grid, 32 * AGG_WARPS, 0, c.stream>>>(gstart, members, G, g.ptr, g.nbr, g.w, d_grp,
+                                                               cap.get(), capstart.get(), loops, tnbr.get(), tw.get(),
+                                                               cnt.get(), c.d_status);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    if (nlarge) {
+        DBuf<uint64_t> lh(c, nlarge + 1), hoff(c, nlarge + 1);
+        k_gather_u64<<<grid_for(nlarge, TB), TB, 0, c.stream>>>(rows.get(), nlarge, hcap.get(), lh.get());
+        zero(c, lh.get() + nlarge, 1);
+        exclusive_sum(c, lh.get(), hoff.get(), nlarge + 1);
+        const uint64_t hsize = to_host(c, hoff.get() + nlarge);
+        DBuf<uint32_t> hkeys(c, hsize);
+        DBuf<double> hvals(c, hsize);
+        const unsigned grid = (unsigned)std::min<uint64_t>(nlarge, (uint64_t)c.sm_count * 4);
+        k_contract_block<<<grid, 256, 0, c.stream>>>(rows.get(), nlarge, hoff.get(), gstart, members, g.ptr, g.nbr,
+                                                     g.w, d_grp, cap.get(), capstart.get(), loops, hkeys.get(),
+                                                     hvals.get(), tnbr.get(), tw.get(), cnt.get(), c.d_status);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+        // sort the large rows' kept entries by neighbour
+        DBuf<uint64_t> sb(c, nlarge), se(c, nlarge);
+        k_segments_of<<<grid_for(nlarge, TB), TB, 0, c.stream>>>(rows.get(), nlarge, capstart.get(), cnt.get(),
+                                                                 sb.get(), se.get());
+        SC_LAUNCH_CHECK();
+        DBuf<uint32_t> knbr(c, g.E);
+        DBuf<float> kw(c, g.E);
+        size_t bytes = 0;
+        SC_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, bytes, tnbr.get(), knbr.get(), tw.get(), kw.get(),
+                                                    (int64_t)g.E, (int64_t)nlarge, sb.get(), se.get(), c.stream));
+        DBuf<unsigned char> tmp(c, bytes);
+        SC_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.get(), bytes, tnbr.get(), knbr.get(), tw.get(), kw.get(),
+                                                    (int64_t)g.E, (int64_t)nlarge, sb.get(), se.get(), c.stream));
+        k_copy_segments<<<grid_for(nlarge * 32, TB), TB, 0, c.stream>>>(sb.get(), se.get(), nlarge, knbr.get(),
+                                                                        kw.get(), tnbr.get(), tw.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 4;
+    }
+    check_device_status(c);
+    // assemble
+    DBuf<uint64_t> cnt64(c, G + 1), optr(c, G + 1);
+    k_u32_to_u64<<<grid_for(G + 1, TB), TB, 0, c.stream>>>(cnt.get(), G + 1, cnt64.get());
+    exclusive_sum(c, cnt64.get(), optr.get(), G + 1);
+    const uint64_t E2 = to_host(c, optr.get() + G);
+    galloc(c, *out, G, E2);
+    d2d(c, out->ptr, optr.get(), G + 1);
+    d2d(c, out->node_w, nw_new, G);
+    if (E2) {
+        k_pack_rows<<<grid_for(G * 32, TB), TB, 0, c.stream>>>(optr.get(), capstart.get(), G, tnbr.get(), tw.get(),
+                                                               out->nbr, out->w);
+        k_fill_erow<<<grid_for(G * 32, TB), TB, 0, c.stream>>>(out->ptr, G, out->erow);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    c.launches++;
+    return out.release();
+}
+
+}  // namespace
+
+// Stats and checks of an aggregated graph; its rows mirror each other exactly.
+void finish_aggregate(Ctx& c, DevGraph& out) {
+    // aggregate cannot fail in the reference (csr_network.rs:605-607)
+    try {
+        finalize(c, out, true);
+    } catch (Failure& f) {
+        if (f.info.code == SC_E_ASYMMETRIC_GRAPH) {
+            f.info.code = SC_E_INTERNAL;
+            std::snprintf(f.info.message, sizeof f.info.message,
+                          "aggregate produced a graph failing the degree-sum check");
+        }
+        throw;
+    }
+    out.sym_state.store(1, std::memory_order_relaxed);
+    sync(c);
+}
+
 DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t G) {
     const uint64_t n = g.n, E = g.E;
     std::unique_ptr<DevGraph> out(new DevGraph());
@@ -843,6 +1255,14 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
     }
     idx.release();
     grp_s.release();
+    if (g.exact_w && graph_bitwise_symmetric(c, g)) {
+        std::unique_ptr<DevGraph> fast(contract_exact(c, g, d_grp, G, gstart.get(), members.get(), nw_new.get(),
+                                                      loops.get()));
+        members.release();
+        gstart.release();
+        finish_aggregate(c, *fast);
+        return fast.release();
+    }
     members.release();
     gstart.release();
 
@@ -964,18 +1384,7 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         }
         c.launches += 3;
     }
-    // aggregate cannot fail in the reference (csr_network.rs:605-607)
-    try {
-        finalize(c, *out, true);
-    } catch (Failure& f) {
-        if (f.info.code == SC_E_ASYMMETRIC_GRAPH) {
-            f.info.code = SC_E_INTERNAL;
-            std::snprintf(f.info.message, sizeof f.info.message,
-                          "aggregate produced a graph failing the degree-sum check");
-        }
-        throw;
-    }
-    sync(c);
+    finish_aggregate(c, *out);
     return out.release();
 }
 

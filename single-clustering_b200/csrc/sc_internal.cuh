@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <memory>
@@ -69,6 +70,7 @@ struct Ctx {
     uint64_t launches = 0;             // kernels launched by the current call
     int sm_count = 148;
     size_t smem_optin = 0;
+    sc_tuning tuning{8, 16, 32, 4096};  // decide-kernel routing (sc_set_tuning / sc_autotune)
 };
 
 // Stream-ordered device buffer of T (cudaMallocAsync on the context stream).
@@ -141,6 +143,9 @@ struct DevGraph {
     bool exact_nw = true;
     double total_node_weight = 0.0;  // Σ node_w, Rust `sum()` order
     uint64_t n_hubs = 0;      // nodes whose degree exceeds the shared-memory hash
+    // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
+    // once, on first need; a benign race between contexts computes it twice)
+    mutable std::atomic<int> sym_state{0};
     // Arrays come from the stream-ordered pool. A graph owned by a running call
     // (a coarse level) returns them on that stream; a graph handed to the user
     // (stream == nullptr) frees them with cudaFree.
@@ -212,6 +217,7 @@ DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint6
                            const double* w, uint64_t m, const double* node_w);
 DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t n_groups);
 void graph_validate_symmetry(Ctx& c, const DevGraph& g);
+bool graph_bitwise_symmetric(Ctx& c, const DevGraph& g);
 void graph_copy_csr(Ctx& c, const DevGraph& g, uint64_t* ptr, uint32_t* nbr, float* w);
 void graph_copy_node_data(Ctx& c, const DevGraph& g, double* node_w, double* strength);
 
@@ -247,6 +253,10 @@ struct LeidenOut {
 };
 void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64_t* initial_host,
             uint32_t* d_labels_out, uint64_t* n_clusters);
+bool tuning_valid(const sc_tuning& t);
+// Times the first level under candidate routings, keeps the fastest on c.
+uint32_t autotune(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, sc_tuning* chosen, double* ms_chosen,
+                  double* ms_default);
 
 // knn.cu
 void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k,

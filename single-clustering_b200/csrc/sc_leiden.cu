@@ -160,7 +160,8 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 // the constraint, randomised choice among non-negative candidates).
 template <int G, bool REFINE>
 __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t* __restrict__ list,
-                                                     uint32_t count) {
+                                                        const uint64_t* __restrict__ lbeg,
+                                                        const uint32_t* __restrict__ ldeg, uint32_t count) {
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31;
     const int sub = lane & (G - 1);
@@ -178,8 +179,8 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
         const uint32_t v = have ? ro(list + (i)) : 0;
         uint64_t b = 0, e = 0;
         if (have) {
-            b = ro(p.ptr + (v));
-            e = ro(p.ptr + (v + 1));
+            b = ro(lbeg + i);
+            e = b + ro(ldeg + i);
         }
         const int deg = (int)(e - b);
         const uint32_t own = have ? ro(p.memb + (v)) : 0;
@@ -387,6 +388,8 @@ __device__ void block_argmax(double& g, uint32_t& c, double* sg, uint32_t* sc) {
 // by every lane over its slots, warp argmax.
 template <bool REFINE>
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, const uint32_t* __restrict__ list,
+                                                                      const uint64_t* __restrict__ lbeg,
+                                                                      const uint32_t* __restrict__ ldeg,
                                                                       uint32_t count) {
     __shared__ uint32_t s_keys[WARPS_PER_BLOCK][WCAP];
     __shared__ long long s_vals[WARPS_PER_BLOCK][WCAP];
@@ -399,7 +402,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = warp; i < count; i += nwarps) {
         const uint32_t v = ro(list + (i));
-        const uint64_t b = ro(p.ptr + (v)), e = ro(p.ptr + (v + 1));
+        const uint64_t b = ro(lbeg + i), e = b + ro(ldeg + i);
         const uint32_t deg = (uint32_t)(e - b);
         const uint32_t own = ro(p.memb + (v));
         if (REFINE && ro(p.csize + (own)) != 1) continue;  // warp-uniform
@@ -519,8 +522,9 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
 // grid never exceeds the number of slices.
 template <bool REFINE, bool HUB>
 __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* __restrict__ list,
-                                                     uint32_t count, uint32_t* gkeys, long long* gvals,
-                                                     uint64_t gcap) {
+                                                     const uint64_t* __restrict__ lbeg,
+                                                     const uint32_t* __restrict__ ldeg, uint32_t count,
+                                                     uint32_t* gkeys, long long* gvals, uint64_t gcap) {
     extern __shared__ __align__(16) unsigned char smem[];
     long long* s_vals = (long long*)smem;
     uint32_t* s_keys = (uint32_t*)(smem + HCAP_SMEM * sizeof(long long));
@@ -531,7 +535,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const uint32_t v = ro(list + (i));
-        const uint64_t b = ro(p.ptr + (v)), e = ro(p.ptr + (v + 1));
+        const uint64_t b = ro(lbeg + i), e = b + ro(ldeg + i);
         const uint32_t deg = (uint32_t)(e - b);
         const uint32_t own = ro(p.memb + (v));
         if (REFINE && ro(p.csize + (own)) != 1) continue;  // uniform over the block
@@ -714,12 +718,20 @@ __global__ void k_claim(Params p, const uint32_t* __restrict__ list, uint32_t co
 }
 
 // ------------------------------------------------------------ bucketing
-__device__ __forceinline__ int bucket_of(uint32_t deg) {
-    return deg <= 8 ? 0 : deg <= 16 ? 1 : deg <= 32 ? 2 : deg <= WARP_DEGREE ? 3 : deg <= HUB_DEGREE ? 4 : 5;
+// Degree buckets; the lane-group limits come from the context's tuning
+// (lanes8 <= 8 <= ..., each at most its group size). Any routing gives the same
+// decisions: every decide kernel scores the same candidates with the same
+// arithmetic and tie rule.
+struct Route {
+    uint32_t g8, g16, g32;
+};
+
+__device__ __forceinline__ int bucket_of(uint32_t deg, Route r) {
+    return deg <= r.g8 ? 0 : deg <= r.g16 ? 1 : deg <= r.g32 ? 2 : deg <= WARP_DEGREE ? 3 : deg <= HUB_DEGREE ? 4 : 5;
 }
 
 __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
-                               uint64_t n, uint64_t seed, uint32_t sweep, int B, uint32_t* counts) {
+                               uint64_t n, uint64_t seed, uint32_t sweep, int B, Route route, uint32_t* counts) {
     __shared__ uint32_t sc[64];
     for (int t = threadIdx.x; t < B * NBUCKET; t += blockDim.x) sc[t] = 0;
     __syncthreads();
@@ -727,7 +739,7 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* 
          v += (uint64_t)gridDim.x * blockDim.x) {
         if (active && !active[v]) continue;
         int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
-        int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
+        int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]), route);
         atomicAdd(&sc[b * NBUCKET + k], 1u);
     }
     __syncthreads();
@@ -737,16 +749,20 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* 
 
 // One warp-aggregated atomic per distinct (batch, bucket) per warp.
 __global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
-                                 uint64_t n, uint64_t seed, uint32_t sweep, int B, uint32_t* cursor,
-                                 uint32_t* list) {
+                                 uint64_t n, uint64_t seed, uint32_t sweep, int B, Route route,
+                                 uint32_t* cursor, uint32_t* list, uint64_t* lbeg, uint32_t* ldeg) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
         const uint64_t v = base + lane;
         int slot = -1;
+        uint64_t rb = 0;
+        uint32_t deg = 0;
         if (v < n && (!active || active[v])) {
             int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
-            int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]));
+            rb = ptr[v];
+            deg = (uint32_t)(ptr[v + 1] - rb);
+            int k = bucket_of(deg, route);
             slot = b * NBUCKET + k;
         }
         const unsigned mm = __match_any_sync(0xFFFFFFFFu, slot < 0 ? 1000 + (int)lane : slot);
@@ -754,7 +770,12 @@ __global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint8_t
         uint32_t pos0 = 0;
         if (slot >= 0 && (int)lane == leader) pos0 = atomicAdd(cursor + slot, (uint32_t)__popc(mm));
         pos0 = __shfl_sync(0xFFFFFFFFu, pos0, leader);
-        if (slot >= 0) list[pos0 + __popc(mm & ((1u << lane) - 1u))] = (uint32_t)v;
+        if (slot >= 0) {
+            const uint32_t pos = pos0 + __popc(mm & ((1u << lane) - 1u));
+            list[pos] = (uint32_t)v;
+            lbeg[pos] = rb;
+            ldeg[pos] = deg;
+        }
     }
 }
 
@@ -818,6 +839,8 @@ Scales scales_for(const DevGraph& g) {
 
 struct Workspace {
     DBuf<uint32_t> tgt, hint, from, epoch, list, moved;
+    DBuf<uint64_t> lbeg;  // row start of each list entry (written by the bucket scatter)
+    DBuf<uint32_t> ldeg;  // degree of each list entry
     DBuf<long long> dgain;
     DBuf<uint8_t> active, next_active;
     DBuf<uint32_t> counts;
@@ -861,6 +884,8 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.epoch.alloc(c, n);
     ws.moved.alloc(c, n);
     ws.list.alloc(c, n);
+    ws.lbeg.alloc(c, n);
+    ws.ldeg.alloc(c, n);
     ws.dgain.alloc(c, n);
     ws.active.alloc(c, n);
     ws.next_active.alloc(c, n);
@@ -887,29 +912,32 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
 }
 
 template <bool REFINE>
-void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list, uint32_t cnt) {
+void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32_t cnt) {
     if (!cnt) return;
+    const uint32_t* list = ws.list.get() + off;
+    const uint64_t* lbeg = ws.lbeg.get() + off;
+    const uint32_t* ldeg = ws.ldeg.get() + off;
     if (k == 0) {
         unsigned warps = (cnt + 3) / 4;
-        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 1) {
         unsigned warps = (cnt + 1) / 2;
-        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 2) {
-        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, cnt);
+        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 3) {
         const uint64_t warps = cnt;
         k_decide_warp<REFINE><<<grid_for(warps * 32, 32 * WARPS_PER_BLOCK, 148u * 64u), 32 * WARPS_PER_BLOCK, 0,
-                                c.stream>>>(p, list, cnt);
+                                c.stream>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 4) {
         size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
         unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
-        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, cnt, nullptr, nullptr, 0);
+        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, lbeg, ldeg, cnt, nullptr, nullptr, 0);
     } else {
         if (ws.nblk_large < 1 || ws.gcap == 0) fail(SC_E_INTERNAL, "hub scratch missing");
         unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
-        k_decide_block<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, cnt, ws.gkeys.get(), ws.gvals.get(),
-                                                               ws.gcap);
+        k_decide_block<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt, ws.gkeys.get(),
+                                                               ws.gvals.get(), ws.gcap);
     }
     SC_LAUNCH_CHECK();
     c.launches++;
@@ -921,17 +949,18 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, const uint32_t* list
 // decision for them as the lane-group kernels (fixed-point sums are exact in
 // any order, ties go to the lower id), and the launches saved are the cost
 // that dominates a batch of a few thousand nodes.
-constexpr uint32_t SMALL_BATCH = 4096;
+Route route_of(const Ctx& c) { return Route{c.tuning.lanes8_max_degree, c.tuning.lanes16_max_degree,
+                                             c.tuning.lanes32_max_degree}; }
 
 template <bool REFINE>
 void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs, int b) {
     const uint32_t* o = offs + b * NBUCKET;
-    if (o[4] - o[0] <= SMALL_BATCH) {
-        launch_decide<REFINE>(c, p, ws, 3, ws.list.get() + o[0], o[4] - o[0]);
-        for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, ws.list.get() + o[k], o[k + 1] - o[k]);
+    if (o[4] - o[0] <= c.tuning.small_batch) {
+        launch_decide<REFINE>(c, p, ws, 3, o[0], o[4] - o[0]);
+        for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
         return;
     }
-    for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, ws.list.get() + o[k], o[k + 1] - o[k]);
+    for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
 }
 
 struct MoveResult {
@@ -1011,7 +1040,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
         zero(c, ws.counts.get(), B * NBUCKET);
         zero(c, ws.next_active.get(), n);
-        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B,
+        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B, route_of(c),
                                                              ws.counts.get());
         SC_LAUNCH_CHECK();
         c.launches++;
@@ -1033,8 +1062,9 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         if (offs[B * NBUCKET] == 0) break;
         DBuf<uint32_t> cursor(c, 64);
         h2d(c, cursor.get(), offs, B * NBUCKET);
-        k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B,
-                                                               cursor.get(), ws.list.get());
+        k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B, route_of(c),
+                                                               cursor.get(), ws.list.get(), ws.lbeg.get(),
+                                                               ws.ldeg.get());
         SC_LAUNCH_CHECK();
         c.launches++;
         for (int b = 0; b < B; ++b) {
@@ -1128,7 +1158,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     zero(c, ws.epoch.get(), n);
     const int B = RF_BATCHES;
     zero(c, ws.counts.get(), B * NBUCKET);
-    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B,
+    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
                                                          ws.counts.get());
     SC_LAUNCH_CHECK();
     c.launches++;
@@ -1140,8 +1170,9 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
     DBuf<uint32_t> cursor(c, 64);
     h2d(c, cursor.get(), offs, B * NBUCKET);
-    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B,
-                                                           cursor.get(), ws.list.get());
+    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
+                                                           cursor.get(), ws.list.get(), ws.lbeg.get(),
+                                                           ws.ldeg.get());
     SC_LAUNCH_CHECK();
     c.launches++;
     for (int b = 0; b < B; ++b) {
@@ -1333,6 +1364,58 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
     c.stats.ms_other = c.stats.ms_total - c.stats.ms_local_move - c.stats.ms_refine - c.stats.ms_aggregate;
     c.stats.kernel_launches = c.launches;
     *n_clusters = clusters;
+}
+
+bool tuning_valid(const sc_tuning& t) {
+    return t.lanes8_max_degree <= 8 && t.lanes8_max_degree <= t.lanes16_max_degree && t.lanes16_max_degree <= 16 &&
+           t.lanes16_max_degree <= t.lanes32_max_degree && t.lanes32_max_degree <= 32;
+}
+
+uint32_t autotune(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, sc_tuning* chosen, double* ms_chosen,
+                  double* ms_default) {
+    validate_config(cfg);
+    static const sc_tuning candidates[] = {
+        {8, 16, 32, 4096},   // default
+        {0, 16, 32, 4096},   // no 8-lane groups
+        {8, 8, 32, 4096},    // no 16-lane groups
+        {8, 16, 16, 4096},   // degree 17-32 on the warp kernel
+        {0, 0, 32, 4096},    // 32-lane groups only
+        {8, 16, 32, 0},      // never fuse a small batch
+        {8, 16, 32, 1024},
+        {8, 16, 32, 16384},
+    };
+    sc_leiden_config one = cfg;
+    one.n_iterations = 1;
+    one.max_levels = 1;
+    const sc_tuning saved = c.tuning;
+    DBuf<uint32_t> lab(c, g.n);
+    uint64_t ncl = 0;
+    double best = INFINITY, def = 0.0;
+    sc_tuning pick = candidates[0];
+    try {
+        c.tuning = candidates[0];
+        leiden(c, g, one, nullptr, lab.get(), &ncl);  // warm-up: pools, caches, first-call costs
+        uint32_t k = 0;
+        for (const sc_tuning& t : candidates) {
+            c.tuning = t;
+            leiden(c, g, one, nullptr, lab.get(), &ncl);
+            const double ms = c.stats.ms_total;
+            if (k == 0) def = ms;
+            if (ms < best) {
+                best = ms;
+                pick = t;
+            }
+            ++k;
+        }
+    } catch (...) {
+        c.tuning = saved;
+        throw;
+    }
+    c.tuning = pick;
+    if (chosen) *chosen = pick;
+    if (ms_chosen) *ms_chosen = best;
+    if (ms_default) *ms_default = def;
+    return (uint32_t)(sizeof candidates / sizeof candidates[0]);
 }
 
 }  // namespace sc

@@ -522,6 +522,38 @@ def quality(graph: CSRNetwork, membership, objective: ObjectiveKind = Rb()) -> f
     return out.value
 
 
+def get_tuning(device: int | None = None) -> dict:
+    """The decide-kernel routing of this thread's context on `device`."""
+    t = _lib.Tuning()
+    ctx = context(device)
+    _check(lib().sc_get_tuning(ctx.h, C.byref(t)), ctx)
+    return {name: getattr(t, name) for name, _ in _lib.Tuning._fields_}
+
+
+def set_tuning(tuning: dict, device: int | None = None) -> None:
+    t = _lib.Tuning()
+    lib().sc_tuning_default(C.byref(t))
+    for k, v in tuning.items():
+        setattr(t, k, int(v))
+    ctx = context(device)
+    _check(lib().sc_set_tuning(ctx.h, C.byref(t)), ctx)
+
+
+def autotune(graph: CSRNetwork, config: LeidenConfig | None = None) -> dict:
+    """Times the first Leiden level under candidate routings on `graph`, keeps
+    the fastest on the graph's context; returns it with the timings (ms)."""
+    cfg = (config or LeidenConfig()).to_c()
+    t = _lib.Tuning()
+    best, default = C.c_double(), C.c_double()
+    k = C.c_uint32()
+    ctx = graph._ctx
+    _check(lib().sc_autotune(ctx.h, graph._h, C.byref(cfg), C.byref(t), C.byref(best), C.byref(default),
+                             C.byref(k)), ctx)
+    out = {name: getattr(t, name) for name, _ in _lib.Tuning._fields_}
+    out.update(ms_chosen=best.value, ms_default=default.value, candidates=k.value)
+    return out
+
+
 def last_run_stats(device: int | None = None) -> dict:
     return context(device).run_stats()
 
@@ -531,7 +563,7 @@ __all__ = [
     "leiden_batch", "modularity", "quality", "ClusteringError", "NodeIndexOutOfRange", "NonFiniteWeight",
     "NegativeWeight", "InvalidNodeWeight", "NodeWeightLengthMismatch", "MembershipLengthMismatch",
     "InvalidConfig", "TooManyNodes", "InvalidCsr", "AsymmetricGraph", "DeviceError", "MAX_NODES", "NOISE",
-    "last_run_stats", "context", "sweep_plan", "leiden_sweep",
+    "last_run_stats", "context", "sweep_plan", "leiden_sweep", "get_tuning", "set_tuning", "autotune",
 ]
 
 

@@ -72,6 +72,15 @@ class RunStats(C.Structure):
     ]
 
 
+class Tuning(C.Structure):
+    _fields_ = [
+        ("lanes8_max_degree", C.c_uint32),
+        ("lanes16_max_degree", C.c_uint32),
+        ("lanes32_max_degree", C.c_uint32),
+        ("small_batch", C.c_uint32),
+    ]
+
+
 class KnnOpts(C.Structure):
     _fields_ = [
         ("sigma", C.c_int32),
@@ -91,6 +100,11 @@ SIGNATURES = [
     ("sc_last_error_info", C.c_int, [vp, C.POINTER(ErrorInfo)]),
     ("sc_last_run_stats", C.c_int, [vp, C.POINTER(RunStats)]),
     ("sc_ctx_synchronize", C.c_int, [vp]),
+    ("sc_tuning_default", None, [C.POINTER(Tuning)]),
+    ("sc_get_tuning", C.c_int, [vp, C.POINTER(Tuning)]),
+    ("sc_set_tuning", C.c_int, [vp, C.POINTER(Tuning)]),
+    ("sc_autotune", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), C.POINTER(Tuning), f64p, f64p,
+                              C.POINTER(C.c_uint32)]),
     ("sc_leiden_config_default", None, [C.POINTER(LeidenConfigC)]),
     ("sc_graph_from_csr", C.c_int, [vp, u64p, C.c_uint64, u32p, C.c_uint64, f32p, C.c_uint64, f64p,
                                      C.c_uint64, vpp]),

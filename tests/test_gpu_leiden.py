@@ -235,3 +235,54 @@ def test_batch_matches_single_runs():
     batch = sc_gpu.leiden_batch([g] * len(cfgs), cfgs)
     for cfg, got in zip(cfgs, batch):
         assert got == sc_gpu.leiden(g, cfg)
+
+
+TUNINGS = [
+    dict(lanes8_max_degree=8, lanes16_max_degree=16, lanes32_max_degree=32, small_batch=4096),
+    dict(lanes8_max_degree=0, lanes16_max_degree=0, lanes32_max_degree=0, small_batch=0),
+    dict(lanes8_max_degree=0, lanes16_max_degree=16, lanes32_max_degree=16, small_batch=1 << 30),
+    dict(lanes8_max_degree=8, lanes16_max_degree=8, lanes32_max_degree=32, small_batch=0),
+]
+
+
+def test_tuning_never_changes_labels():
+    """Every decide-kernel routing gives the same decisions, so the labels of a
+    fixed-seed run are identical under every tuning (local moving, refinement,
+    Louvain mode, CPM, a community-weight cap)."""
+    src, dst, w, _ = synth.planted_partition(6000, 30, 10, 3, seed=9)
+    g = sc_gpu.CSRNetwork.from_edge_arrays(6000, src, dst, w)
+    lat = synth.knn_like_graph(20000, k=12, seed=3)
+    h = sc_gpu.CSRNetwork.from_csr_parts(*lat)
+    configs = [sc_gpu.LeidenConfig(seed=5), sc_gpu.LeidenConfig(seed=6, refine=False),
+               sc_gpu.LeidenConfig(objective=sc_gpu.Cpm(0.05), seed=7),
+               sc_gpu.LeidenConfig(seed=8, max_community_weight=40.0)]
+    before = sc_gpu.get_tuning()
+    try:
+        for graph in (g, h):
+            for cfg in configs:
+                runs = []
+                for t in TUNINGS:
+                    sc_gpu.set_tuning(t)
+                    runs.append(sc_gpu.leiden(graph, cfg).labels())
+                for r in runs[1:]:
+                    assert np.array_equal(r, runs[0])
+    finally:
+        sc_gpu.set_tuning(before)
+
+
+def test_autotune_keeps_a_candidate_and_rejects_bad_limits():
+    lat = synth.knn_like_graph(50000, k=12, seed=4)
+    g = sc_gpu.CSRNetwork.from_csr_parts(*lat)
+    before = sc_gpu.get_tuning()
+    try:
+        res = sc_gpu.autotune(g, sc_gpu.LeidenConfig(seed=1))
+        assert res["candidates"] >= 2 and res["ms_chosen"] <= res["ms_default"]
+        now = sc_gpu.get_tuning()
+        assert all(now[k] == res[k] for k in now)
+        with pytest.raises(sc_gpu.ClusteringError):
+            sc_gpu.set_tuning(dict(lanes8_max_degree=9))
+        with pytest.raises(sc_gpu.ClusteringError):
+            sc_gpu.set_tuning(dict(lanes16_max_degree=4, lanes8_max_degree=8))
+        assert sc_gpu.get_tuning() == now
+    finally:
+        sc_gpu.set_tuning(before)

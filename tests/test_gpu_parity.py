@@ -195,6 +195,29 @@ def test_aggregate_planted_partition_20k():
         assert same_f64([og.quality(p)], [sc_gpu.quality(gg, p)])
 
 
+def test_aggregate_of_balanced_asymmetric_graph():
+    """A graph whose degree sums balance but whose rows do not mirror
+    (csr_network.rs:968-979) takes the ordered sort path of aggregate; a
+    symmetric one in the exact regime takes the per-row hash contraction. Both
+    must give the reference's bits."""
+    ptrs, nbrs, ws = [0, 2, 3, 4], [1, 2, 0, 0], [1.0, 3.0, 3.0, 1.0]
+    og = O.Graph.from_csr_parts(np.array(ptrs, np.uint64), np.array(nbrs, np.uint32), np.array(ws, np.float32))
+    gg = sc_gpu.CSRNetwork.from_csr_parts(ptrs, nbrs, ws)
+    for p in ([0, 0, 1], [0, 1, 1], [0, 1, 2], [0, 0, 0]):
+        assert_same_graph(og.aggregate(np.array(p, np.uint64)), gg.aggregate(p))
+
+
+def test_aggregate_large_rows_use_the_block_contraction():
+    """Groups whose members hold more than 256 entries (a block per row, table
+    in global memory, segmented sort) next to small ones (a warp per row)."""
+    src, dst, w, truth = synth.planted_partition(6000, 6, 12, 3, seed=4)
+    og = O.Graph.from_edges(6000, src=src, dst=dst, w=w)
+    gg = sc_gpu.CSRNetwork.from_edge_arrays(6000, src, dst, w)
+    mixed = np.where(truth < 2, truth, 2 + np.arange(6000) // 3).astype(np.uint64)
+    for p in (truth, mixed, np.zeros(6000, np.uint64)):
+        assert_same_graph(og.aggregate(p), gg.aggregate(p))
+
+
 def test_leidenalg_fixture_definitions():
     # tests/reference.rs:164-209 on the GPU quality and modularity
     d = leidenalg_fixture()
