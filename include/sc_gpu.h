@@ -359,8 +359,11 @@ sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const fl
  * The model is a 2-layer MLP (sc_mlp_feature_count() inputs, 128 hidden units,
  * ReLU, one logit) scoring each undirected edge with the probability that its
  * endpoints share a community, from endpoint degree/strength, the edge weight,
- * the RB null-model term at the given resolution and the endpoints' common
- * neighbourhood. Forward passes use BF16 weights with FP32 accumulation; Adam
+ * the RB null-model term at the given resolution, the endpoints' common
+ * neighbourhood and, when given, whether they share a community in the
+ * partitions found at a neighbouring lower (`coarse`) and higher (`fine`)
+ * resolution: host label arrays of n entries, each nullable. A model trained
+ * with these context partitions is meant to be used with them. Forward passes use BF16 weights with FP32 accumulation; Adam
  * updates an FP32 master copy. Parameters are laid out W1[f*128+u], b1[u],
  * w2[u], b2 (sc_mlp_param_count() floats). The feature scaler (means, then
  * inverse standard deviations, 2 * feature_count floats) is fitted on the first
@@ -386,19 +389,21 @@ sc_status sc_mlp_set(sc_ctx* ctx, sc_mlp* m, const float* params, const float* s
 /* The scaled edge features the model sees for g at `resolution`, edges (i < j)
  * in ascending (i, j) order: feat[e * feature_count + f], endpoints ei/ej (each
  * nullable). `capacity` is the room in edges; *n_edges receives the count. */
-sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, float* feat,
-                          uint32_t* ei, uint32_t* ej, uint64_t capacity, uint64_t* n_edges);
+sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, const uint64_t* coarse,
+                          const uint64_t* fine, float* feat, uint32_t* ei, uint32_t* ej, uint64_t capacity,
+                          uint64_t* n_edges);
 /* `epochs` full-batch Adam steps (learning rate lr) of the mean binary
  * cross-entropy against "same community in `membership`". *loss_out receives the
  * loss before the last step; grad_out (nullable, param_count floats) the last
  * gradient. epochs == 0 evaluates loss and gradient without a step. */
 sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
-                       double resolution, uint32_t epochs, double lr, double* loss_out, float* grad_out);
+                       double resolution, const uint64_t* coarse, const uint64_t* fine, uint32_t epochs, double lr,
+                       double* loss_out, float* grad_out);
 /* Initial membership for sc_leiden_from (see above); prob_out (nullable) gets
  * the edge probabilities in sc_mlp_features order, prob_capacity entries. */
-sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
-                         double core_fraction, uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out,
-                         uint64_t prob_capacity);
+sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, const uint64_t* coarse,
+                         const uint64_t* fine, double threshold, double core_fraction, uint64_t* labels_out,
+                         uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity);
 
 #ifdef __cplusplus
 }

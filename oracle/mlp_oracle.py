@@ -18,7 +18,7 @@ from __future__ import annotations
 
 import numpy as np
 
-F = 10
+F = 12
 H = 128
 GAMMA_FEATURE = 6
 
@@ -45,8 +45,9 @@ def unpack(params):
     return W1, b1, w2, b2
 
 
-def edge_features(ptr, nbr, w, strength, total_weight, gamma):
-    """Raw features of the undirected edges (sc_mlp.cu k_edge_features)."""
+def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=None):
+    """Raw features of the undirected edges (sc_mlp.cu k_edge_features);
+    coarse / fine: labels of the neighbouring-resolution partitions or None."""
     ptr = np.asarray(ptr, np.int64)
     nbr = np.asarray(nbr, np.int64)
     w = np.asarray(w, np.float32)
@@ -73,7 +74,9 @@ def edge_features(ptr, nbr, w, strength, total_weight, gamma):
             f = [wij, lki + lkj, abs(lki - lkj), ldi + ldj, abs(ldi - ldj),
                  wij / max(ki, 1e-300) + wij / max(kj, 1e-300), np.log(gamma),
                  gamma * ki * kj / (two_m * max(wij, 1e-300)) if two_m > 0 else 0.0,
-                 cw / max(min(ki, kj), 1e-300), len(common) / max(min(di, dj), 1.0)]
+                 cw / max(min(ki, kj), 1e-300), len(common) / max(min(di, dj), 1.0),
+                 0.0 if coarse is None else float(coarse[i] == coarse[j]),
+                 0.0 if fine is None else float(fine[i] == fine[j])]
             ei.append(i)
             ej.append(j)
             feats.append(f)

@@ -605,6 +605,17 @@ sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const fl
 }
 
 // ---------------------------------------------------------------- learned warm start
+namespace {
+// Host labels (n entries, nullable) -> compact device ids; empty buffer for NULL.
+void upload_labels(sc::Ctx& c, const uint64_t* host, uint64_t n, sc::DBuf<uint32_t>& out) {
+    if (!host || n == 0) return;
+    sc::DBuf<uint64_t> d(c, n);
+    out.alloc(c, n);
+    sc::h2d(c, d.get(), host, n);
+    sc::renumber_u64_labels(c, d.get(), n, out.get(), nullptr);
+}
+}  // namespace
+
 uint32_t sc_mlp_param_count(void) { return sc::mlp_param_count(); }
 
 uint32_t sc_mlp_feature_count(void) { return sc::mlp_feature_count(); }
@@ -645,19 +656,24 @@ sc_status sc_mlp_set(sc_ctx* ctx, sc_mlp* m, const float* params, const float* s
     });
 }
 
-sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, float* feat,
-                          uint32_t* ei, uint32_t* ej, uint64_t capacity, uint64_t* n_edges) {
+sc_status sc_mlp_features(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, const uint64_t* coarse,
+                          const uint64_t* fine, float* feat, uint32_t* ei, uint32_t* ej, uint64_t capacity,
+                          uint64_t* n_edges) {
     return guarded(ctx, [&](sc::Ctx& c) {
         require(m && m->m && g && g->g && n_edges, "model, graph or n_edges is NULL");
         if (m->device != c.device) bad_arg("model lives on another device than the context");
         require_same_device(c, *g->g);
         require(resolution > 0.0 && std::isfinite(resolution), "resolution must be positive and finite");
-        sc::mlp_features(c, *m->m, *g->g, resolution, feat, ei, ej, capacity, n_edges);
+        sc::DBuf<uint32_t> dc, df;
+        upload_labels(c, coarse, g->g->n, dc);
+        upload_labels(c, fine, g->g->n, df);
+        sc::mlp_features(c, *m->m, *g->g, resolution, dc.get(), df.get(), feat, ei, ej, capacity, n_edges);
     });
 }
 
 sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t* membership, uint64_t n_membership,
-                       double resolution, uint32_t epochs, double lr, double* loss_out, float* grad_out) {
+                       double resolution, const uint64_t* coarse, const uint64_t* fine, uint32_t epochs, double lr,
+                       double* loss_out, float* grad_out) {
     return guarded(ctx, [&](sc::Ctx& c) {
         require(m && m->m && g && g->g, "model or graph is NULL");
         if (m->device != c.device) bad_arg("model lives on another device than the context");
@@ -671,14 +687,17 @@ sc_status sc_mlp_train(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, const uint64_t
         sc::DBuf<uint32_t> ids(c, G.n);
         sc::h2d(c, dl.get(), membership, G.n);
         if (G.n) sc::renumber_u64_labels(c, dl.get(), G.n, ids.get(), nullptr);
-        const double loss = sc::mlp_train(c, *m->m, G, ids.get(), resolution, epochs, lr, grad_out);
+        sc::DBuf<uint32_t> dc, df;
+        upload_labels(c, coarse, G.n, dc);
+        upload_labels(c, fine, G.n, df);
+        const double loss = sc::mlp_train(c, *m->m, G, ids.get(), resolution, dc.get(), df.get(), epochs, lr, grad_out);
         if (loss_out) *loss_out = loss;
     });
 }
 
-sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, double threshold,
-                         double core_fraction, uint64_t* labels_out, uint64_t* n_clusters_out, float* prob_out,
-                         uint64_t prob_capacity) {
+sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resolution, const uint64_t* coarse,
+                         const uint64_t* fine, double threshold, double core_fraction, uint64_t* labels_out,
+                         uint64_t* n_clusters_out, float* prob_out, uint64_t prob_capacity) {
     return guarded(ctx, [&](sc::Ctx& c) {
         require(m && m->m && g && g->g && n_clusters_out, "model, graph or n_clusters_out is NULL");
         if (m->device != c.device) bad_arg("model lives on another device than the context");
@@ -689,8 +708,11 @@ sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resol
         const sc::DevGraph& G = *g->g;
         require(labels_out || G.n == 0, "labels_out is NULL");
         sc::DBuf<uint32_t> lab(c, G.n);
-        const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, threshold, core_fraction, lab.get(), prob_out,
-                                             prob_capacity);
+        sc::DBuf<uint32_t> dc, df;
+        upload_labels(c, coarse, G.n, dc);
+        upload_labels(c, fine, G.n, df);
+        const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, dc.get(), df.get(), threshold, core_fraction,
+                                           lab.get(), prob_out, prob_capacity);
         if (G.n) {
             std::vector<uint32_t> h(G.n);
             sc::d2h(c, h.data(), lab.get(), G.n);

@@ -277,12 +277,14 @@ uint32_t mlp_param_count();
 uint32_t mlp_feature_count();
 bool mlp_get(Ctx& c, const Mlp& m, float* params, float* scaler);  // returns whether a scaler is set
 void mlp_set(Ctx& c, Mlp& m, const float* params, const float* scaler);
-void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_host, uint32_t* ei_host,
-                  uint32_t* ej_host, uint64_t cap, uint64_t* M_out);
-double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, uint32_t epochs,
-                 double lr, float* grad_out_host);
-uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, double core_fraction,
-                     uint32_t* d_labels, float* prob_host, uint64_t prob_cap);
+// coarse / fine: compact device labels of the partitions at the neighbouring
+// lower / higher resolutions (nullable)
+void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                  float* feat_host, uint32_t* ei_host, uint32_t* ej_host, uint64_t cap, uint64_t* M_out);
+double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, const uint32_t* coarse,
+                 const uint32_t* fine, uint32_t epochs, double lr, float* grad_out_host);
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                     double thr, double core_fraction, uint32_t* d_labels, float* prob_host, uint64_t prob_cap);
 
 // common.cu
 void check_device_status(Ctx& c);

@@ -3,16 +3,17 @@
 //
 // Community ids are arbitrary (any permutation of a partition is the same
 // partition), so the network does not classify nodes into ids: it scores each
-// undirected edge (i, j) from the features of its two endpoints and their
-// shared neighbourhood, F = 10 of them,
+// undirected edge (i, j) from the features of its two endpoints, their shared
+// neighbourhood and the partitions found at neighbouring resolutions, F = 12:
 //   w, log1p(k_i) + log1p(k_j), |log1p(k_i) - log1p(k_j)|, log(d_i) + log(d_j),
 //   |log d_i - log d_j|, w/k_i + w/k_j, log(gamma), gamma k_i k_j / (2 m w),
-//   sum_c min(w_ic, w_jc) / min(k_i, k_j), |N(i) & N(j)| / min(d_i, d_j)
+//   sum_c min(w_ic, w_jc) / min(k_i, k_j), |N(i) & N(j)| / min(d_i, d_j),
+//   [i, j together at the coarser neighbour], [i, j together at the finer one]
 // (w edge weight, k strength, d degree, gamma the RB resolution; the 8th is the
 // configuration-model null term relative to the edge, the quantity local moving
-// weighs; the last two compare the endpoints' neighbour histograms, c over the
-// common neighbours other than i and j) and outputs the logit that i and j
-// share a community:
+// weighs; the 9th and 10th compare the endpoints' neighbour histograms, c over
+// the common neighbours other than i and j; the last two are 0 without a
+// context) and outputs the logit that i and j share a community:
 //   h = relu(x W1 + b1) (hidden H), z = h . w2 + b2.
 // Weights are BF16 in the forward pass with FP32 accumulation; an FP32 master
 // copy is updated by Adam. Training labels are partitions plain Leiden found;
@@ -32,7 +33,7 @@
 
 namespace sc {
 
-constexpr int MLP_F = 10;
+constexpr int MLP_F = 12;
 constexpr int MLP_H = 128;
 constexpr int MLP_UPL = MLP_H / 32;  // hidden units per lane
 constexpr int MLP_NPARAM = MLP_F * MLP_H + MLP_H + MLP_H + 1;  // W1, b1, w2, b2
@@ -84,7 +85,8 @@ __device__ void common_neighbours(const uint64_t* __restrict__ ptr, const uint32
 // Features of the undirected edges (stored entries with row < neighbour).
 __global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                                 const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
-                                const double* __restrict__ strength, double two_m, double gamma, float* feat,
+                                const double* __restrict__ strength, double two_m, double gamma,
+                                const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine, float* feat,
                                 uint32_t* ei, uint32_t* ej, unsigned long long* count) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
          e += (uint64_t)gridDim.x * blockDim.x) {
@@ -109,6 +111,8 @@ __global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t
         f[7] = (float)(two_m > 0.0 ? gamma * ki * kj / (two_m * fmax(wij, 1e-300)) : 0.0);
         f[8] = (float)(cw / fmax(fmin(ki, kj), 1e-300));
         f[9] = (float)((double)cn / fmax(fmin(di, dj), 1.0));
+        f[10] = coarse ? (coarse[i] == coarse[j] ? 1.0f : 0.0f) : 0.0f;
+        f[11] = fine ? (fine[i] == fine[j] ? 1.0f : 0.0f) : 0.0f;
         ei[pos] = i;
         ej[pos] = j;
     }
@@ -390,7 +394,8 @@ struct EdgeSet {
     DBuf<uint32_t> ei, ej;
 };
 
-void build_edges(Ctx& c, const DevGraph& g, double gamma, EdgeSet& es) {
+void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                 EdgeSet& es) {
     const uint64_t cap = g.E;
     DBuf<float> feat(c, cap * MLP_F);
     DBuf<uint32_t> ei(c, cap), ej(c, cap);
@@ -398,8 +403,8 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, EdgeSet& es) {
     zero(c, cnt.get(), 1);
     if (g.E) {
         k_edge_features<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, g.strength,
-                                                                2.0 * g.total_weight, gamma, feat.get(), ei.get(),
-                                                                ej.get(), cnt.get());
+                                                                2.0 * g.total_weight, gamma, coarse, fine, feat.get(),
+                                                                ei.get(), ej.get(), cnt.get());
         SC_LAUNCH_CHECK();
         c.launches++;
     }
@@ -514,10 +519,10 @@ void mlp_set(Ctx& c, Mlp& m, const float* params, const float* scaler) {
 
 // Edge features of g at resolution gamma as the model sees them (standardised
 // by its scaler, which this fits if the model has none), sorted by (i, j).
-void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_host, uint32_t* ei_host,
-                  uint32_t* ej_host, uint64_t cap, uint64_t* M_out) {
+void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                  float* feat_host, uint32_t* ei_host, uint32_t* ej_host, uint64_t cap, uint64_t* M_out) {
     EdgeSet es;
-    build_edges(c, g, gamma, es);
+    build_edges(c, g, gamma, coarse, fine, es);
     *M_out = es.M;
     if (es.M > cap)
         fail(SC_E_INVALID_ARGUMENT, "capacity %llu is below the %llu undirected edges", (unsigned long long)cap,
@@ -532,10 +537,10 @@ void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, float* feat_h
 // `epochs` full-batch Adam steps on (g, membership) at gamma; returns the mean
 // loss at the weights before the last step. epochs == 0 only evaluates the loss
 // and gradient. grad_out_host (nullable) receives the last gradient.
-double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, uint32_t epochs,
-                 double lr, float* grad_out_host) {
+double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, double gamma, const uint32_t* coarse,
+                 const uint32_t* fine, uint32_t epochs, double lr, float* grad_out_host) {
     EdgeSet es;
-    build_edges(c, g, gamma, es);
+    build_edges(c, g, gamma, coarse, fine, es);
     scale_edges(c, m, es, true);
     DBuf<uint8_t> lab(c, es.M);
     if (es.M) {
@@ -562,10 +567,10 @@ double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, doub
 }
 
 // Proposal: components of the edges whose predicted probability exceeds thr.
-uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, double thr, double core_fraction,
-                     uint32_t* d_labels, float* prob_host, uint64_t prob_cap) {
+uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                     double thr, double core_fraction, uint32_t* d_labels, float* prob_host, uint64_t prob_cap) {
     EdgeSet es;
-    build_edges(c, g, gamma, es);
+    build_edges(c, g, gamma, coarse, fine, es);
     scale_edges(c, m, es, false);
     DBuf<__nv_bfloat16> wb(c, MLP_NPARAM);
     k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());

@@ -477,28 +477,41 @@ def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig], 
 
 
 def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb, warm_start: bool = True,
-               base: LeidenConfig | None = None):
+               base: LeidenConfig | None = None, split: int = 1):
     """Configs and warm-start links of a resolution x seed sweep.
 
     Instances are ordered seed-major with resolutions descending; with warm_start
     each instance starts from the previous (finer) resolution's result of the
-    same seed, so a chain coarsens a partition instead of rebuilding it."""
+    same seed, so a chain coarsens a partition instead of rebuilding it. With
+    split = k each seed's chain is cut into k contiguous pieces: the first piece
+    starts from singletons, the head of every other piece from the first
+    instance of the seed (the finest resolution), so k pieces per seed run
+    concurrently. Returns (configs, warm_from, keys)."""
     base = base or LeidenConfig()
     res = sorted(resolutions, reverse=True)
+    split = max(1, min(int(split), len(res))) if res else 1
+    bounds = [round(i * len(res) / split) for i in range(split + 1)]
+    heads = set(bounds[:-1])
     configs, warm, keys = [], [], []
     for s in seeds:
+        first = len(configs)
         for j, r in enumerate(res):
             cfg = LeidenConfig(**{**base.__dict__, "objective": objective(r), "seed": int(s)})
             configs.append(cfg)
-            warm.append(len(configs) - 2 if (warm_start and j > 0) else -1)
+            if not warm_start or j == 0:
+                warm.append(-1)
+            elif j in heads:
+                warm.append(first)
+            else:
+                warm.append(len(configs) - 2)
             keys.append((float(r), int(s)))
     return configs, warm, keys
 
 
 def leiden_sweep(graph: CSRNetwork, resolutions, seeds, objective=Rb, warm_start: bool = True,
-                 n_streams: int = 0, base: LeidenConfig | None = None) -> dict:
+                 n_streams: int = 0, base: LeidenConfig | None = None, split: int = 1) -> dict:
     """Resolution x seed sweep on one graph: {(resolution, seed): Clustering}."""
-    configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base)
+    configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base, split)
     res = leiden_batch([graph] * len(configs), configs, warm if warm_start else None, n_streams)
     return dict(zip(keys, res))
 

@@ -141,9 +141,11 @@ SIGNATURES = [
     ("sc_mlp_destroy", None, [vp]),
     ("sc_mlp_get", C.c_int, [vp, vp, f32p, f32p, i32p]),
     ("sc_mlp_set", C.c_int, [vp, vp, f32p, f32p]),
-    ("sc_mlp_features", C.c_int, [vp, vp, vp, C.c_double, f32p, u32p, u32p, C.c_uint64, u64p]),
-    ("sc_mlp_train", C.c_int, [vp, vp, vp, u64p, C.c_uint64, C.c_double, C.c_uint32, C.c_double, f64p, f32p]),
-    ("sc_mlp_propose", C.c_int, [vp, vp, vp, C.c_double, C.c_double, C.c_double, u64p, u64p, f32p, C.c_uint64]),
+    ("sc_mlp_features", C.c_int, [vp, vp, vp, C.c_double, u64p, u64p, f32p, u32p, u32p, C.c_uint64, u64p]),
+    ("sc_mlp_train", C.c_int, [vp, vp, vp, u64p, C.c_uint64, C.c_double, u64p, u64p, C.c_uint32, C.c_double, f64p,
+                               f32p]),
+    ("sc_mlp_propose", C.c_int, [vp, vp, vp, C.c_double, u64p, u64p, C.c_double, C.c_double, u64p, u64p, f32p,
+                                 C.c_uint64]),
 ]
 
 _lib = None

@@ -24,6 +24,20 @@ def _check(rc, ctx):
     chk(rc, ctx)
 
 
+def _ctx_labels(context):
+    """(coarse, fine) host label arrays of a neighbouring-resolution context, or Nones."""
+    if context is None:
+        return None, None
+    coarse, fine = context
+    c = None if coarse is None else np.ascontiguousarray(coarse, np.uint64)
+    f = None if fine is None else np.ascontiguousarray(fine, np.uint64)
+    return c, f
+
+
+def _p64(a):
+    return None if a is None else a.ctypes.data_as(_lib.u64p)
+
+
 def param_count() -> int:
     return int(lib().sc_mlp_param_count())
 
@@ -75,15 +89,18 @@ class EdgeMlp:
                                 None if s is None else s.ctypes.data_as(_lib.f32p)), self._ctx)
 
     # device work ------------------------------------------------------------
-    def features(self, graph, resolution: float):
-        """(features (M, F) float32, ei, ej) as the model sees them."""
+    def features(self, graph, resolution: float, context=None):
+        """(features (M, F) float32, ei, ej) as the model sees them. `context` is
+        (coarse, fine): the partitions found at a neighbouring lower and higher
+        resolution (either may be None)."""
+        cl, fl = _ctx_labels(context)
         cap = graph.entry_count()
         F = feature_count()
         feat = np.zeros((max(cap, 1), F), np.float32)
         ei = np.zeros(max(cap, 1), np.uint32)
         ej = np.zeros(max(cap, 1), np.uint32)
         M = C.c_uint64()
-        _check(lib().sc_mlp_features(self._ctx.h, self._h, graph._h, float(resolution),
+        _check(lib().sc_mlp_features(self._ctx.h, self._h, graph._h, float(resolution), _p64(cl), _p64(fl),
                                      feat.ctypes.data_as(_lib.f32p), ei.ctypes.data_as(_lib.u32p),
                                      ej.ctypes.data_as(_lib.u32p),
                                      cap, C.byref(M)), self._ctx)
@@ -91,26 +108,29 @@ class EdgeMlp:
         return feat[:m], ei[:m], ej[:m]
 
     def train(self, graph, membership, resolution: float, epochs: int = 1, lr: float = 1e-2,
-              return_grad: bool = False):
+              return_grad: bool = False, context=None):
         """`epochs` Adam steps; returns the loss before the last step (and the gradient)."""
         m = np.ascontiguousarray(membership, np.uint64)
+        cl, fl = _ctx_labels(context)
         loss = C.c_double()
         grad = np.zeros(param_count(), np.float32) if return_grad else None
         _check(lib().sc_mlp_train(self._ctx.h, self._h, graph._h, m.ctypes.data_as(_lib.u64p), len(m),
-                                  float(resolution), int(epochs), float(lr), C.byref(loss),
+                                  float(resolution), _p64(cl), _p64(fl), int(epochs), float(lr), C.byref(loss),
                                   None if grad is None else grad.ctypes.data_as(_lib.f32p)), self._ctx)
         return (loss.value, grad) if return_grad else loss.value
 
     def propose(self, graph, resolution: float, threshold: float = 0.9, core_fraction: float = 1.0,
-                return_prob: bool = False):
+                return_prob: bool = False, context=None):
         """Initial membership: components of the confident edges (p > threshold)
         between core nodes (>= core_fraction of their edges confident)."""
+        cl, fl = _ctx_labels(context)
         n = graph.node_count()
         labels = np.zeros(n, np.uint64)
         k = C.c_uint64()
         prob = np.zeros(max(graph.entry_count(), 1), np.float32) if return_prob else None
-        _check(lib().sc_mlp_propose(self._ctx.h, self._h, graph._h, float(resolution), float(threshold),
-                                    float(core_fraction), labels.ctypes.data_as(_lib.u64p), C.byref(k),
+        _check(lib().sc_mlp_propose(self._ctx.h, self._h, graph._h, float(resolution), _p64(cl), _p64(fl),
+                                    float(threshold), float(core_fraction), labels.ctypes.data_as(_lib.u64p),
+                                    C.byref(k),
                                     None if prob is None else prob.ctypes.data_as(_lib.f32p),
                                     0 if prob is None else prob.size), self._ctx)
         if return_prob:
@@ -133,14 +153,16 @@ class WarmStartResult:
 
 
 def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
-                      judge: bool = True, tolerance: float = 1e-4) -> WarmStartResult:
+                      judge: bool = True, tolerance: float = 1e-4, context=None) -> WarmStartResult:
     """leiden_from(model's proposal). With `judge`, the plain singleton start also
     runs and the proposal is kept only if its final modularity is at least the
-    plain one minus `tolerance`; otherwise the plain result is returned."""
+    plain one minus `tolerance`; otherwise the plain result is returned.
+    `context` is (coarse, fine), the partitions at the neighbouring lower and
+    higher resolutions the model was trained to read."""
     from . import leiden, leiden_from, modularity, Rb
     gamma = config.objective.resolution if isinstance(config.objective, Rb) else 1.0
     t0 = time.perf_counter()
-    prop, kprop = model.propose(graph, gamma, threshold, core_fraction)
+    prop, kprop = model.propose(graph, gamma, threshold, core_fraction, context=context)
     t_prop = (time.perf_counter() - t0) * 1e3
     warm = leiden_from(graph, config, prop)
     sw = graph._ctx.run_stats()

@@ -8,10 +8,11 @@
   deterministic for a fixed seed;
 * proposal: components of the confident edges between core nodes, from the
   GPU probabilities, equal the oracle's from the same probabilities;
-* gain: trained on plain-GPU Leiden partitions at RB {0.5, 1, 2}, the proposal
-  used as a warm start at RB {0.8, 1.5} needs fewer local-moving sweeps than the
-  plain singleton start, with final modularity >= plain - 1e-4 or the judge
-  falling back to the plain result.
+* gain: trained on plain-GPU Leiden partitions at RB {0.5, 1, 2} (each with the
+  partitions of its neighbouring resolutions as context), the proposal used as
+  a warm start at RB {0.8, 1.5} needs fewer local-moving sweeps than the plain
+  singleton start, with final modularity >= plain - 1e-4 or the judge falling
+  back to the plain result.
 """
 import numpy as np
 import pytest
@@ -38,12 +39,14 @@ def test_features_match_oracle():
     from sc_gpu.learned import EdgeMlp
     from helpers import karate
     edges, _ = karate()
+    rng = np.random.default_rng(0)
     for g in (sc_gpu.CSRNetwork.from_edges(34, edges), _planted(800, 8)[0]):
-        for gamma in (1.0, 0.3):
+        n = g.node_count()
+        for gamma, ctx in ((1.0, None), (0.3, (rng.integers(0, 3, n) * 7, rng.integers(0, 9, n)))):
             m = EdgeMlp(seed=1)
-            feat, ei, ej = m.features(g, gamma)
+            feat, ei, ej = m.features(g, gamma, context=ctx)
             ptr, nbr, w, st, tw = _graph_arrays(g)
-            raw, oi, oj = mo.edge_features(ptr, nbr, w, st, tw, gamma)
+            raw, oi, oj = mo.edge_features(ptr, nbr, w, st, tw, gamma, *(ctx or (None, None)))
             assert np.array_equal(ei, oi) and np.array_equal(ej, oj)
             mean, istd = m.scaler()
             omean, oistd = mo.scaler_fit(raw)
@@ -122,6 +125,27 @@ def test_untrained_model_cannot_propose():
     assert "scaler" in str(e.value)
 
 
+def train_context_model(g, epochs=6):
+    """An edge MLP trained on plain-GPU partitions at RB {0.5, 1, 2} (seeds 101-103),
+    each with the partitions of its neighbouring resolutions as context; at the
+    ends of the range the context's missing side is an independent run (seeds
+    201, 203) at the same resolution. Returns the model and the partitions."""
+    import sc_gpu
+    from sc_gpu.learned import EdgeMlp
+
+    def run(gamma, seed):
+        return sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=seed)).labels()
+
+    labs = {0.5: run(0.5, 101), 1.0: run(1.0, 102), 2.0: run(2.0, 103)}
+    alt = {0.5: run(0.5, 201), 2.0: run(2.0, 203)}
+    ctx = {0.5: (alt[0.5], labs[1.0]), 1.0: (labs[0.5], labs[2.0]), 2.0: (labs[1.0], alt[2.0])}
+    m = EdgeMlp(seed=4)
+    for _ in range(epochs):
+        for gamma in (0.5, 1.0, 2.0):
+            m.train(g, labs[gamma], gamma, epochs=20, lr=5e-3, context=ctx[gamma])
+    return m, labs
+
+
 def test_warm_start_gain_over_plain_start():
     """Train at RB {0.5, 1, 2} on plain-GPU partitions, evaluate at {0.8, 1.5}."""
     import sc_gpu
@@ -130,15 +154,11 @@ def test_warm_start_gain_over_plain_start():
     X, _ = synth.gaussian_mixture(60000, 50, 200, 5, sigma=(0.5, 2.0))
     r = sc_gpu.knn_gaussian(X, 15, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
     g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w)
-    m = EdgeMlp(seed=4)
-    for epoch in range(6):
-        for gamma, seed in ((0.5, 101), (1.0, 102), (2.0, 103)):
-            lab = sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=seed)).labels()
-            m.train(g, lab, gamma, epochs=20, lr=5e-3)
+    m, labs = train_context_model(g)
     saved = []
-    for gamma in (0.8, 1.5):
+    for gamma, ctx in ((0.8, (labs[0.5], labs[1.0])), (1.5, (labs[1.0], labs[2.0]))):
         cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=9)
-        res = warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=1.0)
+        res = warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=0.0, context=ctx)
         assert res.q_warm >= res.q_plain - 1e-4 or not res.used_proposal
         final_q = sc_gpu.modularity(g, res.labels, gamma)
         assert final_q >= res.q_plain - 1e-4

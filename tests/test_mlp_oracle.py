@@ -74,6 +74,10 @@ def test_features_on_triangle_with_tail():
     # the tail edge has no common neighbour
     assert feats[3][8] == 0.0 and feats[3][9] == 0.0
     assert np.allclose(feats[:, mo.GAMMA_FEATURE], 0.0)
+    assert np.all(feats[:, 10:] == 0.0)  # no context partitions
+    feats2, _, _ = mo.edge_features(ptr, nbr, w, strength, 7.0, 1.0, coarse=[0, 0, 0, 1], fine=[0, 1, 1, 2])
+    # edges (0,1) (0,2) (1,2) (2,3): together at coarse 1 1 1 0, at fine 0 0 1 0
+    assert list(feats2[:, 10]) == [1, 1, 1, 0] and list(feats2[:, 11]) == [0, 0, 1, 0]
 
 
 def test_scaler_passes_gamma_through():

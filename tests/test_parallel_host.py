@@ -30,6 +30,13 @@ def test_sweep_plan_chains_descending_resolutions():
     assert all(c.seed == k[1] and c.objective.resolution == k[0] for c, k in zip(cfgs, keys))
     _, warm_plain, _ = sweep_plan([0.5, 2.0], [1], warm_start=False)
     assert warm_plain == [-1, -1]
+    # split chains: pieces [0..2] [3..4] [5..7] of 8 resolutions (bounds round(i*8/3));
+    # piece heads warm from the seed's first (finest) instance
+    _, warm_split, keys = sweep_plan([float(x) for x in range(1, 9)], [1, 2], split=3)
+    assert warm_split[:8] == [-1, 0, 1, 0, 3, 0, 5, 6]
+    assert warm_split[8:] == [-1, 8, 9, 8, 11, 8, 13, 14]
+    assert [k[0] for k in keys[:8]] == [8.0, 7.0, 6.0, 5.0, 4.0, 3.0, 2.0, 1.0]
+    assert parallel.chains(warm_split) == [list(range(8)), list(range(8, 16))]
 
 
 def _free_port():
