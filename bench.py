@@ -23,7 +23,7 @@ with from_csr_parts. A "step" is one full leiden() call on that graph.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--n POINTS] [--no-sweep] [--no-cpu-baseline]
-  python bench.py --part knn [--n POINTS] [--steps K] [--warmup W]
+  python bench.py --part knn [--n POINTS] [--steps K] [--warmup W] [--knn-precision bf16|fp8]
              times the kNN graph builder alone (points/s) on the same data.
 """
 from __future__ import annotations
@@ -124,9 +124,10 @@ SWEEP_RESOLUTIONS = 32
 SWEEP_SEEDS = (1, 2, 3, 4)
 
 
-def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=4):
+def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=4):
     """128-instance resolution x seed sweep: sequential plain runs vs
-    warm-started chains on concurrent streams (same graph, same configs)."""
+    warm-started chains (each seed's chain cut in `split` pieces whose heads
+    start from the seed's finest partition) on concurrent streams."""
     import sc_gpu
     from sc_gpu import synth
     X, _ = synth.gaussian_mixture(n_points, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_SEED, sigma=(0.7, 1.5))
@@ -138,7 +139,7 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=4):
     out = {}
     for name, warm, streams in (("plain_sequential", False, 1), ("warm_chains", True, n_streams)):
         t = time.perf_counter()
-        sw = sc_gpu.leiden_sweep(g, res, SWEEP_SEEDS, warm_start=warm, n_streams=streams)
+        sw = sc_gpu.leiden_sweep(g, res, SWEEP_SEEDS, warm_start=warm, n_streams=streams, split=split if warm else 1)
         dt = time.perf_counter() - t
         out[name] = (dt, {k: sc_gpu.modularity(g, v.labels(), k[0]) for k, v in sw.items()})
     base_s, base_q = out["plain_sequential"]
@@ -146,7 +147,7 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=4):
     d = np.array([warm_q[k] - base_q[k] for k in base_q])
     return {"workload": f"sweep_rb{SWEEP_RESOLUTIONS}x{len(SWEEP_SEEDS)}_knn{SWEEP_K}_gmm{n_points}x{SWEEP_DIMS}",
             "instances": len(base_q), "edge_count": g.edge_count(), "plain_sequential_s": base_s,
-            "warm_chains_s": warm_s, "streams": n_streams, "speedup": base_s / warm_s,
+            "warm_chains_s": warm_s, "streams": n_streams, "chain_split": split, "speedup": base_s / warm_s,
             "dQ_min": float(d.min()), "dQ_mean": float(d.mean()), "dQ_max": float(d.max()),
             "frac_dQ_ge_-1e-4": float(np.mean(d >= -1e-4))}
 
@@ -155,16 +156,19 @@ def run_knn_part(args, device_index):
     """The kNN graph builder alone on the bench's point set."""
     import sc_gpu
     from sc_gpu import synth
+    prec = sc_gpu.KNN_FP8 if args.knn_precision == "fp8" else sc_gpu.KNN_BF16
     X, _ = synth.gaussian_mixture(args.n, DIMS, COMPONENTS, GRAPH_SEED, sigma=(0.7, 1.5))
     for _ in range(args.warmup):
-        sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+        sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec, device=device_index)
     t = time.perf_counter()
     for _ in range(args.steps):
-        r = sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+        r = sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
+                                device=device_index)
     dt = (time.perf_counter() - t) / args.steps
-    line = {"metric": "kNN graph build points/s (exact k=10, BF16 tcgen05 candidates + FP32 re-rank)",
+    line = {"metric": f"kNN graph build points/s (exact k=10, {args.knn_precision.upper()} tcgen05 candidates "
+                      "+ FP32 re-rank)",
             "value": args.n / dt, "unit": "points/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": dt * 1e3, "higher_is_better": True, "dtype": "bf16", "data": "synthetic",
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "dtype": args.knn_precision, "data": "synthetic",
             "config": {"workload": f"knn{K}_gmm{args.n}x{DIMS}", "n_points": args.n, "dims": DIMS, "k": K},
             "timing": "host wall clock around the C ABI call (host input, host CSR output)",
             "conn_nnz": int(len(r.conn_w))}
@@ -265,6 +269,7 @@ def main():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--sweep-points", type=int, default=SWEEP_POINTS)
     ap.add_argument("--part", default="leiden", choices=["leiden", "knn"])
+    ap.add_argument("--knn-precision", default="bf16", choices=["bf16", "fp8"])
     args = ap.parse_args()
 
     rank = int(os.environ.get("RANK", "0"))

@@ -1048,12 +1048,125 @@ __global__ void __launch_bounds__(256)
     }
 }
 
-__global__ void k_flag_large(const uint64_t* __restrict__ cap, uint64_t G, uint8_t* flag, uint64_t* hcap) {
+constexpr uint64_t AGG_SMEM_SLOTS = 4096;  // shared table of the block kernel (48 KB)
+constexpr uint64_t AGG_SMEM_KEEP = AGG_SMEM_SLOTS / 2;
+
+// A row has at most min(cap, G) distinct neighbour groups; its table needs twice that.
+__device__ __forceinline__ uint64_t agg_slots(uint64_t cap, uint64_t G) {
+    const uint64_t d = cap < G ? cap : G;
+    uint64_t s = 64;
+    while (s < 2 * d) s <<= 1;
+    return s;
+}
+
+// mid: rows past the warp kernel whose table fits the block kernel's shared
+// memory; big: the rest (table in global memory, sized by the row's entries).
+__global__ void k_flag_large(const uint64_t* __restrict__ cap, uint64_t G, uint8_t* mid, uint8_t* big,
+                             uint64_t* hcap, uint64_t* lcap) {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const bool large = cap[g] > AGG_WARP_CAP;
-        flag[g] = large;
-        hcap[g] = large ? 2 * cap[g] : 0;
+        const bool m = large && agg_slots(cap[g], G) <= AGG_SMEM_SLOTS;
+        mid[g] = m;
+        big[g] = large && !m;
+        hcap[g] = large && !m ? 2 * cap[g] : 0;
+        lcap[g] = large ? cap[g] : 0;
+    }
+}
+
+// One block per row of the mid list: integer fixed-point sums (exact in this
+// regime: every weight is a multiple of 2^e0 and every sum below 2^(52+e0)) in
+// a shared table, kept entries sorted by neighbour with a block bitonic sort.
+__global__ void __launch_bounds__(256)
+    k_contract_smem(const uint32_t* __restrict__ rows, uint64_t nrows, uint64_t G,
+                    const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
+                    const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                    const float* __restrict__ w, const uint32_t* __restrict__ grp, const uint64_t* __restrict__ cap,
+                    const uint64_t* __restrict__ capstart, const double* __restrict__ loops, double inv_scale,
+                    double scale, uint32_t* tnbr, float* tw, uint32_t* cnt, uint32_t* status) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    unsigned long long* vals = (unsigned long long*)smem_raw;          // AGG_SMEM_SLOTS
+    uint32_t* keys = (uint32_t*)(vals + AGG_SMEM_SLOTS);               // AGG_SMEM_SLOTS
+    uint32_t* sk = keys + AGG_SMEM_SLOTS;                              // AGG_SMEM_KEEP
+    float* sv = (float*)(sk + AGG_SMEM_KEEP);                          // AGG_SMEM_KEEP
+    __shared__ uint32_t s_n;
+    const int wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
+        const uint32_t g = rows[i];
+        const uint64_t size = agg_slots(cap[g], G);
+        const uint64_t mask = size - 1;
+        for (uint64_t s2 = threadIdx.x; s2 < size; s2 += blockDim.x) {
+            keys[s2] = AGG_EMPTY;
+            vals[s2] = 0ull;
+        }
+        if (threadIdx.x == 0) s_n = 0;
+        __syncthreads();
+        const uint64_t m0 = gstart[g], m1 = gstart[g + 1];
+        for (uint64_t mb = m0 + (uint64_t)wib * 32; mb < m1; mb += (uint64_t)nw * 32) {
+            const uint64_t me = mb + 32 < m1 ? mb + 32 : m1;
+            warp_member_entries(ptr, members, mb, me, [&](uint64_t j) {
+                const uint32_t h = grp[nbr[j]];
+                const unsigned long long x = (unsigned long long)__double2ll_rn(__dmul_rn((double)w[j], inv_scale));
+                uint64_t slot = agg_hash(h) & mask;
+                for (uint64_t probe = 0; probe < size; ++probe) {
+                    const uint32_t prev = atomicCAS(keys + slot, AGG_EMPTY, h);
+                    if (prev == AGG_EMPTY || prev == h) {
+                        atomicAdd(vals + slot, x);
+                        return;
+                    }
+                    slot = (slot + 1) & mask;
+                }
+                atomicOr(status, DEV_OVERFLOW);
+            });
+        }
+        __syncthreads();
+        for (uint64_t s2 = threadIdx.x; s2 < size; s2 += blockDim.x) {
+            const uint32_t h = keys[s2];
+            if (h == AGG_EMPTY) continue;
+            bool keep;
+            const double acc = __dmul_rn(__ll2double_rn((long long)vals[s2]), scale);
+            const float val = agg_value(g, h, acc, loops, &keep);
+            if (keep) {
+                const uint32_t pos = atomicAdd(&s_n, 1u);
+                if (pos < AGG_SMEM_KEEP) {
+                    sk[pos] = h;
+                    sv[pos] = val;
+                } else {
+                    atomicOr(status, DEV_OVERFLOW);
+                }
+            }
+        }
+        __syncthreads();
+        const uint32_t nk = s_n < AGG_SMEM_KEEP ? s_n : (uint32_t)AGG_SMEM_KEEP;
+        uint32_t P = 1;
+        while (P < nk) P <<= 1;
+        for (uint32_t t = nk + threadIdx.x; t < P; t += blockDim.x) sk[t] = AGG_EMPTY;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1)
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = threadIdx.x; t < P; t += blockDim.x) {
+                    const uint32_t o = t ^ j;
+                    if (o > t) {
+                        const bool up = (t & k) == 0;
+                        const uint32_t a = sk[t], b = sk[o];
+                        if ((a > b) == up) {
+                            sk[t] = b;
+                            sk[o] = a;
+                            const float va = sv[t];
+                            sv[t] = sv[o];
+                            sv[o] = va;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        const uint64_t o = capstart[g];
+        for (uint32_t t = threadIdx.x; t < nk; t += blockDim.x) {
+            tnbr[o + t] = sk[t];
+            tw[o + t] = sv[t];
+        }
+        if (threadIdx.x == 0) cnt[g] = nk;
+        __syncthreads();
     }
 }
 
@@ -1143,18 +1256,40 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
     DBuf<uint32_t> tnbr(c, g.E), cnt(c, G + 1);
     DBuf<float> tw(c, g.E);
     zero(c, cnt.get(), G + 1);
-    // large rows: list, table offsets, table size
-    DBuf<uint8_t> flag(c, G);
-    DBuf<uint64_t> hcap(c, G), nl(c, 1);
-    DBuf<uint32_t> iota(c, G), rows(c, G);
-    uint64_t nlarge = 0;
+    // rows past the warp kernel: shared-table rows (mid) and global-table rows (large)
+    DBuf<uint8_t> fmid(c, G), flag(c, G);
+    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 3);
+    DBuf<uint32_t> iota(c, G), rows(c, G), mrows(c, G);
+    uint64_t nlarge = 0, nmid = 0;
     if (G) {
-        k_flag_large<<<grid_for(G, TB), TB, 0, c.stream>>>(cap.get(), G, flag.get(), hcap.get());
+        k_flag_large<<<grid_for(G, TB), TB, 0, c.stream>>>(cap.get(), G, fmid.get(), flag.get(), hcap.get(),
+                                                           lcap.get());
         k_iota<<<grid_for(G, TB), TB, 0, c.stream>>>(iota.get(), G);
         SC_LAUNCH_CHECK();
         c.launches += 2;
         select_flagged(c, iota.get(), flag.get(), rows.get(), nl.get(), G);
-        nlarge = to_host(c, nl.get());
+        select_flagged(c, iota.get(), fmid.get(), mrows.get(), nl.get() + 1, G);
+        device_sum(c, lcap.get(), nl.get() + 2, G);
+        uint64_t counts[3];
+        d2h(c, counts, nl.get(), 3);
+        sync(c);
+        nlarge = counts[0];
+        nmid = counts[1];
+        // Rows past the warp kernel are served by one block each; when they hold
+        // more than a tenth of the entries the sort path is faster.
+        if (counts[2] * 10 > g.E) return nullptr;
+    }
+    if (nmid) {
+        const size_t smem = AGG_SMEM_SLOTS * (sizeof(unsigned long long) + sizeof(uint32_t)) +
+                            AGG_SMEM_KEEP * (sizeof(uint32_t) + sizeof(float));
+        SC_CUDA(cudaFuncSetAttribute(k_contract_smem, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const double scale = std::ldexp(1.0, g.e0_w), inv = std::ldexp(1.0, -g.e0_w);
+        const unsigned grid = (unsigned)std::min<uint64_t>(nmid, (uint64_t)c.sm_count * 3);
+        k_contract_smem<<<grid, 256, smem, c.stream>>>(mrows.get(), nmid, G, gstart, members, g.ptr, g.nbr, g.w,
+                                                       d_grp, cap.get(), capstart.get(), loops, inv, scale,
+                                                       tnbr.get(), tw.get(), cnt.get(), c.d_status);
+        SC_LAUNCH_CHECK();
+        c.launches++;
     }
     if (G) {
         const unsigned grid = grid_for(G * 32, 32 * AGG_WARPS, 148u * 16u);
@@ -1258,10 +1393,12 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
     if (g.exact_w && graph_bitwise_symmetric(c, g)) {
         std::unique_ptr<DevGraph> fast(contract_exact(c, g, d_grp, G, gstart.get(), members.get(), nw_new.get(),
                                                       loops.get()));
-        members.release();
-        gstart.release();
-        finish_aggregate(c, *fast);
-        return fast.release();
+        if (fast) {
+            members.release();
+            gstart.release();
+            finish_aggregate(c, *fast);
+            return fast.release();
+        }
     }
     members.release();
     gstart.release();

@@ -5,6 +5,14 @@
 //                     A . B = |c|^2 - 2 q.c = |q - c|^2 - |q|^2: the row-constant
 //                     |q|^2 does not change a row's ranking, so the contraction
 //                     yields ranking scores directly.
+//    k_knn_prep_f8    the FP8 (e4m3) operands, 64 one-byte columns (D <= 61): B =
+//                     [x / S, three e4m3 terms of |x|^2 / S_n, 0..] with one scale
+//                     for the point set, A = f_q [-2 x S / S_n, 1, 1, 1, 0..] with a
+//                     power-of-two scale f_q per query row. A . B = (f_q / S_n) (|c|^2
+//                     - 2 q.c): a positive factor per row, so the ranking is kept
+//                     (a per-point scale on B would rescale columns and break it).
+//                     64-byte rows: the tile geometry, swizzle and descriptors of the
+//                     BF16 KA = 32 path; each K step is one kind::f8f6f4 MMA of K = 32.
 // 2. k_knn_tc         persistent tcgen05 kernel, one CTA per SM. A group of 256
 //                     queries (two M = 128 tiles) stays in shared memory; every
 //                     128-candidate tile of B streams in by TMA (no multicast)
@@ -27,6 +35,7 @@
 // returns; the host turns the status into SC_E_TIMEOUT.
 #include <cuda.h>
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cudaTypedefs.h>
 
 #include "sc_prims.cuh"
@@ -120,6 +129,21 @@ __device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// Instruction descriptor, kind::f8f6f4: D f32, A/B e4m3 (format 0), both K-major, N = 128, M = 128.
+__host__ __device__ constexpr uint32_t idesc_e4m3_128x128() {
+    return (1u << 4) | ((uint32_t)(TILE >> 3) << 17) | ((uint32_t)(TILE >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_e4m3(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                         uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
@@ -222,6 +246,82 @@ __global__ void k_knn_prep(const float* __restrict__ X, uint64_t n, uint32_t d, 
     }
 }
 
+// max |x_ik| and max |x_i|^2 over the point set (non-negative floats order like
+// their bit patterns, so an integer atomicMax finds them).
+__global__ void k_knn_scales(const float* __restrict__ X, uint64_t n, uint32_t d, unsigned* maxabs,
+                             unsigned* maxnorm) {
+    float ma = 0.0f, mn = 0.0f;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* x = X + i * d;
+        float nrm = 0.0f;
+        for (uint32_t j = 0; j < d; ++j) {
+            ma = fmaxf(ma, fabsf(x[j]));
+            nrm = __fmaf_rn(x[j], x[j], nrm);
+        }
+        mn = fmaxf(mn, nrm);
+    }
+    for (int o = 16; o; o >>= 1) {
+        ma = fmaxf(ma, __shfl_xor_sync(0xFFFFFFFFu, ma, o));
+        mn = fmaxf(mn, __shfl_xor_sync(0xFFFFFFFFu, mn, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMax(maxabs, __float_as_uint(ma));
+        atomicMax(maxnorm, __float_as_uint(mn));
+    }
+}
+
+__device__ __forceinline__ uint8_t to_e4m3(float x) { return (uint8_t)__nv_cvt_float_to_fp8(x, __NV_SATFINITE, __NV_E4M3); }
+
+__device__ __forceinline__ float from_e4m3(uint8_t b) {
+    __nv_fp8_e4m3 v;
+    v.__x = (__nv_fp8_storage_t)b;
+    return (float)v;
+}
+
+// FP8 operands (64 one-byte columns, D <= 61): see the file comment.
+__global__ void k_knn_prep_f8(const float* __restrict__ X, uint64_t n, uint32_t d, const unsigned* __restrict__ maxabs,
+                              const unsigned* __restrict__ maxnorm, uint8_t* A, uint8_t* B) {
+    constexpr uint32_t W = 64;
+    const float ma = __uint_as_float(*maxabs), mn = __uint_as_float(*maxnorm);
+    const float S = ma > 0.0f ? ma / 256.0f : 1.0f;
+    const float Sn = mn > 0.0f ? mn / 256.0f : 1.0f;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* x = X + i * d;
+        uint8_t* a = A + i * W;
+        uint8_t* b = B + i * W;
+        float nrm = 0.0f, m = 0.0f;
+        for (uint32_t j = 0; j < d; ++j) {
+            nrm = __fmaf_rn(x[j], x[j], nrm);
+            m = fmaxf(m, fabsf(2.0f * x[j] * S / Sn));
+        }
+        // power-of-two row factor f with m f <= 448, f in [2^-9, 2^8] (both e4m3-exact)
+        int e = 8;
+        if (m > 0.0f) {
+            e = (int)floorf(log2f(448.0f / m));
+            e = e < -9 ? -9 : (e > 8 ? 8 : e);
+        }
+        const float f = ldexpf(1.0f, e);
+        for (uint32_t j = 0; j < d; ++j) {
+            a[j] = to_e4m3(-2.0f * x[j] * S / Sn * f);
+            b[j] = to_e4m3(x[j] / S);
+        }
+        // |x|^2 / S_n as three e4m3 terms (each takes the remainder of the last)
+        float v = nrm / Sn;
+        for (uint32_t t = 0; t < 3; ++t) {
+            const uint8_t q = to_e4m3(v);
+            b[d + t] = q;
+            a[d + t] = to_e4m3(f);
+            v -= from_e4m3(q);
+        }
+        for (uint32_t j = d + 3; j < W; ++j) {
+            a[j] = 0;
+            b[j] = 0;
+        }
+    }
+}
+
 // ------------------------------------------------------------ tensor-core candidate search
 template <int KA>
 struct KnnSmem {
@@ -238,7 +338,8 @@ struct KnnSmem {
     static constexpr uint32_t BYTES = MISC_OFF + 64 + 1024;  // + alignment slack
 };
 
-template <int KA>
+// F8: the operands are e4m3 bytes with the row size of BF16 KA columns.
+template <int KA, bool F8>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
              uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status) {
@@ -327,7 +428,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
     } else if (warp == 1) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            constexpr uint32_t idesc = idesc_bf16_128x128();
+            constexpr uint32_t idesc = F8 ? idesc_e4m3_128x128() : idesc_bf16_128x128();
             uint64_t it = 0;
             uint32_t gi = 0;
             for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x, ++gi) {
@@ -355,9 +456,14 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                         const uint32_t abase = smem_u32(sA + q * L::TILE_BYTES);
                         const uint32_t d = tmem + b * (QT * TILE) + q * TILE;
 #pragma unroll
-                        for (int kk = 0; kk < KA / 16; ++kk)
-                            mma_bf16(d, smem_desc<KA>(abase + kk * 32), smem_desc<KA>(bbase + kk * 32), idesc,
-                                     kk > 0 ? 1u : 0u);
+                        for (int kk = 0; kk < KA / 16; ++kk) {  // 32 bytes of K per MMA
+                            if constexpr (F8)
+                                mma_e4m3(d, smem_desc<KA>(abase + kk * 32), smem_desc<KA>(bbase + kk * 32), idesc,
+                                         kk > 0 ? 1u : 0u);
+                            else
+                                mma_bf16(d, smem_desc<KA>(abase + kk * 32), smem_desc<KA>(bbase + kk * 32), idesc,
+                                         kk > 0 ? 1u : 0u);
+                        }
                     }
                     mma_commit(empty + s);
                     mma_commit(accfull + b);
@@ -601,19 +707,33 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     return fn;
 }
 
-template <int KA>
-CUtensorMap make_map(const __nv_bfloat16* base, uint64_t n) {
+// 2-D map of n rows of `row_bytes` bytes, tiles of 128 rows, swizzled by the row size.
+CUtensorMap make_map(const void* base, uint64_t n, uint32_t row_bytes, bool bytes_type) {
     CUtensorMap m;
-    cuuint64_t dims[2] = {(cuuint64_t)KA, (cuuint64_t)n};
-    cuuint64_t strides[1] = {(cuuint64_t)KA * 2};
-    cuuint32_t box[2] = {(cuuint32_t)KA, (cuuint32_t)TILE};
+    const uint32_t esize = bytes_type ? 1 : 2;
+    cuuint64_t dims[2] = {(cuuint64_t)(row_bytes / esize), (cuuint64_t)n};
+    cuuint64_t strides[1] = {(cuuint64_t)row_bytes};
+    cuuint32_t box[2] = {(cuuint32_t)(row_bytes / esize), (cuuint32_t)TILE};
     cuuint32_t estr[2] = {1, 1};
-    CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, (void*)base, dims, strides, box, estr,
-                             CU_TENSOR_MAP_INTERLEAVE_NONE,
-                             KA == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+    CUresult r = encode_fn()(&m, bytes_type ? CU_TENSOR_MAP_DATA_TYPE_UINT8 : CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2,
+                             (void*)base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                             row_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
                              CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) fail(SC_E_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return m;
+}
+
+template <int KA, bool F8>
+void launch_tc(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, uint64_t n, uint64_t nq, float* cand_score,
+               uint32_t* cand_idx) {
+    using L = KnnSmem<KA>;
+    SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
+    const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
+    const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
+    k_knn_tc<KA, F8><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
+                                                                 cand_idx, c.d_status);
+    SC_LAUNCH_CHECK();
+    c.launches++;
 }
 
 // Candidates of the queries q0 .. q0 + nq - 1 against all n points. A is the
@@ -625,22 +745,33 @@ void candidates(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0, ui
     DBuf<__nv_bfloat16> A(c, n * KA), B(c, n * KA);
     k_knn_prep<KA><<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, A.get(), B.get());
     SC_LAUNCH_CHECK();
-    CUtensorMap ta = make_map<KA>(A.get() + q0 * KA, nq), tb = make_map<KA>(B.get(), n);
-    using L = KnnSmem<KA>;
-    SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
-    const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
-    const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
-    k_knn_tc<KA><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
-                                                             cand_idx, c.d_status);
+    c.launches++;
+    CUtensorMap ta = make_map(A.get() + q0 * KA, nq, KA * 2, false), tb = make_map(B.get(), n, KA * 2, false);
+    launch_tc<KA, false>(c, ta, tb, n, nq, cand_score, cand_idx);
+}
+
+// The same search with e4m3 operands (64-byte rows, the geometry of BF16 KA = 32).
+void candidates_f8(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0, uint64_t nq, float* cand_score,
+                   uint32_t* cand_idx) {
+    DBuf<uint8_t> A(c, n * 64), B(c, n * 64);
+    DBuf<unsigned> mx(c, 2);
+    zero(c, mx.get(), 2);
+    k_knn_scales<<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, mx.get(), mx.get() + 1);
+    k_knn_prep_f8<<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, mx.get(), mx.get() + 1, A.get(), B.get());
     SC_LAUNCH_CHECK();
     c.launches += 2;
+    CUtensorMap ta = make_map(A.get() + q0 * 64, nq, 64, true), tb = make_map(B.get(), n, 64, true);
+    launch_tc<32, true>(c, ta, tb, n, nq, cand_score, cand_idx);
 }
 
 void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
     if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
     if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
     if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
-    if (opts.precision != SC_KNN_BF16) fail(SC_E_UNSUPPORTED, "only the BF16 contraction is built");
+    if (opts.precision != SC_KNN_BF16 && opts.precision != SC_KNN_FP8)
+        fail(SC_E_UNSUPPORTED, "the candidate contraction runs in BF16 or FP8 (e4m3)");
+    if (opts.precision == SC_KNN_FP8 && d > 61)
+        fail(SC_E_UNSUPPORTED, "the FP8 contraction supports 1..61 dimensions, got %llu", (unsigned long long)d);
 }
 
 // Exact (brute-force) k+1 nearest points of the queries q0 .. q0 + nq - 1
@@ -649,11 +780,12 @@ void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
 // scores, ranked exactly in FP32. idx/d2 are nq x (k+1), self first, then
 // ascending squared distance, ties by lower index.
 void knn_search_device(Ctx& c, const float* dX, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t nq,
-                       uint32_t* idx, float* d2) {
+                       bool f8, uint32_t* idx, float* d2) {
     if (!nq) return;
     DBuf<float> cscore(c, nq * RTOTAL);
     DBuf<uint32_t> cidx(c, nq * RTOTAL);
-    if (d <= 30) candidates<32>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    if (f8) candidates_f8(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    else if (d <= 30) candidates<32>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
     else candidates<64>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
     k_knn_rerank<<<grid_for(nq * 32, 256), 256, 0, c.stream>>>(dX, n, (uint32_t)d, (uint32_t)k, q0, nq,
                                                                 cidx.get(), idx, d2);
@@ -740,7 +872,7 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, co
     h2d(c, dX.get(), X, n * d);
     DBuf<uint32_t> idx(c, n * (k + 1));
     DBuf<float> d2(c, n * (k + 1));
-    knn_search_device(c, dX.get(), n, d, k, 0, n, idx.get(), d2.get());
+    knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
     copy_lists_out(c, idx.get(), d2.get(), n, k, opts.squared_kiddo, knn_index, knn_dist);
     if (!conn_ptrs && !graph_out) return;
     knn_connectivities_device(c, idx.get(), d2.get(), n, k, opts, conn_ptrs, conn_nbrs, conn_w, conn_cap, conn_nnz,
@@ -759,7 +891,7 @@ void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint
     h2d(c, dX.get(), X, n * d);
     DBuf<uint32_t> idx(c, nq * (k + 1));
     DBuf<float> d2(c, nq * (k + 1));
-    knn_search_device(c, dX.get(), n, d, k, q0, nq, idx.get(), d2.get());
+    knn_search_device(c, dX.get(), n, d, k, q0, nq, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
     copy_lists_out(c, idx.get(), d2.get(), nq, k, 1, knn_index, knn_d2);
 }
 

@@ -159,10 +159,11 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 // REFINE=false: local moving. REFINE=true: refinement (singletons only, inside
 // the constraint, randomised choice among non-negative candidates).
 template <int G, bool REFINE>
-__global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(TB, 5) k_decide_small(Params p, const uint32_t* __restrict__ list,
                                                         const uint64_t* __restrict__ lbeg,
                                                         const uint32_t* __restrict__ ldeg, uint32_t count) {
     const unsigned FULL = 0xFFFFFFFFu;
+    __shared__ unsigned long long s_acc[TB];
     const int lane = threadIdx.x & 31;
     const int sub = lane & (G - 1);
     const int gw = lane / G;  // group within warp
@@ -200,12 +201,14 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
         const uint64_t key = valid ? (((uint64_t)gw << 32) | cu) : (0xFFFFFFFF00000000ull | (uint64_t)lane);
         const unsigned mm = __match_any_sync(FULL, key);
         const bool leader = valid && (__ffs(mm) - 1 == lane);
-        long long acc = 0;
-#pragma unroll
-        for (int t = 0; t < G; ++t) {
-            long long x = __shfl_sync(FULL, wf, gbase + t);
-            if ((mm >> (gbase + t)) & 1u) acc += x;
-        }
+        // per-community sums: every lane adds into its group leader's shared slot
+        // (integer adds, so the order does not matter); only leaders read theirs
+        s_acc[threadIdx.x] = 0ull;
+        __syncwarp();
+        if (valid) atomicAdd(&s_acc[(threadIdx.x & ~31u) + (unsigned)(__ffs(mm) - 1)], (unsigned long long)wf);
+        __syncwarp();
+        const long long acc = (long long)s_acc[threadIdx.x];
+        __syncwarp();
         // node quantities (identical in all lanes of the group)
         long long kf = 0, af = 0;
         double sl = 0.0;
@@ -333,6 +336,31 @@ __device__ bool hinsert(uint32_t* keys, long long* vals, uint32_t mask, uint32_t
     return false;
 }
 
+// hinsert that also appends every slot it claims to `list` (the distinct keys,
+// in no particular order; the caller sized `list` for all of them).
+__device__ void hinsert_listed(uint32_t* keys, long long* vals, uint32_t mask, uint32_t c, long long x,
+                               uint32_t* status, uint32_t* list, uint32_t* count, uint32_t list_cap) {
+    uint32_t h = hslot(c, mask);
+    for (uint32_t probe = 0; probe <= mask; ++probe) {
+        uint32_t k = keys[h];
+        if (k == EMPTYK) {
+            const uint32_t prev = atomicCAS(keys + h, EMPTYK, c);
+            if (prev == EMPTYK) {
+                const uint32_t i = atomicAdd(count, 1u);
+                if (i < list_cap) list[i] = h;
+                else atomicOr(status, DEV_OVERFLOW);
+            }
+            k = prev == EMPTYK ? c : prev;
+        }
+        if (k == c) {
+            atomicAdd((unsigned long long*)(vals + h), (unsigned long long)x);
+            return;
+        }
+        h = (h + 1) & mask;
+    }
+    atomicOr(status, DEV_OVERFLOW);
+}
+
 __device__ long long hlookup(const uint32_t* keys, const long long* vals, uint32_t mask, uint32_t c) {
     uint32_t h = hslot(c, mask);
     for (uint32_t probe = 0; probe <= mask; ++probe) {
@@ -393,6 +421,8 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
                                                                       uint32_t count) {
     __shared__ uint32_t s_keys[WARPS_PER_BLOCK][WCAP];
     __shared__ long long s_vals[WARPS_PER_BLOCK][WCAP];
+    __shared__ uint32_t s_list[WARPS_PER_BLOCK][WARP_DEGREE];  // claimed slots: the distinct communities
+    __shared__ uint32_t s_cnt[WARPS_PER_BLOCK];
     const unsigned FULL = 0xFFFFFFFFu;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     uint32_t* keys = s_keys[wib];
@@ -417,15 +447,18 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
             keys[s] = EMPTYK;
             vals[s] = 0;
         }
+        if (lane == 0) s_cnt[wib] = 0;
         __syncwarp();
         const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
         for (uint64_t j = b + lane; j < e; j += 32) {
             const uint32_t u = ro(p.nbr + (j));
             if (u == v) continue;
             if (REFINE && ro(p.constraint + (u)) != cv) continue;
-            hinsert(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status);
+            hinsert_listed(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status,
+                           s_list[wib], &s_cnt[wib], WARP_DEGREE);
         }
         __syncwarp();
+        const uint32_t ndist = min(s_cnt[wib], WARP_DEGREE);
         const long long kf = to_fix(ro(p.strength + (v)), p.inv_scale);
         const long long af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
         const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = ro(p.self_loop + (v));
@@ -435,9 +468,10 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         double g = -INFINITY;
         uint32_t c = NONE32;
         uint32_t lc = 0;
-        for (uint32_t s = lane; s < cap; s += 32) {
+        for (uint32_t t = lane; t < ndist; t += 32) {  // the distinct communities only
+            const uint32_t s = s_list[wib][t];
             const uint32_t cu = keys[s];
-            if (cu == EMPTYK || cu == own) continue;
+            if (cu == own) continue;
             lc++;
             const double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;

@@ -208,13 +208,17 @@ def test_aggregate_of_balanced_asymmetric_graph():
 
 
 def test_aggregate_large_rows_use_the_block_contraction():
-    """Groups whose members hold more than 256 entries (a block per row, table
-    in global memory, segmented sort) next to small ones (a warp per row)."""
+    """Each row-size path of the exact-regime contraction: small rows (a warp
+    per row), one large row whose table fits shared memory, one large row with
+    more distinct neighbour groups than that (table in global memory), and
+    large rows holding most entries (the sort path)."""
     src, dst, w, truth = synth.planted_partition(6000, 6, 12, 3, seed=4)
     og = O.Graph.from_edges(6000, src=src, dst=dst, w=w)
     gg = sc_gpu.CSRNetwork.from_edge_arrays(6000, src, dst, w)
-    mixed = np.where(truth < 2, truth, 2 + np.arange(6000) // 3).astype(np.uint64)
-    for p in (truth, mixed, np.zeros(6000, np.uint64)):
+    v = np.arange(6000)
+    shared_row = np.where(v < 300, 0, 1 + (v - 300) // 3).astype(np.uint64)
+    global_row = np.where(v < 200, 0, v - 199).astype(np.uint64)
+    for p in (shared_row, global_row, truth, np.zeros(6000, np.uint64)):
         assert_same_graph(og.aggregate(p), gg.aggregate(p))
 
 
