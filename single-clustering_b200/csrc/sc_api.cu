@@ -100,6 +100,7 @@ void release_ctx(sc::Ctx& c) {
     }
     if (c.d_status) cudaFree(c.d_status);
     c.d_status = nullptr;
+    c.pool = nullptr;  // the device's default pool: not ours to destroy
 }
 
 // Runs instance i of a batch on worker context w (labels copied to the host).

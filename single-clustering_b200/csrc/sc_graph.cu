@@ -735,10 +735,16 @@ __device__ __forceinline__ void seg_emit(uint64_t s, uint64_t b, double acc, con
     keep[s] = (acc > 0.0) && ((double)val != 0.0);
 }
 
+// Segments at least SEG_BLOCK long, in the exact regime, are summed by a whole
+// block (k_seg_values_long): any order gives the exact sum, and one warp folding
+// a segment of a coarse community's internal entries alone takes milliseconds.
+constexpr uint64_t SEG_BLOCK = 4096;
+
 __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
                              const uint64_t* __restrict__ keys, const float* __restrict__ w,
                              uint64_t G, const double* __restrict__ loops, uint32_t* prow,
-                             uint32_t* pcol, float* pw, uint8_t* keep, int exact) {
+                             uint32_t* pcol, float* pw, uint8_t* keep, int exact, uint32_t* long_list,
+                             uint32_t* long_count, uint32_t long_cap) {
     constexpr uint64_t SHORT = 64;
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -761,9 +767,42 @@ __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P,
             const int src = __ffs(long_mask) - 1;
             long_mask &= long_mask - 1;
             const uint64_t bb = __shfl_sync(0xFFFFFFFFu, b, src), ee = __shfl_sync(0xFFFFFFFFu, e, src);
+            if (exact && ee - bb >= SEG_BLOCK && long_list) {  // warp-uniform
+                if ((int)lane == src) {
+                    const uint32_t i = atomicAdd(long_count, 1u);
+                    if (i < long_cap) long_list[i] = (uint32_t)s;
+                }
+                continue;
+            }
             const double acc = warp_fold(bb, ee, 0.0, exact, [&](uint64_t i) { return (double)w[i]; });
             if ((int)lane == src) seg_emit(s, b, acc, keys, G, loops, prow, pcol, pw, keep);
         }
+    }
+}
+
+// One block per listed long segment (exact regime): block-wide sum, then the
+// same emission as k_seg_values.
+__global__ void k_seg_values_long(const uint32_t* __restrict__ long_list, const uint32_t* __restrict__ long_count,
+                                  const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
+                                  const uint64_t* __restrict__ keys, const float* __restrict__ w, uint64_t G,
+                                  const double* __restrict__ loops, uint32_t* prow, uint32_t* pcol, float* pw,
+                                  uint8_t* keep) {
+    __shared__ double red[32];
+    const uint32_t cnt = *long_count;
+    for (uint32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+        const uint32_t s = long_list[li];
+        const uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
+        double acc = 0.0;
+        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) acc += (double)w[i];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double t = 0.0;
+            for (unsigned k = 0; k < (blockDim.x >> 5); ++k) t += red[k];
+            seg_emit(s, b, t, keys, G, loops, prow, pcol, pw, keep);
+        }
+        __syncthreads();
     }
 }
 
@@ -937,6 +976,86 @@ __device__ __forceinline__ void warp_member_entries(const uint64_t* __restrict__
     }
 }
 
+// The member entries of one group flattened across the whole block: members
+// in chunks of blockDim, a block-wide prefix of their degrees in shared memory,
+// every thread takes entries t, t + blockDim, ... and finds its member by binary
+// search. f(j, valid) is called by every thread of the block the same number
+// of times (valid false past the end), so f may use warp-collective operations.
+template <class F>
+__device__ __forceinline__ void block_member_entries(const uint64_t* __restrict__ ptr,
+                                                     const uint32_t* __restrict__ members, uint64_t m0, uint64_t m1,
+                                                     uint64_t* s_pref, uint64_t* s_beg, uint64_t* s_wsum, F&& f) {
+    const unsigned tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5, nw = blockDim.x >> 5;
+    for (uint64_t mb = m0; mb < m1; mb += blockDim.x) {
+        const uint64_t mi = mb + tid;
+        uint64_t b = 0, d = 0;
+        if (mi < m1) {
+            const uint32_t v = members[mi];
+            b = ptr[v];
+            d = ptr[v + 1] - b;
+        }
+        uint64_t incl = d;
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint64_t t = __shfl_up_sync(0xFFFFFFFFu, incl, o);
+            if ((int)lane >= o) incl += t;
+        }
+        if (lane == 31) s_wsum[wid] = incl;
+        __syncthreads();
+        uint64_t off = 0;
+        for (unsigned k = 0; k < wid; ++k) off += s_wsum[k];
+        s_pref[tid + 1] = off + incl;
+        s_beg[tid] = b;
+        if (tid == 0) s_pref[0] = 0;
+        __syncthreads();
+        const uint64_t nmem = (m1 - mb) < blockDim.x ? (m1 - mb) : blockDim.x;
+        const uint64_t total = s_pref[nmem];
+        for (uint64_t base = 0; base < total; base += blockDim.x) {
+            const uint64_t t = base + tid;
+            const bool valid = t < total;
+            uint64_t j = 0;
+            if (valid) {
+                uint64_t lo = 0, hi = nmem;  // largest L with s_pref[L] <= t
+                while (hi - lo > 1) {
+                    const uint64_t mid = (lo + hi) >> 1;
+                    if (s_pref[mid] <= t) lo = mid;
+                    else hi = mid;
+                }
+                j = s_beg[lo] + (t - s_pref[lo]);
+            }
+            f(j, valid);
+        }
+        __syncthreads();
+        (void)nw;
+    }
+}
+
+// Warp-combined insert: lanes with the same key add their values through the
+// lowest such lane, so a key hit by many lanes costs one shared atomic.
+__device__ __forceinline__ void agg_insert_fix_combined(uint32_t* keys, unsigned long long* vals, uint64_t size,
+                                                        uint64_t mask, bool valid, uint32_t h,
+                                                        unsigned long long x, uint32_t* status) {
+    const unsigned lane = threadIdx.x & 31u;
+    const unsigned long long key = valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | lane);
+    const unsigned mm = __match_any_sync(0xFFFFFFFFu, key);
+    unsigned long long acc = 0;
+#pragma unroll
+    for (int L = 0; L < 32; ++L) {
+        const unsigned long long y = __shfl_sync(0xFFFFFFFFu, x, L);
+        if ((mm >> L) & 1u) acc += y;
+    }
+    if (!valid || (int)lane != __ffs(mm) - 1) return;
+    uint64_t slot = agg_hash(h) & mask;
+    for (uint64_t probe = 0; probe < size; ++probe) {
+        const uint32_t prev = atomicCAS(keys + slot, AGG_EMPTY, h);
+        if (prev == AGG_EMPTY || prev == h) {
+            atomicAdd(vals + slot, acc);
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+    atomicOr(status, DEV_OVERFLOW);
+}
+
 __global__ void __launch_bounds__(32 * AGG_WARPS)
     k_contract_warp(const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members, uint64_t G,
                     const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
@@ -1090,7 +1209,7 @@ __global__ void __launch_bounds__(256)
     uint32_t* sk = keys + AGG_SMEM_SLOTS;                              // AGG_SMEM_KEEP
     float* sv = (float*)(sk + AGG_SMEM_KEEP);                          // AGG_SMEM_KEEP
     __shared__ uint32_t s_n;
-    const int wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ uint64_t s_pref[257], s_beg[256], s_wsum[8];
     for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
         const uint32_t g = rows[i];
         const uint64_t size = agg_slots(cap[g], G);
@@ -1101,25 +1220,16 @@ __global__ void __launch_bounds__(256)
         }
         if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
-        const uint64_t m0 = gstart[g], m1 = gstart[g + 1];
-        for (uint64_t mb = m0 + (uint64_t)wib * 32; mb < m1; mb += (uint64_t)nw * 32) {
-            const uint64_t me = mb + 32 < m1 ? mb + 32 : m1;
-            warp_member_entries(ptr, members, mb, me, [&](uint64_t j) {
-                const uint32_t h = grp[nbr[j]];
-                const unsigned long long x = (unsigned long long)__double2ll_rn(__dmul_rn((double)w[j], inv_scale));
-                uint64_t slot = agg_hash(h) & mask;
-                for (uint64_t probe = 0; probe < size; ++probe) {
-                    const uint32_t prev = atomicCAS(keys + slot, AGG_EMPTY, h);
-                    if (prev == AGG_EMPTY || prev == h) {
-                        atomicAdd(vals + slot, x);
-                        return;
-                    }
-                    slot = (slot + 1) & mask;
-                }
-                atomicOr(status, DEV_OVERFLOW);
-            });
-        }
-        __syncthreads();
+        block_member_entries(ptr, members, gstart[g], gstart[g + 1], s_pref, s_beg, s_wsum,
+                             [&](uint64_t j, bool valid) {
+                                 uint32_t h = 0;
+                                 unsigned long long x = 0;
+                                 if (valid) {
+                                     h = grp[nbr[j]];
+                                     x = (unsigned long long)__double2ll_rn(__dmul_rn((double)w[j], inv_scale));
+                                 }
+                                 agg_insert_fix_combined(keys, vals, size, mask, valid, h, x, status);
+                             });
         for (uint64_t s2 = threadIdx.x; s2 < size; s2 += blockDim.x) {
             const uint32_t h = keys[s2];
             if (h == AGG_EMPTY) continue;
@@ -1445,11 +1555,19 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         pcol.alloc(c, P);
         pw.alloc(c, P);
         keep.alloc(c, P);
+        const uint32_t long_cap = (uint32_t)(N / SEG_BLOCK + 1);
+        DBuf<uint32_t> long_list(c, long_cap), long_count(c, 1);
+        zero(c, long_count.get(), 1);
         k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
                                                            uw_s.get(), G, loops.get(), prow.get(),
-                                                           pcol.get(), pw.get(), keep.get(), (int)g.exact_w);
+                                                           pcol.get(), pw.get(), keep.get(), (int)g.exact_w,
+                                                           long_list.get(), long_count.get(), long_cap);
+        if (g.exact_w)
+            k_seg_values_long<<<std::min<unsigned>(long_cap, (unsigned)c.sm_count * 2), TB, 0, c.stream>>>(
+                long_list.get(), long_count.get(), seg.get(), P, N, ukeys_s.get(), uw_s.get(), G, loops.get(),
+                prow.get(), pcol.get(), pw.get(), keep.get());
         SC_LAUNCH_CHECK();
-        c.launches++;
+        c.launches += 2;
     }
     ukeys_s.release();
     uw_s.release();

@@ -63,7 +63,7 @@ constexpr uint32_t HUB_DEGREE = 1024;  // degree above which a node's hash lives
 struct Ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
-    cudaMemPool_t pool = nullptr;
+    cudaMemPool_t pool = nullptr;      // the device's default pool (stream-ordered temporaries)
     uint32_t* d_status = nullptr;      // device status word
     Error last;
     sc_run_stats stats{};
@@ -73,7 +73,7 @@ struct Ctx {
     sc_tuning tuning{8, 16, 32, 4096};  // decide-kernel routing (sc_set_tuning / sc_autotune)
 };
 
-// Stream-ordered device buffer of T (cudaMallocAsync on the context stream).
+// Stream-ordered device buffer of T, from the context's pool on its stream.
 template <class T>
 struct DBuf {
     T* p = nullptr;
@@ -86,12 +86,12 @@ struct DBuf {
         s = c.stream;
         n = count;
         if (count) {
-            cudaError_t e = cudaMallocAsync((void**)&p, count * sizeof(T), s);
+            cudaError_t e = cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), c.pool, s);
             if (e == cudaErrorMemoryAllocation) {
                 cudaGetLastError();
                 fail(SC_E_OUT_OF_MEMORY, "device allocation of %zu bytes failed", count * sizeof(T));
             }
-            if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
+            if (e != cudaSuccess) throw_cuda(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
         }
     }
     void release() {

@@ -159,7 +159,7 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 // REFINE=false: local moving. REFINE=true: refinement (singletons only, inside
 // the constraint, randomised choice among non-negative candidates).
 template <int G, bool REFINE>
-__global__ void __launch_bounds__(TB, 5) k_decide_small(Params p, const uint32_t* __restrict__ list,
+__global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t* __restrict__ list,
                                                         const uint64_t* __restrict__ lbeg,
                                                         const uint32_t* __restrict__ ldeg, uint32_t count) {
     const unsigned FULL = 0xFFFFFFFFu;
@@ -174,26 +174,42 @@ __global__ void __launch_bounds__(TB, 5) k_decide_small(Params p, const uint32_t
     const int per_warp = 32 / G;
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
 
-    for (uint64_t wb = warp * per_warp; wb < count; wb += nwarps * per_warp) {
+    // Software pipeline: the list entry and this lane's neighbour id / weight of
+    // the group's next node are loaded one iteration ahead, so their round trip
+    // overlaps the current node's membership gathers and scoring.
+    const uint64_t step = nwarps * per_warp;
+    uint32_t nv = 0, nu = 0;
+    uint64_t nb = 0;
+    int ndeg = 0;
+    float nwt = 0.0f;
+    auto fetch = [&](uint64_t w0) {
+        const uint64_t i = w0 + gw;
+        nv = 0, nu = 0, nb = 0, ndeg = 0, nwt = 0.0f;
+        if (i < count) {
+            nv = ro(list + i);
+            nb = ro(lbeg + i);
+            ndeg = (int)ro(ldeg + i);
+            if (sub < ndeg) {
+                nu = ro(p.nbr + (nb + sub));
+                nwt = ro(p.w + (nb + sub));
+            }
+        }
+    };
+    fetch(warp * per_warp);
+    for (uint64_t wb = warp * per_warp; wb < count; wb += step) {
         const uint64_t i = wb + gw;
         const bool have = i < count;
-        const uint32_t v = have ? ro(list + (i)) : 0;
-        uint64_t b = 0, e = 0;
-        if (have) {
-            b = ro(lbeg + i);
-            e = b + ro(ldeg + i);
-        }
-        const int deg = (int)(e - b);
+        const uint32_t v = nv;
+        const int deg = ndeg;
+        const uint32_t u_next = nu;
+        const float wt_next = nwt;
+        fetch(wb + step);
         const uint32_t own = have ? ro(p.memb + (v)) : 0;
         bool eligible = have;
         if (REFINE && have) eligible = ro(p.csize + (own)) == 1;  // refine.rs:60-62
         bool valid = eligible && sub < deg;
-        uint32_t u = 0;
-        float wt = 0.0f;
-        if (valid) {
-            u = ro(p.nbr + (b + sub));
-            wt = ro(p.w + (b + sub));
-        }
+        const uint32_t u = valid ? u_next : 0;
+        const float wt = valid ? wt_next : 0.0f;
         valid = valid && u != v;
         if (REFINE && valid) valid = ro(p.constraint + (u)) == ro(p.constraint + (v));
         const uint32_t cu = valid ? ro(p.memb + (u)) : NONE32;
@@ -694,8 +710,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
 
 // ------------------------------------------------------------ commit
 template <bool REFINE>
-__global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t count,
-                        uint8_t* next_active) {
+__global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t count) {
     unsigned long long nmoves = 0;
     long long gsum = 0;
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
@@ -725,7 +740,10 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
 // Re-queue the neighbours of every node that moved in this batch and now sits
 // in a different community from them (local_move.rs:113-118). Runs after the
 // commit, so every membership it reads is final.
-__global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t count, uint8_t* next_active) {
+// A node enters the next sweep's list once: its stamp is raised to `mark` (the
+// next sweep's number + 1) and only the lane that raised it appends it.
+__global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t count, uint32_t* stamp,
+                           uint32_t mark, uint32_t* next_list, uint32_t* next_count) {
     // one warp per node of the batch, lanes over its row (coalesced)
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -735,9 +753,22 @@ __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t
         if (p.moved[v] != p.cur) continue;
         const uint32_t t = p.memb[v];
         const uint64_t e = p.ptr[v + 1];
-        for (uint64_t j = p.ptr[v] + lane; j < e; j += 32) {
-            const uint32_t u = p.nbr[j];
-            if (u != v && p.memb[u] != t) next_active[u] = 1;
+        for (uint64_t j0 = p.ptr[v]; j0 < e; j0 += 32) {
+            const uint64_t j = j0 + lane;
+            uint32_t u = 0;
+            bool add = false;
+            if (j < e) {
+                u = p.nbr[j];
+                add = u != v && p.memb[u] != t && atomicMax(stamp + u, mark) < mark;
+            }
+            const unsigned bal = __ballot_sync(0xFFFFFFFFu, add);
+            if (bal) {
+                const int leader = __ffs(bal) - 1;
+                uint32_t base = 0;
+                if ((int)lane == leader) base = atomicAdd(next_count, (uint32_t)__popc(bal));
+                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                if (add) next_list[base + __popc(bal & ((1u << lane) - 1u))] = u;
+            }
         }
     }
 }
@@ -764,14 +795,17 @@ __device__ __forceinline__ int bucket_of(uint32_t deg, Route r) {
     return deg <= r.g8 ? 0 : deg <= r.g16 ? 1 : deg <= r.g32 ? 2 : deg <= WARP_DEGREE ? 3 : deg <= HUB_DEGREE ? 4 : 5;
 }
 
-__global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
-                               uint64_t n, uint64_t seed, uint32_t sweep, int B, Route route, uint32_t* counts) {
+// The nodes of a sweep: alist[0 .. *acount) or, with alist == nullptr, all n.
+__global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ alist,
+                               const uint32_t* __restrict__ acount, uint64_t n, uint64_t seed, uint32_t sweep, int B,
+                               Route route, uint32_t* counts) {
     __shared__ uint32_t sc[64];
     for (int t = threadIdx.x; t < B * NBUCKET; t += blockDim.x) sc[t] = 0;
     __syncthreads();
-    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
-         v += (uint64_t)gridDim.x * blockDim.x) {
-        if (active && !active[v]) continue;
+    const uint64_t m = alist ? *acount : n;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t v = alist ? alist[i] : i;
         int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
         int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]), route);
         atomicAdd(&sc[b * NBUCKET + k], 1u);
@@ -782,17 +816,20 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint8_t* 
 }
 
 // One warp-aggregated atomic per distinct (batch, bucket) per warp.
-__global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint8_t* __restrict__ active,
-                                 uint64_t n, uint64_t seed, uint32_t sweep, int B, Route route,
-                                 uint32_t* cursor, uint32_t* list, uint64_t* lbeg, uint32_t* ldeg) {
+__global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ alist,
+                                 const uint32_t* __restrict__ acount, uint64_t n, uint64_t seed, uint32_t sweep,
+                                 int B, Route route, uint32_t* cursor, uint32_t* list, uint64_t* lbeg,
+                                 uint32_t* ldeg) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) - lane; base < n; base += stride) {
-        const uint64_t v = base + lane;
+    const uint64_t m = alist ? *acount : n;
+    for (uint64_t base = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) - lane; base < m; base += stride) {
+        const uint64_t i = base + lane;
+        const uint64_t v = i < m ? (alist ? alist[i] : i) : 0;
         int slot = -1;
         uint64_t rb = 0;
         uint32_t deg = 0;
-        if (v < n && (!active || active[v])) {
+        if (i < m) {
             int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
             rb = ptr[v];
             deg = (uint32_t)(ptr[v + 1] - rb);
@@ -845,12 +882,6 @@ __global__ void k_gather(const uint32_t* __restrict__ map, uint32_t* x, uint64_t
         x[i] = map[x[i]];
 }
 
-__global__ void k_fill_u8(uint8_t* p, uint64_t n, uint8_t v) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        p[i] = v;
-}
-
 // ------------------------------------------------------------ host side
 struct Scales {
     double scale, inv, nscale, ninv;
@@ -876,7 +907,9 @@ struct Workspace {
     DBuf<uint64_t> lbeg;  // row start of each list entry (written by the bucket scatter)
     DBuf<uint32_t> ldeg;  // degree of each list entry
     DBuf<long long> dgain;
-    DBuf<uint8_t> active, next_active;
+    DBuf<uint32_t> alist, nlist;    // this sweep's active nodes, the next sweep's
+    DBuf<uint32_t> acount, ncount;  // their counts (device)
+    DBuf<uint32_t> stamp;           // per node: 1 + the last sweep it was queued for
     DBuf<uint32_t> counts;
     DBuf<unsigned long long> counters;
     DBuf<long long> gain_acc;
@@ -921,8 +954,11 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.lbeg.alloc(c, n);
     ws.ldeg.alloc(c, n);
     ws.dgain.alloc(c, n);
-    ws.active.alloc(c, n);
-    ws.next_active.alloc(c, n);
+    ws.alist.alloc(c, n);
+    ws.nlist.alloc(c, n);
+    ws.acount.alloc(c, 1);
+    ws.ncount.alloc(c, 1);
+    ws.stamp.alloc(c, n);
     ws.counts.alloc(c, 64);
     ws.counters.alloc(c, 4);
     ws.gain_acc.alloc(c, 1);
@@ -1062,8 +1098,8 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     zero(c, ws.gain_acc.get(), 1);
     zero(c, ws.epoch.get(), n);
     zero(c, ws.moved.get(), n);
-    k_fill_u8<<<grid_for(n, TB), TB, 0, c.stream>>>(ws.active.get(), n, 1);
-    c.launches++;
+    zero(c, ws.stamp.get(), n);
+    bool all_active = true;  // sweep 0 visits every node
     const int B = LM_BATCHES;
     uint32_t epoch = 0;
     uint64_t moves_before = 0;
@@ -1073,9 +1109,10 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     const double tail = std::getenv("SC_LM_TAIL") ? std::atof(std::getenv("SC_LM_TAIL")) : 0.0;
     for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
         zero(c, ws.counts.get(), B * NBUCKET);
-        zero(c, ws.next_active.get(), n);
-        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B, route_of(c),
-                                                             ws.counts.get());
+        zero(c, ws.ncount.get(), 1);
+        const uint32_t* alist = all_active ? nullptr : ws.alist.get();
+        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, alist, ws.acount.get(), n, seed, sweep, B,
+                                                             route_of(c), ws.counts.get());
         SC_LAUNCH_CHECK();
         c.launches++;
         uint32_t counts[64];
@@ -1096,9 +1133,9 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         if (offs[B * NBUCKET] == 0) break;
         DBuf<uint32_t> cursor(c, 64);
         h2d(c, cursor.get(), offs, B * NBUCKET);
-        k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, ws.active.get(), n, seed, sweep, B, route_of(c),
-                                                               cursor.get(), ws.list.get(), ws.lbeg.get(),
-                                                               ws.ldeg.get());
+        k_bucket_scatter<<<grid_for(offs[B * NBUCKET], TB), TB, 0, c.stream>>>(
+            g.ptr, alist, ws.acount.get(), n, seed, sweep, B, route_of(c), cursor.get(), ws.list.get(),
+            ws.lbeg.get(), ws.ldeg.get());
         SC_LAUNCH_CHECK();
         c.launches++;
         for (int b = 0; b < B; ++b) {
@@ -1112,14 +1149,15 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
                 k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
                 c.launches++;
             }
-            k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo,
-                                                                       ws.next_active.get());
+            k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
             k_activate<<<grid_for((uint64_t)(hi - lo) * 32, TB, 148u * 64u), TB, 0, c.stream>>>(
-                p, ws.list.get() + lo, hi - lo, ws.next_active.get());
+                p, ws.list.get() + lo, hi - lo, ws.stamp.get(), sweep + 2, ws.nlist.get(), ws.ncount.get());
             SC_LAUNCH_CHECK();
             c.launches += 2;
         }
-        std::swap(ws.active, ws.next_active);
+        std::swap(ws.alist, ws.nlist);
+        std::swap(ws.acount, ws.ncount);
+        all_active = false;
         r.sweeps++;
     }
     unsigned long long ctr[4];
@@ -1192,7 +1230,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     zero(c, ws.epoch.get(), n);
     const int B = RF_BATCHES;
     zero(c, ws.counts.get(), B * NBUCKET);
-    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
+    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
                                                          ws.counts.get());
     SC_LAUNCH_CHECK();
     c.launches++;
@@ -1204,7 +1242,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
     DBuf<uint32_t> cursor(c, 64);
     h2d(c, cursor.get(), offs, B * NBUCKET);
-    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
+    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
                                                            cursor.get(), ws.list.get(), ws.lbeg.get(),
                                                            ws.ldeg.get());
     SC_LAUNCH_CHECK();
@@ -1218,7 +1256,7 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
             k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
             c.launches++;
         }
-        k_apply<true><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo, nullptr);
+        k_apply<true><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
         SC_LAUNCH_CHECK();
         c.launches++;
     }
