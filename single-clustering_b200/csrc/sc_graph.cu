@@ -1127,7 +1127,7 @@ __global__ void __launch_bounds__(256)
                      const uint64_t* __restrict__ capstart, const double* __restrict__ loops, uint32_t* hkeys,
                      double* hvals, uint32_t* tnbr, float* tw, uint32_t* cnt, uint32_t* status) {
     __shared__ unsigned long long s_n;
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __shared__ uint64_t s_pref[257], s_beg[256], s_wsum[8];
     for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
         const uint32_t g = rows[i];
         const uint64_t size = 2 * cap[g];
@@ -1139,15 +1139,28 @@ __global__ void __launch_bounds__(256)
         }
         if (threadIdx.x == 0) s_n = 0;
         __syncthreads();
-        // members dealt to the warps in chunks of 32
-        const uint64_t m0 = gstart[g], m1 = gstart[g + 1];
-        for (uint64_t mb = m0 + (uint64_t)wib * 32; mb < m1; mb += (uint64_t)nw * 32) {
-            const uint64_t me = mb + 32 < m1 ? mb + 32 : m1;
-            warp_member_entries(ptr, members, mb, me, [&](uint64_t j) {
-                agg_insert(keys, vals, size, grp[nbr[j]], (double)w[j], status);
-            });
-        }
-        __syncthreads();
+        block_member_entries(ptr, members, gstart[g], gstart[g + 1], s_pref, s_beg, s_wsum,
+                             [&](uint64_t j, bool valid) {
+                                 uint32_t h = 0;
+                                 double x = 0.0;
+                                 if (valid) {
+                                     h = grp[nbr[j]];
+                                     x = (double)w[j];
+                                 }
+                                 // lanes with the same key add through the lowest one
+                                 const unsigned lane = threadIdx.x & 31u;
+                                 const unsigned long long key =
+                                     valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | lane);
+                                 const unsigned mm = __match_any_sync(0xFFFFFFFFu, key);
+                                 double acc = 0.0;
+#pragma unroll
+                                 for (int L = 0; L < 32; ++L) {
+                                     const double y = __shfl_sync(0xFFFFFFFFu, x, L);
+                                     if ((mm >> L) & 1u) acc += y;
+                                 }
+                                 if (valid && (int)lane == __ffs(mm) - 1)
+                                     agg_insert(keys, vals, size, h, acc, status);
+                             });
         const uint64_t o = capstart[g];
         for (uint64_t s = threadIdx.x; s < size; s += blockDim.x) {
             const uint32_t h = keys[s];
@@ -1163,7 +1176,6 @@ __global__ void __launch_bounds__(256)
         __syncthreads();
         if (threadIdx.x == 0) cnt[g] = (uint32_t)s_n;
         __syncthreads();
-        (void)lane;
     }
 }
 
@@ -1368,7 +1380,7 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
     zero(c, cnt.get(), G + 1);
     // rows past the warp kernel: shared-table rows (mid) and global-table rows (large)
     DBuf<uint8_t> fmid(c, G), flag(c, G);
-    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 3);
+    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 4);
     DBuf<uint32_t> iota(c, G), rows(c, G), mrows(c, G);
     uint64_t nlarge = 0, nmid = 0;
     if (G) {
@@ -1380,14 +1392,19 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         select_flagged(c, iota.get(), flag.get(), rows.get(), nl.get(), G);
         select_flagged(c, iota.get(), fmid.get(), mrows.get(), nl.get() + 1, G);
         device_sum(c, lcap.get(), nl.get() + 2, G);
-        uint64_t counts[3];
-        d2h(c, counts, nl.get(), 3);
+        device_sum(c, hcap.get(), nl.get() + 3, G);
+        uint64_t counts[4];
+        d2h(c, counts, nl.get(), 4);
         sync(c);
         nlarge = counts[0];
         nmid = counts[1];
-        // Rows past the warp kernel are served by one block each; when they hold
-        // more than a tenth of the entries the sort path is faster.
-        if (counts[2] * 10 > g.E) return nullptr;
+        // Rows past the warp kernel are served by one block each. The sort path is
+        // faster when a few such rows (fewer than 4 per SM) hold more than a tenth
+        // of the entries (the blocks cannot fill the GPU), or when rows whose table
+        // must live in global memory hold more than a twentieth.
+        const uint64_t global_entries = counts[3] / 2;
+        if (global_entries * 20 > g.E) return nullptr;
+        if (counts[2] * 10 > g.E && counts[0] + counts[1] < 4ull * (uint64_t)c.sm_count) return nullptr;
     }
     if (nmid) {
         const size_t smem = AGG_SMEM_SLOTS * (sizeof(unsigned long long) + sizeof(uint32_t)) +

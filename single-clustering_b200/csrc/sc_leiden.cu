@@ -446,16 +446,46 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
+    // Software pipeline: the next node's list entry is loaded at the top of an
+    // iteration, its first 32 neighbour ids / weights once this node's entries
+    // are in the table; both round trips overlap this node's work.
+    uint32_t nv = 0, nu = 0, ndeg = 0;
+    uint64_t nb = 0;
+    float nw = 0.0f;
+    auto fetch_head = [&](uint64_t i) {
+        nv = 0, nb = 0, ndeg = 0;
+        if (i < count) {
+            nv = ro(list + i);
+            nb = ro(lbeg + i);
+            ndeg = ro(ldeg + i);
+        }
+    };
+    auto fetch_chunk = [&]() {
+        nu = 0, nw = 0.0f;
+        if ((uint32_t)lane < ndeg) {
+            nu = ro(p.nbr + (nb + lane));
+            nw = ro(p.w + (nb + lane));
+        }
+    };
+    fetch_head(warp);
+    fetch_chunk();
     for (uint64_t i = warp; i < count; i += nwarps) {
-        const uint32_t v = ro(list + (i));
-        const uint64_t b = ro(lbeg + i), e = b + ro(ldeg + i);
-        const uint32_t deg = (uint32_t)(e - b);
+        const uint32_t v = nv;
+        const uint64_t b = nb, e = b + ndeg;
+        const uint32_t deg = ndeg;
+        const uint32_t u_first = nu;
+        const float w_first = nw;
+        fetch_head(i + nwarps);
         const uint32_t own = ro(p.memb + (v));
-        if (REFINE && ro(p.csize + (own)) != 1) continue;  // warp-uniform
+        if (REFINE && ro(p.csize + (own)) != 1) {  // warp-uniform
+            fetch_chunk();
+            continue;
+        }
         uint32_t cap = 64;
         while (cap < 2 * deg) cap <<= 1;
         if (cap > (uint32_t)WCAP) {  // not this bucket's node
             if (lane == 0) atomicOr(p.status, DEV_OVERFLOW);
+            fetch_chunk();
             continue;
         }
         const uint32_t mask = cap - 1;
@@ -467,12 +497,15 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         __syncwarp();
         const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
         for (uint64_t j = b + lane; j < e; j += 32) {
-            const uint32_t u = ro(p.nbr + (j));
+            const bool first = j < b + 32;
+            const uint32_t u = first ? u_first : ro(p.nbr + (j));
             if (u == v) continue;
             if (REFINE && ro(p.constraint + (u)) != cv) continue;
-            hinsert_listed(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status,
+            const float wj = first ? w_first : ro(p.w + (j));
+            hinsert_listed(keys, vals, mask, ro(p.memb + (u)), to_fix((double)wj, p.inv_scale), p.status,
                            s_list[wib], &s_cnt[wib], WARP_DEGREE);
         }
+        fetch_chunk();
         __syncwarp();
         const uint32_t ndist = min(s_cnt[wib], WARP_DEGREE);
         const long long kf = to_fix(ro(p.strength + (v)), p.inv_scale);
