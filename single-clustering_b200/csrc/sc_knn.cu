@@ -178,6 +178,10 @@ struct Worst {
     int slot;
 };
 
+// A chunk whose candidates fall in at most this many of a warp's 32 rows is
+// processed by the whole warp, row by row; denser chunks by each lane alone.
+constexpr int COOP_ROWS = 8;
+
 __device__ __noinline__ Worst cand_insert(float* cs, uint32_t* ci, int qrow, int slot, float v, uint32_t idx) {
     constexpr int S = QT * HALVES * TILE;
     cs[slot * S + qrow] = v;
@@ -335,7 +339,10 @@ struct KnnSmem {
     static constexpr uint32_t BAR_OFF = I_OFF + RCAND * SLOTS * 4;
     static constexpr uint32_t NBAR = 2 * STAGES + 4 + 2;
     static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR * 8;
-    static constexpr uint32_t BYTES = MISC_OFF + 64 + 1024;  // + alignment slack
+    static constexpr uint32_t ROW_OFF = MISC_OFF + 64;                       // one staged row chunk per epilogue warp
+    static constexpr uint32_t BYTES = ROW_OFF + NUM_EPI_WARPS * 32 * 4 + 1024;  // + alignment slack
+    static_assert(BYTES <= 227 * 1024, "shared memory of the kNN kernel exceeds 227 KB");
+    static_assert(ROW_OFF % 16 == 0, "staged rows must be 16-byte aligned");
 };
 
 // F8: the operands are e4m3 bytes with the row size of BF16 KA columns.
@@ -482,6 +489,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
         const int row = lq * 32 + lane;         // row within the query tile
         const int owner = combo * TILE + row;   // candidate-buffer column
         constexpr int S = L::SLOTS;
+        float* srow = (float*)(smem + L::ROW_OFF) + ew * 32;  // this warp's staged row chunk
         uint64_t it = 0;
         for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x) {
             float thr = INFINITY;
@@ -511,14 +519,68 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     for (int w2 = 8; w2 >= 1; w2 >>= 1)
 #pragma unroll
                         for (int j = 0; j < w2; ++j) m[j] = fminf(m[j], m[j + w2]);
-                    if (m[0] < thr) {
-                        const uint32_t base_idx = t * TILE + h * (TILE / HALVES) + c0;
+                    const uint32_t base_idx = t * TILE + h * (TILE / HALVES) + c0;
+                    unsigned hits = __ballot_sync(0xFFFFFFFFu, m[0] < thr);
+                    if (__popc(hits) > COOP_ROWS) {
+                        // many rows have candidates: each lane scans its own row
+                        if (m[0] < thr) {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) {
-                            if (r[j] < thr && base_idx + j < n) {
-                                const Worst w = cand_insert(cs, ci, owner, thr_slot, r[j], base_idx + j);
-                                thr = w.thr;
-                                thr_slot = w.slot;
+                            for (int j = 0; j < 32; ++j) {
+                                if (r[j] < thr && base_idx + j < n) {
+                                    const Worst w = cand_insert(cs, ci, owner, thr_slot, r[j], base_idx + j);
+                                    thr = w.thr;
+                                    thr_slot = w.slot;
+                                }
+                            }
+                        }
+                    } else {
+                        // few rows: the warp takes them one at a time, lane j holding
+                        // column j; inserts in ascending column order with a warp argmax
+                        // over the row's kept slots (same operations as the lane path)
+                        while (hits) {
+                            const int L = __ffs(hits) - 1;
+                            hits &= hits - 1;
+                            if (lane == L) {
+#pragma unroll
+                                for (int j = 0; j < 32; j += 4)
+                                    *(float4*)(srow + j) = make_float4(r[j], r[j + 1], r[j + 2], r[j + 3]);
+                            }
+                            __syncwarp();
+                            const float v = srow[lane];
+                            __syncwarp();
+                            const int ownerL = owner - lane + L;
+                            float thrL = __shfl_sync(0xFFFFFFFFu, thr, L);
+                            int slotL = __shfl_sync(0xFFFFFFFFu, thr_slot, L);
+                            const bool inrange = base_idx + lane < n;
+                            unsigned cand = __ballot_sync(0xFFFFFFFFu, inrange && v < thrL);
+                            while (cand) {
+                                const int jc = __ffs(cand) - 1;
+                                if (lane == jc) {
+                                    cs[slotL * S + ownerL] = v;
+                                    ci[slotL * S + ownerL] = base_idx + jc;
+                                }
+                                __syncwarp();
+                                // new worst of the row: highest score, lowest slot on ties
+                                float wv = cs[lane * S + ownerL];
+                                int ws = lane;
+#pragma unroll
+                                for (int o = 16; o; o >>= 1) {
+                                    const float ov = __shfl_xor_sync(0xFFFFFFFFu, wv, o);
+                                    const int os = __shfl_xor_sync(0xFFFFFFFFu, ws, o);
+                                    if (ov > wv || (ov == wv && os < ws)) {
+                                        wv = ov;
+                                        ws = os;
+                                    }
+                                }
+                                thrL = wv;
+                                slotL = ws;
+                                // later columns of this row that still beat the new worst
+                                cand &= ~((2u << jc) - 1u);
+                                cand &= __ballot_sync(0xFFFFFFFFu, inrange && v < thrL);
+                            }
+                            if (lane == L) {
+                                thr = thrL;
+                                thr_slot = slotL;
                             }
                         }
                     }

@@ -944,6 +944,7 @@ struct Workspace {
     DBuf<uint32_t> acount, ncount;  // their counts (device)
     DBuf<uint32_t> stamp;           // per node: 1 + the last sweep it was queued for
     DBuf<uint32_t> counts;
+    DBuf<uint32_t> cursor;  // scatter cursors of the (batch, bucket) lists
     DBuf<unsigned long long> counters;
     DBuf<long long> gain_acc;
     DBuf<uint32_t> gkeys;
@@ -993,6 +994,7 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     ws.ncount.alloc(c, 1);
     ws.stamp.alloc(c, n);
     ws.counts.alloc(c, 64);
+    ws.cursor.alloc(c, 64);
     ws.counters.alloc(c, 4);
     ws.gain_acc.alloc(c, 1);
     zero(c, ws.epoch.get(), n);
@@ -1164,10 +1166,9 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         if (ctr[0] >= budget) break;
         moves_before = ctr[0];
         if (offs[B * NBUCKET] == 0) break;
-        DBuf<uint32_t> cursor(c, 64);
-        h2d(c, cursor.get(), offs, B * NBUCKET);
+        h2d(c, ws.cursor.get(), offs, B * NBUCKET);
         k_bucket_scatter<<<grid_for(offs[B * NBUCKET], TB), TB, 0, c.stream>>>(
-            g.ptr, alist, ws.acount.get(), n, seed, sweep, B, route_of(c), cursor.get(), ws.list.get(),
+            g.ptr, alist, ws.acount.get(), n, seed, sweep, B, route_of(c), ws.cursor.get(), ws.list.get(),
             ws.lbeg.get(), ws.ldeg.get());
         SC_LAUNCH_CHECK();
         c.launches++;
@@ -1273,10 +1274,9 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     uint32_t offs[65];
     offs[0] = 0;
     for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
-    DBuf<uint32_t> cursor(c, 64);
-    h2d(c, cursor.get(), offs, B * NBUCKET);
+    h2d(c, ws.cursor.get(), offs, B * NBUCKET);
     k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
-                                                           cursor.get(), ws.list.get(), ws.lbeg.get(),
+                                                           ws.cursor.get(), ws.list.get(), ws.lbeg.get(),
                                                            ws.ldeg.get());
     SC_LAUNCH_CHECK();
     c.launches++;
