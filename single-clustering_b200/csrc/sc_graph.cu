@@ -1380,7 +1380,7 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
     zero(c, cnt.get(), G + 1);
     // rows past the warp kernel: shared-table rows (mid) and global-table rows (large)
     DBuf<uint8_t> fmid(c, G), flag(c, G);
-    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 4);
+    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 3);
     DBuf<uint32_t> iota(c, G), rows(c, G), mrows(c, G);
     uint64_t nlarge = 0, nmid = 0;
     if (G) {
@@ -1392,19 +1392,15 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         select_flagged(c, iota.get(), flag.get(), rows.get(), nl.get(), G);
         select_flagged(c, iota.get(), fmid.get(), mrows.get(), nl.get() + 1, G);
         device_sum(c, lcap.get(), nl.get() + 2, G);
-        device_sum(c, hcap.get(), nl.get() + 3, G);
-        uint64_t counts[4];
-        d2h(c, counts, nl.get(), 4);
+        uint64_t counts[3];
+        d2h(c, counts, nl.get(), 3);
         sync(c);
         nlarge = counts[0];
         nmid = counts[1];
-        // Rows past the warp kernel are served by one block each. The sort path is
-        // faster when a few such rows (fewer than 4 per SM) hold more than a tenth
-        // of the entries (the blocks cannot fill the GPU), or when rows whose table
-        // must live in global memory hold more than a twentieth.
-        const uint64_t global_entries = counts[3] / 2;
-        if (global_entries * 20 > g.E) return nullptr;
-        if (counts[2] * 10 > g.E && counts[0] + counts[1] < 4ull * (uint64_t)c.sm_count) return nullptr;
+        // Rows past the warp kernel are served by one block each; when they hold
+        // more than a tenth of the entries the sort path is faster (measured on
+        // kNN graphs at every level of a run).
+        if (counts[2] * 10 > g.E) return nullptr;
     }
     if (nmid) {
         const size_t smem = AGG_SMEM_SLOTS * (sizeof(unsigned long long) + sizeof(uint32_t)) +
