@@ -53,11 +53,14 @@ def exact_dist_matrix_rows(X, rows, cols):
 
 
 def sigmas(dist: np.ndarray, kth: bool = False) -> np.ndarray:
-    k1 = dist.shape[1]
-    if kth:
-        return dist[:, k1 - 1].copy()
+    """Per-row sigma over the neighbours actually returned (finite entries; a
+    search over fewer than k + 1 points returns fewer)."""
     out = np.ones(dist.shape[0])
     for i, row in enumerate(dist):
+        row = row[np.isfinite(row)]
+        if kth:
+            out[i] = row[-1] if len(row) else 1.0
+            continue
         pos = np.sort(row[row > 0])
         if len(pos):
             out[i] = pos[len(pos) // 2]
@@ -71,6 +74,8 @@ def connectivities(idx: np.ndarray, dist: np.ndarray, sigma: np.ndarray, union: 
     for i in range(n):
         for t in range(1, k1):
             j = int(idx[i, t])
+            if j >= n:  # an empty slot (fewer points than k + 1)
+                continue
             if union:
                 if j == i:
                     continue

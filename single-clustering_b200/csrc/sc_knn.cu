@@ -675,18 +675,22 @@ __global__ void k_knn_sigma(const float* __restrict__ d2, uint64_t n, uint32_t k
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const float* r = d2 + i * (k + 1);
+        // with fewer than k + 1 points the trailing slots are empty (infinite):
+        // only the neighbours the search returned count, as in the reference
+        uint32_t m = 0;
+        while (m <= k && isfinite(r[m])) ++m;
         if (kth) {
-            sigma[i] = sqrtf(r[k]);
+            sigma[i] = m ? sqrtf(r[m - 1]) : 1.0f;
             continue;
         }
         uint32_t pos = 0;
-        for (uint32_t t = 0; t <= k; ++t) pos += r[t] > 0.0f;
+        for (uint32_t t = 0; t < m; ++t) pos += r[t] > 0.0f;
         if (pos == 0) {
             sigma[i] = 1.0f;
             continue;
         }
-        // rows are sorted ascending, positive entries are the last `pos`
-        uint32_t first = (k + 1) - pos;
+        // rows are sorted ascending, positive entries are the last `pos` of the m
+        uint32_t first = m - pos;
         sigma[i] = sqrtf(r[first + pos / 2]);
     }
 }

@@ -127,3 +127,38 @@ def test_precision_limits():
         sc_gpu.knn_gaussian(X, 5, precision=sc_gpu.KNN_FP8)  # 62 dims need 65 e4m3 columns
     with pytest.raises(sc_gpu.ClusteringError):
         sc_gpu.knn_gaussian(X[:, :20], 5, precision=sc_gpu.KNN_FP32)
+
+
+@pytest.mark.parametrize("n", [1, 2, 5, 11])
+def test_fewer_points_than_neighbours(n):
+    """k + 1 > n: every row lists all n points (self first, ascending distance),
+    the missing slots hold no index (0xFFFFFFFF) and an infinite distance; the
+    connectivities only use real neighbours."""
+    X, _ = synth.gaussian_mixture(max(n, 1), 4, 1, seed=n)
+    X = X[:n]
+    k = 10
+    r = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH if n > k else sc_gpu.SIGMA_MEDIAN)
+    assert r.index.shape == (n, k + 1)
+    for q in range(n):
+        real = [int(j) for j in r.index[q] if j != 0xFFFFFFFF]
+        assert real[0] == q and sorted(real) == list(range(n))
+        assert np.all(np.isinf(r.distances[q, n:]))
+        assert np.all(np.diff(r.distances[q, :n]) >= 0)
+    assert np.all(r.conn_nbrs < n)
+    # connectivities from the real neighbours only, as the FP64 formula gives them
+    idx64 = r.index.astype(np.int64)
+    d64 = np.full(r.distances.shape, np.inf)
+    for q in range(n):
+        d64[q, :n] = np.sqrt(((X[q].astype(np.float64) - X[idx64[q, :n]]) ** 2).sum(1))
+    sig = K.sigmas(d64, kth=n > k)
+    rows, cols, w = K.connectivities(np.where(idx64 == 0xFFFFFFFF, n, idx64), d64, sig)
+    ptr = r.conn_ptrs.astype(np.int64)
+    assert np.array_equal(np.repeat(np.arange(n), np.diff(ptr)), rows)
+    assert np.array_equal(r.conn_nbrs.astype(np.int64), cols)
+    assert np.allclose(r.conn_w, w, rtol=1e-5)
+
+
+def test_empty_point_set():
+    X = np.zeros((0, 8), np.float32)
+    r = sc_gpu.knn_gaussian(X, 5)
+    assert r.index.shape == (0, 6) and len(r.conn_w) == 0 and len(r.conn_ptrs) == 1

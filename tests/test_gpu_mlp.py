@@ -164,3 +164,16 @@ def test_warm_start_gain_over_plain_start():
         assert final_q >= res.q_plain - 1e-4
         saved.append(res.sweeps_plain - res.sweeps_warm)
     assert sum(saved) > 0, saved
+
+
+def test_graph_without_edges():
+    import sc_gpu
+    from sc_gpu.learned import EdgeMlp
+    g = sc_gpu.CSRNetwork.from_edges(5, [])
+    m = EdgeMlp(seed=1)
+    feat, ei, ej = m.features(g, 1.0)
+    assert feat.shape == (0, mo.F) and len(ei) == 0
+    loss = m.train(g, np.zeros(5, np.uint64), 1.0, epochs=2)
+    assert loss == 0.0
+    lab, k = m.propose(g, 1.0)
+    assert list(lab) == [0, 1, 2, 3, 4] and k == 5
