@@ -75,13 +75,21 @@ void require_same_device(sc::Ctx& c, const sc::DevGraph& g) {
 }
 
 // Stream, pool and status word of a context on `device` (SC_OK or the failure).
-sc_status init_ctx(sc::Ctx& c, int device) {
+// side_streams: the decide kernels of one batch may fork onto 3 extra streams;
+// workers of a concurrent batch skip them (the instances already fill the GPU).
+sc_status init_ctx(sc::Ctx& c, int device, bool side_streams = true) {
     c.device = device;
     if (cudaSetDevice(device) != cudaSuccess) return SC_E_CUDA;
     if (cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
     if (cudaDeviceGetDefaultMemPool(&c.pool, device) != cudaSuccess) return SC_E_CUDA;
     uint64_t thresh = UINT64_MAX;  // keep freed blocks cached in the pool
     cudaMemPoolSetAttribute(c.pool, cudaMemPoolAttrReleaseThreshold, &thresh);
+    for (int t = 0; side_streams && t < sc::SIDE_STREAMS; ++t) {
+        if (cudaStreamCreateWithFlags(&c.side[t], cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
+        if (cudaEventCreateWithFlags(&c.ev_join[t], cudaEventDisableTiming) != cudaSuccess) return SC_E_CUDA;
+    }
+    if (side_streams && cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming) != cudaSuccess)
+        return SC_E_CUDA;
     if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
     cudaMemset(c.d_status, 0, sizeof(uint32_t));
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
@@ -98,6 +106,17 @@ void release_ctx(sc::Ctx& c) {
         cudaStreamDestroy(c.stream);
         c.stream = nullptr;
     }
+    for (int t = 0; t < sc::SIDE_STREAMS; ++t) {
+        if (c.side[t]) {
+            cudaStreamSynchronize(c.side[t]);
+            cudaStreamDestroy(c.side[t]);
+        }
+        if (c.ev_join[t]) cudaEventDestroy(c.ev_join[t]);
+        c.side[t] = nullptr;
+        c.ev_join[t] = nullptr;
+    }
+    if (c.ev_fork) cudaEventDestroy(c.ev_fork);
+    c.ev_fork = nullptr;
     if (c.d_status) cudaFree(c.d_status);
     c.d_status = nullptr;
     c.pool = nullptr;  // the device's default pool: not ours to destroy
@@ -492,7 +511,7 @@ sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs, const s
         sc_error_info first_err{};
         auto worker = [&]() {
             sc::Ctx w;
-            sc_status st = init_ctx(w, c.device);
+            sc_status st = init_ctx(w, c.device, W == 1);
             if (st != SC_OK) {
                 std::lock_guard<std::mutex> lk(mu);
                 if (!failed) {

@@ -71,7 +71,12 @@ struct Ctx {
     int sm_count = 148;
     size_t smem_optin = 0;
     sc_tuning tuning{8, 16, 32, 4096};  // decide-kernel routing (sc_set_tuning / sc_autotune)
+    // side streams for kernels of one step that may run concurrently (fork / join by events)
+    cudaStream_t side[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev_fork = nullptr;
+    cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
 };
+constexpr int SIDE_STREAMS = 3;
 
 // Stream-ordered device buffer of T, from the context's pool on its stream.
 template <class T>

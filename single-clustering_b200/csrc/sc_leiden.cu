@@ -1017,31 +1017,33 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
 }
 
 template <bool REFINE>
-void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32_t cnt) {
+void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32_t cnt,
+                   cudaStream_t st = nullptr) {
     if (!cnt) return;
+    if (!st) st = c.stream;
     const uint32_t* list = ws.list.get() + off;
     const uint64_t* lbeg = ws.lbeg.get() + off;
     const uint32_t* ldeg = ws.ldeg.get() + off;
     if (k == 0) {
         unsigned warps = (cnt + 3) / 4;
-        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 1) {
         unsigned warps = (cnt + 1) / 2;
-        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 2) {
-        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 3) {
         const uint64_t warps = cnt;
         k_decide_warp<REFINE><<<grid_for(warps * 32, 32 * WARPS_PER_BLOCK, 148u * 64u), 32 * WARPS_PER_BLOCK, 0,
-                                c.stream>>>(p, list, lbeg, ldeg, cnt);
+                                st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 4) {
         size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
         unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
-        k_decide_block<REFINE, false><<<grid, TB, sm, c.stream>>>(p, list, lbeg, ldeg, cnt, nullptr, nullptr, 0);
+        k_decide_block<REFINE, false><<<grid, TB, sm, st>>>(p, list, lbeg, ldeg, cnt, nullptr, nullptr, 0);
     } else {
         if (ws.nblk_large < 1 || ws.gcap == 0) fail(SC_E_INTERNAL, "hub scratch missing");
         unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
-        k_decide_block<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, lbeg, ldeg, cnt, ws.gkeys.get(),
+        k_decide_block<REFINE, true><<<grid, TB, 0, st>>>(p, list, lbeg, ldeg, cnt, ws.gkeys.get(),
                                                                ws.gvals.get(), ws.gcap);
     }
     SC_LAUNCH_CHECK();
@@ -1065,7 +1067,34 @@ void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs,
         for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
         return;
     }
-    for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+    // Buckets of one batch read the same snapshot and write disjoint nodes: the
+    // non-empty ones run concurrently on the context's side streams (fork and
+    // join by events), so one kernel's ramp and last partial wave overlap another.
+    int nonempty = 0;
+    for (int k = 0; k < NBUCKET; ++k) nonempty += o[k + 1] > o[k];
+    if (nonempty < 2 || !c.side[0]) {
+        for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+        return;
+    }
+    SC_CUDA(cudaEventRecord(c.ev_fork, c.stream));
+    int used = 0;
+    bool first = true;
+    for (int k = 0; k < NBUCKET; ++k) {
+        if (o[k + 1] == o[k]) continue;
+        if (first) {  // the first non-empty bucket runs on the main stream
+            launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+            first = false;
+            continue;
+        }
+        cudaStream_t st = c.side[used % SIDE_STREAMS];
+        if (used < SIDE_STREAMS) SC_CUDA(cudaStreamWaitEvent(st, c.ev_fork, 0));
+        launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k], st);
+        ++used;
+    }
+    for (int t = 0; t < used && t < SIDE_STREAMS; ++t) {
+        SC_CUDA(cudaEventRecord(c.ev_join[t], c.side[t]));
+        SC_CUDA(cudaStreamWaitEvent(c.stream, c.ev_join[t], 0));
+    }
 }
 
 struct MoveResult {
