@@ -124,7 +124,7 @@ SWEEP_RESOLUTIONS = 32
 SWEEP_SEEDS = (1, 2, 3, 4)
 
 
-def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=4):
+def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=8, split=2):
     """128-instance resolution x seed sweep: sequential plain runs vs
     warm-started chains (each seed's chain cut in `split` pieces whose heads
     start from the seed's finest partition) on concurrent streams."""
@@ -317,6 +317,8 @@ def main():
 
     if args.impl == "reference":
         if rank != 0:
+            if dist:
+                dist.destroy_process_group()
             return
         ptr, nbr, w = make_graph(args, device)
         g, lab, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
@@ -331,11 +333,15 @@ def main():
                                  "cpu": cpu_model(), "nproc": os.cpu_count()},
                 "e2e": {"value": eps, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
+        if dist:
+            dist.destroy_process_group()
         return
 
     if args.part == "knn":
         if rank == 0:
             run_knn_part(args, local_rank)
+        if dist:
+            dist.destroy_process_group()
         return
 
     import sc_gpu

@@ -76,7 +76,8 @@ void require_same_device(sc::Ctx& c, const sc::DevGraph& g) {
 
 // Stream, pool and status word of a context on `device` (SC_OK or the failure).
 // side_streams: the decide kernels of one batch may fork onto 3 extra streams;
-// workers of a concurrent batch skip them (the instances already fill the GPU).
+// a batch with more than 8 workers gives its workers none (the instances
+// already fill the GPU; measured on a 128-instance sweep).
 sc_status init_ctx(sc::Ctx& c, int device, bool side_streams = true) {
     c.device = device;
     if (cudaSetDevice(device) != cudaSuccess) return SC_E_CUDA;
@@ -90,6 +91,11 @@ sc_status init_ctx(sc::Ctx& c, int device, bool side_streams = true) {
     }
     if (side_streams && cudaEventCreateWithFlags(&c.ev_fork, cudaEventDisableTiming) != cudaSuccess)
         return SC_E_CUDA;
+    if (side_streams) {
+        if (cudaStreamCreateWithFlags(&c.aux, cudaStreamNonBlocking) != cudaSuccess) return SC_E_CUDA;
+        if (cudaEventCreateWithFlags(&c.ev_aux_start, cudaEventDisableTiming) != cudaSuccess) return SC_E_CUDA;
+        if (cudaEventCreateWithFlags(&c.ev_aux_done, cudaEventDisableTiming) != cudaSuccess) return SC_E_CUDA;
+    }
     if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
     cudaMemset(c.d_status, 0, sizeof(uint32_t));
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
@@ -117,6 +123,14 @@ void release_ctx(sc::Ctx& c) {
     }
     if (c.ev_fork) cudaEventDestroy(c.ev_fork);
     c.ev_fork = nullptr;
+    if (c.aux) {
+        cudaStreamSynchronize(c.aux);
+        cudaStreamDestroy(c.aux);
+    }
+    if (c.ev_aux_start) cudaEventDestroy(c.ev_aux_start);
+    if (c.ev_aux_done) cudaEventDestroy(c.ev_aux_done);
+    c.aux = nullptr;
+    c.ev_aux_start = c.ev_aux_done = nullptr;
     if (c.d_status) cudaFree(c.d_status);
     c.d_status = nullptr;
     c.pool = nullptr;  // the device's default pool: not ours to destroy
@@ -511,7 +525,7 @@ sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs, const s
         sc_error_info first_err{};
         auto worker = [&]() {
             sc::Ctx w;
-            sc_status st = init_ctx(w, c.device, W == 1);
+            sc_status st = init_ctx(w, c.device, W <= 8);
             if (st != SC_OK) {
                 std::lock_guard<std::mutex> lk(mu);
                 if (!failed) {

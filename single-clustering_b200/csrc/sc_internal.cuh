@@ -75,6 +75,9 @@ struct Ctx {
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr;
     cudaEvent_t ev_join[3] = {nullptr, nullptr, nullptr};
+    // auxiliary stream for work that overlaps the next step (local moving's re-queue)
+    cudaStream_t aux = nullptr;
+    cudaEvent_t ev_aux_start = nullptr, ev_aux_done = nullptr;
 };
 constexpr int SIDE_STREAMS = 3;
 

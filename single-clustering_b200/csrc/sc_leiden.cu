@@ -1201,6 +1201,11 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             ws.lbeg.get(), ws.ldeg.get());
         SC_LAUNCH_CHECK();
         c.launches++;
+        // A batch's re-queue reads memberships and writes only the next sweep's
+        // list, so with an auxiliary stream it runs while the next batch decides;
+        // it must end before the next batch commits (which changes memberships).
+        const bool overlap = c.aux != nullptr;
+        bool act_pending = false;
         for (int b = 0; b < B; ++b) {
             ++epoch;
             p.cur = epoch;
@@ -1212,12 +1217,27 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
                 k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
                 c.launches++;
             }
+            if (act_pending) {
+                SC_CUDA(cudaStreamWaitEvent(c.stream, c.ev_aux_done, 0));
+                act_pending = false;
+            }
             k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
-            k_activate<<<grid_for((uint64_t)(hi - lo) * 32, TB, 148u * 64u), TB, 0, c.stream>>>(
+            cudaStream_t as = c.stream;
+            if (overlap) {
+                SC_CUDA(cudaEventRecord(c.ev_aux_start, c.stream));
+                SC_CUDA(cudaStreamWaitEvent(c.aux, c.ev_aux_start, 0));
+                as = c.aux;
+            }
+            k_activate<<<grid_for((uint64_t)(hi - lo) * 32, TB, 148u * 64u), TB, 0, as>>>(
                 p, ws.list.get() + lo, hi - lo, ws.stamp.get(), sweep + 2, ws.nlist.get(), ws.ncount.get());
+            if (overlap) {
+                SC_CUDA(cudaEventRecord(c.ev_aux_done, c.aux));
+                act_pending = true;
+            }
             SC_LAUNCH_CHECK();
             c.launches += 2;
         }
+        if (act_pending) SC_CUDA(cudaStreamWaitEvent(c.stream, c.ev_aux_done, 0));
         std::swap(ws.alist, ws.nlist);
         std::swap(ws.acount, ws.ncount);
         all_active = false;
