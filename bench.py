@@ -383,9 +383,15 @@ def main():
     torch.cuda.synchronize()
     t = time.perf_counter()
     e2e_steps = max(1, min(args.steps, 2))
+    graph_s = leiden_s = 0.0
     for _ in range(e2e_steps):
+        t1 = time.perf_counter()
         g2 = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
+        t2 = time.perf_counter()
         c2 = sc_gpu.leiden(g2, cfg)
+        t3 = time.perf_counter()
+        graph_s += t2 - t1
+        leiden_s += t3 - t2
         del g2
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t) / e2e_steps
@@ -413,6 +419,7 @@ def main():
                          "peak_kind": peak_kind},
             "clocks": clk,
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
+                    "graph_upload_s": graph_s / e2e_steps, "leiden_call_s": leiden_s / e2e_steps,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
     if KNN_INFO:
         line["knn_graph_build_s"] = KNN_INFO["seconds"]
