@@ -384,6 +384,7 @@ def main():
     t = time.perf_counter()
     e2e_steps = max(1, min(args.steps, 2))
     graph_s = leiden_s = 0.0
+    e2e_each = []
     for _ in range(e2e_steps):
         t1 = time.perf_counter()
         g2 = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
@@ -392,6 +393,8 @@ def main():
         t3 = time.perf_counter()
         graph_s += t2 - t1
         leiden_s += t3 - t2
+        e2e_each.append({"graph_upload_s": t2 - t1, "leiden_call_s": t3 - t2,
+                         "leiden_device_ms": sc_gpu.last_run_stats(local_rank)["ms_total"]})
         del g2
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t) / e2e_steps
@@ -420,7 +423,7 @@ def main():
             "clocks": clk,
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
                     "graph_upload_s": graph_s / e2e_steps, "leiden_call_s": leiden_s / e2e_steps,
-                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)}}
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "each": e2e_each}}
     if KNN_INFO:
         line["knn_graph_build_s"] = KNN_INFO["seconds"]
     if not args.no_sweep:

@@ -96,8 +96,14 @@ sc_status init_ctx(sc::Ctx& c, int device, bool side_streams = true) {
         if (cudaEventCreateWithFlags(&c.ev_aux_start, cudaEventDisableTiming) != cudaSuccess) return SC_E_CUDA;
         if (cudaEventCreateWithFlags(&c.ev_aux_done, cudaEventDisableTiming) != cudaSuccess) return SC_E_CUDA;
     }
+    if (cudaHostAlloc((void**)&c.mailbox, sc::MAILBOX_BYTES, cudaHostAllocDefault) != cudaSuccess) {
+        c.mailbox = nullptr;
+        return SC_E_CUDA;
+    }
     if (cudaMalloc(&c.d_status, sizeof(uint32_t)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
     cudaMemset(c.d_status, 0, sizeof(uint32_t));
+    if (cudaMalloc(&c.d_refine_ctr, 4 * sizeof(unsigned long long)) != cudaSuccess) return SC_E_OUT_OF_MEMORY;
+    cudaMemset(c.d_refine_ctr, 0, 4 * sizeof(unsigned long long));
     cudaDeviceGetAttribute(&c.sm_count, cudaDevAttrMultiProcessorCount, device);
     int optin = 0;
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
@@ -131,8 +137,12 @@ void release_ctx(sc::Ctx& c) {
     if (c.ev_aux_done) cudaEventDestroy(c.ev_aux_done);
     c.aux = nullptr;
     c.ev_aux_start = c.ev_aux_done = nullptr;
+    if (c.mailbox) cudaFreeHost(c.mailbox);
+    c.mailbox = nullptr;
     if (c.d_status) cudaFree(c.d_status);
     c.d_status = nullptr;
+    if (c.d_refine_ctr) cudaFree(c.d_refine_ctr);
+    c.d_refine_ctr = nullptr;
     c.pool = nullptr;  // the device's default pool: not ours to destroy
 }
 

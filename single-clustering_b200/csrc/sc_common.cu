@@ -95,9 +95,13 @@ void fail_info(sc_error_info i) {
 }
 
 void check_device_status(Ctx& c) {
-    uint32_t st = 0;
-    SC_CUDA(cudaMemcpyAsync(&st, c.d_status, sizeof st, cudaMemcpyDeviceToHost, c.stream));
-    SC_CUDA(cudaStreamSynchronize(c.stream));
+    Mailbox mb(c);
+    const uint32_t* h = mb.get(c.d_status, 1);
+    mb.wait();
+    raise_device_status(c, *h);
+}
+
+void raise_device_status(Ctx& c, uint32_t st) {
     if (st == DEV_OK) return;
     SC_CUDA(cudaMemsetAsync(c.d_status, 0, sizeof(uint32_t), c.stream));
     if (st & DEV_TIMEOUT) fail(SC_E_TIMEOUT, "a bounded device wait gave up (status 0x%x)", st);

@@ -251,56 +251,23 @@ struct Totals {
     uint64_t edge_count;
 };
 
-// total_weight (csr_network.rs:321-324) and edge_count of a clean CSR.
-Totals ordered_total(Ctx& c, const DevGraph& g, bool exact) {
-    Totals t{0.0, 0};
-    if (g.E == 0) return t;
-    DBuf<double> terms(c, g.E);
-    DBuf<uint8_t> flags(c, g.E);
-    k_upper_terms<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.erow, g.nbr, g.w, g.E, terms.get(),
-                                                          flags.get());
-    SC_LAUNCH_CHECK();
-    c.launches++;
-    DBuf<uint64_t> f64s(c, g.E);
-    k_u8_to_u64<<<grid_for(g.E, TB), TB, 0, c.stream>>>(flags.get(), g.E, f64s.get());
-    c.launches++;
-    DBuf<uint64_t> cnt(c, 1);
-    device_sum(c, f64s.get(), cnt.get(), g.E);
-    t.edge_count = to_host(c, cnt.get());
-    if (exact) {
-        DBuf<double> s(c, 1);
-        device_sum(c, terms.get(), s.get(), g.E);
-        t.total_weight = to_host(c, s.get());
-    } else {
-        DBuf<double> up(c, g.E);
-        DBuf<uint64_t> nup(c, 1);
-        select_flagged(c, terms.get(), flags.get(), up.get(), nup.get(), g.E);
-        uint64_t k = to_host(c, nup.get());
-        t.total_weight = ordered_sum_from(c, up.get(), k, 0.0);
-    }
-    return t;
-}
-
-// Rust-order Σ of an f64 array (fold from -0.0), exact or chained.
-double rust_sum_dev(Ctx& c, const double* d, uint64_t n, bool exact) {
-    if (n == 0) return -0.0;
-    if (exact) {
-        DBuf<double> s(c, 1);
-        device_sum(c, d, s.get(), n);
-        double x = to_host(c, s.get());
-        return x;  // n > 0 terms, each >= +0.0: the -0.0 start never shows
-    }
-    return ordered_sum(c, d, n);
-}
-
 // Stats, regime, totals and check_degree_sum of a graph whose rows are clean.
+// Every reduction that the exact regime can use is queued first and read back
+// with one synchronisation; the ordered folds of the other regime follow only
+// when the regime needs them.
+//   total_weight (csr_network.rs:321-324): Σ over the v <= u entries of f64(w)
+//   (self-loops once), in (v asc, u asc) order; edge_count: their number.
 void finalize(Ctx& c, DevGraph& g, bool check_sum) {
-    const uint64_t n = g.n;
+    const uint64_t n = g.n, E = g.E;
     DBuf<int> d_low(c, 2);
     DBuf<unsigned> d_flags(c, 3);
+    DBuf<double> d_sums(c, 3);  // Σ strength, Σ node weight, Σ upper-triangle terms
+    DBuf<uint64_t> d_ecount(c, 1);
     int init_low[2] = {0x7FFFFFFF, 0x7FFFFFFF};
     h2d(c, d_low.get(), init_low, 2);
     zero(c, d_flags.get(), 3);
+    zero(c, d_sums.get(), 3);
+    zero(c, d_ecount.get(), 1);
     if (n) {
         k_row_stats<<<grid_for(n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength,
                                                           g.self_loop, d_low.get(), d_flags.get(),
@@ -309,12 +276,38 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
         k_lowbit_f64<<<grid_for(n, TB), TB, 0, c.stream>>>(g.node_w, n, d_low.get() + 1);
         SC_LAUNCH_CHECK();
         c.launches += 2;
+        device_sum(c, g.strength, d_sums.get(), n);
+        device_sum(c, g.node_w, d_sums.get() + 1, n);
+    }
+    DBuf<double> terms;
+    DBuf<uint8_t> upper;
+    if (E) {
+        terms.alloc(c, E);
+        upper.alloc(c, E);
+        k_upper_terms<<<grid_for(E, TB), TB, 0, c.stream>>>(g.erow, g.nbr, g.w, E, terms.get(), upper.get());
+        SC_LAUNCH_CHECK();
+        DBuf<uint64_t> f64s(c, E);
+        k_u8_to_u64<<<grid_for(E, TB), TB, 0, c.stream>>>(upper.get(), E, f64s.get());
+        c.launches += 2;
+        device_sum(c, f64s.get(), d_ecount.get(), E);
+        device_sum(c, terms.get(), d_sums.get() + 2, E);  // exact in the exact regime; unused otherwise
     }
     int low[2];
     unsigned flags[3];
-    d2h(c, low, d_low.get(), 2);
-    d2h(c, flags, d_flags.get(), 3);
-    sync(c);
+    double sums[3];
+    uint64_t ecount;
+    {
+        Mailbox mb(c);
+        const int* hl = mb.get(d_low.get(), 2);
+        const unsigned* hf = mb.get(d_flags.get(), 3);
+        const double* hs = mb.get(d_sums.get(), 3);
+        const uint64_t* he = mb.get(d_ecount.get(), 1);
+        mb.wait();
+        std::memcpy(low, hl, sizeof low);
+        std::memcpy(flags, hf, sizeof flags);
+        std::memcpy(sums, hs, sizeof sums);
+        ecount = *he;
+    }
     g.any_self_loops = flags[0] != 0;
     g.max_degree = flags[1];
     g.n_hubs = flags[2];
@@ -322,32 +315,34 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
     g.e0_nw = low[1];
 
     // approximate Σ strength (= 2m) decides the regime; exact inside it
-    double approx2m = 0.0;
-    if (n) {
-        DBuf<double> s(c, 1);
-        device_sum(c, g.strength, s.get(), n);
-        approx2m = to_host(c, s.get());
-    }
+    const double approx2m = n ? sums[0] : 0.0;
     g.exact_w = (g.e0_w == 0x7FFFFFFF) || (approx2m < std::ldexp(1.0, 52 + g.e0_w));
-    double approx_nw = 0.0;
-    if (n) {
-        DBuf<double> s(c, 1);
-        device_sum(c, g.node_w, s.get(), n);
-        approx_nw = to_host(c, s.get());
-    }
+    const double approx_nw = n ? sums[1] : 0.0;
     g.exact_nw = (g.e0_nw == 0x7FFFFFFF) || (approx_nw < std::ldexp(1.0, 52 + g.e0_nw));
-    g.total_node_weight = rust_sum_dev(c, g.node_w, n, g.exact_nw);
+    // Rust-order Σ of the node weights (a fold from -0.0): in the exact regime any
+    // order gives these bits, and n > 0 terms >= +0.0 never leave the -0.0 start
+    if (n == 0) g.total_node_weight = -0.0;
+    else g.total_node_weight = g.exact_nw ? approx_nw : ordered_sum(c, g.node_w, n);
 
-    Totals t = ordered_total(c, g, g.exact_w);
-    g.total_weight = t.total_weight;
-    g.edge_count = t.edge_count;
+    g.edge_count = E ? ecount : 0;
+    if (E == 0) {
+        g.total_weight = 0.0;
+    } else if (g.exact_w) {
+        g.total_weight = sums[2];
+    } else {
+        DBuf<double> up(c, E);
+        DBuf<uint64_t> nup(c, 1);
+        select_flagged(c, terms.get(), upper.get(), up.get(), nup.get(), E);
+        const uint64_t k = to_host(c, nup.get());
+        g.total_weight = ordered_sum_from(c, up.get(), k, 0.0);
+    }
 
     if (check_sum) {
         // check_degree_sum (csr_network.rs:712-723)
         double expected = 2.0 * g.total_weight;
         double tol = 1e-6 * std::max(std::fabs(expected), 1.0);
         double sum = g.exact_w ? (n ? approx2m : -0.0) : approx2m;
-        if (!g.exact_w && std::fabs(sum - expected) > 0.25 * tol) sum = rust_sum_dev(c, g.strength, n, false);
+        if (!g.exact_w && std::fabs(sum - expected) > 0.25 * tol) sum = n ? ordered_sum(c, g.strength, n) : -0.0;
         if (std::fabs(sum - expected) > tol) {
             sc_error_info i{};
             i.code = SC_E_ASYMMETRIC_GRAPH;
@@ -735,9 +730,10 @@ __device__ __forceinline__ void seg_emit(uint64_t s, uint64_t b, double acc, con
     keep[s] = (acc > 0.0) && ((double)val != 0.0);
 }
 
-// Segments at least SEG_BLOCK long, in the exact regime, are summed by a whole
-// block (k_seg_values_long): any order gives the exact sum, and one warp folding
-// a segment of a coarse community's internal entries alone takes milliseconds.
+// Segments at least SEG_BLOCK long, in the exact regime, are summed in chunks
+// by many blocks (k_seg_long_partial): any order gives the exact sum, and one
+// warp folding a segment of a coarse community's internal entries alone takes
+// milliseconds.
 constexpr uint64_t SEG_BLOCK = 4096;
 
 __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
@@ -780,29 +776,60 @@ __global__ void k_seg_values(const uint64_t* __restrict__ seg_start, uint64_t P,
     }
 }
 
-// One block per listed long segment (exact regime): block-wide sum, then the
-// same emission as k_seg_values.
-__global__ void k_seg_values_long(const uint32_t* __restrict__ long_list, const uint32_t* __restrict__ long_count,
-                                  const uint64_t* __restrict__ seg_start, uint64_t P, uint64_t N,
-                                  const uint64_t* __restrict__ keys, const float* __restrict__ w, uint64_t G,
-                                  const double* __restrict__ loops, uint32_t* prow, uint32_t* pcol, float* pw,
-                                  uint8_t* keep) {
-    __shared__ double red[32];
-    const uint32_t cnt = *long_count;
-    for (uint32_t li = blockIdx.x; li < cnt; li += gridDim.x) {
+// Long segments (exact regime) in chunks of SEG_CHUNK entries spread over all
+// blocks: chunk ch of listed segment li goes to block (li + ch) mod gridDim, so
+// one segment of a coarse community's internal entries (hundreds of thousands
+// of them) keeps the whole GPU busy instead of one block. Every partial sum is
+// exact, so the atomic accumulation gives the same bits in any order.
+constexpr uint64_t SEG_CHUNK = 8192;
+
+__global__ void __launch_bounds__(256) k_seg_long_partial(const uint32_t* __restrict__ long_list,
+                                                          const uint32_t* __restrict__ long_count,
+                                                          uint32_t long_cap, const uint64_t* __restrict__ seg_start,
+                                                          uint64_t P, uint64_t N, const float* __restrict__ w,
+                                                          double* part) {
+    __shared__ double red[8];
+    const uint32_t cnt = min(*long_count, long_cap);
+    for (uint32_t li = 0; li < cnt; ++li) {
         const uint32_t s = long_list[li];
         const uint64_t b = seg_start[s], e = s + 1 < P ? seg_start[s + 1] : N;
-        double acc = 0.0;
-        for (uint64_t i = b + threadIdx.x; i < e; i += blockDim.x) acc += (double)w[i];
-        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double t = 0.0;
-            for (unsigned k = 0; k < (blockDim.x >> 5); ++k) t += red[k];
-            seg_emit(s, b, t, keys, G, loops, prow, pcol, pw, keep);
+        const uint64_t nch = (e - b + SEG_CHUNK - 1) / SEG_CHUNK;
+        uint64_t ch = (blockIdx.x + gridDim.x - (li % gridDim.x)) % gridDim.x;
+        for (; ch < nch; ch += gridDim.x) {
+            const uint64_t cb = b + ch * SEG_CHUNK, ce = cb + SEG_CHUNK < e ? cb + SEG_CHUNK : e;
+            double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;  // four loads in flight per thread
+            uint64_t i = cb + threadIdx.x;
+            for (; i + 3 * blockDim.x < ce; i += 4 * blockDim.x) {
+                a0 += (double)w[i];
+                a1 += (double)w[i + blockDim.x];
+                a2 += (double)w[i + 2 * blockDim.x];
+                a3 += (double)w[i + 3 * blockDim.x];
+            }
+            for (; i < ce; i += blockDim.x) a0 += (double)w[i];
+            double acc = (a0 + a1) + (a2 + a3);
+            for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double t = 0.0;
+                for (unsigned k = 0; k < (blockDim.x >> 5); ++k) t += red[k];
+                atomicAdd(part + li, t);
+            }
+            __syncthreads();
         }
-        __syncthreads();
+    }
+}
+
+// The emission of every listed long segment from its accumulated sum.
+__global__ void k_seg_long_emit(const uint32_t* __restrict__ long_list, const uint32_t* __restrict__ long_count,
+                                uint32_t long_cap, const uint64_t* __restrict__ seg_start,
+                                const double* __restrict__ part, const uint64_t* __restrict__ keys, uint64_t G,
+                                const double* __restrict__ loops, uint32_t* prow, uint32_t* pcol, float* pw,
+                                uint8_t* keep) {
+    const uint32_t cnt = min(*long_count, long_cap);
+    for (uint32_t li = blockIdx.x * blockDim.x + threadIdx.x; li < cnt; li += gridDim.x * blockDim.x) {
+        const uint32_t s = long_list[li];
+        seg_emit(s, seg_start[s], part[li], keys, G, loops, prow, pcol, pw, keep);
     }
 }
 
@@ -941,7 +968,9 @@ __device__ __forceinline__ float agg_value(uint32_t g, uint32_t h, double acc, c
 }
 
 // The member entries of one group, flattened across the 32 lanes: calls
-// f(j) for every stored entry j of every member, in no particular order.
+// f(j, valid) for every stored entry j of every member, in no particular
+// order; every lane calls it the same number of times (valid false past the
+// end), so f may use warp-collective operations.
 template <class F>
 __device__ __forceinline__ void warp_member_entries(const uint64_t* __restrict__ ptr,
                                                     const uint32_t* __restrict__ members, uint64_t m0, uint64_t m1,
@@ -971,7 +1000,7 @@ __device__ __forceinline__ void warp_member_entries(const uint64_t* __restrict__
                 if (e <= t) L += step;
             }
             const uint64_t eL = __shfl_sync(FULL, excl, L), bL = __shfl_sync(FULL, b, L);
-            if (t < total) f(bL + (t - eL));
+            f(bL + (t - eL), t < total);
         }
     }
 }
@@ -1037,12 +1066,7 @@ __device__ __forceinline__ void agg_insert_fix_combined(uint32_t* keys, unsigned
     const unsigned lane = threadIdx.x & 31u;
     const unsigned long long key = valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | lane);
     const unsigned mm = __match_any_sync(0xFFFFFFFFu, key);
-    unsigned long long acc = 0;
-#pragma unroll
-    for (int L = 0; L < 32; ++L) {
-        const unsigned long long y = __shfl_sync(0xFFFFFFFFu, x, L);
-        if ((mm >> L) & 1u) acc += y;
-    }
+    const unsigned long long acc = peer_sum(mm, valid ? x : 0ull);
     if (!valid || (int)lane != __ffs(mm) - 1) return;
     uint64_t slot = agg_hash(h) & mask;
     for (uint64_t probe = 0; probe < size; ++probe) {
@@ -1084,8 +1108,18 @@ __global__ void __launch_bounds__(32 * AGG_WARPS)
             vals[s] = 0.0;
         }
         __syncwarp();
-        warp_member_entries(ptr, members, gstart[g], gstart[g + 1], [&](uint64_t j) {
-            agg_insert(keys, vals, size, grp[nbr[j]], (double)w[j], status);
+        warp_member_entries(ptr, members, gstart[g], gstart[g + 1], [&](uint64_t j, bool valid) {
+            uint32_t h = 0;
+            double x = 0.0;
+            if (valid) {
+                h = grp[nbr[j]];
+                x = (double)w[j];
+            }
+            // lanes with the same key add through the lowest one (exact regime: any grouping)
+            const unsigned long long key = valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | (unsigned)lane);
+            const unsigned mm = __match_any_sync(FULL, key);
+            const double acc = peer_sum(mm, x);
+            if (valid && lane == __ffs(mm) - 1) agg_insert(keys, vals, size, h, acc, status);
         });
         __syncwarp();
         uint32_t nk = 0;
@@ -1152,12 +1186,7 @@ __global__ void __launch_bounds__(256)
                                  const unsigned long long key =
                                      valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | lane);
                                  const unsigned mm = __match_any_sync(0xFFFFFFFFu, key);
-                                 double acc = 0.0;
-#pragma unroll
-                                 for (int L = 0; L < 32; ++L) {
-                                     const double y = __shfl_sync(0xFFFFFFFFu, x, L);
-                                     if ((mm >> L) & 1u) acc += y;
-                                 }
+                                 const double acc = peer_sum(mm, x);  // exact regime: any grouping
                                  if (valid && (int)lane == __ffs(mm) - 1)
                                      agg_insert(keys, vals, size, h, acc, status);
                              });
@@ -1393,8 +1422,12 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         select_flagged(c, iota.get(), fmid.get(), mrows.get(), nl.get() + 1, G);
         device_sum(c, lcap.get(), nl.get() + 2, G);
         uint64_t counts[3];
-        d2h(c, counts, nl.get(), 3);
-        sync(c);
+        {
+            Mailbox mb(c);
+            const uint64_t* hc = mb.get(nl.get(), 3);
+            mb.wait();
+            std::memcpy(counts, hc, sizeof counts);
+        }
         nlarge = counts[0];
         nmid = counts[1];
         // Rows past the warp kernel are served by one block each; when they hold
@@ -1454,12 +1487,20 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         SC_LAUNCH_CHECK();
         c.launches += 4;
     }
-    check_device_status(c);
-    // assemble
+    // assemble (the status word of the contraction kernels is read with the size)
     DBuf<uint64_t> cnt64(c, G + 1), optr(c, G + 1);
     k_u32_to_u64<<<grid_for(G + 1, TB), TB, 0, c.stream>>>(cnt.get(), G + 1, cnt64.get());
     exclusive_sum(c, cnt64.get(), optr.get(), G + 1);
-    const uint64_t E2 = to_host(c, optr.get() + G);
+    uint64_t E2;
+    {
+        Mailbox mb(c);
+        const uint32_t* hs = mb.get(c.d_status, 1);
+        const uint64_t* he = mb.get(optr.get() + G, 1);
+        mb.wait();
+        const uint32_t st = *hs;
+        E2 = *he;
+        raise_device_status(c, st);
+    }
     galloc(c, *out, G, E2);
     d2d(c, out->ptr, optr.get(), G + 1);
     d2d(c, out->node_w, nw_new, G);
@@ -1575,12 +1616,20 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
                                                            uw_s.get(), G, loops.get(), prow.get(),
                                                            pcol.get(), pw.get(), keep.get(), (int)g.exact_w,
                                                            long_list.get(), long_count.get(), long_cap);
-        if (g.exact_w)
-            k_seg_values_long<<<std::min<unsigned>(long_cap, (unsigned)c.sm_count * 2), TB, 0, c.stream>>>(
-                long_list.get(), long_count.get(), seg.get(), P, N, ukeys_s.get(), uw_s.get(), G, loops.get(),
-                prow.get(), pcol.get(), pw.get(), keep.get());
+        c.launches++;
+        if (g.exact_w) {
+            DBuf<double> part(c, long_cap);
+            zero(c, part.get(), long_cap);
+            const unsigned pgrid = (unsigned)std::min<uint64_t>(N / SEG_CHUNK + 1, (uint64_t)c.sm_count * 4);
+            k_seg_long_partial<<<pgrid, TB, 0, c.stream>>>(long_list.get(), long_count.get(), long_cap, seg.get(), P, N,
+                                                           uw_s.get(), part.get());
+            k_seg_long_emit<<<grid_for(long_cap, TB), TB, 0, c.stream>>>(long_list.get(), long_count.get(),
+                                                                         long_cap, seg.get(), part.get(), ukeys_s.get(), G,
+                                                                         loops.get(), prow.get(), pcol.get(),
+                                                                         pw.get(), keep.get());
+            c.launches += 2;
+        }
         SC_LAUNCH_CHECK();
-        c.launches += 2;
     }
     ukeys_s.release();
     uw_s.release();

@@ -65,6 +65,7 @@ struct Ctx {
     cudaStream_t stream = nullptr;
     cudaMemPool_t pool = nullptr;      // the device's default pool (stream-ordered temporaries)
     uint32_t* d_status = nullptr;      // device status word
+    unsigned long long* d_refine_ctr = nullptr;  // refinement counters summed over a run (3 words)
     Error last;
     sc_run_stats stats{};
     uint64_t launches = 0;             // kernels launched by the current call
@@ -78,8 +79,13 @@ struct Ctx {
     // auxiliary stream for work that overlaps the next step (local moving's re-queue)
     cudaStream_t aux = nullptr;
     cudaEvent_t ev_aux_start = nullptr, ev_aux_done = nullptr;
+    // pinned host buffer for the small device->host reads that steer the host loop
+    // (bucket counts, counters, sizes): copies into it are truly asynchronous, so
+    // several can be queued and completed by one stream synchronisation
+    uint8_t* mailbox = nullptr;
 };
 constexpr int SIDE_STREAMS = 3;
+constexpr size_t MAILBOX_BYTES = 4096;
 
 // Stream-ordered device buffer of T, from the context's pool on its stream.
 template <class T>
@@ -296,6 +302,8 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
 
 // common.cu
 void check_device_status(Ctx& c);
+// the failure for a status word already read back (none for DEV_OK); clears it
+void raise_device_status(Ctx& c, uint32_t st);
 // Rust-style shortest round-trip text of an f64 (Display of f64).
 std::string fmt_f64(double x);
 

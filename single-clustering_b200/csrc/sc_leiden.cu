@@ -499,14 +499,24 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         if (lane == 0) s_cnt[wib] = 0;
         __syncwarp();
         const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
-        for (uint64_t j = b + lane; j < e; j += 32) {
-            const bool first = j < b + 32;
-            const uint32_t u = first ? u_first : ro(p.nbr + (j));
-            if (u == v) continue;
-            if (REFINE && ro(p.constraint + (u)) != cv) continue;
-            const float wj = first ? w_first : ro(p.w + (j));
-            hinsert_listed(keys, vals, mask, ro(p.memb + (u)), to_fix((double)wj, p.inv_scale), p.status,
-                           s_list[wib], &s_cnt[wib], WARP_DEGREE);
+        for (uint64_t base0 = b; base0 < e; base0 += 32) {  // warp-uniform trip count
+            const uint64_t j = base0 + lane;
+            const bool first = base0 == b;
+            bool ok = j < e;
+            uint32_t u = 0;
+            float wj = 0.0f;
+            if (ok) {
+                u = first ? u_first : ro(p.nbr + (j));
+                wj = first ? w_first : ro(p.w + (j));
+            }
+            ok = ok && u != v;
+            if (REFINE && ok) ok = ro(p.constraint + (u)) == cv;
+            const uint32_t cu = ok ? ro(p.memb + (u)) : 0u;
+            const uint64_t key = ok ? (uint64_t)cu : (0xFFFFFFFF00000000ull | lane);
+            const unsigned peers = __match_any_sync(FULL, key);
+            const long long x = peer_sum(peers, ok ? to_fix((double)wj, p.inv_scale) : 0ll);
+            if (ok && __ffs(peers) - 1 == lane)
+                hinsert_listed(keys, vals, mask, cu, x, p.status, s_list[wib], &s_cnt[wib], WARP_DEGREE);
         }
         fetch_chunk();
         __syncwarp();
@@ -651,11 +661,21 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
         }
         __syncthreads();
         const uint32_t cv = REFINE ? ro(p.constraint + (v)) : 0;
-        for (uint64_t j = b + threadIdx.x; j < e; j += blockDim.x) {
-            uint32_t u = ro(p.nbr + (j));
-            if (u == v) continue;
-            if (REFINE && ro(p.constraint + (u)) != cv) continue;
-            hinsert(keys, vals, mask, ro(p.memb + (u)), to_fix((double)ro(p.w + (j)), p.inv_scale), p.status);
+        {
+            const unsigned lane = threadIdx.x & 31u;
+            // each warp walks its own 32-entry chunks: trip counts are warp-uniform
+            for (uint64_t base0 = b + (threadIdx.x & ~31u); base0 < e; base0 += blockDim.x) {
+                const uint64_t j = base0 + lane;
+                bool ok = j < e;
+                const uint32_t u = ok ? ro(p.nbr + (j)) : 0u;
+                ok = ok && u != v;
+                if (REFINE && ok) ok = ro(p.constraint + (u)) == cv;
+                const uint32_t cu = ok ? ro(p.memb + (u)) : 0u;
+                const uint64_t key = ok ? (uint64_t)cu : (0xFFFFFFFF00000000ull | lane);
+                const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+                const long long x = peer_sum(peers, ok ? to_fix((double)ro(p.w + (j)), p.inv_scale) : 0ll);
+                if (ok && __ffs(peers) - 1 == (int)lane) hinsert(keys, vals, mask, cu, x, p.status);
+            }
         }
         __syncthreads();
         const long long kf = to_fix(ro(p.strength + (v)), p.inv_scale);
@@ -795,7 +815,9 @@ __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t
             bool add = false;
             if (j < e) {
                 u = p.nbr[j];
-                add = u != v && p.memb[u] != t && atomicMax(stamp + u, mark) < mark;
+                // a plain read first: a node already queued for the next sweep
+                // (the common case once many of its neighbours moved) costs no atomic
+                add = u != v && p.memb[u] != t && stamp[u] < mark && atomicMax(stamp + u, mark) < mark;
             }
             const unsigned bal = __ballot_sync(0xFFFFFFFFu, add);
             if (bal) {
@@ -956,28 +978,54 @@ struct Workspace {
     int nblk_large = 0;
 };
 
-class Timer {
+// Phase times of a run: events recorded around each phase on the context's
+// stream, read after the run's last synchronisation, so timing adds none.
+class PhaseClock {
    public:
-    explicit Timer(Ctx& c) : c_(c) {
-        cudaEventCreate(&a_);
-        cudaEventCreate(&b_);
-        cudaEventRecord(a_, c.stream);
+    explicit PhaseClock(Ctx& c) : c_(c) {}
+    PhaseClock(const PhaseClock&) = delete;
+    PhaseClock& operator=(const PhaseClock&) = delete;
+    ~PhaseClock() {
+        for (Span& s : spans_) {
+            cudaEventDestroy(s.a);
+            cudaEventDestroy(s.b);
+        }
     }
-    double stop() {
-        cudaEventRecord(b_, c_.stream);
-        cudaEventSynchronize(b_);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a_, b_);
-        return ms;
+    size_t start() {
+        Span s{};
+        SC_CUDA(cudaEventCreate(&s.a));
+        if (cudaEventCreate(&s.b) != cudaSuccess) {
+            cudaEventDestroy(s.a);
+            SC_CUDA(cudaErrorMemoryAllocation);
+        }
+        spans_.push_back(s);
+        SC_CUDA(cudaEventRecord(s.a, c_.stream));
+        return spans_.size() - 1;
     }
-    ~Timer() {
-        cudaEventDestroy(a_);
-        cudaEventDestroy(b_);
+    // the span's time is added to *into when collect() runs
+    void stop(size_t i, double* into) {
+        SC_CUDA(cudaEventRecord(spans_[i].b, c_.stream));
+        spans_[i].into = into;
+    }
+    // waits for every stopped span and adds its time to its target
+    void collect() {
+        for (Span& s : spans_) {
+            if (!s.into) continue;
+            SC_CUDA(cudaEventSynchronize(s.b));
+            float ms = 0.0f;
+            SC_CUDA(cudaEventElapsedTime(&ms, s.a, s.b));
+            *s.into += ms;
+            s.into = nullptr;
+        }
     }
 
    private:
+    struct Span {
+        cudaEvent_t a, b;
+        double* into;
+    };
     Ctx& c_;
-    cudaEvent_t a_, b_;
+    std::vector<Span> spans_;
 };
 
 void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
@@ -1174,6 +1222,9 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     static const int trace = std::getenv("SC_TRACE") ? std::atoi(std::getenv("SC_TRACE")) : 0;
     // experimental: stop once a sweep moves fewer than tail * n nodes (0 = run to a local optimum)
     const double tail = std::getenv("SC_LM_TAIL") ? std::atof(std::getenv("SC_LM_TAIL")) : 0.0;
+    unsigned long long last_ctr[4] = {0, 0, 0, 0};
+    long long last_gacc = 0;
+    bool read_fresh = false;  // last_ctr / last_gacc hold the counters' current values
     for (uint32_t sweep = 0; sweep < (uint32_t)MAX_SWEEPS; ++sweep) {
         zero(c, ws.counts.get(), B * NBUCKET);
         zero(c, ws.ncount.get(), 1);
@@ -1184,9 +1235,18 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         c.launches++;
         uint32_t counts[64];
         unsigned long long ctr[4];
-        d2h(c, counts, ws.counts.get(), B * NBUCKET);
-        d2h(c, ctr, ws.counters.get(), 4);
-        sync(c);
+        {
+            Mailbox mb(c);
+            const uint32_t* hc = mb.get(ws.counts.get(), B * NBUCKET);
+            const unsigned long long* hk = mb.get(ws.counters.get(), 4);
+            const long long* hg = mb.get(ws.gain_acc.get(), 1);
+            mb.wait();
+            std::memcpy(counts, hc, sizeof(uint32_t) * B * NBUCKET);
+            std::memcpy(ctr, hk, sizeof ctr);
+            std::memcpy(last_ctr, hk, sizeof ctr);
+            last_gacc = *hg;
+            read_fresh = true;  // nothing that changes the counters runs before the next launch below
+        }
         uint32_t offs[65];
         offs[0] = 0;
         for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
@@ -1198,6 +1258,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         if (ctr[0] >= budget) break;
         moves_before = ctr[0];
         if (offs[B * NBUCKET] == 0) break;
+        read_fresh = false;
         h2d(c, ws.cursor.get(), offs, B * NBUCKET);
         k_bucket_scatter<<<grid_for(offs[B * NBUCKET], TB), TB, 0, c.stream>>>(
             g.ptr, alist, ws.acount.get(), n, seed, sweep, B, route_of(c), ws.cursor.get(), ws.list.get(),
@@ -1207,7 +1268,9 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         // A batch's re-queue reads memberships and writes only the next sweep's
         // list, so with an auxiliary stream it runs while the next batch decides;
         // it must end before the next batch commits (which changes memberships).
-        const bool overlap = c.aux != nullptr;
+        // (a sweep of a few thousand nodes gains nothing from the overlap and
+        // would pay three extra stream operations per batch)
+        const bool overlap = c.aux != nullptr && offs[B * NBUCKET] > c.tuning.small_batch;
         bool act_pending = false;
         for (int b = 0; b < B; ++b) {
             ++epoch;
@@ -1246,11 +1309,16 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         all_active = false;
         r.sweeps++;
     }
-    unsigned long long ctr[4];
-    long long gacc = 0;
-    d2h(c, ctr, ws.counters.get(), 4);
-    d2h(c, &gacc, ws.gain_acc.get(), 1);
-    sync(c);
+    if (!read_fresh) {  // the sweep limit ended the loop after launching a sweep
+        Mailbox mb(c);
+        const unsigned long long* hk = mb.get(ws.counters.get(), 4);
+        const long long* hg = mb.get(ws.gain_acc.get(), 1);
+        mb.wait();
+        std::memcpy(last_ctr, hk, sizeof last_ctr);
+        last_gacc = *hg;
+    }
+    const unsigned long long* ctr = last_ctr;
+    const long long gacc = last_gacc;
     r.moves = ctr[0];
     r.improvement = (double)gacc * sc.scale;
     // algorithmic bytes: 16 per node visit + 12 per scanned entry + 8 per candidate
@@ -1259,10 +1327,24 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
 }
 
 // refine (refine.rs:29-103): refined ids < n; constraint = working membership.
-double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint, uint32_t* refined,
-              const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
+// Adds a refinement's node, entry and candidate counters to the run's totals.
+__global__ void k_add_refine_counters(const unsigned long long* __restrict__ ctr, unsigned long long* run) {
+    if (threadIdx.x == 0) {
+        run[0] += ctr[3];
+        run[1] += ctr[1];
+        run[2] += ctr[2];
+    }
+}
+
+// Algorithmic bytes of the refinements of a run, from the counters summed on the device.
+double refine_alg_bytes(const unsigned long long* run) {
+    return 16.0 * (double)run[0] + 16.0 * (double)run[1] + 8.0 * (double)run[2];
+}
+
+void refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint, uint32_t* refined,
+            const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
     const uint64_t n = g.n;
-    if (n == 0) return 0.0;
+    if (n == 0) return;
     DBuf<long long> Kf(c, n), Wf(c, n);
     DBuf<uint32_t> csize(c, n);
     DBuf<unsigned long long> claim(c, cfg.has_max_community_weight ? n : 0);
@@ -1321,8 +1403,12 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
     SC_LAUNCH_CHECK();
     c.launches++;
     uint32_t counts[64];
-    d2h(c, counts, ws.counts.get(), B * NBUCKET);
-    sync(c);
+    {
+        Mailbox mb(c);
+        const uint32_t* hc = mb.get(ws.counts.get(), B * NBUCKET);
+        mb.wait();
+        std::memcpy(counts, hc, sizeof(uint32_t) * B * NBUCKET);
+    }
     uint32_t offs[65];
     offs[0] = 0;
     for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
@@ -1345,10 +1431,10 @@ double refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constrai
         SC_LAUNCH_CHECK();
         c.launches++;
     }
-    unsigned long long ctr[4];
-    d2h(c, ctr, ws.counters.get(), 4);
-    sync(c);
-    return 16.0 * (double)ctr[3] + 16.0 * (double)ctr[1] + 8.0 * (double)ctr[2];
+    // counters go to the run's totals on the device (read once, at the end of the run)
+    k_add_refine_counters<<<1, 32, 0, c.stream>>>(ws.counters.get(), c.d_refine_ctr);
+    SC_LAUNCH_CHECK();
+    c.launches++;
 }
 
 struct PassOut {
@@ -1359,7 +1445,7 @@ struct PassOut {
 
 // run_once (mod.rs:214-289) from compact initial ids `init` (< C0).
 void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, const sc_leiden_config& cfg,
-              uint64_t pass_seed, PassOut& out, sc_run_stats& st) {
+              uint64_t pass_seed, PassOut& out, sc_run_stats& st, PhaseClock& clock) {
     const uint64_t n0 = g0.n;
     const double gamma = cfg.resolution;
     std::unique_ptr<DevGraph> owned;
@@ -1372,7 +1458,7 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
     double improvement = 0.0;
     static const bool trace = std::getenv("SC_TRACE") != nullptr;
     for (uint64_t level = 0; level < cfg.max_levels; ++level) {
-        const uint64_t nl = gl->n;
+        const uint64_t nl = gl->n, level_E = gl->E;
         const sc_run_stats before = st;
         const uint64_t lvl_seed = hash3(pass_seed, level, 0x1eafull);
         Scales sc = scales_for(*gl);
@@ -1380,9 +1466,9 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         prepare_workspace(c, ws, *gl);
         // ids of memb are < C; fresh ids live in [C, C + nl)
         {
-            Timer t(c);
+            const size_t t = clock.start();
             MoveResult mr = local_move(c, *gl, ws, memb.get(), C, cfg, lvl_seed, sc, gamma);
-            st.ms_local_move += t.stop();
+            clock.stop(t, &st.ms_local_move);
             improvement += mr.improvement;
             st.local_move_sweeps += mr.sweeps;
             st.moves += mr.moves;
@@ -1391,25 +1477,25 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         DBuf<uint32_t> collapse(c, nl);
         uint64_t id_space;
         if (cfg.refine) {
-            Timer t(c);
-            st.alg_bytes_refine += refine(c, *gl, ws, memb.get(), collapse.get(), cfg,
-                                          hash3(lvl_seed, 0x7e71eull, 1), sc, gamma);
-            st.ms_refine += t.stop();
+            const size_t t = clock.start();
+            refine(c, *gl, ws, memb.get(), collapse.get(), cfg, hash3(lvl_seed, 0x7e71eull, 1), sc, gamma);
+            clock.stop(t, &st.ms_refine);
             id_space = nl;
         } else {
             d2d(c, collapse.get(), memb.get(), nl);
             id_space = C + nl;
         }
-        Timer t_agg(c);
+        const size_t t_agg = clock.start();
         DBuf<uint32_t> grp(c, nl);
         uint32_t G = renumber_ids(c, collapse.get(), nl, id_space, grp.get());
         st.levels++;
         auto trace_level = [&](uint64_t ng) {
             if (!trace) return;
+            clock.collect();
             std::fprintf(stderr,
                          "[sc] level %llu n=%llu E=%llu exact=%d/%d groups=%llu sweeps=%llu moves=%llu "
                          "lm=%.3fms ref=%.3fms agg=%.3fms\n",
-                         (unsigned long long)level, (unsigned long long)nl, (unsigned long long)gl->E,
+                         (unsigned long long)level, (unsigned long long)nl, (unsigned long long)level_E,
                          (int)gl->exact_w, (int)gl->exact_nw,
                          (unsigned long long)ng,
                          (unsigned long long)(st.local_move_sweeps - before.local_move_sweeps),
@@ -1417,7 +1503,7 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
                          st.ms_refine - before.ms_refine, st.ms_aggregate - before.ms_aggregate);
         };
         if (G >= nl) {
-            st.ms_aggregate += t_agg.stop();
+            clock.stop(t_agg, &st.ms_aggregate);
             trace_level(G);
             break;
         }
@@ -1435,7 +1521,7 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         memb = std::move(cm2);
         owned = std::move(coarse);
         gl = owned.get();
-        st.ms_aggregate += t_agg.stop();
+        clock.stop(t_agg, &st.ms_aggregate);
         trace_level(G);
     }
     // final ascending renumber (mod.rs:282-286)
@@ -1480,7 +1566,9 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
             uint32_t* d_labels_out, uint64_t* n_clusters) {
     validate_config(cfg);
     std::memset(&c.stats, 0, sizeof c.stats);
-    Timer total(c);
+    PhaseClock clock(c);
+    const size_t t_total = clock.start();
+    zero(c, c.d_refine_ctr, 3);
     const uint64_t n = g.n;
     if (n == 0) {
         *n_clusters = 0;
@@ -1502,7 +1590,7 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
     uint64_t stagnant = 0;
     for (uint64_t it = 0; it < cfg.n_iterations; ++it) {
         PassOut po;
-        run_pass(c, g, labels.get(), C, cfg, hash3(seed, it, 0x9a55ull), po, c.stats);
+        run_pass(c, g, labels.get(), C, cfg, hash3(seed, it, 0x9a55ull), po, c.stats, clock);
         labels = std::move(po.labels);
         C = po.n_clusters;
         clusters = C;
@@ -1516,8 +1604,17 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
         }
     }
     d2d(c, d_labels_out, labels.get(), n);
-    check_device_status(c);
-    c.stats.ms_total = total.stop();
+    clock.stop(t_total, &c.stats.ms_total);
+    {
+        Mailbox mb(c);
+        const uint32_t* hs = mb.get(c.d_status, 1);
+        const unsigned long long* hr = mb.get(c.d_refine_ctr, 3);
+        mb.wait();
+        const uint32_t status = *hs;
+        c.stats.alg_bytes_refine = refine_alg_bytes(hr);
+        raise_device_status(c, status);
+    }
+    clock.collect();
     c.stats.ms_other = c.stats.ms_total - c.stats.ms_local_move - c.stats.ms_refine - c.stats.ms_aggregate;
     c.stats.kernel_launches = c.launches;
     *n_clusters = clusters;

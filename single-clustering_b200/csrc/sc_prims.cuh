@@ -85,12 +85,32 @@ void select_flagged(Ctx& c, const T* in, const F* flags, T* out, uint64_t* d_cou
     c.launches += 2;
 }
 
+// Small device->host reads through the context's pinned mailbox: get() queues
+// an asynchronous copy and returns where its result will be; wait() completes
+// every copy queued so far with one synchronisation of the context's stream.
+// Results are valid until the next Mailbox of the same context is used.
+struct Mailbox {
+    Ctx& c;
+    size_t off = 0;
+    explicit Mailbox(Ctx& ctx) : c(ctx) {}
+    template <class T>
+    const T* get(const T* d, size_t n) {
+        off = (off + 15) & ~size_t(15);
+        if (off + n * sizeof(T) > MAILBOX_BYTES) fail(SC_E_INTERNAL, "mailbox overflow (%zu bytes)", off + n * sizeof(T));
+        T* h = reinterpret_cast<T*>(c.mailbox + off);
+        if (n) SC_CUDA(cudaMemcpyAsync(h, d, n * sizeof(T), cudaMemcpyDeviceToHost, c.stream));
+        off += n * sizeof(T);
+        return h;
+    }
+    void wait() { SC_CUDA(cudaStreamSynchronize(c.stream)); }
+};
+
 template <class T>
 T to_host(Ctx& c, const T* d) {
-    T h;
-    SC_CUDA(cudaMemcpyAsync(&h, d, sizeof(T), cudaMemcpyDeviceToHost, c.stream));
-    SC_CUDA(cudaStreamSynchronize(c.stream));
-    return h;
+    Mailbox mb(c);
+    const T* h = mb.get(d, 1);
+    mb.wait();
+    return *h;
 }
 
 template <class T>
@@ -111,6 +131,31 @@ void zero(Ctx& c, T* d, size_t n) {
 }
 inline void sync(Ctx& c) { SC_CUDA(cudaStreamSynchronize(c.stream)); }
 
+
+// Sum of x over this lane's peers (the lanes holding the same key; `peers` from
+// __match_any_sync), complete in the lowest peer. A tree fold over each peer
+// group's ranks: in round r a peer whose rank has bit r clear adds the value of
+// the next peer above it that is still open, then the peers with bit r set
+// close; five rounds at most. Use it where the grouping cannot change the sum:
+// integers, or doubles whose every partial sum is exact. Neighbour entries of
+// a node (or of a group's members) mostly share one or two keys, and without
+// this fold each of them lands on the same table slot, one atomic after
+// another. Every lane of the warp must call it.
+template <class T>
+__device__ __forceinline__ T peer_sum(unsigned peers, T x) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const unsigned lane = threadIdx.x & 31u;
+    unsigned rank = __popc(peers & ((1u << lane) - 1u));
+    unsigned above = peers & ~((2u << lane) - 1u);  // lane 31: (2u << 31) - 1 = ~0u, nothing above
+    while (__any_sync(FULL, above != 0u)) {
+        const int next = __ffs(above);
+        const T t = __shfl_sync(FULL, x, next ? next - 1 : (int)lane);
+        if (next) x += t;
+        above &= ~__ballot_sync(FULL, rank & 1u);
+        rank >>= 1;
+    }
+    return x;
+}
 
 // Σ_{i in [b, e)} f(i) in index order, by one warp: lanes load 32 terms at a
 // time (coalesced), then every lane folds them in order through shuffles, so
