@@ -137,6 +137,7 @@ void release_ctx(sc::Ctx& c) {
     if (c.ev_aux_done) cudaEventDestroy(c.ev_aux_done);
     c.aux = nullptr;
     c.ev_aux_start = c.ev_aux_done = nullptr;
+    sc::release_staging(c);
     if (c.mailbox) cudaFreeHost(c.mailbox);
     c.mailbox = nullptr;
     if (c.d_status) cudaFree(c.d_status);
@@ -152,10 +153,7 @@ void run_instance(sc::Ctx& w, const sc::DevGraph& G, const sc_leiden_config& cfg
     sc::DBuf<uint32_t> lab(w, G.n);
     uint64_t ncl = 0;
     sc::leiden(w, G, cfg, initial, lab.get(), &ncl);
-    std::vector<uint32_t> h(G.n);
-    sc::d2h(w, h.data(), lab.get(), G.n);
-    sc::sync(w);
-    for (uint64_t j = 0; j < G.n; ++j) labels_out[j] = h[j];
+    sc::download_labels(w, lab.get(), G.n, labels_out);
     *n_clusters = ncl;
 }
 
@@ -491,12 +489,7 @@ sc_status sc_leiden_from(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config*
         sc::DBuf<uint32_t> lab(c, G.n);
         uint64_t ncl = 0;
         sc::leiden(c, G, *cfg, initial, lab.get(), &ncl);
-        if (G.n) {
-            std::vector<uint32_t> h(G.n);
-            sc::d2h(c, h.data(), lab.get(), G.n);
-            sc::sync(c);
-            for (uint64_t i = 0; i < G.n; ++i) labels_out[i] = h[i];
-        }
+        sc::download_labels(c, lab.get(), G.n, labels_out);
         *n_clusters_out = ncl;
     });
 }
@@ -757,12 +750,7 @@ sc_status sc_mlp_propose(sc_ctx* ctx, sc_mlp* m, const sc_graph* g, double resol
         upload_labels(c, fine, G.n, df);
         const uint64_t k = sc::mlp_propose(c, *m->m, G, resolution, dc.get(), df.get(), threshold, core_fraction,
                                            lab.get(), prob_out, prob_capacity);
-        if (G.n) {
-            std::vector<uint32_t> h(G.n);
-            sc::d2h(c, h.data(), lab.get(), G.n);
-            sc::sync(c);
-            for (uint64_t i = 0; i < G.n; ++i) labels_out[i] = h[i];
-        }
+        sc::download_labels(c, lab.get(), G.n, labels_out);
         *n_clusters_out = k;
     });
 }

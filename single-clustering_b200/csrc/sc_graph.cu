@@ -437,10 +437,14 @@ DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint
     const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     std::unique_ptr<DevGraph> g(new DevGraph());
     galloc(c, *g, n, n_nbr);
-    SC_CUDA(cudaMemcpyAsync(g->ptr, ptr, n_ptr * sizeof(uint64_t), kind, c.stream));
+    auto copy_in = [&](void* dst, const void* src, size_t bytes) {
+        if (kind == cudaMemcpyHostToDevice) upload(c, dst, src, bytes);
+        else if (bytes) SC_CUDA(cudaMemcpyAsync(dst, src, bytes, kind, c.stream));
+    };
+    copy_in(g->ptr, ptr, n_ptr * sizeof(uint64_t));
     if (n_nbr) {
-        SC_CUDA(cudaMemcpyAsync(g->nbr, nbr, n_nbr * sizeof(uint32_t), kind, c.stream));
-        SC_CUDA(cudaMemcpyAsync(g->w, w, n_nbr * sizeof(float), kind, c.stream));
+        copy_in(g->nbr, nbr, n_nbr * sizeof(uint32_t));
+        copy_in(g->w, w, n_nbr * sizeof(float));
     }
     uint64_t last = to_host(c, g->ptr + n);
     if (last != n_nbr)
@@ -497,7 +501,7 @@ DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint
             i.expected_len = n;
             fail_info(i);
         }
-        SC_CUDA(cudaMemcpyAsync(g->node_w, node_w, n * sizeof(double), kind, c.stream));
+        copy_in(g->node_w, node_w, n * sizeof(double));
         if (n) {
             h2d(c, first.get(), &NOBAD, 1);
             k_first_bad_nodew<<<grid_for(n, TB), TB, 0, c.stream>>>(g->node_w, n, first.get());

@@ -83,9 +83,22 @@ struct Ctx {
     // (bucket counts, counters, sizes): copies into it are truly asynchronous, so
     // several can be queued and completed by one stream synchronisation
     uint8_t* mailbox = nullptr;
+    // pinned staging lanes of large host -> device uploads (created on first use)
+    struct Staging* staging = nullptr;
 };
 constexpr int SIDE_STREAMS = 3;
 constexpr size_t MAILBOX_BYTES = 4096;
+constexpr int STAGE_LANES = 4;                     // host threads of a staged upload
+constexpr size_t STAGE_CHUNK = size_t(4) << 20;     // bytes per pinned buffer (two per lane)
+constexpr size_t STAGE_MIN_BYTES = size_t(16) << 20;  // smaller uploads use one plain copy
+
+// Host -> device copy of `bytes` from pageable `src`, ordered on the context's
+// stream (large copies go through the pinned staging lanes); src may be reused
+// when it returns.
+void upload(Ctx& c, void* dst, const void* src, size_t bytes);
+void release_staging(Ctx& c);
+// u32 device labels -> u64 host labels (widened on the device, one copy)
+void download_labels(Ctx& c, const uint32_t* d_labels, uint64_t n, uint64_t* host_out);
 
 // Stream-ordered device buffer of T, from the context's pool on its stream.
 template <class T>
