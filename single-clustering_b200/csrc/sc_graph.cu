@@ -166,12 +166,15 @@ __global__ void k_merge_write(const uint64_t* __restrict__ ptr_in, const uint64_
     }
 }
 
-// Per row of a clean CSR, one warp per row: strength in ascending-neighbour
-// order (self-loop twice, csr_network.rs:313-320), self-loop weight, lowest set
-// bit of the stored weights, any self-loop, max degree, hub count.
+// Per row of a clean CSR, one warp per row: strength (self-loop twice,
+// csr_network.rs:313-320), self-loop weight, lowest set bit of the stored
+// weights, any self-loop, max degree, hub count.
 __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                             const float* __restrict__ w, uint64_t n, double* strength,
                             double* self_loop, int* min_low, unsigned* any_loop, unsigned* max_deg) {
+    // One pass per row. The strengths are folded in any order here: exact (and
+    // so equal to the reference's left fold) whenever the graph turns out to be
+    // in the exact regime; otherwise finalize recomputes them in order.
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
@@ -179,23 +182,24 @@ __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __
     unsigned loop = 0, mdeg = 0, hubs = 0;
     for (uint64_t v = warp; v < n; v += nwarps) {
         const uint64_t b = ptr[v], e = ptr[v + 1];
-        double sl = 0.0;
+        double sl = 0.0, acc = 0.0;
         for (uint64_t i = b + lane; i < e; i += 32) {
-            float x = w[i];
+            const float x = w[i];
             low = min(low, lowbit_exp_f32(x));
+            const double st = (double)x;
             if (nbr[i] == (uint32_t)v) {
                 loop = 1;
-                sl = (double)x;
+                sl = st;
+                acc = __dadd_rn(acc, __dmul_rn(2.0, st));
+            } else {
+                acc = __dadd_rn(acc, st);
             }
         }
-        const double s = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) {
-            const double st = (double)w[i];
-            return nbr[i] == (uint32_t)v ? __dmul_rn(2.0, st) : st;
-        });
+        for (int o = 16; o; o >>= 1) acc = __dadd_rn(acc, __shfl_xor_sync(0xFFFFFFFFu, acc, o));
         // at most one lane saw the self-loop
         for (int o = 16; o; o >>= 1) sl = fmax(sl, __shfl_xor_sync(0xFFFFFFFFu, sl, o));
         if (lane == 0) {
-            strength[v] = s;
+            strength[v] = e > b ? __dadd_rn(0.0, acc) : 0.0;
             self_loop[v] = sl;
             mdeg = max(mdeg, (unsigned)(e - b));
             hubs += (e - b) > HUB_DEGREE;
@@ -212,6 +216,23 @@ __global__ void k_row_stats(const uint64_t* __restrict__ ptr, const uint32_t* __
         if (loop) atomicOr(any_loop, 1u);
         atomicMax(max_deg, mdeg);
         if (hubs) atomicAdd(any_loop + 2, hubs);
+    }
+}
+
+// Strengths as the reference folds them (csr_network.rs:313-320): left to
+// right over the row in ascending-neighbour order from 0.0, a self-loop
+// counted twice. For graphs outside the exact regime.
+__global__ void k_row_strength_ordered(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                       const float* __restrict__ w, uint64_t n, double* strength) {
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t v = warp; v < n; v += nwarps) {
+        const uint64_t b = ptr[v], e = ptr[v + 1];
+        const double s = warp_ordered_sum(b, e, 0.0, [&](uint64_t i) {
+            const double st = (double)w[i];
+            return nbr[i] == (uint32_t)v ? __dmul_rn(2.0, st) : st;
+        });
+        if ((threadIdx.x & 31u) == 0) strength[v] = s;
     }
 }
 
@@ -321,6 +342,11 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
     g.exact_nw = (g.e0_nw == 0x7FFFFFFF) || (approx_nw < std::ldexp(1.0, 52 + g.e0_nw));
     // Rust-order Σ of the node weights (a fold from -0.0): in the exact regime any
     // order gives these bits, and n > 0 terms >= +0.0 never leave the -0.0 start
+    if (n && !g.exact_w) {  // the strengths in the reference's order
+        k_row_strength_ordered<<<grid_for(n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, n, g.strength);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
     if (n == 0) g.total_node_weight = -0.0;
     else g.total_node_weight = g.exact_nw ? approx_nw : ordered_sum(c, g.node_w, n);
 
@@ -1213,6 +1239,7 @@ __global__ void __launch_bounds__(256)
 }
 
 constexpr uint64_t AGG_SMEM_SLOTS = 4096;  // shared table of the block kernel (48 KB)
+constexpr uint64_t AGG_SMALL_GRAPH = 1u << 16;  // entries up to which the hash path is always taken
 constexpr uint64_t AGG_SMEM_KEEP = AGG_SMEM_SLOTS / 2;
 
 // A row has at most min(cap, G) distinct neighbour groups; its table needs twice that.
@@ -1436,8 +1463,9 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         nmid = counts[1];
         // Rows past the warp kernel are served by one block each; when they hold
         // more than a tenth of the entries the sort path is faster (measured on
-        // kNN graphs at every level of a run).
-        if (counts[2] * 10 > g.E) return nullptr;
+        // kNN graphs at every level of a run), except on small graphs, where the
+        // sort path's extra launches and read-backs cost more than any block.
+        if (counts[2] * 10 > g.E && g.E > AGG_SMALL_GRAPH) return nullptr;
     }
     if (nmid) {
         const size_t smem = AGG_SMEM_SLOTS * (sizeof(unsigned long long) + sizeof(uint32_t)) +

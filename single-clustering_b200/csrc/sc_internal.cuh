@@ -175,7 +175,7 @@ struct DevGraph {
     mutable std::atomic<int> sym_state{0};
     // Arrays come from the stream-ordered pool. A graph owned by a running call
     // (a coarse level) returns them on that stream; a graph handed to the user
-    // (stream == nullptr) frees them with cudaFree.
+    // (stream == nullptr) returns them once the device is idle.
     cudaStream_t stream = nullptr;
     void free_all();
     ~DevGraph() { free_all(); }

@@ -776,12 +776,14 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
         if (lost(p, v)) continue;
         const uint32_t t = p.tgt[v], old = p.from[v];
         const long long kf = to_fix(p.strength[v], p.inv_scale);
-        const long long af = to_fix(p.node_w[v], p.inv_nscale);
         p.memb[v] = t;
         atomicAdd((unsigned long long*)(p.Kf + old), (unsigned long long)(-kf));
         atomicAdd((unsigned long long*)(p.Kf + t), (unsigned long long)kf);
-        atomicAdd((unsigned long long*)(p.Wf + old), (unsigned long long)(-af));
-        atomicAdd((unsigned long long*)(p.Wf + t), (unsigned long long)af);
+        if (p.need_nc) {  // community node weights: read only by CPM and the weight cap
+            const long long af = to_fix(p.node_w[v], p.inv_nscale);
+            atomicAdd((unsigned long long*)(p.Wf + old), (unsigned long long)(-af));
+            atomicAdd((unsigned long long*)(p.Wf + t), (unsigned long long)af);
+        }
         atomicSub(p.csize + old, 1u);
         atomicAdd(p.csize + t, 1u);
         nmoves++;
@@ -798,19 +800,31 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
 // commit, so every membership it reads is final.
 // A node enters the next sweep's list once: its stamp is raised to `mark` (the
 // next sweep's number + 1) and only the lane that raised it appends it.
+// Half a warp per node (k-NN rows hold 10-30 entries, so a whole warp per row
+// would leave most lanes idle); both halves walk max(their chunk counts) chunks
+// so that the ballot and the shuffle see every lane.
 __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t count, uint32_t* stamp,
                            uint32_t mark, uint32_t* next_list, uint32_t* next_count) {
-    // one warp per node of the batch, lanes over its row (coalesced)
-    const unsigned lane = threadIdx.x & 31u;
+    const unsigned FULL = 0xFFFFFFFFu;
+    const unsigned lane = threadIdx.x & 31u, half = lane >> 4, sub = lane & 15u;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = warp; i < count; i += nwarps) {
-        const uint32_t v = list[i];
-        if (p.moved[v] != p.cur) continue;
-        const uint32_t t = p.memb[v];
-        const uint64_t e = p.ptr[v + 1];
-        for (uint64_t j0 = p.ptr[v]; j0 < e; j0 += 32) {
-            const uint64_t j = j0 + lane;
+    for (uint64_t i0 = warp * 2; i0 < count; i0 += nwarps * 2) {  // warp-uniform
+        const uint64_t i = i0 + half;
+        uint32_t v = 0, t = 0;
+        uint64_t b = 0, e = 0;
+        if (i < count) {
+            v = list[i];
+            if (p.moved[v] == p.cur) {
+                t = p.memb[v];
+                b = p.ptr[v];
+                e = p.ptr[v + 1];
+            }
+        }
+        const uint64_t my_chunks = (e - b + 15) >> 4;
+        const uint64_t chunks = max(my_chunks, __shfl_xor_sync(FULL, my_chunks, 16));
+        for (uint64_t ch = 0; ch < chunks; ++ch) {
+            const uint64_t j = b + ch * 16 + sub;
             uint32_t u = 0;
             bool add = false;
             if (j < e) {
@@ -819,12 +833,12 @@ __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t
                 // (the common case once many of its neighbours moved) costs no atomic
                 add = u != v && p.memb[u] != t && stamp[u] < mark && atomicMax(stamp + u, mark) < mark;
             }
-            const unsigned bal = __ballot_sync(0xFFFFFFFFu, add);
+            const unsigned bal = __ballot_sync(FULL, add);
             if (bal) {
                 const int leader = __ffs(bal) - 1;
                 uint32_t base = 0;
                 if ((int)lane == leader) base = atomicAdd(next_count, (uint32_t)__popc(bal));
-                base = __shfl_sync(0xFFFFFFFFu, base, leader);
+                base = __shfl_sync(FULL, base, leader);
                 if (add) next_list[base + __popc(bal & ((1u << lane) - 1u))] = u;
             }
         }
@@ -916,7 +930,7 @@ __global__ void k_init_comm(const uint32_t* __restrict__ memb, uint64_t n, const
          v += (uint64_t)gridDim.x * blockDim.x) {
         uint32_t c = memb[v];
         atomicAdd((unsigned long long*)(Kf + c), (unsigned long long)to_fix(strength[v], inv_scale));
-        atomicAdd((unsigned long long*)(Wf + c), (unsigned long long)to_fix(node_w[v], inv_nscale));
+        if (Wf) atomicAdd((unsigned long long*)(Wf + c), (unsigned long long)to_fix(node_w[v], inv_nscale));
         atomicAdd(csize + c, 1u);
     }
 }
@@ -1162,12 +1176,13 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     const uint64_t n = g.n;
     if (n == 0) return r;
     const uint64_t S = S0 + n;
-    DBuf<long long> Kf(c, S), Wf(c, S);
+    const bool need_nc = cfg.objective == SC_OBJECTIVE_CPM || cfg.has_max_community_weight;
+    DBuf<long long> Kf(c, S), Wf(c, need_nc ? S : 0);  // Wf only where CPM or the cap reads it
     DBuf<uint32_t> csize(c, S);
     DBuf<unsigned long long> claim(c, cfg.has_max_community_weight ? S : 0);
     zero(c, claim.get(), claim.n);
     zero(c, Kf.get(), S);
-    zero(c, Wf.get(), S);
+    zero(c, Wf.get(), Wf.n);
     zero(c, csize.get(), S);
     k_init_comm<<<grid_for(n, TB), TB, 0, c.stream>>>(memb, n, g.strength, g.node_w, sc.inv, sc.ninv,
                                                       Kf.get(), Wf.get(), csize.get());
@@ -1294,7 +1309,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
                 SC_CUDA(cudaStreamWaitEvent(c.aux, c.ev_aux_start, 0));
                 as = c.aux;
             }
-            k_activate<<<grid_for((uint64_t)(hi - lo) * 32, TB, 148u * 64u), TB, 0, as>>>(
+            k_activate<<<grid_for((uint64_t)(hi - lo) * 16, TB, 148u * 64u), TB, 0, as>>>(
                 p, ws.list.get() + lo, hi - lo, ws.stamp.get(), sweep + 2, ws.nlist.get(), ws.ncount.get());
             if (overlap) {
                 SC_CUDA(cudaEventRecord(c.ev_aux_done, c.aux));
@@ -1345,12 +1360,13 @@ void refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint
             const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
     const uint64_t n = g.n;
     if (n == 0) return;
-    DBuf<long long> Kf(c, n), Wf(c, n);
+    const bool need_nc = cfg.objective == SC_OBJECTIVE_CPM || cfg.has_max_community_weight;
+    DBuf<long long> Kf(c, n), Wf(c, need_nc ? n : 0);  // Wf only where CPM or the cap reads it
     DBuf<uint32_t> csize(c, n);
     DBuf<unsigned long long> claim(c, cfg.has_max_community_weight ? n : 0);
     zero(c, claim.get(), claim.n);
     zero(c, Kf.get(), n);
-    zero(c, Wf.get(), n);
+    zero(c, Wf.get(), Wf.n);
     zero(c, csize.get(), n);
     k_identity<<<grid_for(n, TB), TB, 0, c.stream>>>(refined, n);
     k_init_comm<<<grid_for(n, TB), TB, 0, c.stream>>>(refined, n, g.strength, g.node_w, sc.inv, sc.ninv,
