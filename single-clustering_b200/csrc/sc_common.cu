@@ -140,15 +140,21 @@ void DevGraph::free_all() {
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != device) cudaSetDevice(device);
-        // Pool memory goes back to the pool only through cudaFreeAsync (a plain
-        // cudaFree leaves it counted as in use, so every destroyed user graph
-        // would stay allocated). A user graph may still be read by work queued on
-        // any context's stream: wait for the device, free on the legacy stream
-        // and wait for that, so the call stays synchronous for the caller.
-        if (!stream) cudaDeviceSynchronize();
-        for (void* p : ps)
-            if (p) cudaFreeAsync(p, stream ? stream : (cudaStream_t)0);
-        if (!stream) cudaStreamSynchronize((cudaStream_t)0);
+        // cudaMalloc'd arrays: cudaFree (it waits for the device). Pool memory
+        // goes back to the pool only through cudaFreeAsync (a plain cudaFree
+        // leaves it counted as in use). A pooled graph handed to the user may
+        // still be read by work queued on any context's stream: wait for the
+        // device, free on the legacy stream and wait for that, so the call stays
+        // synchronous for the caller.
+        if (!pooled) {
+            for (void* p : ps)
+                if (p) cudaFree(p);
+        } else {
+            if (!stream) cudaDeviceSynchronize();
+            for (void* p : ps)
+                if (p) cudaFreeAsync(p, stream ? stream : (cudaStream_t)0);
+            if (!stream) cudaStreamSynchronize((cudaStream_t)0);
+        }
         if (prev != device) cudaSetDevice(prev);
     }
     ptr = nullptr;

@@ -14,31 +14,41 @@ namespace {
 
 constexpr unsigned TB = 256;
 
+// A graph array: from the stream-ordered pool for the graphs of a running call,
+// from cudaMalloc for graphs handed to the user (see DevGraph::pooled).
 template <class T>
-void palloc(Ctx& c, T** p, uint64_t count) {
-    cudaError_t e = cudaMallocAsync((void**)p, count * sizeof(T), c.stream);
+void palloc(Ctx& c, bool pooled, T** p, uint64_t count) {
+    cudaError_t e = pooled ? cudaMallocAsync((void**)p, count * sizeof(T), c.stream)
+                           : cudaMalloc((void**)p, count * sizeof(T));
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
         fail(SC_E_OUT_OF_MEMORY, "device allocation of %llu bytes failed",
              (unsigned long long)(count * sizeof(T)));
     }
-    if (e != cudaSuccess) throw_cuda(e, "cudaMallocAsync", __FILE__, __LINE__);
+    if (e != cudaSuccess) throw_cuda(e, pooled ? "cudaMallocAsync" : "cudaMalloc", __FILE__, __LINE__);
+}
+
+// Frees an array palloc gave out (a plain cudaFree waits for the device first).
+void pfree(Ctx& c, bool pooled, void* p) {
+    if (!p) return;
+    if (pooled) cudaFreeAsync(p, c.stream);
+    else cudaFree(p);
 }
 
 void galloc(Ctx& c, DevGraph& g, uint64_t n, uint64_t E) {
     SC_CUDA(cudaGetDevice(&g.device));
     g.n = n;
     g.E = E;
-    palloc(c, &g.ptr, n + 1);
+    palloc(c, g.pooled, &g.ptr, n + 1);
     if (E) {
-        palloc(c, &g.nbr, E);
-        palloc(c, &g.w, E);
-        palloc(c, &g.erow, E);
+        palloc(c, g.pooled, &g.nbr, E);
+        palloc(c, g.pooled, &g.w, E);
+        palloc(c, g.pooled, &g.erow, E);
     }
     if (n) {
-        palloc(c, &g.node_w, n);
-        palloc(c, &g.strength, n);
-        palloc(c, &g.self_loop, n);
+        palloc(c, g.pooled, &g.node_w, n);
+        palloc(c, g.pooled, &g.strength, n);
+        palloc(c, g.pooled, &g.self_loop, n);
     }
 }
 
@@ -411,18 +421,18 @@ void finish(Ctx& c, DevGraph& g) {
             float* w2 = nullptr;
             uint32_t* erow2 = nullptr;
             if (E2) {
-                palloc(c, &nbr2, E2);
-                palloc(c, &w2, E2);
-                palloc(c, &erow2, E2);
+                palloc(c, g.pooled, &nbr2, E2);
+                palloc(c, g.pooled, &w2, E2);
+                palloc(c, g.pooled, &erow2, E2);
             }
             k_merge_write<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, keys_s.get(), w_s.get(), n,
                                                                 nptr.get(), nbr2, w2);
             SC_LAUNCH_CHECK();
             c.launches += 2;
             d2d(c, g.ptr, nptr.get(), n + 1);
-            cudaFreeAsync(g.nbr, c.stream);
-            cudaFreeAsync(g.w, c.stream);
-            cudaFreeAsync(g.erow, c.stream);
+            pfree(c, g.pooled, g.nbr);
+            pfree(c, g.pooled, g.w);
+            pfree(c, g.pooled, g.erow);
             g.nbr = nbr2;
             g.w = w2;
             g.erow = erow2;
@@ -462,6 +472,7 @@ DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint
              (unsigned long long)n_nbr, (unsigned long long)n_w);
     const cudaMemcpyKind kind = device_inputs ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
     std::unique_ptr<DevGraph> g(new DevGraph());
+    g->pooled = false;  // the user's graph keeps out of the pool a run's temporaries cycle through
     galloc(c, *g, n, n_nbr);
     auto copy_in = [&](void* dst, const void* src, size_t bytes) {
         if (kind == cudaMemcpyHostToDevice) upload(c, dst, src, bytes);
@@ -582,6 +593,7 @@ __global__ void k_split_keys(const uint64_t* __restrict__ keys, uint64_t N, uint
 DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint64_t* to,
                            const double* w, uint64_t m, const double* node_w) {
     std::unique_ptr<DevGraph> g(new DevGraph());
+    g->pooled = false;
     DBuf<unsigned long long> first(c, 1);
     const unsigned long long NOBAD = ~0ull;
     if (n > MAX_NODES) {

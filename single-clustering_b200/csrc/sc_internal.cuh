@@ -173,9 +173,14 @@ struct DevGraph {
     // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
     // once, on first need; a benign race between contexts computes it twice)
     mutable std::atomic<int> sym_state{0};
-    // Arrays come from the stream-ordered pool. A graph owned by a running call
-    // (a coarse level) returns them on that stream; a graph handed to the user
-    // (stream == nullptr) returns them once the device is idle.
+    // Arrays of graphs built from user input come from cudaMalloc (pooled ==
+    // false): a graph held across runs would otherwise take pool blocks that a
+    // run's large temporaries reuse from one run to the next, and a pool that
+    // has to grow in the middle of a run stalls it. The graphs a run builds
+    // (coarse levels, aggregates) come from the stream-ordered pool; one owned
+    // by a running call returns them on that stream, one handed to the user
+    // (stream == nullptr) once the device is idle.
+    bool pooled = true;
     cudaStream_t stream = nullptr;
     void free_all();
     ~DevGraph() { free_all(); }

@@ -22,6 +22,14 @@ def _pool_used():
     return int(v)
 
 
+def _device_free():
+    from cuda.bindings import runtime as rt
+    rt.cudaDeviceSynchronize()
+    err, free, total = rt.cudaMemGetInfo()
+    assert int(err) == 0
+    return int(free)
+
+
 def test_destroyed_graphs_return_their_memory():
     import sc_gpu
     rng = np.random.default_rng(3)
@@ -32,12 +40,19 @@ def test_destroyed_graphs_return_their_memory():
     g0 = sc_gpu.CSRNetwork.from_edge_arrays(n, src, dst, w)
     ptr, nbr, ww = g0.to_csr_parts()
     graph_bytes = ptr.nbytes + 3 * nbr.nbytes + 3 * n * 8  # ptr, nbr, w, row ids, three per-node arrays
-    sc_gpu.leiden(g0)  # the context's first run: its temporaries settle in the pool
-    before = _pool_used()
-    for _ in range(3):
+
+    def cycle():
         g = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, ww)
-        sc_gpu.leiden(g)
+        labels = sc_gpu.leiden(g).labels()
+        sc_gpu.leiden(g.aggregate(labels))  # a pooled aggregate handed to the user, then dropped
         del g
         gc.collect()
-    after = _pool_used()
+
+    cycle()  # the first cycle settles the run's temporaries in the pool
+    before, free_before = _pool_used(), _device_free()
+    for _ in range(3):
+        cycle()
+    after, free_after = _pool_used(), _device_free()
+    # three leaked graphs would hold three times graph_bytes
     assert after - before < graph_bytes, (before, after, graph_bytes)
+    assert free_before - free_after < graph_bytes, (free_before, free_after, graph_bytes)
