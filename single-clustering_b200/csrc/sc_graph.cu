@@ -948,12 +948,21 @@ constexpr int AGG_WARPS = 4;
 constexpr uint32_t AGG_EMPTY = 0xFFFFFFFFu;
 
 // Whether every stored entry (v, u, w) has its mirror (u, v) with the same bits.
+// Rows hold distinct neighbours, so mapping every upper entry (v, u > v) to its
+// mirror (u, v) is one-to-one; when each mirror exists with the same bits and
+// the upper and lower entries are equally many, every lower entry is some upper
+// entry's mirror. So only the upper entries are searched, and the two counts
+// compared afterwards (counts[0] upper, counts[1] lower).
 __global__ void k_symmetric_bits(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                                  const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
-                                 unsigned* bad) {
+                                 unsigned* bad, unsigned long long* counts) {
+    unsigned long long up = 0, down = 0;
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
          e += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = erow[e], u = nbr[e];
+        if (u < v) ++down;
+        if (u <= v) continue;
+        ++up;
         uint64_t lo = ptr[u], hi = ptr[u + 1];
         const uint64_t end = hi;
         while (lo < hi) {
@@ -962,6 +971,14 @@ __global__ void k_symmetric_bits(const uint64_t* __restrict__ ptr, const uint32_
             else hi = mid;
         }
         if (!(lo < end && nbr[lo] == v && __float_as_uint(w[lo]) == __float_as_uint(w[e]))) *bad = 1u;
+    }
+    for (int o = 16; o; o >>= 1) {
+        up += __shfl_xor_sync(0xFFFFFFFFu, up, o);
+        down += __shfl_xor_sync(0xFFFFFFFFu, down, o);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+        if (up) atomicAdd(counts, up);
+        if (down) atomicAdd(counts + 1, down);
     }
 }
 
@@ -1423,13 +1440,20 @@ bool graph_bitwise_symmetric(Ctx& c, const DevGraph& g) {
     int st = g.sym_state.load(std::memory_order_relaxed);
     if (st != 0) return st == 1;
     DBuf<unsigned> bad(c, 1);
+    DBuf<unsigned long long> counts(c, 2);
     zero(c, bad.get(), 1);
+    zero(c, counts.get(), 2);
     if (g.E) {
-        k_symmetric_bits<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, bad.get());
+        k_symmetric_bits<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, bad.get(),
+                                                                counts.get());
         SC_LAUNCH_CHECK();
         c.launches++;
     }
-    const bool sym = to_host(c, bad.get()) == 0;
+    Mailbox mb(c);
+    const unsigned* hb = mb.get(bad.get(), 1);
+    const unsigned long long* hc = mb.get(counts.get(), 2);
+    mb.wait();
+    const bool sym = *hb == 0 && hc[0] == hc[1];
     g.sym_state.store(sym ? 1 : 2, std::memory_order_relaxed);
     return sym;
 }
