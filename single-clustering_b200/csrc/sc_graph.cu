@@ -875,6 +875,47 @@ __global__ void k_seg_long_emit(const uint32_t* __restrict__ long_list, const ui
     }
 }
 
+// The (g, h) segments of keys sorted by (g, h) (values beside them) summed and
+// emitted (seg_emit's rule): prow/pcol/pw/keep of P segments, P returned.
+uint64_t segment_sums(Ctx& c, const uint64_t* keys_s, const float* w_s, uint64_t N, uint64_t G,
+                      const double* loops, bool exact, DBuf<uint32_t>& prow, DBuf<uint32_t>& pcol,
+                      DBuf<float>& pw, DBuf<uint8_t>& keep) {
+    if (N == 0) return 0;
+    DBuf<uint8_t> head(c, N);
+    k_seg_heads<<<grid_for(N, TB), TB, 0, c.stream>>>(keys_s, N, head.get());
+    DBuf<uint64_t> iota(c, N), seg(c, N), cnt(c, 1);
+    k_iota64<<<grid_for(N, TB), TB, 0, c.stream>>>(iota.get(), N);
+    SC_LAUNCH_CHECK();
+    c.launches += 2;
+    select_flagged(c, iota.get(), head.get(), seg.get(), cnt.get(), N);
+    const uint64_t P = to_host(c, cnt.get());
+    prow.alloc(c, P);
+    pcol.alloc(c, P);
+    pw.alloc(c, P);
+    keep.alloc(c, P);
+    const uint32_t long_cap = (uint32_t)(N / SEG_BLOCK + 1);
+    DBuf<uint32_t> long_list(c, long_cap), long_count(c, 1);
+    zero(c, long_count.get(), 1);
+    k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, keys_s, w_s, G, loops, prow.get(),
+                                                       pcol.get(), pw.get(), keep.get(), (int)exact,
+                                                       long_list.get(), long_count.get(), long_cap);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    if (exact) {
+        DBuf<double> part(c, long_cap);
+        zero(c, part.get(), long_cap);
+        const unsigned pgrid = (unsigned)std::min<uint64_t>(N / SEG_CHUNK + 1, (uint64_t)c.sm_count * 4);
+        k_seg_long_partial<<<pgrid, TB, 0, c.stream>>>(long_list.get(), long_count.get(), long_cap, seg.get(), P, N,
+                                                       w_s, part.get());
+        k_seg_long_emit<<<grid_for(long_cap, TB), TB, 0, c.stream>>>(long_list.get(), long_count.get(), long_cap,
+                                                                     seg.get(), part.get(), keys_s, G, loops,
+                                                                     prow.get(), pcol.get(), pw.get(), keep.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    return P;
+}
+
 // Mirror keys (h, g) of the kept off-diagonal pairs.
 __global__ void k_mirror(const uint32_t* __restrict__ prow, const uint32_t* __restrict__ pcol,
                          const float* __restrict__ pw, uint64_t P, uint64_t G, uint64_t* mkeys,
@@ -1067,13 +1108,16 @@ __device__ __forceinline__ void warp_member_entries(const uint64_t* __restrict__
 // The member entries of one group flattened across the whole block: members
 // in chunks of blockDim, a block-wide prefix of their degrees in shared memory,
 // every thread takes entries t, t + blockDim, ... and finds its member by binary
-// search. f(j, valid) is called by every thread of the block the same number
-// of times (valid false past the end), so f may use warp-collective operations.
+// search. f(j, valid, flat) is called by every thread of the block the same
+// number of times (valid false past the end), so f may use warp-collective
+// operations; flat numbers the group's entries 0, 1, ... in member order.
 template <class F>
-__device__ __forceinline__ void block_member_entries(const uint64_t* __restrict__ ptr,
-                                                     const uint32_t* __restrict__ members, uint64_t m0, uint64_t m1,
-                                                     uint64_t* s_pref, uint64_t* s_beg, uint64_t* s_wsum, F&& f) {
+__device__ __forceinline__ void block_member_entries_at(const uint64_t* __restrict__ ptr,
+                                                        const uint32_t* __restrict__ members, uint64_t m0,
+                                                        uint64_t m1, uint64_t* s_pref, uint64_t* s_beg,
+                                                        uint64_t* s_wsum, F&& f) {
     const unsigned tid = threadIdx.x, lane = tid & 31u, wid = tid >> 5, nw = blockDim.x >> 5;
+    uint64_t flat0 = 0;  // entries of the earlier member chunks
     for (uint64_t mb = m0; mb < m1; mb += blockDim.x) {
         const uint64_t mi = mb + tid;
         uint64_t b = 0, d = 0;
@@ -1110,11 +1154,21 @@ __device__ __forceinline__ void block_member_entries(const uint64_t* __restrict_
                 }
                 j = s_beg[lo] + (t - s_pref[lo]);
             }
-            f(j, valid);
+            f(j, valid, flat0 + t);
         }
+        flat0 += total;
         __syncthreads();
         (void)nw;
     }
+}
+
+// block_member_entries_at without the flattened index: f(j, valid).
+template <class F>
+__device__ __forceinline__ void block_member_entries(const uint64_t* __restrict__ ptr,
+                                                     const uint32_t* __restrict__ members, uint64_t m0, uint64_t m1,
+                                                     uint64_t* s_pref, uint64_t* s_beg, uint64_t* s_wsum, F&& f) {
+    block_member_entries_at(ptr, members, m0, m1, s_pref, s_beg, s_wsum,
+                            [&](uint64_t j, bool valid, uint64_t) { f(j, valid); });
 }
 
 // Warp-combined insert: lanes with the same key add their values through the
@@ -1210,65 +1264,50 @@ __global__ void __launch_bounds__(32 * AGG_WARPS)
     }
 }
 
-// One block per large row; its table is `2 cap` slots of the global scratch at
-// hoff[i]. Kept entries are written unsorted; a segmented sort follows.
+// Rows too large for a shared table (the "big" rows): every member entry as a
+// (g, h) key and its weight, row i's entries at loff[i] .., one block per row.
 __global__ void __launch_bounds__(256)
-    k_contract_block(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ hoff,
-                     const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
-                     const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
-                     const float* __restrict__ w, const uint32_t* __restrict__ grp, const uint64_t* __restrict__ cap,
-                     const uint64_t* __restrict__ capstart, const double* __restrict__ loops, uint32_t* hkeys,
-                     double* hvals, uint32_t* tnbr, float* tw, uint32_t* cnt, uint32_t* status) {
-    __shared__ unsigned long long s_n;
+    k_big_row_keys(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ loff,
+                   const uint64_t* __restrict__ gstart, const uint32_t* __restrict__ members,
+                   const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr, const float* __restrict__ w,
+                   const uint32_t* __restrict__ grp, uint64_t G, uint64_t* keys, float* vals) {
     __shared__ uint64_t s_pref[257], s_beg[256], s_wsum[8];
     for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
         const uint32_t g = rows[i];
-        const uint64_t size = 2 * cap[g];
-        uint32_t* keys = hkeys + hoff[i];
-        double* vals = hvals + hoff[i];
-        for (uint64_t s = threadIdx.x; s < size; s += blockDim.x) {
-            keys[s] = AGG_EMPTY;
-            vals[s] = 0.0;
+        const uint64_t o = loff[i];
+        block_member_entries_at(ptr, members, gstart[g], gstart[g + 1], s_pref, s_beg, s_wsum,
+                                [&](uint64_t j, bool valid, uint64_t t) {
+                                    if (!valid) return;
+                                    keys[o + t] = (uint64_t)g * G + grp[nbr[j]];
+                                    vals[o + t] = w[j];
+                                });
+    }
+}
+
+// The kept (g, h, w) of the big rows, sorted by (g, h) with row starts kstart,
+// into each row's slot range: one block per big row.
+__global__ void k_place_big_rows(const uint32_t* __restrict__ rows, uint64_t nrows,
+                                 const uint64_t* __restrict__ kstart, const uint32_t* __restrict__ kcol,
+                                 const float* __restrict__ kw, const uint64_t* __restrict__ capstart, uint32_t* tnbr,
+                                 float* tw, uint32_t* cnt) {
+    for (uint64_t i = blockIdx.x; i < nrows; i += gridDim.x) {
+        const uint32_t g = rows[i];
+        const uint64_t b = kstart[g], e = kstart[g + 1], o = capstart[g];
+        for (uint64_t t = b + threadIdx.x; t < e; t += blockDim.x) {
+            tnbr[o + (t - b)] = kcol[t];
+            tw[o + (t - b)] = kw[t];
         }
-        if (threadIdx.x == 0) s_n = 0;
-        __syncthreads();
-        block_member_entries(ptr, members, gstart[g], gstart[g + 1], s_pref, s_beg, s_wsum,
-                             [&](uint64_t j, bool valid) {
-                                 uint32_t h = 0;
-                                 double x = 0.0;
-                                 if (valid) {
-                                     h = grp[nbr[j]];
-                                     x = (double)w[j];
-                                 }
-                                 // lanes with the same key add through the lowest one
-                                 const unsigned lane = threadIdx.x & 31u;
-                                 const unsigned long long key =
-                                     valid ? (unsigned long long)h : (0xFFFFFFFF00000000ull | lane);
-                                 const unsigned mm = __match_any_sync(0xFFFFFFFFu, key);
-                                 const double acc = peer_sum(mm, x);  // exact regime: any grouping
-                                 if (valid && (int)lane == __ffs(mm) - 1)
-                                     agg_insert(keys, vals, size, h, acc, status);
-                             });
-        const uint64_t o = capstart[g];
-        for (uint64_t s = threadIdx.x; s < size; s += blockDim.x) {
-            const uint32_t h = keys[s];
-            if (h == AGG_EMPTY) continue;
-            bool keep;
-            const float val = agg_value(g, h, vals[s], loops, &keep);
-            if (keep) {
-                const unsigned long long pos = atomicAdd(&s_n, 1ull);
-                tnbr[o + pos] = h;
-                tw[o + pos] = val;
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) cnt[g] = (uint32_t)s_n;
-        __syncthreads();
+        if (threadIdx.x == 0) cnt[g] = (uint32_t)(e - b);
     }
 }
 
 constexpr uint64_t AGG_SMEM_SLOTS = 4096;  // shared table of the block kernel (48 KB)
 constexpr uint64_t AGG_SMALL_GRAPH = 1u << 16;  // entries up to which the hash path is always taken
+// The share of the entries in rows past the warp kernel, as 1/AGG_SORT_SHARE,
+// above which the whole graph takes the sort path (0: never). Measured on the
+// kNN graphs of a run: never taking it (big rows sorted on their own, below)
+// made aggregation twice as slow; a tenth is the best of the rules tried.
+constexpr uint64_t AGG_SORT_SHARE = 10;
 constexpr uint64_t AGG_SMEM_KEEP = AGG_SMEM_SLOTS / 2;
 
 // A row has at most min(cap, G) distinct neighbour groups; its table needs twice that.
@@ -1280,16 +1319,15 @@ __device__ __forceinline__ uint64_t agg_slots(uint64_t cap, uint64_t G) {
 }
 
 // mid: rows past the warp kernel whose table fits the block kernel's shared
-// memory; big: the rest (table in global memory, sized by the row's entries).
+// memory; big: the rest (their entries are sorted, k_big_row_keys).
 __global__ void k_flag_large(const uint64_t* __restrict__ cap, uint64_t G, uint8_t* mid, uint8_t* big,
-                             uint64_t* hcap, uint64_t* lcap) {
+                             uint64_t* lcap) {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G;
          g += (uint64_t)gridDim.x * blockDim.x) {
         const bool large = cap[g] > AGG_WARP_CAP;
         const bool m = large && agg_slots(cap[g], G) <= AGG_SMEM_SLOTS;
         mid[g] = m;
         big[g] = large && !m;
-        hcap[g] = large && !m ? 2 * cap[g] : 0;
         lcap[g] = large ? cap[g] : 0;
     }
 }
@@ -1388,29 +1426,6 @@ __global__ void k_gather_u64(const uint32_t* __restrict__ idx, uint64_t n, const
         dst[i] = src[idx[i]];
 }
 
-__global__ void k_segments_of(const uint32_t* __restrict__ rows, uint64_t nrows, const uint64_t* __restrict__ capstart,
-                              const uint32_t* __restrict__ cnt, uint64_t* sb, uint64_t* se) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nrows;
-         i += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t g = rows[i];
-        sb[i] = capstart[g];
-        se[i] = capstart[g] + cnt[g];
-    }
-}
-
-__global__ void k_copy_segments(const uint64_t* __restrict__ sb, const uint64_t* __restrict__ se, uint64_t nseg,
-                                const uint32_t* __restrict__ kin, const float* __restrict__ vin, uint32_t* kout,
-                                float* vout) {
-    const unsigned lane = threadIdx.x & 31u;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    for (uint64_t i = warp; i < nseg; i += nwarps)
-        for (uint64_t j = sb[i] + lane; j < se[i]; j += 32) {
-            kout[j] = kin[j];
-            vout[j] = vin[j];
-        }
-}
-
 // Final rows: ptr from the kept counts, entries copied from the row slots.
 __global__ void k_pack_rows(const uint64_t* __restrict__ optr, const uint64_t* __restrict__ capstart, uint64_t G,
                             const uint32_t* __restrict__ tnbr, const float* __restrict__ tw, uint32_t* nbr,
@@ -1476,12 +1491,11 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
     zero(c, cnt.get(), G + 1);
     // rows past the warp kernel: shared-table rows (mid) and global-table rows (large)
     DBuf<uint8_t> fmid(c, G), flag(c, G);
-    DBuf<uint64_t> hcap(c, G), lcap(c, G), nl(c, 3);
+    DBuf<uint64_t> lcap(c, G), nl(c, 3);
     DBuf<uint32_t> iota(c, G), rows(c, G), mrows(c, G);
     uint64_t nlarge = 0, nmid = 0;
     if (G) {
-        k_flag_large<<<grid_for(G, TB), TB, 0, c.stream>>>(cap.get(), G, fmid.get(), flag.get(), hcap.get(),
-                                                           lcap.get());
+        k_flag_large<<<grid_for(G, TB), TB, 0, c.stream>>>(cap.get(), G, fmid.get(), flag.get(), lcap.get());
         k_iota<<<grid_for(G, TB), TB, 0, c.stream>>>(iota.get(), G);
         SC_LAUNCH_CHECK();
         c.launches += 2;
@@ -1501,7 +1515,7 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         // more than a tenth of the entries the sort path is faster (measured on
         // kNN graphs at every level of a run), except on small graphs, where the
         // sort path's extra launches and read-backs cost more than any block.
-        if (counts[2] * 10 > g.E && g.E > AGG_SMALL_GRAPH) return nullptr;
+        if (AGG_SORT_SHARE && counts[2] * AGG_SORT_SHARE > g.E && g.E > AGG_SMALL_GRAPH) return nullptr;
     }
     if (nmid) {
         const size_t smem = AGG_SMEM_SLOTS * (sizeof(unsigned long long) + sizeof(uint32_t)) +
@@ -1524,36 +1538,44 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
         c.launches++;
     }
     if (nlarge) {
-        DBuf<uint64_t> lh(c, nlarge + 1), hoff(c, nlarge + 1);
-        k_gather_u64<<<grid_for(nlarge, TB), TB, 0, c.stream>>>(rows.get(), nlarge, hcap.get(), lh.get());
-        zero(c, lh.get() + nlarge, 1);
-        exclusive_sum(c, lh.get(), hoff.get(), nlarge + 1);
-        const uint64_t hsize = to_host(c, hoff.get() + nlarge);
-        DBuf<uint32_t> hkeys(c, hsize);
-        DBuf<double> hvals(c, hsize);
+        // big rows: their member entries as (g, h) keys, sorted, summed per
+        // segment and placed into their rows (sorted by neighbour already)
+        DBuf<uint64_t> lc(c, nlarge + 1), loff(c, nlarge + 1);
+        k_gather_u64<<<grid_for(nlarge, TB), TB, 0, c.stream>>>(rows.get(), nlarge, cap.get(), lc.get());
+        zero(c, lc.get() + nlarge, 1);
+        exclusive_sum(c, lc.get(), loff.get(), nlarge + 1);
+        c.launches++;
+        const uint64_t L = to_host(c, loff.get() + nlarge);
+        DBuf<uint64_t> keys(c, L), keys_s(c, L);
+        DBuf<float> vals(c, L), vals_s(c, L);
         const unsigned grid = (unsigned)std::min<uint64_t>(nlarge, (uint64_t)c.sm_count * 4);
-        k_contract_block<<<grid, 256, 0, c.stream>>>(rows.get(), nlarge, hoff.get(), gstart, members, g.ptr, g.nbr,
-                                                     g.w, d_grp, cap.get(), capstart.get(), loops, hkeys.get(),
-                                                     hvals.get(), tnbr.get(), tw.get(), cnt.get(), c.d_status);
+        k_big_row_keys<<<grid, 256, 0, c.stream>>>(rows.get(), nlarge, loff.get(), gstart, members, g.ptr, g.nbr,
+                                                   g.w, d_grp, G, keys.get(), vals.get());
         SC_LAUNCH_CHECK();
-        c.launches += 2;
-        // sort the large rows' kept entries by neighbour
-        DBuf<uint64_t> sb(c, nlarge), se(c, nlarge);
-        k_segments_of<<<grid_for(nlarge, TB), TB, 0, c.stream>>>(rows.get(), nlarge, capstart.get(), cnt.get(),
-                                                                 sb.get(), se.get());
-        SC_LAUNCH_CHECK();
-        DBuf<uint32_t> knbr(c, g.E);
-        DBuf<float> kw(c, g.E);
-        size_t bytes = 0;
-        SC_CUDA(cub::DeviceSegmentedSort::SortPairs(nullptr, bytes, tnbr.get(), knbr.get(), tw.get(), kw.get(),
-                                                    (int64_t)g.E, (int64_t)nlarge, sb.get(), se.get(), c.stream));
-        DBuf<unsigned char> tmp(c, bytes);
-        SC_CUDA(cub::DeviceSegmentedSort::SortPairs(tmp.get(), bytes, tnbr.get(), knbr.get(), tw.get(), kw.get(),
-                                                    (int64_t)g.E, (int64_t)nlarge, sb.get(), se.get(), c.stream));
-        k_copy_segments<<<grid_for(nlarge * 32, TB), TB, 0, c.stream>>>(sb.get(), se.get(), nlarge, knbr.get(),
-                                                                        kw.get(), tnbr.get(), tw.get());
-        SC_LAUNCH_CHECK();
-        c.launches += 4;
+        c.launches++;
+        sort_pairs(c, keys.get(), keys_s.get(), vals.get(), vals_s.get(), L, bits_for((uint64_t)G * G - 1));
+        keys.release();
+        vals.release();
+        DBuf<uint32_t> prow, pcol;
+        DBuf<float> pw;
+        DBuf<uint8_t> keep;
+        const uint64_t P = segment_sums(c, keys_s.get(), vals_s.get(), L, G, loops, true, prow, pcol, pw, keep);
+        keys_s.release();
+        vals_s.release();
+        if (P) {
+            DBuf<uint32_t> krow(c, P), kcol(c, P);
+            DBuf<float> kw(c, P);
+            DBuf<uint64_t> kc(c, 1), kstart(c, (uint64_t)G + 1);
+            select_flagged(c, prow.get(), keep.get(), krow.get(), kc.get(), P);
+            select_flagged(c, pcol.get(), keep.get(), kcol.get(), kc.get(), P);
+            select_flagged(c, pw.get(), keep.get(), kw.get(), kc.get(), P);
+            const uint64_t K = to_host(c, kc.get());
+            k_starts_from_sorted<<<grid_for(K + 1, TB), TB, 0, c.stream>>>(krow.get(), K, G, kstart.get());
+            k_place_big_rows<<<grid, 256, 0, c.stream>>>(rows.get(), nlarge, kstart.get(), kcol.get(), kw.get(),
+                                                         capstart.get(), tnbr.get(), tw.get(), cnt.get());
+            SC_LAUNCH_CHECK();
+            c.launches += 2;
+        }
     }
     // assemble (the status word of the contraction kernels is read with the size)
     DBuf<uint64_t> cnt64(c, G + 1), optr(c, G + 1);
@@ -1660,45 +1682,11 @@ DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint
         uw.release();
     }
     // segments = distinct (g, h)
-    uint64_t P = 0;
     DBuf<uint32_t> prow, pcol;
     DBuf<float> pw;
     DBuf<uint8_t> keep;
-    if (N) {
-        DBuf<uint8_t> head(c, N);
-        k_seg_heads<<<grid_for(N, TB), TB, 0, c.stream>>>(ukeys_s.get(), N, head.get());
-        c.launches++;
-        DBuf<uint64_t> iota(c, N), seg(c, N), cnt(c, 1);
-        k_iota64<<<grid_for(N, TB), TB, 0, c.stream>>>(iota.get(), N);
-        c.launches++;
-        select_flagged(c, iota.get(), head.get(), seg.get(), cnt.get(), N);
-        P = to_host(c, cnt.get());
-        prow.alloc(c, P);
-        pcol.alloc(c, P);
-        pw.alloc(c, P);
-        keep.alloc(c, P);
-        const uint32_t long_cap = (uint32_t)(N / SEG_BLOCK + 1);
-        DBuf<uint32_t> long_list(c, long_cap), long_count(c, 1);
-        zero(c, long_count.get(), 1);
-        k_seg_values<<<grid_for(P, TB), TB, 0, c.stream>>>(seg.get(), P, N, ukeys_s.get(),
-                                                           uw_s.get(), G, loops.get(), prow.get(),
-                                                           pcol.get(), pw.get(), keep.get(), (int)g.exact_w,
-                                                           long_list.get(), long_count.get(), long_cap);
-        c.launches++;
-        if (g.exact_w) {
-            DBuf<double> part(c, long_cap);
-            zero(c, part.get(), long_cap);
-            const unsigned pgrid = (unsigned)std::min<uint64_t>(N / SEG_CHUNK + 1, (uint64_t)c.sm_count * 4);
-            k_seg_long_partial<<<pgrid, TB, 0, c.stream>>>(long_list.get(), long_count.get(), long_cap, seg.get(), P, N,
-                                                           uw_s.get(), part.get());
-            k_seg_long_emit<<<grid_for(long_cap, TB), TB, 0, c.stream>>>(long_list.get(), long_count.get(),
-                                                                         long_cap, seg.get(), part.get(), ukeys_s.get(), G,
-                                                                         loops.get(), prow.get(), pcol.get(),
-                                                                         pw.get(), keep.get());
-            c.launches += 2;
-        }
-        SC_LAUNCH_CHECK();
-    }
+    const uint64_t P = segment_sums(c, ukeys_s.get(), uw_s.get(), N, G, loops.get(), g.exact_w, prow, pcol, pw,
+                                    keep);
     ukeys_s.release();
     uw_s.release();
     // kept pairs, still in (g, h) order: the upper triangle incl. diagonal
