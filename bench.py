@@ -124,7 +124,7 @@ SWEEP_RESOLUTIONS = 32
 SWEEP_SEEDS = (1, 2, 3, 4)
 
 
-def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=12, split=3):
+def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2):
     """128-instance resolution x seed sweep: sequential plain runs vs
     warm-started chains (each seed's chain cut in `split` pieces whose heads
     start from the seed's finest partition) on concurrent streams."""

@@ -990,6 +990,7 @@ struct Workspace {
     DBuf<long long> gvals;
     uint64_t gcap = 0;
     int nblk_large = 0;
+    uint64_t cap = 0;  // nodes the per-node arrays hold (the largest level seen)
 };
 
 // Phase times of a run: events recorded around each phase on the context's
@@ -1042,26 +1043,34 @@ class PhaseClock {
     std::vector<Span> spans_;
 };
 
+// One workspace serves every level of a run: the per-node arrays are sized by
+// the first (largest) level and only their prefix is used below it, which
+// spares each level some twenty allocations (the bulk of a small level's host
+// time). The hub scratch grows when a level needs more.
 void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     const uint64_t n = g.n;
-    ws.tgt.alloc(c, n);
-    ws.hint.alloc(c, n);
-    ws.from.alloc(c, n);
-    ws.epoch.alloc(c, n);
-    ws.moved.alloc(c, n);
-    ws.list.alloc(c, n);
-    ws.lbeg.alloc(c, n);
-    ws.ldeg.alloc(c, n);
-    ws.dgain.alloc(c, n);
-    ws.alist.alloc(c, n);
-    ws.nlist.alloc(c, n);
-    ws.acount.alloc(c, 1);
-    ws.ncount.alloc(c, 1);
-    ws.stamp.alloc(c, n);
-    ws.counts.alloc(c, 64);
-    ws.cursor.alloc(c, 64);
-    ws.counters.alloc(c, 4);
-    ws.gain_acc.alloc(c, 1);
+    if (ws.cap < n || ws.cap == 0) {
+        const uint64_t m = std::max<uint64_t>(n, 1);
+        ws.tgt.alloc(c, m);
+        ws.hint.alloc(c, m);
+        ws.from.alloc(c, m);
+        ws.epoch.alloc(c, m);
+        ws.moved.alloc(c, m);
+        ws.list.alloc(c, m);
+        ws.lbeg.alloc(c, m);
+        ws.ldeg.alloc(c, m);
+        ws.dgain.alloc(c, m);
+        ws.alist.alloc(c, m);
+        ws.nlist.alloc(c, m);
+        ws.acount.alloc(c, 1);
+        ws.ncount.alloc(c, 1);
+        ws.stamp.alloc(c, m);
+        ws.counts.alloc(c, 64);
+        ws.cursor.alloc(c, 64);
+        ws.counters.alloc(c, 4);
+        ws.gain_acc.alloc(c, 1);
+        ws.cap = m;
+    }
     zero(c, ws.epoch.get(), n);
     zero(c, ws.moved.get(), n);
     zero(c, ws.hint.get(), n);
@@ -1076,8 +1085,10 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
         while (nblk > 1 && (uint64_t)nblk * cap * 12 > budget) nblk >>= 1;
         ws.nblk_large = nblk;
         ws.gcap = cap;
-        ws.gkeys.alloc(c, (uint64_t)nblk * cap);
-        ws.gvals.alloc(c, (uint64_t)nblk * cap);
+        if (ws.gkeys.n < (uint64_t)nblk * cap) {
+            ws.gkeys.alloc(c, (uint64_t)nblk * cap);
+            ws.gvals.alloc(c, (uint64_t)nblk * cap);
+        }
     }
 }
 
@@ -1461,7 +1472,7 @@ struct PassOut {
 
 // run_once (mod.rs:214-289) from compact initial ids `init` (< C0).
 void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, const sc_leiden_config& cfg,
-              uint64_t pass_seed, PassOut& out, sc_run_stats& st, PhaseClock& clock) {
+              uint64_t pass_seed, PassOut& out, sc_run_stats& st, PhaseClock& clock, Workspace& ws) {
     const uint64_t n0 = g0.n;
     const double gamma = cfg.resolution;
     std::unique_ptr<DevGraph> owned;
@@ -1478,7 +1489,6 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
         const sc_run_stats before = st;
         const uint64_t lvl_seed = hash3(pass_seed, level, 0x1eafull);
         Scales sc = scales_for(*gl);
-        Workspace ws;
         prepare_workspace(c, ws, *gl);
         // ids of memb are < C; fresh ids live in [C, C + nl)
         {
@@ -1604,9 +1614,10 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
     }
     uint64_t clusters = C;
     uint64_t stagnant = 0;
+    Workspace ws;  // shared by every level of every pass
     for (uint64_t it = 0; it < cfg.n_iterations; ++it) {
         PassOut po;
-        run_pass(c, g, labels.get(), C, cfg, hash3(seed, it, 0x9a55ull), po, c.stats, clock);
+        run_pass(c, g, labels.get(), C, cfg, hash3(seed, it, 0x9a55ull), po, c.stats, clock, ws);
         labels = std::move(po.labels);
         C = po.n_clusters;
         clusters = C;
