@@ -210,8 +210,9 @@ def test_aggregate_of_balanced_asymmetric_graph():
 def test_aggregate_large_rows_use_the_block_contraction():
     """Each row-size path of the exact-regime contraction: small rows (a warp
     per row), one large row whose table fits shared memory, one large row with
-    more distinct neighbour groups than that (table in global memory), and
-    large rows holding most entries (the sort path)."""
+    more distinct neighbour groups than that (its entries sorted as (g, h) keys
+    and summed per segment), and large rows holding most entries (the sort path
+    of the whole graph, with segments long enough for the chunked sums)."""
     src, dst, w, truth = synth.planted_partition(6000, 6, 12, 3, seed=4)
     og = O.Graph.from_edges(6000, src=src, dst=dst, w=w)
     gg = sc_gpu.CSRNetwork.from_edge_arrays(6000, src, dst, w)
