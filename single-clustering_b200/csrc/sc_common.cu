@@ -1,5 +1,6 @@
 // sc_common.cu — errors, formatting, the ordered f64 chain and graph storage.
 #include <cstdarg>
+#include <mutex>
 
 #include "sc_prims.cuh"
 
@@ -94,6 +95,25 @@ void fail_info(sc_error_info i) {
     throw f;
 }
 
+cudaMemPool_t user_graph_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) fail(SC_E_INVALID_ARGUMENT, "device %d out of range", device);
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        SC_CUDA(cudaMemPoolCreate(&pool, &props));
+        uint64_t keep = UINT64_MAX;  // freed graph memory stays for the next graph
+        SC_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
 void check_device_status(Ctx& c) {
     Mailbox mb(c);
     const uint32_t* h = mb.get(c.d_status, 1);
@@ -140,21 +160,15 @@ void DevGraph::free_all() {
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != device) cudaSetDevice(device);
-        // cudaMalloc'd arrays: cudaFree (it waits for the device). Pool memory
-        // goes back to the pool only through cudaFreeAsync (a plain cudaFree
-        // leaves it counted as in use). A pooled graph handed to the user may
+        // Pool memory goes back to its pool only through cudaFreeAsync (a plain
+        // cudaFree leaves it counted as in use). A graph handed to the user may
         // still be read by work queued on any context's stream: wait for the
         // device, free on the legacy stream and wait for that, so the call stays
         // synchronous for the caller.
-        if (!pooled) {
-            for (void* p : ps)
-                if (p) cudaFree(p);
-        } else {
-            if (!stream) cudaDeviceSynchronize();
-            for (void* p : ps)
-                if (p) cudaFreeAsync(p, stream ? stream : (cudaStream_t)0);
-            if (!stream) cudaStreamSynchronize((cudaStream_t)0);
-        }
+        if (!stream) cudaDeviceSynchronize();
+        for (void* p : ps)
+            if (p) cudaFreeAsync(p, stream ? stream : (cudaStream_t)0);
+        if (!stream) cudaStreamSynchronize((cudaStream_t)0);
         if (prev != device) cudaSetDevice(prev);
     }
     ptr = nullptr;

@@ -14,25 +14,25 @@ namespace {
 
 constexpr unsigned TB = 256;
 
-// A graph array: from the stream-ordered pool for the graphs of a running call,
-// from cudaMalloc for graphs handed to the user (see DevGraph::pooled).
+// A graph array: from the device's default stream-ordered pool for the graphs
+// of a running call, from the device's graph pool for graphs handed to the user
+// (see DevGraph::pooled).
 template <class T>
 void palloc(Ctx& c, bool pooled, T** p, uint64_t count) {
     cudaError_t e = pooled ? cudaMallocAsync((void**)p, count * sizeof(T), c.stream)
-                           : cudaMalloc((void**)p, count * sizeof(T));
+                           : cudaMallocFromPoolAsync((void**)p, count * sizeof(T), user_graph_pool(c.device),
+                                                     c.stream);
     if (e == cudaErrorMemoryAllocation) {
         cudaGetLastError();
         fail(SC_E_OUT_OF_MEMORY, "device allocation of %llu bytes failed",
              (unsigned long long)(count * sizeof(T)));
     }
-    if (e != cudaSuccess) throw_cuda(e, pooled ? "cudaMallocAsync" : "cudaMalloc", __FILE__, __LINE__);
+    if (e != cudaSuccess) throw_cuda(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
 }
 
-// Frees an array palloc gave out (a plain cudaFree waits for the device first).
-void pfree(Ctx& c, bool pooled, void* p) {
-    if (!p) return;
-    if (pooled) cudaFreeAsync(p, c.stream);
-    else cudaFree(p);
+// Frees an array palloc gave out, in the order of the context's stream.
+void pfree(Ctx& c, bool /*pooled*/, void* p) {
+    if (p) cudaFreeAsync(p, c.stream);
 }
 
 void galloc(Ctx& c, DevGraph& g, uint64_t n, uint64_t E) {

@@ -97,6 +97,8 @@ constexpr size_t STAGE_MIN_BYTES = size_t(16) << 20;  // smaller uploads use one
 // when it returns.
 void upload(Ctx& c, void* dst, const void* src, size_t bytes);
 void release_staging(Ctx& c);
+// The device's pool of user-graph arrays (created on first use, kept until exit).
+cudaMemPool_t user_graph_pool(int device);
 // u32 device labels -> u64 host labels (widened on the device, one copy)
 void download_labels(Ctx& c, const uint32_t* d_labels, uint64_t n, uint64_t* host_out);
 
@@ -173,13 +175,14 @@ struct DevGraph {
     // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
     // once, on first need; a benign race between contexts computes it twice)
     mutable std::atomic<int> sym_state{0};
-    // Arrays of graphs built from user input come from cudaMalloc (pooled ==
-    // false): a graph held across runs would otherwise take pool blocks that a
-    // run's large temporaries reuse from one run to the next, and a pool that
-    // has to grow in the middle of a run stalls it. The graphs a run builds
-    // (coarse levels, aggregates) come from the stream-ordered pool; one owned
-    // by a running call returns them on that stream, one handed to the user
-    // (stream == nullptr) once the device is idle.
+    // Arrays of graphs built from user input come from a pool of their own,
+    // one per device (pooled == false): in the default pool a graph held across
+    // runs would take blocks that a run's large temporaries reuse from one run
+    // to the next, and a pool that has to grow in the middle of a run stalls
+    // it; cudaMalloc / cudaFree instead cost up to 0.1 s per graph. The graphs a
+    // run builds (coarse levels, aggregates) come from the default pool. A graph
+    // owned by a running call returns its arrays on that call's stream, one
+    // handed to the user (stream == nullptr) once the device is idle.
     bool pooled = true;
     cudaStream_t stream = nullptr;
     void free_all();

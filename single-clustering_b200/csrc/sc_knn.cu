@@ -935,7 +935,7 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, co
                   uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out) {
     knn_check(n, d, k, opts);
     DBuf<float> dX(c, n * d);
-    h2d(c, dX.get(), X, n * d);
+    upload(c, dX.get(), X, n * d * sizeof(float));
     DBuf<uint32_t> idx(c, n * (k + 1));
     DBuf<float> d2(c, n * (k + 1));
     knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
@@ -954,7 +954,7 @@ void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint
                                 (unsigned long long)q0, (unsigned long long)q1, (unsigned long long)n);
     const uint64_t nq = q1 - q0;
     DBuf<float> dX(c, n * d);
-    h2d(c, dX.get(), X, n * d);
+    upload(c, dX.get(), X, n * d * sizeof(float));
     DBuf<uint32_t> idx(c, nq * (k + 1));
     DBuf<float> d2(c, nq * (k + 1));
     knn_search_device(c, dX.get(), n, d, k, q0, nq, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
