@@ -200,6 +200,8 @@ sc_status sc_graph_from_csr_matrix(sc_ctx* ctx,
                                    uint64_t nnz, const double* node_weights,
                                    sc_graph** out);
 
+/* Drop(CSRNetwork): waits for the device, then returns the graph's arrays to
+ * the library's graph pool (kept for the next graph until the process exits). */
 void sc_graph_destroy(sc_graph* g);
 
 /* node_count, stored entries, edge_count, total_weight, has_self_loops
