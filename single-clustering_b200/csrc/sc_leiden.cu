@@ -30,7 +30,7 @@ constexpr uint32_t WARP_DEGREE = 256;  // largest degree of the warp-per-node bu
 constexpr int WCAP = 2 * WARP_DEGREE;  // per-warp shared hash entries
 constexpr int WARPS_PER_BLOCK = 4;
 constexpr int HCAP_SMEM = 2 * HUB_DEGREE;  // shared hash entries per block (u32 key + i64 val): 24 KB
-constexpr int LM_BATCHES = 4;
+constexpr int LM_BATCHES = 2;
 constexpr int RF_BATCHES = 8;
 constexpr int MAX_SLOTS = 64;  // (batch, bucket) counters, cursors and offsets are sized for this
 static_assert(LM_BATCHES * NBUCKET <= MAX_SLOTS && RF_BATCHES * NBUCKET <= MAX_SLOTS,
