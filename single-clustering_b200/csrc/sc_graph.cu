@@ -1621,7 +1621,6 @@ void finish_aggregate(Ctx& c, DevGraph& out) {
         throw;
     }
     out.sym_state.store(1, std::memory_order_relaxed);
-    sync(c);
 }
 
 DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t G) {

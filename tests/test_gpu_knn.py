@@ -68,6 +68,29 @@ def test_recall_at_k_on_larger_mixture():
     assert rec >= 0.999, rec
 
 
+def test_staged_point_upload_sampled_rows_exact():
+    """Points past the 16 MB staging threshold (150k x 30 f32 = 18 MB) go up in
+    pinned chunks from several host threads; sampled rows' neighbour lists must
+    equal an exact FP64 search of those rows against every point."""
+    n, d, k = 150_000, 30, 10
+    X, _ = synth.gaussian_mixture(n, d, 20, seed=5, sigma=(0.7, 1.5))
+    assert X.astype(np.float32).nbytes > (16 << 20)
+    r = sc_gpu.knn_gaussian(X, k)
+    rows = np.random.Generator(np.random.PCG64(1)).choice(n, 64, replace=False)
+    X64 = X.astype(np.float32).astype(np.float64)
+    sq = (X64 * X64).sum(axis=1)
+    for q in rows:
+        d2 = sq + sq[q] - 2.0 * (X64 @ X64[q])
+        d2[q] = -1.0  # self first
+        want = np.argsort(d2, kind="stable")[:k + 1]
+        got = r.index[q]
+        # equal sets, allowing exchanges among distances tied to 1e-6 relative
+        kth = np.sort(np.maximum(d2, 0.0))[k]
+        if set(got.tolist()) != set(want.tolist()):
+            for j in set(got.tolist()) ^ set(want.tolist()):
+                assert abs(max(d2[j], 0.0) - kth) <= 1e-6 * max(kth, 1e-12), (q, j)
+
+
 def test_squared_kiddo_semantics():
     X, _ = synth.gaussian_mixture(500, 20, 4, seed=3)
     a = sc_gpu.knn_gaussian(X, 8)

@@ -1,8 +1,11 @@
-"""Device memory of destroyed graphs goes back to the device's pool.
+"""Graph memory: large uploads and the memory of destroyed graphs.
 
-Graph arrays come from the stream-ordered pool; a graph dropped by its user
-must return them there, or every graph a long-lived process builds stays
-allocated (read through the pool's own used-memory counter).
+* Uploads of 16 MB and more go through pinned staging lanes (several host
+  threads, double-buffered): the arrays must arrive bit for bit.
+* Graph arrays come from stream-ordered pools; a graph dropped by its user
+  must return them, or every graph a long-lived process builds stays
+  allocated (read through the default pool's used-memory counter and the
+  device's free memory).
 """
 import gc
 
@@ -56,3 +59,22 @@ def test_destroyed_graphs_return_their_memory():
     # three leaked graphs would hold three times graph_bytes
     assert after - before < graph_bytes, (before, after, graph_bytes)
     assert free_before - free_after < graph_bytes, (free_before, free_after, graph_bytes)
+
+
+def test_staged_upload_round_trips_bit_for_bit():
+    import sc_gpu
+    rng = np.random.default_rng(11)
+    n, k = 600_000, 8  # 9.6M entries: neighbour ids and weights are 38 MB each, past the staging threshold
+    src = np.repeat(np.arange(n, dtype=np.uint64), k)
+    dst = rng.integers(0, n, n * k).astype(np.uint64)
+    w = rng.uniform(0.5, 1.5, n * k).astype(np.float32)
+    g0 = sc_gpu.CSRNetwork.from_edge_arrays(n, src, dst, w)
+    ptr, nbr, ww = g0.to_csr_parts()
+    assert nbr.nbytes > (16 << 20)
+    for _ in range(2):  # the second upload reuses the staging buffers
+        g = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, ww)
+        p2, n2, w2 = g.to_csr_parts()
+        assert np.array_equal(p2, ptr) and np.array_equal(n2, nbr)
+        assert np.array_equal(w2.view(np.uint32), ww.view(np.uint32))
+        assert g.total_weight() == g0.total_weight() and g.edge_count() == g0.edge_count()
+        assert np.array_equal(g.strengths().view(np.uint64), g0.strengths().view(np.uint64))
