@@ -1246,8 +1246,6 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     uint64_t moves_before = 0;
     const uint64_t budget = n * 100;  // MAX_MOVES_PER_NODE, local_move.rs:32
     static const int trace = std::getenv("SC_TRACE") ? std::atoi(std::getenv("SC_TRACE")) : 0;
-    // experimental: stop once a sweep moves fewer than tail * n nodes (0 = run to a local optimum)
-    const double tail = std::getenv("SC_LM_TAIL") ? std::atof(std::getenv("SC_LM_TAIL")) : 0.0;
     unsigned long long last_ctr[4] = {0, 0, 0, 0};
     long long last_gacc = 0;
     bool read_fresh = false;  // last_ctr / last_gacc hold the counters' current values
@@ -1280,7 +1278,6 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             std::fprintf(stderr, "[sc]   sweep %u moves=%llu next_active=%u\n", sweep - 1,
                          (unsigned long long)(ctr[0] - moves_before), offs[B * NBUCKET]);
         if (sweep > 0 && ctr[0] == moves_before) break;  // last sweep moved nothing
-        if (sweep > 1 && tail > 0.0 && (double)(ctr[0] - moves_before) < tail * (double)n) break;
         if (ctr[0] >= budget) break;
         moves_before = ctr[0];
         if (offs[B * NBUCKET] == 0) break;

@@ -153,8 +153,8 @@ class WarmStartResult:
 
 
 def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
-                      judge: bool = True, tolerance: float = 1e-4, context=None) -> WarmStartResult:
-    """leiden_from(model's proposal). With `judge`, the plain singleton start also
+                      verify: bool = True, tolerance: float = 1e-4, context=None) -> WarmStartResult:
+    """leiden_from(model's proposal). With `verify`, the plain singleton start also
     runs and the proposal is kept only if its final modularity is at least the
     plain one minus `tolerance`; otherwise the plain result is returned.
     `context` is (coarse, fine), the partitions at the neighbouring lower and
@@ -169,7 +169,7 @@ def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, 
     q_w = modularity(graph, warm.labels(), gamma)
     res = WarmStartResult(warm.labels(), warm.n_clusters(), True, q_w, None, sw["local_move_sweeps"], None,
                           t_prop + sw["ms_total"], None, kprop)
-    if not judge:
+    if not verify:
         return res
     plain = leiden(graph, config)
     sp = graph._ctx.run_stats()

@@ -11,7 +11,7 @@
 * gain: trained on plain-GPU Leiden partitions at RB {0.5, 1, 2} (each with the
   partitions of its neighbouring resolutions as context), the proposal used as
   a warm start at RB {0.8, 1.5} needs fewer local-moving sweeps than the plain
-  singleton start, with final modularity >= plain - 1e-4 or the judge falling
+  singleton start, with final modularity >= plain - 1e-4 or the check falling
   back to the plain result.
 """
 import numpy as np
