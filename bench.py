@@ -20,6 +20,9 @@ with from_csr_parts. A "step" is one full leiden() call on that graph.
              log-spaced in [0.1, 3] x 4 seeds = 128 instances, timed as 128
              sequential plain runs and as warm-started chains on concurrent
              streams; speed-up and per-instance modularity differences.
+  many_graphs (also in the line, skipped with the sweep) 512 independent
+             planted-partition graphs (n log-uniform in [100, 50,000]) in one
+             batch call: sequential vs concurrent workers, identical labels.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                   [--n POINTS] [--no-sweep] [--no-cpu-baseline]
@@ -153,6 +156,38 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2):
             "warm_chains_s": warm_s, "streams": n_streams, "chain_split": split, "speedup": base_s / warm_s,
             "dQ_min": float(d.min()), "dQ_mean": float(d.mean()), "dQ_max": float(d.max()),
             "frac_dQ_ge_-1e-4": float(np.mean(d >= -1e-4))}
+
+
+MANY_GRAPHS, MANY_SEED, MANY_STREAMS = 512, 21, 16
+
+
+def run_many_graphs(device_index, count=MANY_GRAPHS, n_streams=MANY_STREAMS):
+    """512 independent planted-partition graphs (node counts log-uniform in
+    [100, 50,000], 5-200 blocks, mean degree U[10, 30], 80% of the draws inside
+    the block, f32 weights U[0.5, 1.5]), RB(1) seed 42 on each: one batch call
+    with sequential instances vs one with concurrent workers. The labels of
+    the two must be identical (a fixed seed is bit-reproducible)."""
+    import sc_gpu
+    from sc_gpu import synth
+    graphs = []
+    nodes = edges = 0
+    for n, src, dst, w, _ in synth.many_planted_graphs(count, MANY_SEED):
+        g = sc_gpu.CSRNetwork.from_edge_arrays(n, src, dst, w, device=device_index)
+        graphs.append(g)
+        nodes += n
+        edges += g.edge_count()
+    cfgs = [sc_gpu.LeidenConfig(objective=sc_gpu.Rb(1.0), seed=42)] * count
+    sc_gpu.leiden_batch(graphs, cfgs, n_streams=n_streams)  # warm-up: workers' temporaries settle in the pool
+    t = time.perf_counter()
+    seq = sc_gpu.leiden_batch(graphs, cfgs, n_streams=1)
+    seq_s = time.perf_counter() - t
+    t = time.perf_counter()
+    bat = sc_gpu.leiden_batch(graphs, cfgs, n_streams=n_streams)
+    bat_s = time.perf_counter() - t
+    same = all(a == b for a, b in zip(seq, bat))
+    return {"workload": f"many_planted{count}_n100-50000", "graphs": count, "nodes": nodes, "edges": edges,
+            "sequential_s": seq_s, "batched_s": bat_s, "streams": n_streams, "speedup": seq_s / bat_s,
+            "graphs_per_s": count / bat_s, "edges_per_s": edges / bat_s, "labels_identical": bool(same)}
 
 
 def run_knn_part(args, device_index):
@@ -433,6 +468,7 @@ def main():
     if not args.no_sweep:
         del g
         line["sweep"] = run_sweep(local_rank, args.sweep_points)
+        line["many_graphs"] = run_many_graphs(local_rank)
     if not args.no_cpu_baseline:
         og, lab_o, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
         q_o = og.modularity(lab_o)

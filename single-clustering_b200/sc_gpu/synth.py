@@ -36,6 +36,26 @@ def planted_partition(n: int = 20_000, blocks: int = 40, intra: int = 12, inter:
     return src, dst, w, block.astype(np.uint64)
 
 
+def many_planted_graphs(count: int = 512, seed: int = 21, n_range=(100, 50_000), blocks_range=(5, 200),
+                        degree_range=(10.0, 30.0), intra_share: float = 0.8):
+    """Many independent planted-partition graphs: node counts log-uniform in
+    n_range, block counts uniform in blocks_range (at most n/5), mean degree
+    uniform in degree_range with intra_share of each node's draws inside its
+    block, f32 weights U[0.5, 1.5]. Yields (n, src, dst, w, truth) per graph."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    ns = np.exp(rng.uniform(np.log(n_range[0]), np.log(n_range[1]), count)).astype(np.int64)
+    bs = rng.integers(blocks_range[0], blocks_range[1] + 1, count)
+    ds = rng.uniform(degree_range[0], degree_range[1], count)
+    for i in range(count):
+        n = int(ns[i])
+        blocks = int(max(1, min(bs[i], n // 5)))
+        draws = ds[i] / 2.0  # each draw adds one entry to both endpoints' rows
+        intra = max(1, int(round(intra_share * draws)))
+        inter = max(0, int(round(draws)) - intra)
+        src, dst, w, truth = planted_partition(n, blocks, intra, inter, seed * 100_003 + i)
+        yield n, src, dst, w, truth
+
+
 def gaussian_mixture(n: int, d: int, components: int, seed: int, sigma=(1.0, 1.0),
                      centre_scale: float = 2.0):
     """Isotropic Gaussian mixture, f32 row-major [n, d]: centres ~ N(0, centre_scale^2 I),
