@@ -1,6 +1,6 @@
 // sc_upload.cu — host -> device copies of large pageable buffers.
 //
-// A pageable cudaMemcpyAsync is staged by the driver through its own pinned
+// A pageable cudaMemcpyAsync is staged by the CUDA driver through its own pinned
 // buffers by one thread, about 10 GB/s here. For the graph arrays (hundreds
 // of MB) that copy is most of an end-to-end call, so large uploads go through
 // the context's own pinned staging instead: STAGE_LANES host threads each copy
