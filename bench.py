@@ -4,7 +4,11 @@ Workload (the large single-graph configuration): 4,000,000 points x 30 dims
 f32 from a 100-component Gaussian mixture (sigma ~ U[0.7, 1.5], centres
 N(0, 4I)); exact kNN k = 10; Gaussian connectivities with per-point sigma =
 distance to the k-th neighbour; union-symmetrised u32 / f32 CSR handed over
-with from_csr_parts. A "step" is one full leiden() call on that graph.
+with from_csr_parts. A "step" is one full leiden() call on that graph. The
+graph is built with torch alone (synth.knn_graph_exact_torch, an exact FP64
+search), identically in both arms, so the reference arm never loads this
+library; the library's own kNN builder is timed on the same points beside it
+(`library_knn`: build time, recall@k and connectivity error against FP64).
 
   value      undirected edges / s of leiden() with the graph resident in HBM
              (edge_count / device time of the run, CUDA events on the
@@ -24,8 +28,21 @@ with from_csr_parts. A "step" is one full leiden() call on that graph.
              planted-partition graphs (n log-uniform in [100, 50,000]) in one
              batch call: sequential vs concurrent workers, identical labels.
 
+  c2         (also in the line) 200,000 x 50 points, 30 components, k = 15:
+             the graph from FP32 CUDA-core and from BF16 tensor-core candidate
+             distances (both re-ranked in FP32), recall and connectivity error
+             of each, Leiden RB 1.0 and CPM 0.05 on each, the CPU oracle's
+             quality on the same graphs.
+  c5         (also in the line) 2,000,000 x 50 points, 200 components, k = 15
+             from FP8 e4m3 candidates (BF16 beside it): recall, then the edge
+             MLP trained at RB {0.5, 1, 2} and evaluated as a warm start at
+             RB {0.8, 1.5} against the plain start.
+  cpu_baseline.calibration  the CPU oracle on the reference benchmark's own
+             100k-node shape beside its published ~110 ms.
+
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--n POINTS] [--no-sweep] [--no-cpu-baseline]
+                  [--n POINTS] [--no-sweep] [--no-c2] [--no-c5] [--no-accuracy]
+                  [--no-cpu-baseline]
   python bench.py --part knn [--n POINTS] [--steps K] [--warmup W] [--knn-precision bf16|fp8]
              times the kNN graph builder alone (points/s) on the same data.
 """
@@ -58,55 +75,6 @@ def log(*a):
 
 
 # ---------------------------------------------------------------- workload
-def knn_graph_torch(n, d, comps, seed, k, device):
-    """Synthetic input only: exact fp32 brute-force kNN with torch, Gaussian
-    weights with sigma = k-th neighbour distance, union symmetrisation."""
-    import torch
-    from sc_gpu import synth
-    X, _ = synth.gaussian_mixture(n, d, comps, seed, sigma=(0.7, 1.5))
-    x = torch.from_numpy(X).to(device)
-    torch.backends.cuda.matmul.allow_tf32 = False
-    norms = (x * x).sum(1)
-    idx = torch.empty((n, k + 1), dtype=torch.int64, device=device)
-    dist = torch.empty((n, k + 1), dtype=torch.float32, device=device)
-    chunk = 512
-    for s in range(0, n, chunk):
-        e = min(n, s + chunk)
-        d2 = norms[s:e, None] + norms[None, :] - 2.0 * (x[s:e] @ x.T)
-        v, i = torch.topk(d2, k + 1, dim=1, largest=False, sorted=True)
-        idx[s:e] = i
-        dist[s:e] = v.clamp_min_(0).sqrt_()
-    sig = dist[:, k]
-    rows = torch.arange(n, device=device).repeat_interleave(k)
-    cols = idx[:, 1:].reshape(-1)
-    dd = dist[:, 1:].reshape(-1)
-    si, sj = sig[rows], sig[cols]
-    den = si * si + sj * sj
-    w = torch.sqrt(2 * si * sj / den) * torch.exp(-dd * dd / den)
-    keep = rows != cols
-    rows, cols, w = rows[keep], cols[keep], w[keep]
-    lo, hi = torch.minimum(rows, cols), torch.maximum(rows, cols)
-    key = lo * n + hi
-    key, order = torch.sort(key, stable=True)
-    w = w[order]
-    first = torch.ones_like(key, dtype=torch.bool)
-    first[1:] = key[1:] != key[:-1]
-    key, w = key[first], w[first]
-    lo, hi = key // n, key % n
-    r = torch.cat([lo, hi])
-    c = torch.cat([hi, lo])
-    ww = torch.cat([w, w]).float()
-    k2, order = torch.sort(r * n + c)
-    r, c, ww = r[order], c[order], ww[order]
-    ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
-    ptr[1:] = torch.cumsum(torch.bincount(r, minlength=n), 0)
-    out = (ptr.cpu().numpy().astype(np.uint64), c.to(torch.int32).cpu().numpy().view(np.uint32).copy(),
-           ww.cpu().numpy())
-    del x, norms, idx, dist
-    torch.cuda.empty_cache()
-    return out
-
-
 def knn_graph_sc(n, d, comps, seed, k, device_index):
     """The library's own kNN builder: exact search (BF16 tcgen05 candidates +
     FP32 re-rank), sigma = k-th distance, union symmetrisation."""
@@ -117,6 +85,8 @@ def knn_graph_sc(n, d, comps, seed, k, device_index):
     r = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
     KNN_INFO["seconds"] = time.perf_counter() - t
     KNN_INFO["stats"] = sc_gpu.last_run_stats(device_index)
+    KNN_INFO["points"] = X
+    KNN_INFO["index"] = r.index
     return r.conn_ptrs, r.conn_nbrs, r.conn_w
 
 
@@ -127,7 +97,7 @@ SWEEP_RESOLUTIONS = 32
 SWEEP_SEEDS = (1, 2, 3, 4)
 
 
-def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2):
+def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2, accuracy=True):
     """128-instance resolution x seed sweep: sequential plain runs vs
     warm-started chains (each seed's chain cut in `split` pieces whose heads
     start from the seed's finest partition) on concurrent streams."""
@@ -135,6 +105,8 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2):
     from sc_gpu import synth
     X, _ = synth.gaussian_mixture(n_points, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_SEED, sigma=(0.7, 1.5))
     r = sc_gpu.knn_gaussian(X, SWEEP_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    acc = (knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, SWEEP_K, f"cuda:{device_index}")
+           if accuracy else None)
     g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w, device=device_index)
     del X, r
     res = np.geomspace(0.1, 3.0, SWEEP_RESOLUTIONS)
@@ -155,7 +127,7 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=2):
             "instances": len(base_q), "edge_count": g.edge_count(), "plain_sequential_s": base_s,
             "warm_chains_s": warm_s, "streams": n_streams, "chain_split": split, "speedup": base_s / warm_s,
             "dQ_min": float(d.min()), "dQ_mean": float(d.mean()), "dQ_max": float(d.max()),
-            "frac_dQ_ge_-1e-4": float(np.mean(d >= -1e-4))}
+            "frac_dQ_ge_-1e-4": float(np.mean(d >= -1e-4)), "knn_accuracy": acc}
 
 
 MANY_GRAPHS, MANY_SEED, MANY_STREAMS = 512, 21, 16
@@ -237,13 +209,260 @@ def knn_cpu_baseline(X, gpu_index, sample=20000):
              "tree build amortised over n", "build_s": build, "query_s": dt}, hits / idx.size)
 
 
+# ---------------------------------------------------------------- kNN accuracy
+def fp64_knn(Xd, nrm, rows, k, device, block=64, margin=8):
+    """Exact FP64 k+1 nearest points (self included) of the points `rows` of the
+    device array Xd (float64): candidates from the norm-expanded FP64 distances
+    with a margin, then exact FP64 differences ordered by (distance, self first,
+    index). Returns host (idx int64, dist float64), len(rows) x (k+1)."""
+    import torch
+    n = Xd.shape[0]
+    kk = min(n, k + 1 + margin)
+    out_i = np.empty((len(rows), k + 1), np.int64)
+    out_d = np.empty((len(rows), k + 1), np.float64)
+    for s in range(0, len(rows), block):
+        r = torch.from_numpy(np.asarray(rows[s:s + block], np.int64)).to(device)
+        d2 = nrm[r, None] + nrm[None, :] - 2.0 * (Xd[r] @ Xd.T)
+        _, cand = torch.topk(d2, kk, dim=1, largest=False)
+        del d2
+        dd = ((Xd[cand] - Xd[r][:, None, :]) ** 2).sum(-1)
+        cand, dd, rr = cand.cpu().numpy(), dd.cpu().numpy(), r.cpu().numpy()
+        order = np.lexsort((cand, cand != rr[:, None], dd), axis=-1)[:, : k + 1]
+        out_i[s:s + block] = np.take_along_axis(cand, order, 1)
+        out_d[s:s + block] = np.sqrt(np.take_along_axis(dd, order, 1))
+    return out_i, out_d
+
+
+def knn_accuracy(X, index, ptrs, nbrs, w, k, device, sample=2000, seed=0):
+    """recall@k of the library's k-nearest lists and the largest connectivity
+    error against an FP64 exact search, on `sample` seeded query points.
+
+    recall_at_k         |library's k neighbours (self excluded) & FP64's| / k
+    recall_at_k_ties    the same, a library neighbour whose FP64 distance ties
+                        the true k-th within 1e-6 relative counted as a hit
+    max_rel_conn_err    over the FP64 neighbours j of each sampled i: the
+                        library's CSR weight (i, j) against the FP64 Gaussian
+                        weight with sigma = FP64 k-th distance (union
+                        symmetrisation, the bench's setting); edges the library
+                        lacks are counted in missing_edges instead."""
+    import torch
+    n = X.shape[0]
+    rng = np.random.Generator(np.random.PCG64(seed))
+    q = np.sort(rng.choice(n, min(sample, n), replace=False))
+    Xd = torch.from_numpy(np.ascontiguousarray(X)).to(device, torch.float64)
+    nrm = (Xd * Xd).sum(1)
+    t = time.perf_counter()
+    ti, td = fp64_knn(Xd, nrm, q, k, device)
+    nb = np.unique(ti[:, 1:].reshape(-1))
+    si, sd = fp64_knn(Xd, nrm, nb, k, device)
+    sig = dict(zip(nb.tolist(), sd[:, k].tolist()))
+    hits = hits_t = 0
+    max_rel = max_abs = 0.0
+    missing = 0
+    X64 = X.astype(np.float64)
+    for r, i in enumerate(q):
+        truth = set(ti[r, 1:].tolist())
+        got = [j for j in index[i, 1:].tolist() if j != i]
+        kth = td[r, k]
+        for j in got:
+            if j in truth:
+                hits += 1
+                hits_t += 1
+            else:
+                dj = float(np.sqrt(((X64[i] - X64[j]) ** 2).sum()))
+                hits_t += abs(dj - kth) <= 1e-6 * max(kth, 1e-30)
+        row = nbrs[int(ptrs[i]):int(ptrs[i + 1])]
+        for t2 in range(1, k + 1):
+            j = int(ti[r, t2])
+            s_i, s_j, dist = td[r, k], sig[j], td[r, t2]
+            den = s_i * s_i + s_j * s_j
+            w64 = np.sqrt(2 * s_i * s_j / den) * np.exp(-dist * dist / den)
+            pos = np.searchsorted(row, j)
+            if pos >= len(row) or row[pos] != j:
+                missing += 1
+                continue
+            err = abs(float(w[int(ptrs[i]) + pos]) - w64)
+            max_abs = max(max_abs, err)
+            max_rel = max(max_rel, err / w64)
+    del Xd, nrm
+    torch.cuda.empty_cache()
+    return {"recall_at_k": hits / (len(q) * k), "recall_at_k_ties": hits_t / (len(q) * k),
+            "max_rel_conn_err": max_rel, "max_abs_conn_err": max_abs, "missing_edges": missing,
+            "sample": f"{len(q)} seeded query points (PCG64 seed {seed}) against all {n}, FP64 exact search "
+                      "(torch float64 on the device) incl. the k-th distances of their neighbours",
+            "check_s": time.perf_counter() - t}
+
+
+# ---------------------------------------------------------------- C2
+C2_POINTS, C2_DIMS, C2_COMPONENTS, C2_K, C2_SEED = 200_000, 50, 30, 15, 2
+
+
+def run_c2(device_index, cpu=True):
+    """kNN + Gaussian connectivities + Leiden on 200,000 x 50 points of a
+    30-component mixture (centres N(0, 4I), sigma 1, Dirichlet(1) weights):
+    exact k = 15 with sigma = k-th distance, union symmetrisation; candidates
+    from FP32 CUDA-core distances and from BF16 tensor-core distances, both
+    re-ranked in exact FP32; Leiden RB 1.0 and CPM 0.05 on each graph, and the
+    CPU oracle on the same graphs."""
+    import sc_gpu
+    from sc_gpu import synth
+    X, _ = synth.gaussian_mixture(C2_POINTS, C2_DIMS, C2_COMPONENTS, C2_SEED, sigma=(1.0, 1.0))
+    out = {"workload": f"knn{C2_K}_gmm{C2_POINTS}x{C2_DIMS}_c{C2_COMPONENTS}", "sigma": "kth",
+           "symmetrisation": "union", "arms": {}}
+    csr = {}
+    for name, prec in (("fp32", sc_gpu.KNN_FP32), ("bf16", sc_gpu.KNN_BF16)):
+        sc_gpu.knn_gaussian(X, C2_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
+                            device=device_index)  # warm-up
+        t = time.perf_counter()
+        r = sc_gpu.knn_gaussian(X, C2_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
+                                device=device_index)
+        arm = {"knn_build_s": time.perf_counter() - t,
+               "accuracy": knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, C2_K,
+                                        f"cuda:{device_index}")}
+        csr[name] = (r.conn_ptrs, r.conn_nbrs, r.conn_w)
+        g = sc_gpu.CSRNetwork.from_csr_parts(*csr[name], device=device_index)
+        arm["edge_count"] = g.edge_count()
+        for oname, obj in (("rb1.0", sc_gpu.Rb(1.0)), ("cpm0.05", sc_gpu.Cpm(0.05))):
+            cfg = sc_gpu.LeidenConfig(objective=obj, seed=42)
+            sc_gpu.leiden(g, cfg)
+            c = sc_gpu.leiden(g, cfg)
+            st = sc_gpu.last_run_stats(device_index)
+            res = {"ms": st["ms_total"], "n_clusters": c.n_clusters(),
+                   "quality": sc_gpu.quality(g, c.labels(), obj)}
+            if oname.startswith("rb"):
+                res["modularity"] = sc_gpu.modularity(g, c.labels(), 1.0)
+            arm[oname] = res
+        out["arms"][name] = arm
+    a, b = csr["fp32"], csr["bf16"]
+    out["graphs_identical"] = bool(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+                                   and np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32)))
+    if cpu:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        cb = {}
+        for name in ("fp32", "bf16"):
+            og = O.Graph.from_csr_parts(*csr[name])
+            for oname, kind, gamma in (("rb1.0", O.RB, 1.0), ("cpm0.05", O.CPM, 0.05)):
+                t = time.perf_counter()
+                lab, ncl = og.leiden(objective=kind, resolution=gamma, seed=42)
+                dt = time.perf_counter() - t
+                qo = og.quality(lab, kind, gamma)
+                gpu = out["arms"][name][oname]
+                # quality per unit of total edge weight (modularity's scale for RB)
+                tw = og.total_weight()
+                cb[f"{name}/{oname}"] = {"s": dt, "quality": qo, "n_clusters": int(ncl),
+                                         "dQ_per_weight": (gpu["quality"] - qo) / tw}
+        out["cpu_baseline"] = {"kind": "port", "cores": 1, "runs": cb,
+                               "sample": "one full leiden() run of the CPU oracle per graph and objective"}
+    return out
+
+
+# ---------------------------------------------------------------- C5
+C5_POINTS, C5_DIMS, C5_COMPONENTS, C5_K, C5_SEED = 2_000_000, 50, 200, 15, 5
+
+
+def run_c5(device_index):
+    """Learned warm start + FP8 kNN on 2,000,000 x 50 points of a 200-component
+    mixture (sigma U[0.5, 2.0]): kNN k = 15 from FP8 e4m3 per-row-scaled
+    candidates re-ranked in FP32 (BF16 candidates beside it for their recall);
+    the edge MLP trained on plain-GPU partitions at RB {0.5, 1.0, 2.0}
+    (independent seeds), evaluated as a warm start at RB {0.8, 1.5} against the
+    plain singleton start, which is also the fallback."""
+    import sc_gpu
+    from sc_gpu import synth
+    from sc_gpu.learned import EdgeMlp, warm_start_leiden
+    X, _ = synth.gaussian_mixture(C5_POINTS, C5_DIMS, C5_COMPONENTS, C5_SEED, sigma=(0.5, 2.0))
+    dev = f"cuda:{device_index}"
+    out = {"workload": f"knn{C5_K}_gmm{C5_POINTS}x{C5_DIMS}_c{C5_COMPONENTS}", "knn": {}}
+    keep = None
+    for name, prec in (("fp8", sc_gpu.KNN_FP8), ("bf16", sc_gpu.KNN_BF16)):
+        t = time.perf_counter()
+        r = sc_gpu.knn_gaussian(X, C5_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
+                                device=device_index)
+        out["knn"][name] = {"build_s": time.perf_counter() - t,
+                            "accuracy": knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, C5_K, dev)}
+        if name == "fp8":
+            keep = (r.conn_ptrs, r.conn_nbrs, r.conn_w)
+        del r
+    del X
+    g = sc_gpu.CSRNetwork.from_csr_parts(*keep, device=device_index)
+    del keep
+    out["edge_count"] = g.edge_count()
+
+    def run(gamma, seed):
+        return sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=seed)).labels()
+
+    sc_gpu.leiden(g)  # warm-up
+    t = time.perf_counter()
+    labs = {0.5: run(0.5, 101), 1.0: run(1.0, 102), 2.0: run(2.0, 103)}
+    alt = {0.5: run(0.5, 201), 2.0: run(2.0, 203)}
+    ctx = {0.5: (alt[0.5], labs[1.0]), 1.0: (labs[0.5], labs[2.0]), 2.0: (labs[1.0], alt[2.0])}
+    t_part = time.perf_counter() - t
+    m = EdgeMlp(seed=4)
+    t = time.perf_counter()
+    rounds, epochs = 6, 20
+    for _ in range(rounds):
+        for gamma in (0.5, 1.0, 2.0):
+            loss = m.train(g, labs[gamma], gamma, epochs=epochs, lr=5e-3, context=ctx[gamma])
+    out["training"] = {"resolutions": [0.5, 1.0, 2.0], "seeds": [101, 102, 103], "calls": 3 * rounds,
+                       "epochs_per_call": epochs, "train_s": time.perf_counter() - t, "final_loss": loss,
+                       "partition_runs_s": t_part}
+    ev = {}
+    for gamma, c in ((0.8, (labs[0.5], labs[1.0])), (1.5, (labs[1.0], labs[2.0]))):
+        cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=9)
+        warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=0.0, context=c)  # warm-up
+        res = warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=0.0, context=c)
+        ev[str(gamma)] = {"used_proposal": res.used_proposal, "q_warm": res.q_warm, "q_plain": res.q_plain,
+                          "dQ": res.q_warm - res.q_plain, "sweeps_warm": res.sweeps_warm,
+                          "sweeps_plain": res.sweeps_plain, "ms_warm": res.ms_warm, "ms_plain": res.ms_plain,
+                          "ms_saved": res.ms_plain - res.ms_warm, "proposal_clusters": res.proposal_clusters}
+    out["warm_start"] = ev
+    return out
+
+
 def make_graph(args, device):
+    """The Leiden input of both arms. "gmm" (default): the exact kNN graph of the
+    4M-point mixture built with torch alone (synth.knn_graph_exact_torch), so
+    the reference arm never loads this library and both arms cluster the same
+    bytes; the library's own kNN builder is timed and checked on the same
+    points in a leg of its own. "gmm-sc": the library's kNN graph instead."""
+    from sc_gpu import synth
     if args.graph == "lattice":
-        from sc_gpu import synth
         return synth.knn_like_graph(args.n, k=K, seed=GRAPH_SEED)
-    if args.graph == "gmm-torch":
-        return knn_graph_torch(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device)
-    return knn_graph_sc(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device.index or 0)
+    if args.graph == "gmm-sc":
+        return knn_graph_sc(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, device.index or 0)
+    X, comp = synth.gaussian_mixture(args.n, DIMS, COMPONENTS, GRAPH_SEED, sigma=(0.7, 1.5))
+    t = time.perf_counter()
+    ptr, nbr, w, idx, dist = synth.knn_graph_exact_torch(X, comp, K, device)
+    GRAPH_INFO["build_s"] = time.perf_counter() - t
+    GRAPH_INFO["points"] = X
+    return ptr, nbr, w
+
+
+GRAPH_INFO = {}
+
+
+def library_knn_leg(X, ptr, nbr, w, device_index, accuracy=True):
+    """The library's kNN builder (BF16 tcgen05 candidates + FP32 re-rank,
+    sigma = k-th distance, union) on the headline's points: build time, recall
+    and connectivity error against FP64, and how its graph compares with the
+    exact graph the Leiden runs use."""
+    import sc_gpu
+    sc_gpu.knn_gaussian(X[:65536], K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    t = time.perf_counter()
+    r = sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    out = {"build_s": time.perf_counter() - t, "precision": "bf16", "points": int(X.shape[0])}
+    same_ptr = np.array_equal(r.conn_ptrs, ptr)
+    same_nbr = same_ptr and np.array_equal(r.conn_nbrs, nbr)
+    out["same_edges_as_exact_graph"] = bool(same_nbr)
+    if same_nbr:
+        rel = np.abs(r.conn_w.astype(np.float64) - w) / np.maximum(w, 1e-30)
+        out["max_rel_weight_diff_vs_exact_graph"] = float(rel.max())
+    else:
+        out["entries"], out["exact_graph_entries"] = int(len(r.conn_nbrs)), int(len(nbr))
+    if accuracy:
+        out["accuracy"] = knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, K, f"cuda:{device_index}")
+    return out
 
 
 # ---------------------------------------------------------------- clocks
@@ -309,6 +528,48 @@ def run_cpu_baseline(ptr, nbr, w, seed):
     return g, lab, dt
 
 
+def blob_knn_graph(n=100_000, blocks=10, k=15, seed=5):
+    """The shape of the reference's own Leiden benchmark (benches/leiden.rs:17-68):
+    n points in `blocks` squares of side 16 around centres on a circle of radius
+    60, each joined to its k nearest points, unit weights, the undirected union
+    of those pairs (from_edges). Points are drawn with numpy's PCG64, not the
+    reference's ChaCha8, and the neighbours by an exact kd-tree: at this density
+    the reference's +-2-cell grid holds every true neighbour."""
+    from scipy.spatial import cKDTree
+    rng = np.random.Generator(np.random.PCG64(seed))
+    per = n // blocks
+    b = np.minimum(np.arange(n) // per, blocks - 1)
+    a = 2 * np.pi * np.arange(blocks) / blocks
+    pts = np.stack([60 * np.cos(a)[b] + rng.random(n) * 16 - 8, 60 * np.sin(a)[b] + rng.random(n) * 16 - 8], 1)
+    _, idx = cKDTree(pts).query(pts, k + 1)
+    src = np.repeat(np.arange(n), k)
+    dst = idx[:, 1:].reshape(-1)
+    key = np.unique(np.minimum(src, dst).astype(np.int64) * n + np.maximum(src, dst))
+    return n, (key // n).astype(np.uint64), (key % n).astype(np.uint64)
+
+
+README_MS_100K = 110.0  # README.md:18: "100k nodes / 840k edges in ~110 ms single-threaded"
+
+
+def cpu_calibration():
+    """The CPU oracle on the reference benchmark's 100k-node shape, best of 3,
+    beside the reference's published time for it (hardware unstated)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    n, src, dst = blob_knn_graph()
+    g = O.Graph.from_edges(n, src=src, dst=dst, w=np.ones(len(src)))
+    ts = []
+    for _ in range(3):
+        t = time.perf_counter()
+        g.leiden(seed=42)
+        ts.append(time.perf_counter() - t)
+    best = min(ts) * 1e3
+    return {"workload": "benches/leiden.rs knn_graph(100000, 10, 15) shape: 2-D blobs, unit weights",
+            "nodes": n, "edges": g.edge_count(), "oracle_ms_best_of_3": best,
+            "reference_published_ms": README_MS_100K, "oracle_over_published": best / README_MS_100K,
+            "note": "published figure: README.md:18, single-threaded, hardware not stated"}
+
+
 def cpu_model():
     try:
         for line in open("/proc/cpuinfo"):
@@ -326,9 +587,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=N_POINTS)
-    ap.add_argument("--graph", default="gmm", choices=["gmm", "gmm-torch", "lattice"])
+    ap.add_argument("--graph", default="gmm", choices=["gmm", "gmm-sc", "lattice"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-sweep", action="store_true")
+    ap.add_argument("--no-c2", action="store_true", help="skip the 200k x 50 FP32-vs-BF16 configuration")
+    ap.add_argument("--no-c5", action="store_true", help="skip the 2M x 50 FP8 + learned warm start configuration")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 recall / connectivity checks")
     ap.add_argument("--sweep-points", type=int, default=SWEEP_POINTS)
     ap.add_argument("--part", default="leiden", choices=["leiden", "knn"])
     ap.add_argument("--knn-precision", default="bf16", choices=["bf16", "fp8"])
@@ -368,7 +632,8 @@ def main():
                 "modularity": g.modularity(lab),
                 "cpu_baseline": {"value": eps, "unit": "edges/s", "cores": 1, "kind": "port",
                                  "sample": "one full leiden() run on the whole graph",
-                                 "cpu": cpu_model(), "nproc": os.cpu_count()},
+                                 "cpu": cpu_model(), "nproc": os.cpu_count(),
+                                 "calibration": cpu_calibration()},
                 "e2e": {"value": eps, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line), flush=True)
         if dist:
@@ -463,19 +728,34 @@ def main():
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
                     "graph_upload_s": graph_s / e2e_steps, "leiden_call_s": leiden_s / e2e_steps,
                     "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "each": e2e_each}}
+    if GRAPH_INFO:
+        line["input_graph"] = {"builder": "synth.knn_graph_exact_torch (torch only, FP64 exact kNN)",
+                               "build_s": GRAPH_INFO["build_s"]}
+        line["library_knn"] = library_knn_leg(GRAPH_INFO.pop("points"), ptr, nbr, w, local_rank,
+                                              accuracy=not args.no_accuracy)
+        line["knn_graph_build_s"] = line["library_knn"]["build_s"]
     if KNN_INFO:
         line["knn_graph_build_s"] = KNN_INFO["seconds"]
+        if not args.no_accuracy:
+            line["knn_accuracy"] = knn_accuracy(KNN_INFO["points"], KNN_INFO["index"], ptr, nbr, w, K,
+                                                f"cuda:{local_rank}")
+        KNN_INFO.pop("points")
+        KNN_INFO.pop("index")
     if not args.no_sweep:
         del g
-        line["sweep"] = run_sweep(local_rank, args.sweep_points)
+        line["sweep"] = run_sweep(local_rank, args.sweep_points, accuracy=not args.no_accuracy)
         line["many_graphs"] = run_many_graphs(local_rank)
+    if not args.no_c2:
+        line["c2"] = run_c2(local_rank, cpu=not args.no_cpu_baseline)
+    if not args.no_c5:
+        line["c5"] = run_c5(local_rank)
     if not args.no_cpu_baseline:
         og, lab_o, dt = run_cpu_baseline(ptr, nbr, w, LEIDEN_SEED)
         q_o = og.modularity(lab_o)
         line["cpu_baseline"] = {"value": m / dt, "unit": "edges/s", "cores": 1, "kind": "port",
                                 "sample": "one full leiden() run of the CPU oracle on the same graph",
                                 "s_per_run": dt, "modularity": q_o, "cpu": cpu_model(),
-                                "nproc": os.cpu_count()}
+                                "nproc": os.cpu_count(), "calibration": cpu_calibration()}
         line["dQ_vs_cpu"] = q - q_o
     print(json.dumps(line), flush=True)
     if dist:

@@ -149,6 +149,24 @@ sc_status sc_get_tuning(const sc_ctx* ctx, sc_tuning* out);
 /* Validates the limits above (SC_E_INVALID_ARGUMENT otherwise). */
 sc_status sc_set_tuning(sc_ctx* ctx, const sc_tuning* t);
 /*
+ * Bounded device waits (no counterpart in single-clustering, which has no
+ * device code). Each pipeline wait of the kNN candidate kernel (a TMA copy
+ * landing, an accumulator filled or drained) tries at most `limit` times, then
+ * the kernel stops, waits with the library's default limit for the copies and
+ * MMAs it already issued, frees its tensor memory and returns; the call then
+ * fails with SC_E_TIMEOUT and the context stays usable. Default 2^26.
+ */
+sc_status sc_set_wait_limit(sc_ctx* ctx, uint32_t limit);
+sc_status sc_get_wait_limit(const sc_ctx* ctx, uint32_t* out);
+/*
+ * Test hook for the bounded waits: while on, the kNN kernel's producer issues
+ * the query tiles but never a point tile, so the first wait for one runs out
+ * its limit (set a small one with sc_set_wait_limit) and the kNN call returns
+ * SC_E_TIMEOUT without any copy or MMA left in flight. Off by default.
+ */
+sc_status sc_test_knn_hold_tiles(sc_ctx* ctx, int32_t on);
+
+/*
  * Autotuner: times the first level of `cfg` (one pass, one level: the level
  * that dominates a run) on g under each candidate routing, keeps the fastest
  * on the context and returns it with its time and the default's (device time,
@@ -242,9 +260,12 @@ sc_status sc_modularity(sc_ctx* ctx, const sc_graph* g, const uint64_t* labels,
  * as compact uint32 ids (< 65,536, so at most 65,536 communities; larger ids
  * return SC_E_UNSUPPORTED) and no device allocation. Its scratch is a fixed
  * 1 MiB array in the library, held by every GPU that loads the library until
- * the process exits; the first call on a device looks up that array's address,
- * so make that first call before any stream capture. Every call shares the
- * array: calls whose work overlaps on the GPU race and must be serialised.
+ * the process exits; a call looks up that array's address for the current
+ * device and CUDA context the first time it meets them. Every call ends by
+ * synchronising the context's stream and reading the result back, so it must
+ * not be called while that stream is being captured into a CUDA graph. Every
+ * call shares the array: calls whose work overlaps on the GPU race and must be
+ * serialised.
  * Bit-exact with sc_modularity when every sum of the graph's edge weights is
  * exact in f64 (all unit or f32-valued weights below 2^(52+e0) in total);
  * otherwise it may differ in the last bits.
@@ -315,7 +336,9 @@ typedef enum sc_knn_precision { SC_KNN_FP32 = 0, SC_KNN_BF16 = 1, SC_KNN_FP8 = 2
 typedef struct sc_knn_opts {
     int32_t sigma;        /* sc_knn_sigma; median = reference (neighborhood/mod.rs:105-124, :480-499) */
     int32_t sym;          /* sc_knn_sym;   lower_id = reference (neighborhood/mod.rs:138-163)         */
-    int32_t precision;    /* sc_knn_precision of the candidate distance contraction                 */
+    int32_t precision;    /* sc_knn_precision of the candidate distances: BF16 or FP8 e4m3 on the
+                             tensor cores (norm-expanded contraction, FP32 accumulation), or FP32
+                             on the CUDA cores (exact differences, the re-rank's arithmetic)       */
     int32_t rerank_factor;/* candidates kept per row before the exact FP32 re-rank = factor * (k+1)  */
     int32_t squared_kiddo;/* 1: kd-tree path semantics (squared distances, sigma = sqrt(median d^2)) */
 } sc_knn_opts;

@@ -225,6 +225,23 @@ sc_status sc_set_tuning(sc_ctx* ctx, const sc_tuning* t) {
     });
 }
 
+sc_status sc_set_wait_limit(sc_ctx* ctx, uint32_t limit) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        if (limit == 0) sc::fail(SC_E_INVALID_ARGUMENT, "the wait limit must be at least 1");
+        c.wait_limit = limit;
+    });
+}
+
+sc_status sc_get_wait_limit(const sc_ctx* ctx, uint32_t* out) {
+    if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
+    *out = ctx->c.wait_limit;
+    return SC_OK;
+}
+
+sc_status sc_test_knn_hold_tiles(sc_ctx* ctx, int32_t on) {
+    return guarded(ctx, [&](sc::Ctx& c) { c.knn_hold_tiles = on ? 1u : 0u; });
+}
+
 sc_status sc_autotune(sc_ctx* ctx, const sc_graph* g, const sc_leiden_config* cfg, sc_tuning* chosen,
                       double* ms_chosen, double* ms_default, uint32_t* n_candidates) {
     return guarded(ctx, [&](sc::Ctx& c) {

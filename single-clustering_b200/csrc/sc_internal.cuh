@@ -59,6 +59,7 @@ struct Failure {
 
 // ------------------------------------------------------------------ context
 constexpr uint32_t HUB_DEGREE = 1024;  // degree above which a node's hash lives in global memory
+constexpr uint32_t DEFAULT_WAIT_LIMIT = 1u << 26;  // try_wait iterations of a bounded mbarrier wait
 
 struct Ctx {
     int device = 0;
@@ -72,6 +73,13 @@ struct Ctx {
     int sm_count = 148;
     size_t smem_optin = 0;
     sc_tuning tuning{8, 16, 32, 4096};  // decide-kernel routing (sc_set_tuning / sc_autotune)
+    // iterations a pipeline wait of the kNN kernel tries before it gives up
+    // (sc_set_wait_limit); the waits that drain copies already issued keep the
+    // library's default, so nothing can land in shared memory after a CTA exits
+    uint32_t wait_limit = DEFAULT_WAIT_LIMIT;
+    // test hook (sc_test_knn_hold_tiles): the kNN producer issues no point
+    // tiles, so the contraction's first wait runs out and the call times out
+    uint32_t knn_hold_tiles = 0;
     // side streams for kernels of one step that may run concurrently (fork / join by events)
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr;

@@ -53,7 +53,7 @@ constexpr int NUM_EPI_WARPS = 4 * QT * HALVES;  // a full set of 4 TMEM lane qua
 constexpr int KNN_THREADS = 32 * (2 + NUM_EPI_WARPS);
 template <int KA>
 constexpr int stages_for() { return KA == 32 ? 6 : 3; }  // B ring depth within 227 KB
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
+constexpr uint32_t WAIT_LIMIT = DEFAULT_WAIT_LIMIT;  // drain waits: copies / MMAs already issued
 constexpr uint32_t TMEM_COLS = 512;
 
 // ------------------------------------------------------------ PTX helpers
@@ -74,10 +74,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
                  : "memory");
 }
 
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+// Bounded wait for the phase with the given parity to complete: at most
+// `limit` try_wait attempts, false when they ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = WAIT_LIMIT) {
     const uint32_t addr = smem_u32(bar);
-    for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
+    for (uint32_t it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -349,7 +350,8 @@ struct KnnSmem {
 template <int KA, bool F8>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
-             uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status) {
+             uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status,
+             uint32_t lim, uint32_t hold_tiles) {
     using L = KnnSmem<KA>;
     extern __shared__ __align__(1024) unsigned char raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
@@ -404,7 +406,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             uint32_t gi = 0;
             bool a_in_flight = false;
             for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x, ++gi) {
-                if (gi > 0 && !mbar_wait(aempty, (gi - 1) & 1)) {
+                if (gi > 0 && !mbar_wait(aempty, (gi - 1) & 1, lim)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -412,10 +414,14 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 a_in_flight = true;
                 for (int q = 0; q < QT; ++q)
                     tma_load_2d(sA + q * L::TILE_BYTES, &tmA, afull, 0, (int)(g * QT * TILE + q * TILE));
+                if (hold_tiles) {  // test hook: no point tile is ever issued
+                    ++gi;
+                    break;
+                }
                 for (uint32_t t = 0; t < ntiles; ++t, ++it) {
                     const uint32_t s = (uint32_t)(it % L::STAGES);
                     const uint64_t use = it / L::STAGES;
-                    if (use > 0 && !mbar_wait(empty + s, (uint32_t)((use - 1) & 1))) {
+                    if (use > 0 && !mbar_wait(empty + s, (uint32_t)((use - 1) & 1), lim)) {
                         *abort_flag = 1;
                         break;
                     }
@@ -425,8 +431,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 }
             }
             // drain: the copies issued last (one per stage, and the query tiles)
-            // must land before the CTA exits
-            if (*abort_flag) {
+            // must land before the CTA exits (waits with the default limit)
+            if (*abort_flag || hold_tiles) {
                 for (uint64_t x = it > L::STAGES ? it - L::STAGES : 0; x < it; ++x)
                     mbar_wait(full + (x % L::STAGES), (uint32_t)((x / L::STAGES) & 1));
                 if (a_in_flight && gi > 0) mbar_wait(afull, (gi - 1) & 1);
@@ -439,7 +445,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             uint64_t it = 0;
             uint32_t gi = 0;
             for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x, ++gi) {
-                if (!mbar_wait(afull, gi & 1)) {
+                if (!mbar_wait(afull, gi & 1, lim)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -448,11 +454,11 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     const uint32_t s = (uint32_t)(it % L::STAGES);
                     const uint32_t b = (uint32_t)(it & 1);
                     const uint64_t use_b = it >> 1;
-                    if (!mbar_wait(full + s, (uint32_t)((it / L::STAGES) & 1))) {
+                    if (!mbar_wait(full + s, (uint32_t)((it / L::STAGES) & 1), lim)) {
                         *abort_flag = 1;
                         break;
                     }
-                    if (use_b > 0 && !mbar_wait(accempty + b, (uint32_t)((use_b - 1) & 1))) {
+                    if (use_b > 0 && !mbar_wait(accempty + b, (uint32_t)((use_b - 1) & 1), lim)) {
                         *abort_flag = 1;
                         break;
                     }
@@ -477,6 +483,13 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 }
                 mma_commit(aempty);
             }
+            // drain: MMAs complete in issue order, so once the last tile's
+            // accumulator commit has arrived none is left writing TMEM or
+            // arriving on this CTA's barriers (waits with the default limit)
+            if (*abort_flag && it > 0) {
+                const uint64_t x = it - 1;
+                mbar_wait(accfull + (uint32_t)(x & 1), (uint32_t)((x >> 1) & 1));
+            }
         }
     } else {
         // ---------------- epilogue: 16 warps; warp % 4 selects the TMEM lane quarter
@@ -500,7 +513,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             }
             for (uint32_t t = 0; t < ntiles; ++t, ++it) {
                 const uint32_t b = (uint32_t)(it & 1);
-                if (!mbar_wait(accfull + b, (uint32_t)((it >> 1) & 1))) {
+                if (!mbar_wait(accfull + b, (uint32_t)((it >> 1) & 1), lim)) {
                     *abort_flag = 1;
                     break;
                 }
@@ -607,6 +620,94 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS)
                      : "memory");
     }
+}
+
+// ------------------------------------------------------------ FP32 candidate search
+// The FP32 arm: squared distances computed on the CUDA cores as
+// sum_t (q_t - c_t)^2, the re-rank's own operations in the same order
+// (dimensions past d are zero on both sides and add exactly nothing), so the
+// candidates are the exact FP32 nearest points, with no norm expansion and no
+// reduced-precision operand. One thread per query, 256 queries per block, the
+// query's coordinates in registers; points stream through shared memory in
+// tiles of F32_TILE (every thread reads the same point: broadcast loads). Each
+// query keeps its RCAND best (distance, id) in shared memory, the worst kept
+// is the rejection threshold, so most points cost one compare after the
+// distance. The other RCAND candidate slots are written empty.
+constexpr int F32_THREADS = 256;
+constexpr int F32_TILE = 64;
+
+template <int DP>
+__global__ void __launch_bounds__(F32_THREADS) k_knn_fp32(const float* __restrict__ X, uint64_t n, uint32_t d,
+                                                          uint64_t q0, uint64_t nq, uint32_t* __restrict__ cand_idx) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    float* tile = (float*)smem;                           // [F32_TILE][DP]
+    float* cs = tile + F32_TILE * DP;                     // [RCAND][F32_THREADS]
+    uint32_t* ci = (uint32_t*)(cs + RCAND * F32_THREADS);  // [RCAND][F32_THREADS]
+    const uint32_t t = threadIdx.x;
+    const uint64_t lq = (uint64_t)blockIdx.x * F32_THREADS + t;
+    const bool have = lq < nq;
+    float q[DP];
+#pragma unroll
+    for (int j = 0; j < DP; ++j) q[j] = (have && (uint32_t)j < d) ? X[(q0 + lq) * d + j] : 0.0f;
+    for (int s2 = 0; s2 < RCAND; ++s2) {
+        cs[s2 * F32_THREADS + t] = INFINITY;
+        ci[s2 * F32_THREADS + t] = 0xFFFFFFFFu;
+    }
+    float thr = INFINITY;
+    int thr_slot = 0;
+    for (uint64_t base = 0; base < n; base += F32_TILE) {
+        __syncthreads();  // the previous tile is no longer read
+        for (uint32_t e = t; e < (uint32_t)(F32_TILE * DP); e += F32_THREADS) {
+            const uint32_t p = e / DP, j = e % DP;
+            tile[e] = (base + p < n && j < d) ? X[(base + p) * d + j] : 0.0f;
+        }
+        __syncthreads();
+        const uint32_t cnt = (n - base < (uint64_t)F32_TILE) ? (uint32_t)(n - base) : (uint32_t)F32_TILE;
+        for (uint32_t p = 0; p < cnt; ++p) {
+            const float4* c4 = (const float4*)(tile + p * DP);
+            float acc = 0.0f;
+#pragma unroll
+            for (int j4 = 0; j4 < DP / 4; ++j4) {
+                const float4 c = c4[j4];
+                float df = __fsub_rn(q[4 * j4], c.x);
+                acc = __fmaf_rn(df, df, acc);
+                df = __fsub_rn(q[4 * j4 + 1], c.y);
+                acc = __fmaf_rn(df, df, acc);
+                df = __fsub_rn(q[4 * j4 + 2], c.z);
+                acc = __fmaf_rn(df, df, acc);
+                df = __fsub_rn(q[4 * j4 + 3], c.w);
+                acc = __fmaf_rn(df, df, acc);
+            }
+            if (acc < thr) {
+                cs[thr_slot * F32_THREADS + t] = acc;
+                ci[thr_slot * F32_THREADS + t] = (uint32_t)(base + p);
+                thr = -INFINITY;
+                for (int s2 = 0; s2 < RCAND; ++s2) {
+                    const float x = cs[s2 * F32_THREADS + t];
+                    if (x > thr) {
+                        thr = x;
+                        thr_slot = s2;
+                    }
+                }
+            }
+        }
+    }
+    if (have) {
+        for (int s2 = 0; s2 < RCAND; ++s2) {
+            cand_idx[lq * RTOTAL + s2] = ci[s2 * F32_THREADS + t];
+            cand_idx[lq * RTOTAL + RCAND + s2] = 0xFFFFFFFFu;
+        }
+    }
+}
+
+template <int DP>
+void candidates_fp32(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0, uint64_t nq, uint32_t* cand_idx) {
+    const size_t sm = (size_t)F32_TILE * DP * 4 + (size_t)RCAND * F32_THREADS * 8;
+    SC_CUDA(cudaFuncSetAttribute(k_knn_fp32<DP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const uint64_t blocks = (nq + F32_THREADS - 1) / F32_THREADS;
+    k_knn_fp32<DP><<<(unsigned)blocks, F32_THREADS, sm, c.stream>>>(dX, n, d, q0, nq, cand_idx);
+    SC_LAUNCH_CHECK();
+    c.launches++;
 }
 
 // ------------------------------------------------------------ exact re-rank
@@ -797,7 +898,8 @@ void launch_tc(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, uint64_t n,
     const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
     const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
     k_knn_tc<KA, F8><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
-                                                                 cand_idx, c.d_status);
+                                                                 cand_idx, c.d_status, c.wait_limit,
+                                                                 c.knn_hold_tiles);
     SC_LAUNCH_CHECK();
     c.launches++;
 }
@@ -834,25 +936,33 @@ void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
     if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
     if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
     if (n >= 0xFFFFFFFFull) fail(SC_E_TOO_MANY_NODES, "too many points");
-    if (opts.precision != SC_KNN_BF16 && opts.precision != SC_KNN_FP8)
-        fail(SC_E_UNSUPPORTED, "the candidate contraction runs in BF16 or FP8 (e4m3)");
+    if (opts.precision != SC_KNN_FP32 && opts.precision != SC_KNN_BF16 && opts.precision != SC_KNN_FP8)
+        fail(SC_E_INVALID_ARGUMENT, "unknown kNN precision %d", opts.precision);
     if (opts.precision == SC_KNN_FP8 && d > 61)
         fail(SC_E_UNSUPPORTED, "the FP8 contraction supports 1..61 dimensions, got %llu", (unsigned long long)d);
 }
 
 // Exact (brute-force) k+1 nearest points of the queries q0 .. q0 + nq - 1
 // among all n points of the device array dX: 64 candidates per query (the 32
-// best of each half of the candidate columns) from the BF16 tensor-core
-// scores, ranked exactly in FP32. idx/d2 are nq x (k+1), self first, then
-// ascending squared distance, ties by lower index.
+// best of each half of the candidate columns) from the BF16 or FP8 tensor-core
+// scores, or the 32 best exact FP32 distances from the CUDA cores, ranked
+// exactly in FP32. idx/d2 are nq x (k+1), self first, then ascending squared
+// distance, ties by lower index.
 void knn_search_device(Ctx& c, const float* dX, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t nq,
-                       bool f8, uint32_t* idx, float* d2) {
+                       int precision, uint32_t* idx, float* d2) {
     if (!nq) return;
-    DBuf<float> cscore(c, nq * RTOTAL);
+    DBuf<float> cscore(c, precision == SC_KNN_FP32 ? 0 : nq * RTOTAL);
     DBuf<uint32_t> cidx(c, nq * RTOTAL);
-    if (f8) candidates_f8(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
-    else if (d <= 30) candidates<32>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
-    else candidates<64>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    if (precision == SC_KNN_FP32) {
+        if (d <= 32) candidates_fp32<32>(c, dX, n, (uint32_t)d, q0, nq, cidx.get());
+        else candidates_fp32<64>(c, dX, n, (uint32_t)d, q0, nq, cidx.get());
+    } else if (precision == SC_KNN_FP8) {
+        candidates_f8(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    } else if (d <= 30) {
+        candidates<32>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    } else {
+        candidates<64>(c, dX, n, (uint32_t)d, q0, nq, cscore.get(), cidx.get());
+    }
     k_knn_rerank<<<grid_for(nq * 32, 256), 256, 0, c.stream>>>(dX, n, (uint32_t)d, (uint32_t)k, q0, nq,
                                                                 cidx.get(), idx, d2);
     SC_LAUNCH_CHECK();
@@ -938,7 +1048,7 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, co
     upload(c, dX.get(), X, n * d * sizeof(float));
     DBuf<uint32_t> idx(c, n * (k + 1));
     DBuf<float> d2(c, n * (k + 1));
-    knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
+    knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision, idx.get(), d2.get());
     copy_lists_out(c, idx.get(), d2.get(), n, k, opts.squared_kiddo, knn_index, knn_dist);
     if (!conn_ptrs && !graph_out) return;
     knn_connectivities_device(c, idx.get(), d2.get(), n, k, opts, conn_ptrs, conn_nbrs, conn_w, conn_cap, conn_nnz,
@@ -957,7 +1067,7 @@ void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint
     upload(c, dX.get(), X, n * d * sizeof(float));
     DBuf<uint32_t> idx(c, nq * (k + 1));
     DBuf<float> d2(c, nq * (k + 1));
-    knn_search_device(c, dX.get(), n, d, k, q0, nq, opts.precision == SC_KNN_FP8, idx.get(), d2.get());
+    knn_search_device(c, dX.get(), n, d, k, q0, nq, opts.precision, idx.get(), d2.get());
     copy_lists_out(c, idx.get(), d2.get(), nq, k, 1, knn_index, knn_d2);
 }
 

@@ -27,21 +27,48 @@ constexpr uint32_t STATIC_TAIL = 8;                     // result and flags
 __device__ __align__(256) double g_static_scratch[2 * STATIC_MAX_COMMUNITIES + STATIC_TAIL];
 
 constexpr int MAX_DEVICES = 64;
-double* g_scratch_addr[MAX_DEVICES];
+// Per device: the address of g_static_scratch and the CUDA context it was looked
+// up in. A context that is destroyed and re-created (cudaDeviceReset, or the
+// primary context released and retained again) maps the array afresh, so the
+// address is looked up again whenever the current context is not the cached one.
+struct ScratchAddr {
+    void* ctx = nullptr;
+    double* addr = nullptr;
+};
+ScratchAddr g_scratch_addr[MAX_DEVICES];
 std::mutex g_scratch_mu;
 
+using CtxGetCurrentFn = int (*)(void**);  // cuCtxGetCurrent(CUcontext*)
+
+void* current_context() {
+    static CtxGetCurrentFn fn = [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            p = nullptr;
+        return (CtxGetCurrentFn)p;
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) fail(SC_E_CUDA, "cuCtxGetCurrent is unavailable");
+    return ctx;
+}
+
 // Host code must not use g_static_scratch's name as a device address: look the
-// address up once per device, with that device current.
+// address up with the device current, once per device and context.
 double* scratch_for(int device) {
     if (device < 0 || device >= MAX_DEVICES) fail(SC_E_INVALID_ARGUMENT, "device %d out of range", device);
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_addr[device]) {
+    ScratchAddr& a = g_scratch_addr[device];
+    if (!a.addr || a.ctx != ctx) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) throw_cuda(e, "cudaGetSymbolAddress(g_static_scratch)", __FILE__, __LINE__);
-        g_scratch_addr[device] = (double*)p;
+        a.addr = (double*)p;
+        a.ctx = ctx;
     }
-    return g_scratch_addr[device];
+    return a.addr;
 }
 
 __global__ void k_static_clear(double* scratch) {

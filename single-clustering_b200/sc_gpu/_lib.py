@@ -103,6 +103,9 @@ SIGNATURES = [
     ("sc_tuning_default", None, [C.POINTER(Tuning)]),
     ("sc_get_tuning", C.c_int, [vp, C.POINTER(Tuning)]),
     ("sc_set_tuning", C.c_int, [vp, C.POINTER(Tuning)]),
+    ("sc_set_wait_limit", C.c_int, [vp, C.c_uint32]),
+    ("sc_get_wait_limit", C.c_int, [vp, C.POINTER(C.c_uint32)]),
+    ("sc_test_knn_hold_tiles", C.c_int, [vp, C.c_int32]),
     ("sc_autotune", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), C.POINTER(Tuning), f64p, f64p,
                               C.POINTER(C.c_uint32)]),
     ("sc_leiden_config_default", None, [C.POINTER(LeidenConfigC)]),

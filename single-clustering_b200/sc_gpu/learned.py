@@ -155,25 +155,35 @@ class WarmStartResult:
 def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
                       verify: bool = True, tolerance: float = 1e-4, context=None) -> WarmStartResult:
     """leiden_from(model's proposal). With `verify`, the plain singleton start also
-    runs and the proposal is kept only if its final modularity is at least the
-    plain one minus `tolerance`; otherwise the plain result is returned.
+    runs and the proposal is kept only if its final modularity (for CPM: its CPM
+    quality / total weight) is at least the plain one's minus `tolerance`;
+    otherwise the plain result is returned.
     `context` is (coarse, fine), the partitions at the neighbouring lower and
     higher resolutions the model was trained to read."""
-    from . import leiden, leiden_from, modularity, Rb
-    gamma = config.objective.resolution if isinstance(config.objective, Rb) else 1.0
+    from . import leiden, leiden_from, modularity, quality, Rb
+    is_rb = isinstance(config.objective, Rb)
+    gamma = config.objective.resolution if is_rb else 1.0
+
+    def score(labels):
+        # the quantity the run optimises: modularity at gamma for RB; for CPM its
+        # quality (Partition::from_membership then Cpm::quality) per unit of total
+        # edge weight, the scale modularity has, so one tolerance serves both
+        if is_rb:
+            return modularity(graph, labels, gamma)
+        return quality(graph, labels, config.objective) / max(graph.total_weight(), 1e-300)
     t0 = time.perf_counter()
     prop, kprop = model.propose(graph, gamma, threshold, core_fraction, context=context)
     t_prop = (time.perf_counter() - t0) * 1e3
     warm = leiden_from(graph, config, prop)
     sw = graph._ctx.run_stats()
-    q_w = modularity(graph, warm.labels(), gamma)
+    q_w = score(warm.labels())
     res = WarmStartResult(warm.labels(), warm.n_clusters(), True, q_w, None, sw["local_move_sweeps"], None,
                           t_prop + sw["ms_total"], None, kprop)
     if not verify:
         return res
     plain = leiden(graph, config)
     sp = graph._ctx.run_stats()
-    q_p = modularity(graph, plain.labels(), gamma)
+    q_p = score(plain.labels())
     res.q_plain, res.sweeps_plain, res.ms_plain = q_p, sp["local_move_sweeps"], sp["ms_total"]
     if q_w < q_p - tolerance:
         res.labels, res.n_clusters, res.used_proposal = plain.labels(), plain.n_clusters(), False

@@ -112,3 +112,108 @@ def knn_like_graph(n: int, k: int = 10, blocks: int = 100, seed: int = 7):
     ptrs = np.zeros(n + 1, dtype=np.uint64)
     np.cumsum(np.bincount(rows, minlength=n), out=ptrs[1:])
     return ptrs, cols.astype(np.uint32), ww
+
+
+def knn_graph_exact_torch(X, groups, k: int, device, chunk: int = 4096, margin: int = 8):
+    """Exact kNN graph of the points X built with torch alone (no call into this
+    library), for benchmark inputs that must not depend on the code under test:
+    k nearest points by FP64 distance (ties by lower index, the point itself
+    first), Gaussian weights with sigma = the k-th neighbour's distance
+    (w = sqrt(2 s_i s_j / (s_i^2 + s_j^2)) exp(-d^2 / (s_i^2 + s_j^2)), kept if
+    > 1e-14), union symmetrisation, f32 weights. Returns (ptrs u64, nbrs u32,
+    w f32, index (n, k+1) int64, dist (n, k+1) float64).
+
+    `groups` (one id per point, e.g. the mixture component) only orders the
+    search: each query first searches its own group, then every other group
+    whose ball bound |q - centre_g| - radius_g is at most its current k-th
+    distance. The bound is a true lower bound on the distance to any member,
+    so the result is exact whatever the grouping."""
+    import torch
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    groups = np.asarray(groups)
+    n, d = X.shape
+    order = np.argsort(groups, kind="stable")
+    gs = groups[order]
+    bounds = np.flatnonzero(np.r_[True, gs[1:] != gs[:-1], True])
+    starts, ends = bounds[:-1], bounds[1:]
+    G = len(starts)
+    xs = torch.from_numpy(X[order]).to(device, torch.float64)
+    orig = torch.from_numpy(order.astype(np.int64)).to(device)
+    nrm = (xs * xs).sum(1)
+    cen = torch.stack([xs[a:b].mean(0) for a, b in zip(starts, ends)])
+    rad = torch.stack([((xs[a:b] - cen[g]) ** 2).sum(1).max().sqrt() for g, (a, b) in enumerate(zip(starts, ends))])
+    rad = rad * (1 + 1e-12) + 1e-12
+    kk = k + 1 + margin
+    out_i = torch.empty((n, k + 1), dtype=torch.int64, device=device)
+    out_d = torch.empty((n, k + 1), dtype=torch.float64, device=device)
+    for g in range(G):
+        a, b = int(starts[g]), int(ends[g])
+        for s in range(a, b, chunk):
+            e = min(b, s + chunk)
+            q = xs[s:e]
+
+            def cands(pa, pb):
+                d2 = nrm[s:e, None] + nrm[None, pa:pb] - 2.0 * (q @ xs[pa:pb].T)
+                m = min(kk, pb - pa)
+                _, j = torch.topk(d2, m, dim=1, largest=False)
+                return j + pa
+
+            pool = [cands(a, b)]
+
+            def exact(pool_idx):
+                dd = ((xs[pool_idx] - q[:, None, :]) ** 2).sum(-1)
+                return dd
+
+            idx = torch.cat(pool, 1)
+            dd = exact(idx)
+            kth = torch.sort(dd, 1).values[:, min(k, idx.shape[1] - 1)].sqrt()
+            if idx.shape[1] < k + 1:
+                kth = torch.full_like(kth, float("inf"))
+            lb = torch.cdist(q, cen) - rad[None, :]
+            need = (lb <= kth[:, None] * (1 + 1e-9)).any(0)
+            need[g] = False
+            for h in torch.nonzero(need).flatten().tolist():
+                pool.append(cands(int(starts[h]), int(ends[h])))
+            if len(pool) > 1:
+                idx = torch.cat(pool, 1)
+                dd = exact(idx)
+            oi = orig[idx]
+            selfq = orig[s:e]
+            # (distance, self first, original index): a stable sort by index, then by the tag, then by distance
+            o1 = torch.argsort(oi, dim=1, stable=True)
+            oi, dd = torch.gather(oi, 1, o1), torch.gather(dd, 1, o1)
+            o2 = torch.argsort((oi != selfq[:, None]).to(torch.int8), dim=1, stable=True)
+            oi, dd = torch.gather(oi, 1, o2), torch.gather(dd, 1, o2)
+            o3 = torch.argsort(dd, dim=1, stable=True)
+            oi, dd = torch.gather(oi, 1, o3)[:, : k + 1], torch.gather(dd, 1, o3)[:, : k + 1]
+            out_i[selfq] = oi
+            out_d[selfq] = dd.sqrt()
+    sig = out_d[:, k]
+    rows = torch.arange(n, device=device).repeat_interleave(k)
+    cols = out_i[:, 1:].reshape(-1)
+    dd = out_d[:, 1:].reshape(-1)
+    si, sj = sig[rows], sig[cols]
+    den = si * si + sj * sj
+    w = torch.sqrt(2 * si * sj / den) * torch.exp(-dd * dd / den)
+    keep = (rows != cols) & (w > 1e-14)
+    rows, cols, w = rows[keep], cols[keep], w[keep]
+    lo, hi = torch.minimum(rows, cols), torch.maximum(rows, cols)
+    key, o = torch.sort(lo * n + hi, stable=True)
+    w = w[o]
+    first = torch.ones_like(key, dtype=torch.bool)
+    first[1:] = key[1:] != key[:-1]
+    key, w = key[first], w[first]
+    lo, hi = key // n, key % n
+    r = torch.cat([lo, hi])
+    c = torch.cat([hi, lo])
+    ww = torch.cat([w, w]).float()
+    _, o = torch.sort(r * n + c)
+    r, c, ww = r[o], c[o], ww[o]
+    ptr = torch.zeros(n + 1, dtype=torch.int64, device=device)
+    ptr[1:] = torch.cumsum(torch.bincount(r, minlength=n), 0)
+    res = (ptr.cpu().numpy().astype(np.uint64), c.to(torch.int32).cpu().numpy().view(np.uint32).copy(),
+           ww.cpu().numpy(), out_i.cpu().numpy(), out_d.cpu().numpy())
+    del xs, nrm, out_i, out_d
+    if str(device).startswith("cuda"):
+        torch.cuda.empty_cache()
+    return res

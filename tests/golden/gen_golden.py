@@ -9,7 +9,7 @@ Outputs
                               (10 graphs, 160 cases: leidenalg quality and
                               igraph modularity of a given membership)
 
-Usage: python tests/golden/gen_golden.py [/path/to/single-clustering]
+Usage: python tests/golden/gen_golden.py /path/to/single-clustering
 """
 import gzip
 import json
@@ -29,7 +29,9 @@ def parse_karate(testdata_rs: str):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_golden.py /path/to/single-clustering (the reference source tree)")
+    ref = sys.argv[1]
     with open(os.path.join(ref, "src", "testdata.rs")) as f:
         edges, optimum = parse_karate(f.read())
     assert len(edges) == 78 and len(optimum) == 34, (len(edges), len(optimum))

@@ -4,6 +4,8 @@ Bar: neighbour sets equal the FP64 exact search's except for distance ties
 within 1e-6 relative; connectivity weights within 1e-5 relative of the FP64
 formula evaluated on the GPU's own neighbour lists.
 """
+import ctypes as C
+
 import numpy as np
 import pytest
 
@@ -185,3 +187,51 @@ def test_empty_point_set():
     X = np.zeros((0, 8), np.float32)
     r = sc_gpu.knn_gaussian(X, 5)
     assert r.index.shape == (0, 6) and len(r.conn_w) == 0 and len(r.conn_ptrs) == 1
+
+
+def test_bounded_wait_gives_up_and_the_context_stays_usable():
+    """The kNN kernel's bounded waits, driven to their limit without a fault:
+    with the test hook on, the producer never issues a point tile, so the MMA
+    issuer's and the epilogue's waits (limit 4 tries) run out; the kernel drains
+    the query-tile copies it did issue, frees its tensor memory and returns, and
+    the call fails with SC_E_TIMEOUT. The same context then builds the graph
+    correctly."""
+    from sc_gpu import _lib
+    L = _lib.lib()
+    ctx = sc_gpu.context(0)
+    X, _ = synth.gaussian_mixture(2000, 30, 4, seed=5, sigma=(0.7, 1.5))
+    default = C.c_uint32()
+    assert L.sc_get_wait_limit(ctx.h, C.byref(default)) == 0 and default.value == 1 << 26
+    assert L.sc_set_wait_limit(ctx.h, 0) == 20  # SC_E_INVALID_ARGUMENT
+    assert L.sc_set_wait_limit(ctx.h, 4) == 0
+    assert L.sc_test_knn_hold_tiles(ctx.h, 1) == 0
+    try:
+        with pytest.raises(sc_gpu.DeviceError) as e:
+            sc_gpu.knn_gaussian(X, 10)
+        assert e.value.status == 23  # SC_E_TIMEOUT
+        assert "bounded device wait" in L.sc_last_error_message(ctx.h).decode()
+    finally:
+        L.sc_test_knn_hold_tiles(ctx.h, 0)
+        L.sc_set_wait_limit(ctx.h, default.value)
+    r = sc_gpu.knn_gaussian(X, 10)
+    idx_t, dist_t = K.knn_exact(X, 10)
+    assert check_sets(r.index, idx_t, dist_t, X) == 0
+
+
+@pytest.mark.parametrize("n,d,k", [(3000, 50, 15), (1000, 30, 10), (777, 7, 5), (300, 62, 10), (33, 3, 31)])
+def test_fp32_candidates_match_exact_fp64(n, d, k):
+    """FP32 arm: candidate distances on the CUDA cores by exact differences (the
+    re-rank's arithmetic), so the returned lists are the exact FP32 nearest
+    points: equal to the FP64 search except for ties within 1e-6 relative, and
+    identical to the BF16 arm's lists wherever the BF16 candidates held the
+    true neighbours (all of them on these mixtures)."""
+    X, _ = synth.gaussian_mixture(n, d, 8, seed=n + d + 7, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=sc_gpu.KNN_FP32)
+    idx_t, dist_t = K.knn_exact(X, k)
+    assert np.all(r.index[:, 0] == np.arange(n)), "self first"
+    assert check_sets(r.index[:, : min(k + 1, n)], idx_t, dist_t, X) == 0
+    d64 = K.exact_dist_matrix_rows(X, np.arange(n)[:, None], r.index.astype(np.int64))
+    assert np.allclose(r.distances, d64, rtol=1e-5, atol=1e-6)
+    b = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=sc_gpu.KNN_BF16)
+    assert np.array_equal(b.index, r.index)
+    assert np.array_equal(b.conn_w.view(np.uint32), r.conn_w.view(np.uint32))

@@ -1,6 +1,7 @@
 """The seeded synthetic workloads: same bytes for the same seed, and the
 shapes the benchmark configurations name (checked on the CPU)."""
 import numpy as np
+import pytest
 
 from sc_gpu import synth
 
@@ -40,3 +41,22 @@ def test_gaussian_mixture_is_seeded():
     assert x1.dtype == np.float32 and x1.shape == (5000, 7)
     assert np.array_equal(x1, x2) and np.array_equal(c1, c2)
     assert set(np.unique(c1)) <= set(range(4))
+
+
+@pytest.mark.parametrize("n,d,comps,k", [(4000, 30, 10, 10), (2500, 50, 3, 15), (300, 7, 40, 5)])
+def test_exact_torch_knn_graph_matches_the_fp64_oracle(n, d, comps, k):
+    """The benchmark's library-free input builder: its k+1 lists equal the FP64
+    oracle's (pruning by ball bounds is exact for any grouping), and its graph is
+    the oracle's union-symmetrised Gaussian connectivities (sigma = k-th
+    distance) rounded to f32."""
+    import knn_oracle as K
+    X, comp = synth.gaussian_mixture(n, d, comps, seed=n + d, sigma=(0.7, 1.5))
+    it, dt = K.knn_exact(X, k)
+    for groups in (comp, np.random.default_rng(0).integers(0, 7, n)):
+        ptr, nbr, w, idx, dist = synth.knn_graph_exact_torch(X, groups, k, "cpu", chunk=700)
+        assert np.array_equal(idx, it)
+        assert np.abs(dist - dt).max() < 1e-12
+    r, c, ww = K.connectivities(it, dt, K.sigmas(dt, kth=True), union=True)
+    rows = np.repeat(np.arange(n), np.diff(ptr).astype(np.int64))
+    assert np.array_equal(rows, r) and np.array_equal(nbr, c)
+    assert np.array_equal(w, ww.astype(np.float32))

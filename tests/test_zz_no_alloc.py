@@ -60,6 +60,46 @@ def test_static_modularity_matches_allocating_entry_point_twice():
                 assert np.float64(got).view(np.uint64) == np.float64(want).view(np.uint64), (got, want)
 
 
+def _pool_used():
+    from cuda.bindings import runtime as rt
+    err, pool = rt.cudaDeviceGetDefaultMemPool(0)
+    assert int(err) == 0
+    rt.cudaDeviceSynchronize()
+    err, v = rt.cudaMemPoolGetAttribute(pool, rt.cudaMemPoolAttr.cudaMemPoolAttrUsedMemCurrent)
+    assert int(err) == 0
+    return int(v)
+
+
+def _device_free():
+    from cuda.bindings import runtime as rt
+    rt.cudaDeviceSynchronize()
+    err, free, _total = rt.cudaMemGetInfo()
+    assert int(err) == 0
+    return int(free)
+
+
+def test_static_modularity_allocates_nothing():
+    """The property the entry point exists for: after one warm-up call (which
+    loads the kernels and looks up the scratch address), further calls leave the
+    device's default pool (where every other entry point of the library takes
+    its temporaries) and the device's free memory exactly as they were."""
+    import sc_gpu
+    from sc_gpu import synth
+    src, dst, w, truth = synth.planted_partition()
+    g = sc_gpu.CSRNetwork.from_edge_arrays(20000, src, dst, w)
+    d = _device_labels(truth)
+    rc, first = _static_modularity(g, d, 20000, 1.0)
+    assert rc == 0
+    used0, free0 = _pool_used(), _device_free()
+    for gamma in (1.0, 0.5, 2.0, 1.0, 1.0):
+        rc, got = _static_modularity(g, d, 20000, gamma)
+        assert rc == 0
+    used1, free1 = _pool_used(), _device_free()
+    assert used1 == used0, (used0, used1)
+    assert free1 == free0, (free0, free1)
+    assert got == first
+
+
 def test_static_modularity_rejects_labels_past_its_limit():
     import sc_gpu
     from sc_gpu import _lib
