@@ -123,71 +123,105 @@ def knn_graph_exact_torch(X, groups, k: int, device, chunk: int = 4096, margin: 
     > 1e-14), union symmetrisation, f32 weights. Returns (ptrs u64, nbrs u32,
     w f32, index (n, k+1) int64, dist (n, k+1) float64).
 
-    `groups` (one id per point, e.g. the mixture component) only orders the
-    search: each query first searches its own group, then every other group
-    whose ball bound |q - centre_g| - radius_g is at most its current k-th
-    distance. The bound is a true lower bound on the distance to any member,
-    so the result is exact whatever the grouping."""
+    `groups` (one id per point, e.g. the mixture component) only organises the
+    search; the result is exact whatever the grouping. Each query first searches
+    its own group; then group h is searched by exactly the queries whose lower
+    bound on the distance to any member of h is at most their current k-th
+    distance. The bound is the larger of a ball bound (distance to h's centre
+    minus h's radius) and a slab bound: with u the unit vector from the query's
+    group centre to h's, every member x of h projects into [lo, hi] on u, and
+    |q - x| >= the distance from <q, u> to that interval. Candidates come from
+    FP32 scores |c|^2 - 2 q.c (TF32 off) with `margin` spares, then exact FP64
+    differences rank them."""
     import torch
+    torch.backends.cuda.matmul.allow_tf32 = False
     X = np.ascontiguousarray(X, dtype=np.float32)
     groups = np.asarray(groups)
     n, d = X.shape
     order = np.argsort(groups, kind="stable")
     gs = groups[order]
     bounds = np.flatnonzero(np.r_[True, gs[1:] != gs[:-1], True])
-    starts, ends = bounds[:-1], bounds[1:]
+    starts, ends = bounds[:-1].tolist(), bounds[1:].tolist()
     G = len(starts)
-    xs = torch.from_numpy(X[order]).to(device, torch.float64)
+    x32 = torch.from_numpy(X[order]).to(device)
+    x64 = x32.to(torch.float64)
     orig = torch.from_numpy(order.astype(np.int64)).to(device)
-    nrm = (xs * xs).sum(1)
-    cen = torch.stack([xs[a:b].mean(0) for a, b in zip(starts, ends)])
-    rad = torch.stack([((xs[a:b] - cen[g]) ** 2).sum(1).max().sqrt() for g, (a, b) in enumerate(zip(starts, ends))])
-    rad = rad * (1 + 1e-12) + 1e-12
+    nrm32 = (x32 * x32).sum(1)
+    gid = torch.empty(n, dtype=torch.int64, device=device)
+    for g, (a, b) in enumerate(zip(starts, ends)):
+        gid[a:b] = g
+    cen = torch.stack([x64[a:b].mean(0) for a, b in zip(starts, ends)])
+    rad = torch.stack([((x64[a:b] - cen[g]) ** 2).sum(1).max().sqrt() for g, (a, b) in enumerate(zip(starts, ends))])
+    # unit directions between group centres (zero when two centres coincide)
+    diff = cen[None, :, :] - cen[:, None, :]
+    ln = diff.norm(dim=2, keepdim=True)
+    U = torch.where(ln > 0, diff / torch.where(ln > 0, ln, torch.ones_like(ln)), torch.zeros_like(diff))  # U[a, h]
+    lo = torch.empty((G, G), dtype=torch.float64, device=device)
+    hi = torch.empty((G, G), dtype=torch.float64, device=device)
+    for h, (a, b) in enumerate(zip(starts, ends)):
+        pr = x64[a:b] @ U[:, h, :].T  # (|h|, G): member projections on every u_{g,h}
+        lo[:, h] = pr.min(0).values
+        hi[:, h] = pr.max(0).values
     kk = k + 1 + margin
+    best_i = torch.empty((n, k + 1), dtype=torch.int64, device=device)  # sorted positions
+    best_d = torch.empty((n, k + 1), dtype=torch.float64, device=device)
+
+    def candidates(qpos, a, b):
+        """FP32 top-kk positions in [a, b) for the queries at sorted positions qpos."""
+        out = []
+        for s in range(0, len(qpos), chunk):
+            qp = qpos[s:s + chunk]
+            sc = torch.addmm(nrm32[None, a:b], x32[qp], x32[a:b].T, beta=1.0, alpha=-2.0)
+            _, j = torch.topk(sc, min(kk, b - a), dim=1, largest=False)
+            out.append(j + a)
+        return torch.cat(out)
+
+    def rank(qpos, cand):
+        """Exact FP64 (distance, self first, original index) order of the candidate
+        positions (-1: an empty slot, ordered last); returns the first k+1 as
+        (positions, d2), empty slots as (-1, +inf)."""
+        valid = cand >= 0
+        cc = cand.clamp(min=0)
+        dd = ((x64[cc] - x64[qpos][:, None, :]) ** 2).sum(-1)
+        dd = torch.where(valid, dd, torch.full_like(dd, float("inf")))
+        oi = torch.where(valid, orig[cc], torch.full_like(cc, n))
+        o = torch.argsort(oi, dim=1, stable=True)
+        cand, dd, oi = torch.gather(cand, 1, o), torch.gather(dd, 1, o), torch.gather(oi, 1, o)
+        o = torch.argsort((oi != orig[qpos][:, None]).to(torch.int8), dim=1, stable=True)
+        cand, dd = torch.gather(cand, 1, o), torch.gather(dd, 1, o)
+        o = torch.argsort(dd, dim=1, stable=True)
+        cand, dd = torch.gather(cand, 1, o)[:, : k + 1], torch.gather(dd, 1, o)[:, : k + 1]
+        if cand.shape[1] < k + 1:
+            pad = k + 1 - cand.shape[1]
+            cand = torch.cat([cand, torch.full((len(qpos), pad), -1, dtype=torch.int64, device=device)], 1)
+            dd = torch.cat([dd, torch.full((len(qpos), pad), float("inf"), dtype=torch.float64, device=device)], 1)
+        cand = torch.where(torch.isfinite(dd), cand, torch.full_like(cand, -1))
+        return cand, dd
+
+    # 1) every query against its own group
+    for g, (a, b) in enumerate(zip(starts, ends)):
+        qpos = torch.arange(a, b, device=device)
+        c, dd = rank(qpos, candidates(qpos, a, b))
+        best_i[a:b], best_d[a:b] = c, dd
+    # 2) every other group h, searched by the queries whose bound does not exclude it
+    kth = best_d[:, k].sqrt()
+    for h, (a, b) in enumerate(zip(starts, ends)):
+        ga = gid  # the query's own group
+        pq = (x64 * U[ga, h, :]).sum(1)
+        slab = torch.clamp(torch.maximum(lo[ga, h] - pq, pq - hi[ga, h]), min=0.0)
+        ball = torch.clamp((x64 - cen[h]).norm(dim=1) - rad[h], min=0.0)
+        lb = torch.maximum(slab, ball) * (1.0 - 1e-9)
+        need = (lb <= kth) & (ga != h)
+        qpos = torch.nonzero(need).flatten()
+        if len(qpos) == 0:
+            continue
+        # the current best (from groups searched before, never h) and h's candidates
+        cand = torch.cat([best_i[qpos], candidates(qpos, a, b)], 1)
+        best_i[qpos], best_d[qpos] = rank(qpos, cand)
     out_i = torch.empty((n, k + 1), dtype=torch.int64, device=device)
     out_d = torch.empty((n, k + 1), dtype=torch.float64, device=device)
-    for g in range(G):
-        a, b = int(starts[g]), int(ends[g])
-        for s in range(a, b, chunk):
-            e = min(b, s + chunk)
-            q = xs[s:e]
-
-            def cands(pa, pb):
-                d2 = nrm[s:e, None] + nrm[None, pa:pb] - 2.0 * (q @ xs[pa:pb].T)
-                m = min(kk, pb - pa)
-                _, j = torch.topk(d2, m, dim=1, largest=False)
-                return j + pa
-
-            pool = [cands(a, b)]
-
-            def exact(pool_idx):
-                dd = ((xs[pool_idx] - q[:, None, :]) ** 2).sum(-1)
-                return dd
-
-            idx = torch.cat(pool, 1)
-            dd = exact(idx)
-            kth = torch.sort(dd, 1).values[:, min(k, idx.shape[1] - 1)].sqrt()
-            if idx.shape[1] < k + 1:
-                kth = torch.full_like(kth, float("inf"))
-            lb = torch.cdist(q, cen) - rad[None, :]
-            need = (lb <= kth[:, None] * (1 + 1e-9)).any(0)
-            need[g] = False
-            for h in torch.nonzero(need).flatten().tolist():
-                pool.append(cands(int(starts[h]), int(ends[h])))
-            if len(pool) > 1:
-                idx = torch.cat(pool, 1)
-                dd = exact(idx)
-            oi = orig[idx]
-            selfq = orig[s:e]
-            # (distance, self first, original index): a stable sort by index, then by the tag, then by distance
-            o1 = torch.argsort(oi, dim=1, stable=True)
-            oi, dd = torch.gather(oi, 1, o1), torch.gather(dd, 1, o1)
-            o2 = torch.argsort((oi != selfq[:, None]).to(torch.int8), dim=1, stable=True)
-            oi, dd = torch.gather(oi, 1, o2), torch.gather(dd, 1, o2)
-            o3 = torch.argsort(dd, dim=1, stable=True)
-            oi, dd = torch.gather(oi, 1, o3)[:, : k + 1], torch.gather(dd, 1, o3)[:, : k + 1]
-            out_i[selfq] = oi
-            out_d[selfq] = dd.sqrt()
+    out_i[orig] = torch.where(best_i >= 0, orig[best_i.clamp(min=0)], torch.full_like(best_i, -1))
+    out_d[orig] = best_d.sqrt()
     sig = out_d[:, k]
     rows = torch.arange(n, device=device).repeat_interleave(k)
     cols = out_i[:, 1:].reshape(-1)
@@ -197,15 +231,15 @@ def knn_graph_exact_torch(X, groups, k: int, device, chunk: int = 4096, margin: 
     w = torch.sqrt(2 * si * sj / den) * torch.exp(-dd * dd / den)
     keep = (rows != cols) & (w > 1e-14)
     rows, cols, w = rows[keep], cols[keep], w[keep]
-    lo, hi = torch.minimum(rows, cols), torch.maximum(rows, cols)
-    key, o = torch.sort(lo * n + hi, stable=True)
+    lo_, hi_ = torch.minimum(rows, cols), torch.maximum(rows, cols)
+    key, o = torch.sort(lo_ * n + hi_, stable=True)
     w = w[o]
     first = torch.ones_like(key, dtype=torch.bool)
     first[1:] = key[1:] != key[:-1]
     key, w = key[first], w[first]
-    lo, hi = key // n, key % n
-    r = torch.cat([lo, hi])
-    c = torch.cat([hi, lo])
+    lo_, hi_ = key // n, key % n
+    r = torch.cat([lo_, hi_])
+    c = torch.cat([hi_, lo_])
     ww = torch.cat([w, w]).float()
     _, o = torch.sort(r * n + c)
     r, c, ww = r[o], c[o], ww[o]
@@ -213,7 +247,8 @@ def knn_graph_exact_torch(X, groups, k: int, device, chunk: int = 4096, margin: 
     ptr[1:] = torch.cumsum(torch.bincount(r, minlength=n), 0)
     res = (ptr.cpu().numpy().astype(np.uint64), c.to(torch.int32).cpu().numpy().view(np.uint32).copy(),
            ww.cpu().numpy(), out_i.cpu().numpy(), out_d.cpu().numpy())
-    del xs, nrm, out_i, out_d
+    del x32, x64, out_i, out_d, best_i, best_d
     if str(device).startswith("cuda"):
         torch.cuda.empty_cache()
     return res
+

@@ -150,8 +150,9 @@ def test_precision_limits():
     X, _ = synth.gaussian_mixture(200, 62, 3, seed=2)
     with pytest.raises(sc_gpu.ClusteringError):
         sc_gpu.knn_gaussian(X, 5, precision=sc_gpu.KNN_FP8)  # 62 dims need 65 e4m3 columns
-    with pytest.raises(sc_gpu.ClusteringError):
-        sc_gpu.knn_gaussian(X[:, :20], 5, precision=sc_gpu.KNN_FP32)
+    with pytest.raises(sc_gpu.ClusteringError) as e:
+        sc_gpu.knn_gaussian(X[:, :20], 5, precision=7)
+    assert e.value.status == 20  # SC_E_INVALID_ARGUMENT: no such precision
 
 
 @pytest.mark.parametrize("n", [1, 2, 5, 11])
