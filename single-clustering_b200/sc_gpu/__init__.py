@@ -477,7 +477,7 @@ def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig], 
 
 
 def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb, warm_start: bool = True,
-               base: LeidenConfig | None = None, split: int = 1):
+               base: LeidenConfig | None = None, split: int = 1, warm_passes: int | None = 1):
     """Configs and warm-start links of a resolution x seed sweep.
 
     Instances are ordered seed-major with resolutions descending; with warm_start
@@ -486,7 +486,10 @@ def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb,
     split = k each seed's chain is cut into k contiguous pieces: the first piece
     starts from singletons, the head of every other piece from the first
     instance of the seed (the finest resolution), so k pieces per seed run
-    concurrently. Returns (configs, warm_from, keys)."""
+    concurrently. A warm-started instance runs `warm_passes` passes (its start
+    stands in for the first pass of a plain run, which takes a singleton start
+    to a converged partition); None keeps the base config's n_iterations.
+    Returns (configs, warm_from, keys)."""
     base = base or LeidenConfig()
     res = sorted(resolutions, reverse=True)
     split = max(1, min(int(split), len(res))) if res else 1
@@ -496,8 +499,10 @@ def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb,
     for s in seeds:
         first = len(configs)
         for j, r in enumerate(res):
-            cfg = LeidenConfig(**{**base.__dict__, "objective": objective(r), "seed": int(s)})
-            configs.append(cfg)
+            fields = {**base.__dict__, "objective": objective(r), "seed": int(s)}
+            if warm_start and j > 0 and warm_passes is not None:
+                fields["n_iterations"] = int(warm_passes)
+            configs.append(LeidenConfig(**fields))
             if not warm_start or j == 0:
                 warm.append(-1)
             elif j in heads:
@@ -509,9 +514,10 @@ def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb,
 
 
 def leiden_sweep(graph: CSRNetwork, resolutions, seeds, objective=Rb, warm_start: bool = True,
-                 n_streams: int = 0, base: LeidenConfig | None = None, split: int = 1) -> dict:
+                 n_streams: int = 0, base: LeidenConfig | None = None, split: int = 1,
+                 warm_passes: int | None = 1) -> dict:
     """Resolution x seed sweep on one graph: {(resolution, seed): Clustering}."""
-    configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base, split)
+    configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base, split, warm_passes)
     res = leiden_batch([graph] * len(configs), configs, warm if warm_start else None, n_streams)
     return dict(zip(keys, res))
 

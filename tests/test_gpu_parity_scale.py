@@ -60,14 +60,17 @@ def assert_same_evaluation(og, gg, part, what):
         assert np.array_equal(bits(a[key]), bits(b[key])), (what, key)
 
 
-def test_aggregate_and_evaluation_bit_exact_on_a_million_point_knn_graph():
+@pytest.fixture(scope="module")
+def knn_million():
     X, _ = synth.gaussian_mixture(1_000_000, 30, 100, seed=17, sigma=(0.7, 1.5))
     r = sc_gpu.knn_gaussian(X, 10, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
-    del X
-    og = O.Graph.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w)
-    gg = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w)
+    return r.conn_ptrs, r.conn_nbrs, r.conn_w
+
+
+def check_levels(ptrs, nbrs, w):
+    og = O.Graph.from_csr_parts(ptrs, nbrs, w)
+    gg = sc_gpu.CSRNetwork.from_csr_parts(ptrs, nbrs, w)
     assert_same_graph(og, gg, "level-0 graph")
-    assert outside_exact_regime(r.conn_w, gg.total_weight())
     # level 0: the oracle's local-moving partition from singletons
     n = og.node_count()
     part0, _ = og.local_move(np.arange(n, dtype=np.uint64), O.RB, 1.0, seed=3)
@@ -84,6 +87,29 @@ def test_aggregate_and_evaluation_bit_exact_on_a_million_point_knn_graph():
     coarse = (part0 % 7).astype(np.uint64)
     assert_same_evaluation(og, gg, coarse, "7 groups")
     assert_same_graph(og.aggregate(coarse), gg.aggregate(coarse), "7-group graph")
+    return gg
+
+
+def test_bit_exact_on_a_million_point_knn_graph(knn_million):
+    """The Gaussian kNN graph itself (sigma = k-th distance keeps every weight in
+    about [0.3, 1]): inside the exact regime, where aggregation may take its
+    hashed contraction path."""
+    ptrs, nbrs, w = knn_million
+    gg = check_levels(ptrs, nbrs, w)
+    assert not outside_exact_regime(w, gg.total_weight())
+
+
+def test_bit_exact_outside_the_exact_regime_at_scale(knn_million):
+    """The same graph with every weight raised to the 40th power (still
+    symmetric, now spanning some 70 binades): f64 sums round, so aggregation
+    takes the ordered sort path with long segments split across blocks, and the
+    per-community sums their ordered chains."""
+    ptrs, nbrs, w = knn_million
+    w40 = np.power(w.astype(np.float64), 40).astype(np.float32)
+    keep = w40 > 0
+    assert keep.all()
+    gg = check_levels(ptrs, nbrs, w40)
+    assert outside_exact_regime(w40, gg.total_weight())
 
 
 def _planted():

@@ -37,6 +37,13 @@ def test_sweep_plan_chains_descending_resolutions():
     assert warm_split[8:] == [-1, 8, 9, 8, 11, 8, 13, 14]
     assert [k[0] for k in keys[:8]] == [8.0, 7.0, 6.0, 5.0, 4.0, 3.0, 2.0, 1.0]
     assert parallel.chains(warm_split) == [list(range(8)), list(range(8, 16))]
+    # warm-started instances run one pass by default (their start replaces the
+    # plain run's first pass); chain heads keep the base config's passes
+    assert [c.n_iterations for c in cfgs] == [2, 1, 1, 2, 1, 1]
+    cfgs2, _, _ = sweep_plan([0.5, 2.0, 1.0], [1], warm_passes=None)
+    assert [c.n_iterations for c in cfgs2] == [2, 2, 2]
+    cfgs3, _, _ = sweep_plan([0.5, 2.0], [1], warm_start=False)
+    assert [c.n_iterations for c in cfgs3] == [2, 2]
 
 
 def _free_port():
