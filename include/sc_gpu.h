@@ -328,6 +328,25 @@ sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs,
                              uint64_t* labels_out, uint64_t* n_clusters_out,
                              uint32_t n_streams);
 
+/*
+ * sc_leiden_batch_ex's instances as batched device work instead of host
+ * threads: instances whose warm start (warm_from, as in sc_leiden_batch_ex) is
+ * done run together over the disjoint union of their graphs, every kernel
+ * launch covering the nodes of all of them, with each instance's resolution,
+ * seed, totals and stopping state in device arrays. Each instance takes the
+ * decisions of its own leiden() run (hashes and tie rules see instance-local
+ * ids, and an instance stops where its own run stops); inside the exact
+ * summation regime its labels are those of sc_leiden / sc_leiden_from bit for
+ * bit. All instances need one objective kind, refine setting and
+ * max_community_weight. A union holds at most max_union_entries stored entries
+ * (0 = 2^30) and 65,535 instances; larger waves split into several. No
+ * reference counterpart as one call; semantically a loop over leiden
+ * (src/community_search/leiden/mod.rs:168-220).
+ */
+sc_status sc_leiden_batch_union(sc_ctx* ctx, const sc_graph* const* graphs, const sc_leiden_config* cfgs,
+                                uint64_t count, const int64_t* warm_from, const uint64_t* label_offsets,
+                                uint64_t* labels_out, uint64_t* n_clusters_out, uint64_t max_union_entries);
+
 /* ---- kNN graph builder --------------------------------------------------- */
 typedef enum sc_knn_sigma { SC_SIGMA_MEDIAN = 0, SC_SIGMA_KTH = 1 } sc_knn_sigma;
 typedef enum sc_knn_sym { SC_SYM_LOWER_ID = 0, SC_SYM_UNION = 1 } sc_knn_sym;

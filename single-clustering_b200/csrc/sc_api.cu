@@ -607,6 +607,73 @@ sc_status sc_leiden_batch_ex(sc_ctx* ctx, const sc_graph* const* graphs, const s
     });
 }
 
+sc_status sc_leiden_batch_union(sc_ctx* ctx, const sc_graph* const* graphs, const sc_leiden_config* cfgs,
+                                uint64_t count, const int64_t* warm_from, const uint64_t* label_offsets,
+                                uint64_t* labels_out, uint64_t* n_clusters_out, uint64_t max_union_entries) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(count == 0 || (graphs && cfgs && label_offsets && labels_out && n_clusters_out),
+                "batch arrays are NULL");
+        std::vector<uint32_t> depth(count, 0);
+        for (uint64_t i = 0; i < count; ++i) {
+            require(graphs[i] && graphs[i]->g, "a graph of the batch is NULL");
+            require_same_device(c, *graphs[i]->g);
+            if (warm_from) {
+                require(warm_from[i] < (int64_t)i, "warm_from must name an earlier instance or -1");
+                if (warm_from[i] >= 0) {
+                    require(graphs[warm_from[i]]->g->n == graphs[i]->g->n,
+                            "a warm start needs an instance on a graph with the same node count");
+                    depth[i] = depth[warm_from[i]] + 1;
+                }
+            }
+        }
+        if (count == 0) return;
+        const uint64_t cap = max_union_entries ? max_union_entries : (uint64_t(1) << 30);
+        const uint32_t max_depth = *std::max_element(depth.begin(), depth.end());
+        for (uint32_t d = 0; d <= max_depth; ++d) {
+            // the instances whose warm start is done, in index order, packed into unions
+            std::vector<uint64_t> wave;
+            for (uint64_t i = 0; i < count; ++i)
+                if (depth[i] == d) wave.push_back(i);
+            size_t a = 0;
+            while (a < wave.size()) {
+                size_t b = a;
+                uint64_t entries = 0, nodes = 0;
+                while (b < wave.size() && b - a < 65535) {
+                    const sc::DevGraph& g = *graphs[wave[b]]->g;
+                    if (b > a && (entries + g.E > cap || nodes + g.n >= 0x7FFFFFFFull)) break;
+                    entries += g.E;
+                    nodes += g.n;
+                    ++b;
+                }
+                const uint32_t K = (uint32_t)(b - a);
+                std::vector<const sc::DevGraph*> gs(K);
+                std::vector<sc_leiden_config> cf(K);
+                std::vector<uint64_t> n(K), ncl(K);
+                std::vector<const uint64_t*> init(K, nullptr);
+                for (uint32_t t = 0; t < K; ++t) {
+                    const uint64_t i = wave[a + t];
+                    gs[t] = graphs[i]->g;
+                    cf[t] = cfgs[i];
+                    n[t] = gs[t]->n;
+                    if (warm_from && warm_from[i] >= 0) init[t] = labels_out + label_offsets[warm_from[i]];
+                }
+                std::unique_ptr<sc::DevGraph> u(sc::graph_union(c, gs.data(), K));
+                u->stream = c.stream;
+                sc::DBuf<uint32_t> lab(c, std::max<uint64_t>(u->n, 1));
+                sc::leiden_union(c, *u, K, n.data(), cf.data(), init.data(), lab.get(), ncl.data());
+                uint64_t off = 0;
+                for (uint32_t t = 0; t < K; ++t) {
+                    const uint64_t i = wave[a + t];
+                    sc::download_labels(c, lab.get() + off, n[t], labels_out + label_offsets[i]);
+                    n_clusters_out[i] = ncl[t];
+                    off += n[t];
+                }
+                a = b;
+            }
+        }
+    });
+}
+
 void sc_knn_opts_default(sc_knn_opts* o) {
     if (!o) return;
     o->sigma = SC_SIGMA_MEDIAN;

@@ -1605,7 +1605,67 @@ DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint6
     return out.release();
 }
 
+// One instance's arrays inside a union graph.
+struct UnionPart {
+    const uint64_t* ptr;
+    const uint32_t* nbr;
+    const float* w;
+    const uint32_t* erow;
+    const double* node_w;
+    uint64_t n, E, noff, eoff;
+};
+
+// Copies instance blockIdx.y into the union: ids shift by its node offset,
+// entry offsets by its entry offset. Blocks along x stride over its entries
+// and nodes.
+__global__ void k_union_copy(const UnionPart* __restrict__ parts, uint64_t* ptr, uint32_t* nbr, float* w,
+                             uint32_t* erow, double* node_w) {
+    const UnionPart pt = parts[blockIdx.y];
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < pt.E; e += stride) {
+        nbr[pt.eoff + e] = pt.nbr[e] + (uint32_t)pt.noff;
+        erow[pt.eoff + e] = pt.erow[e] + (uint32_t)pt.noff;
+        w[pt.eoff + e] = pt.w[e];
+    }
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < pt.n; v += stride) {
+        ptr[pt.noff + v] = pt.ptr[v] + pt.eoff;
+        node_w[pt.noff + v] = pt.node_w[v];
+    }
+}
+
 }  // namespace
+
+// The disjoint union of graphs (instance i's nodes follow instance i-1's):
+// one graph whose rows are the instances' rows, ids shifted, with its own
+// statistics (from the default pool, like the graphs of a run).
+DevGraph* graph_union(Ctx& c, const DevGraph* const* gs, uint64_t count) {
+    if (count == 0 || count > 65535) fail(SC_E_INVALID_ARGUMENT, "a union takes 1..65535 graphs");
+    std::vector<UnionPart> parts(count);
+    uint64_t n = 0, E = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+        const DevGraph& g = *gs[i];
+        parts[i] = UnionPart{g.ptr, g.nbr, g.w, g.erow, g.node_w, g.n, g.E, n, E};
+        n += g.n;
+        E += g.E;
+    }
+    if (n >= 0x7FFFFFFFull) fail(SC_E_TOO_MANY_NODES, "a union of %llu nodes exceeds 2^31 - 1", (unsigned long long)n);
+    std::unique_ptr<DevGraph> u(new DevGraph());
+    u->pooled = true;
+    galloc(c, *u, n, E);
+    DBuf<UnionPart> d_parts(c, count);
+    h2d(c, d_parts.get(), parts.data(), count);
+    uint64_t most = 0;
+    for (const UnionPart& pt : parts) most = std::max(most, std::max(pt.E, pt.n));
+    const unsigned gx = grid_for(most, TB, 148u * 8u);
+    k_union_copy<<<dim3(gx, (unsigned)count), TB, 0, c.stream>>>(d_parts.get(), u->ptr, u->nbr, u->w, u->erow,
+                                                                  u->node_w);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    SC_CUDA(cudaMemcpyAsync(u->ptr + n, &E, sizeof(uint64_t), cudaMemcpyHostToDevice, c.stream));
+    finalize(c, *u, false);
+    sync(c);  // the host value of E above must outlive the copy
+    return u.release();
+}
 
 // Stats and checks of an aggregated graph; its rows mirror each other exactly.
 void finish_aggregate(Ctx& c, DevGraph& out) {

@@ -259,6 +259,8 @@ DevGraph* graph_from_csr(Ctx& c, const uint64_t* ptr, uint64_t n_ptr, const uint
 DevGraph* graph_from_edges(Ctx& c, uint64_t n, const uint64_t* from, const uint64_t* to,
                            const double* w, uint64_t m, const double* node_w);
 DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t n_groups);
+// disjoint union of `count` graphs, instance i's node ids shifted past instance i-1's
+DevGraph* graph_union(Ctx& c, const DevGraph* const* gs, uint64_t count);
 void graph_validate_symmetry(Ctx& c, const DevGraph& g);
 bool graph_bitwise_symmetric(Ctx& c, const DevGraph& g);
 void graph_copy_csr(Ctx& c, const DevGraph& g, uint64_t* ptr, uint32_t* nbr, float* w);
@@ -296,6 +298,10 @@ struct LeidenOut {
 };
 void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64_t* initial_host,
             uint32_t* d_labels_out, uint64_t* n_clusters);
+// Every instance's leiden() over the disjoint union g of their graphs (instance
+// I owns n[I] nodes, in order), instance I from initial[I] (host labels, nullable).
+void leiden_union(Ctx& c, const DevGraph& g, uint32_t count, const uint64_t* n, const sc_leiden_config* cfgs,
+                  const uint64_t* const* initial, uint32_t* d_labels_out, uint64_t* n_clusters);
 bool tuning_valid(const sc_tuning& t);
 // Times the first level under candidate routings, keeps the fastest on c.
 uint32_t autotune(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, sc_tuning* chosen, double* ms_chosen,

@@ -78,22 +78,52 @@ struct Params {
     // highest claim key wins), so a community never passes the cap
     unsigned long long* claim;
     uint32_t* moved;  // epoch in which the node last committed a move
+    // batched runs over a disjoint union of instances (nullptr: one instance,
+    // the scalars above): each node's instance, the instances' settings, and
+    // each instance's gain accumulator
+    const uint32_t* inst;
+    const struct InstCfg* icfg;
+    long long* gain_inst;
 };
+
+// Settings of one instance of a batched run, for the current level.
+struct InstCfg {
+    double gamma, four_m, thr, theta;
+    uint64_t seed;    // the instance's seed for this level (local moving or refinement)
+    uint32_t base;    // the instance's first node id in the union at this level
+    uint32_t frozen;  // 1: the instance takes no decisions (it stopped, as its own run would)
+};
+
+// What a node's decisions read: the run's scalars, or its instance's. Hashes
+// and tie rules see instance-local ids (node id - base), so a node of a batched
+// run draws exactly what it draws in its instance's own run.
+struct NodeCfg {
+    double gamma, four_m, thr, theta;
+    uint64_t seed;
+    uint32_t base;
+};
+
+template <bool MULTI>
+__device__ __forceinline__ NodeCfg node_cfg(const Params& p, uint32_t v) {
+    if (!MULTI) return NodeCfg{p.gamma, p.four_m, p.thr, p.theta, p.seed, 0u};
+    const InstCfg& c = p.icfg[p.inst[v]];
+    return NodeCfg{c.gamma, c.four_m, c.thr, c.theta, c.seed, c.base};
+}
 
 __device__ __forceinline__ long long to_fix(double x, double inv) { return __double2ll_rn(__dmul_rn(x, inv)); }
 __device__ __forceinline__ double from_fix(long long q, double s) { return __dmul_rn(__ll2double_rn(q), s); }
 
 // Rb::delta_insert (objective.rs:91-106) / Cpm::delta_insert (:158-169)
-__device__ __forceinline__ double gain_of(const Params& p, double wto, double sl, double k, double kc,
-                                          double a, double nc) {
+__device__ __forceinline__ double gain_of(const Params& p, const NodeCfg& q, double wto, double sl, double k,
+                                          double kc, double a, double nc) {
     if (p.objective == SC_OBJECTIVE_RB) {
-        if (p.four_m == 0.0) return 0.0;
+        if (q.four_m == 0.0) return 0.0;
         return __dsub_rn(__dadd_rn(wto, sl),
-                         __ddiv_rn(__dmul_rn(__dmul_rn(p.gamma, k), __dadd_rn(__dmul_rn(2.0, kc), k)),
-                                   p.four_m));
+                         __ddiv_rn(__dmul_rn(__dmul_rn(q.gamma, k), __dadd_rn(__dmul_rn(2.0, kc), k)),
+                                   q.four_m));
     }
     return __dsub_rn(__dadd_rn(wto, sl),
-                     __ddiv_rn(__dmul_rn(__dmul_rn(p.gamma, a),
+                     __ddiv_rn(__dmul_rn(__dmul_rn(q.gamma, a),
                                          __dsub_rn(__dadd_rn(__dmul_rn(2.0, nc), a), 1.0)),
                                2.0));
 }
@@ -106,26 +136,32 @@ __device__ __forceinline__ uint64_t prio(uint64_t seed, uint32_t ep, uint32_t v)
     return hash3(seed ^ 0xA5A5A5A5DEADBEEFull, ep, v);
 }
 
-// Whether node x's move (decided in epoch p.cur) is cancelled.
+// Whether node x's move (decided in epoch p.cur) is cancelled. x and the
+// member h of its target are nodes of the same instance.
+template <bool MULTI>
 __device__ __forceinline__ bool cancelled(const Params& p, uint32_t x) {
     uint32_t h = p.hint[x];
     if (h == NONE32) return false;
     if (p.epoch[h] != p.cur) return false;  // the target's member is not moving
     if (p.hint[h] == x) {                   // mutual: the lower priority yields
-        uint64_t px = prio(p.seed, p.cur, x), ph = prio(p.seed, p.cur, h);
+        const NodeCfg q = node_cfg<MULTI>(p, x);
+        uint64_t px = prio(q.seed, p.cur, x - q.base), ph = prio(q.seed, p.cur, h - q.base);
         return px < ph || (px == ph && x < h);
     }
     return true;
 }
 
+template <bool MULTI>
 __device__ __forceinline__ unsigned long long claim_key(const Params& p, uint32_t v) {
-    return ((unsigned long long)p.cur << 40) | ((prio(p.seed ^ 0x77ull, p.cur, v) & 0xFFull) << 32) | v;
+    const NodeCfg q = node_cfg<MULTI>(p, v);
+    return ((unsigned long long)p.cur << 40) | ((prio(q.seed ^ 0x77ull, p.cur, v - q.base) & 0xFFull) << 32) | v;
 }
 
 // Whether node x's move is dropped: cancelled, or beaten to a capped community.
+template <bool MULTI>
 __device__ __forceinline__ bool lost(const Params& p, uint32_t x) {
-    if (cancelled(p, x)) return true;
-    return p.has_limit && p.claim[p.tgt[x]] != claim_key(p, x);
+    if (cancelled<MULTI>(p, x)) return true;
+    return p.has_limit && p.claim[p.tgt[x]] != claim_key<MULTI>(p, x);
 }
 
 __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t a, uint64_t b) {
@@ -138,11 +174,13 @@ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t a, uint64_t 
 // uniform in (0, 1) from a hash of (seed, epoch, node, c). The result does not
 // depend on the order candidates are visited in, so no candidate list or sort
 // is needed. theta <= 0 is the deterministic argmax (ties to the lower id).
-__device__ __forceinline__ double refine_key(const Params& p, double rel, uint32_t v, uint32_t c) {
-    if (p.theta <= 0.0) return rel;
-    uint64_t h = hash3(p.seed ^ 0x5151515151515151ull, ((uint64_t)p.cur << 32) | v, c);
+// v and c are instance-local ids (refined community ids are node ids).
+__device__ __forceinline__ double refine_key(const Params& p, const NodeCfg& q, double rel, uint32_t v,
+                                             uint32_t c) {
+    if (q.theta <= 0.0) return rel;
+    uint64_t h = hash3(q.seed ^ 0x5151515151515151ull, ((uint64_t)p.cur << 32) | v, c);
     double u = ((double)(h >> 11) + 0.5) * 0x1.0p-53;
-    return __dadd_rn(__ddiv_rn(rel, p.theta), -log(-log(u)));
+    return __dadd_rn(__ddiv_rn(rel, q.theta), -log(-log(u)));
 }
 
 // Read-only load (ld.global.nc): the decide kernels never write the graph, the
@@ -161,7 +199,7 @@ __device__ __forceinline__ void warp_add(unsigned long long* ctr, unsigned long 
 // ------------------------------------------------------------ small-degree decide
 // REFINE=false: local moving. REFINE=true: refinement (singletons only, inside
 // the constraint, randomised choice among non-negative candidates).
-template <int G, bool REFINE>
+template <int G, bool REFINE, bool MULTI>
 __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t* __restrict__ list,
                                                         const uint64_t* __restrict__ lbeg,
                                                         const uint32_t* __restrict__ ldeg, uint32_t count) {
@@ -207,6 +245,7 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
         const uint32_t u_next = nu;
         const float wt_next = nwt;
         fetch(wb + step);
+        const NodeCfg q = node_cfg<MULTI>(p, v);
         const uint32_t own = have ? ro(p.memb + (v)) : 0;
         bool eligible = have;
         if (REFINE && have) eligible = ro(p.csize + (own)) == 1;  // refine.rs:60-62
@@ -243,7 +282,7 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
         if (!ob) wof = 0;
         double base = 0.0;
         if (eligible) {
-            base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
+            base = gain_of(p, q, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
                            (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         }
         // candidates held by leader lanes
@@ -253,12 +292,12 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
         if (leader && cu != own) {
             double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (!p.has_limit || __dadd_rn(nc, a) <= p.limit) {
-                g = gain_of(p, from_fix(acc, p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
+                g = gain_of(p, q, from_fix(acc, p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
                 if (REFINE) {
                     double rel = __dsub_rn(g, base);
                     if (rel >= 0.0) {  // `>=` takes ties (refine.rs:91-95)
                         cand = true;
-                        g = refine_key(p, rel, v, cu);
+                        g = refine_key(p, q, rel, v - q.base, cu - q.base);
                     } else {
                         g = -INFINITY;
                     }
@@ -300,14 +339,14 @@ __global__ void __launch_bounds__(TB, 4) k_decide_small(Params p, const uint32_t
                 const uint32_t fresh = (uint32_t)(p.S0 + v);
                 if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 &&
                     (!p.has_limit || a <= p.limit)) {
-                    double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                    double ge = gain_of(p, q, 0.0, sl, k, 0.0, a, 0.0);
                     if (better(ge, fresh, bg, best)) {
                         best = fresh;
                         bg = ge;
                     }
                 }
                 double d = __dsub_rn(bg, base);
-                if (best != own && d > p.thr) {
+                if (best != own && d > q.thr) {
                     p.tgt[v] = best;
                     p.from[v] = own;
                     p.dgain[v] = to_fix(d, p.inv_scale);
@@ -433,7 +472,7 @@ __device__ void block_argmax(double& g, uint32_t& c, double* sg, uint32_t* sc) {
 // One warp per node of degree 33..WARP_DEGREE: an open-addressing hash of
 // neighbour communities in this warp's slice of shared memory, gains scored
 // by every lane over its slots, warp argmax.
-template <bool REFINE>
+template <bool REFINE, bool MULTI>
 __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, const uint32_t* __restrict__ list,
                                                                       const uint64_t* __restrict__ lbeg,
                                                                       const uint32_t* __restrict__ ldeg,
@@ -479,6 +518,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         const uint32_t u_first = nu;
         const float w_first = nw;
         fetch_head(i + nwarps);
+        const NodeCfg q = node_cfg<MULTI>(p, v);
         const uint32_t own = ro(p.memb + (v));
         if (REFINE && ro(p.csize + (own)) != 1) {  // warp-uniform
             fetch_chunk();
@@ -525,7 +565,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
         const long long af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
         const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = ro(p.self_loop + (v));
         const long long wof = hlookup(keys, vals, mask, own);
-        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
+        const double base = gain_of(p, q, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale), a,
                                     (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         double g = -INFINITY;
         uint32_t c = NONE32;
@@ -537,11 +577,11 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
             lc++;
             const double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
-            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
+            double gg = gain_of(p, q, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
             if (REFINE) {
                 const double rel = __dsub_rn(gg, base);
                 if (!(rel >= 0.0)) continue;
-                gg = refine_key(p, rel, v, cu);
+                gg = refine_key(p, q, rel, v - q.base, cu - q.base);
             }
             if (better(gg, cu, g, c)) {
                 g = gg;
@@ -568,14 +608,14 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
             }
             const uint32_t fresh = (uint32_t)(p.S0 + v);
             if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 && (!p.has_limit || a <= p.limit)) {
-                const double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                const double ge = gain_of(p, q, 0.0, sl, k, 0.0, a, 0.0);
                 if (better(ge, fresh, bg, best)) {
                     best = fresh;
                     bg = ge;
                 }
             }
             const double d = __dsub_rn(bg, base);
-            if (best != own && d > p.thr) {
+            if (best != own && d > q.thr) {
                 target = best;
                 dg = to_fix(d, p.inv_scale);
             }
@@ -616,7 +656,7 @@ __global__ void __launch_bounds__(32 * WARPS_PER_BLOCK) k_decide_warp(Params p, 
 // memory. HUB = true: the table lives in this block's slice of the global
 // scratch (gcap entries), which the host sized for the largest degree; the
 // grid never exceeds the number of slices.
-template <bool REFINE, bool HUB>
+template <bool REFINE, bool HUB, bool MULTI>
 __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* __restrict__ list,
                                                      const uint64_t* __restrict__ lbeg,
                                                      const uint32_t* __restrict__ ldeg, uint32_t count,
@@ -631,6 +671,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
     unsigned long long sdeg = 0, scand = 0, snodes = 0;
     for (uint64_t i = blockIdx.x; i < count; i += gridDim.x) {
         const uint32_t v = ro(list + (i));
+        const NodeCfg q = node_cfg<MULTI>(p, v);
         const uint64_t b = ro(lbeg + i), e = b + ro(ldeg + i);
         const uint32_t deg = (uint32_t)(e - b);
         const uint32_t own = ro(p.memb + (v));
@@ -682,7 +723,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
         const long long af = to_fix(ro(p.node_w + (v)), p.inv_nscale);
         const double k = from_fix(kf, p.scale), a = from_fix(af, p.nscale), sl = ro(p.self_loop + (v));
         const long long wof = hlookup(keys, vals, mask, own);
-        const double base = gain_of(p, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale),
+        const double base = gain_of(p, q, from_fix(wof, p.scale), sl, k, from_fix(ro(p.Kf + (own)) - kf, p.scale),
                                     a, (p.need_nc ? from_fix(ro(p.Wf + (own)) - af, p.nscale) : 0.0));
         double g = -INFINITY;
         uint32_t c = NONE32;
@@ -693,11 +734,11 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
             lc++;
             double nc = (p.need_nc ? from_fix(ro(p.Wf + (cu)), p.nscale) : 0.0);
             if (p.has_limit && __dadd_rn(nc, a) > p.limit) continue;
-            double gg = gain_of(p, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
+            double gg = gain_of(p, q, from_fix(vals[s], p.scale), sl, k, from_fix(ro(p.Kf + (cu)), p.scale), a, nc);
             if (REFINE) {
                 double rel = __dsub_rn(gg, base);
                 if (!(rel >= 0.0)) continue;
-                gg = refine_key(p, rel, v, cu);
+                gg = refine_key(p, q, rel, v - q.base, cu - q.base);
             }
             if (better(gg, cu, g, c)) {
                 g = gg;
@@ -721,14 +762,14 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
                 const uint32_t fresh = (uint32_t)(p.S0 + v);
                 if (fresh != own && ro(p.csize + (own)) > 1 && ro(p.csize + (fresh)) == 0 &&
                     (!p.has_limit || a <= p.limit)) {
-                    double ge = gain_of(p, 0.0, sl, k, 0.0, a, 0.0);
+                    double ge = gain_of(p, q, 0.0, sl, k, 0.0, a, 0.0);
                     if (better(ge, fresh, bg, best)) {
                         best = fresh;
                         bg = ge;
                     }
                 }
                 double d = __dsub_rn(bg, base);
-                s_target = (best != own && d > p.thr) ? best : NONE32;
+                s_target = (best != own && d > q.thr) ? best : NONE32;
                 if (s_target != NONE32) p.dgain[v] = to_fix(d, p.inv_scale);
             } else {
                 s_target = c;  // NONE32 when no candidate has rel >= 0
@@ -765,7 +806,7 @@ __global__ void __launch_bounds__(TB) k_decide_block(Params p, const uint32_t* _
 }
 
 // ------------------------------------------------------------ commit
-template <bool REFINE>
+template <bool REFINE, bool MULTI>
 __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t count) {
     unsigned long long nmoves = 0;
     long long gsum = 0;
@@ -773,7 +814,7 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = list[i];
         if (p.epoch[v] != p.cur) continue;
-        if (lost(p, v)) continue;
+        if (lost<MULTI>(p, v)) continue;
         const uint32_t t = p.tgt[v], old = p.from[v];
         const long long kf = to_fix(p.strength[v], p.inv_scale);
         p.memb[v] = t;
@@ -787,7 +828,11 @@ __global__ void k_apply(Params p, const uint32_t* __restrict__ list, uint32_t co
         atomicSub(p.csize + old, 1u);
         atomicAdd(p.csize + t, 1u);
         nmoves++;
-        gsum += p.dgain[v];
+        if (MULTI) {
+            if (p.dgain[v]) atomicAdd((unsigned long long*)(p.gain_inst + p.inst[v]), (unsigned long long)p.dgain[v]);
+        } else {
+            gsum += p.dgain[v];
+        }
         if (!REFINE) p.moved[v] = p.cur;
     }
     warp_add(p.counters + 0, nmoves);
@@ -845,12 +890,13 @@ __global__ void k_activate(Params p, const uint32_t* __restrict__ list, uint32_t
     }
 }
 
+template <bool MULTI>
 __global__ void k_claim(Params p, const uint32_t* __restrict__ list, uint32_t count) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < count;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t v = list[i];
-        if (p.epoch[v] != p.cur || cancelled(p, v)) continue;
-        atomicMax(p.claim + p.tgt[v], claim_key(p, v));
+        if (p.epoch[v] != p.cur || cancelled<MULTI>(p, v)) continue;
+        atomicMax(p.claim + p.tgt[v], claim_key<MULTI>(p, v));
     }
 }
 
@@ -867,10 +913,21 @@ __device__ __forceinline__ int bucket_of(uint32_t deg, Route r) {
     return deg <= r.g8 ? 0 : deg <= r.g16 ? 1 : deg <= r.g32 ? 2 : deg <= WARP_DEGREE ? 3 : deg <= HUB_DEGREE ? 4 : 5;
 }
 
+// The hash batch of node v in a sweep, or -1 for a node of a frozen instance.
+template <bool MULTI>
+__device__ __forceinline__ int batch_of(uint64_t seed, uint32_t sweep, uint64_t v, int B, const uint32_t* inst,
+                                        const InstCfg* icfg) {
+    if (!MULTI) return (int)(hash3(seed, sweep, v) % (uint64_t)B);
+    const InstCfg& c = icfg[inst[v]];
+    if (c.frozen) return -1;
+    return (int)(hash3(c.seed, sweep, v - c.base) % (uint64_t)B);
+}
+
 // The nodes of a sweep: alist[0 .. *acount) or, with alist == nullptr, all n.
+template <bool MULTI>
 __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ alist,
                                const uint32_t* __restrict__ acount, uint64_t n, uint64_t seed, uint32_t sweep, int B,
-                               Route route, uint32_t* counts) {
+                               Route route, uint32_t* counts, const uint32_t* inst, const InstCfg* icfg) {
     __shared__ uint32_t sc[64];
     for (int t = threadIdx.x; t < B * NBUCKET; t += blockDim.x) sc[t] = 0;
     __syncthreads();
@@ -878,7 +935,8 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint32_t*
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m;
          i += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t v = alist ? alist[i] : i;
-        int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
+        const int b = batch_of<MULTI>(seed, sweep, v, B, inst, icfg);
+        if (b < 0) continue;
         int k = bucket_of((uint32_t)(ptr[v + 1] - ptr[v]), route);
         atomicAdd(&sc[b * NBUCKET + k], 1u);
     }
@@ -888,10 +946,11 @@ __global__ void k_bucket_count(const uint64_t* __restrict__ ptr, const uint32_t*
 }
 
 // One warp-aggregated atomic per distinct (batch, bucket) per warp.
+template <bool MULTI>
 __global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ alist,
                                  const uint32_t* __restrict__ acount, uint64_t n, uint64_t seed, uint32_t sweep,
                                  int B, Route route, uint32_t* cursor, uint32_t* list, uint64_t* lbeg,
-                                 uint32_t* ldeg) {
+                                 uint32_t* ldeg, const uint32_t* inst, const InstCfg* icfg) {
     const unsigned lane = threadIdx.x & 31u;
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     const uint64_t m = alist ? *acount : n;
@@ -902,11 +961,13 @@ __global__ void k_bucket_scatter(const uint64_t* __restrict__ ptr, const uint32_
         uint64_t rb = 0;
         uint32_t deg = 0;
         if (i < m) {
-            int b = (int)(hash3(seed, sweep, v) % (uint64_t)B);
-            rb = ptr[v];
-            deg = (uint32_t)(ptr[v + 1] - rb);
-            int k = bucket_of(deg, route);
-            slot = b * NBUCKET + k;
+            const int b = batch_of<MULTI>(seed, sweep, v, B, inst, icfg);
+            if (b >= 0) {
+                rb = ptr[v];
+                deg = (uint32_t)(ptr[v + 1] - rb);
+                int k = bucket_of(deg, route);
+                slot = b * NBUCKET + k;
+            }
         }
         const unsigned mm = __match_any_sync(0xFFFFFFFFu, slot < 0 ? 1000 + (int)lane : slot);
         const int leader = __ffs(mm) - 1;
@@ -1092,7 +1153,7 @@ void prepare_workspace(Ctx& c, Workspace& ws, const DevGraph& g) {
     }
 }
 
-template <bool REFINE>
+template <bool REFINE, bool MULTI>
 void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32_t cnt,
                    cudaStream_t st = nullptr) {
     if (!cnt) return;
@@ -1102,24 +1163,24 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32
     const uint32_t* ldeg = ws.ldeg.get() + off;
     if (k == 0) {
         unsigned warps = (cnt + 3) / 4;
-        k_decide_small<8, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<8, REFINE, MULTI><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 1) {
         unsigned warps = (cnt + 1) / 2;
-        k_decide_small<16, REFINE><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<16, REFINE, MULTI><<<grid_for((uint64_t)warps * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 2) {
-        k_decide_small<32, REFINE><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
+        k_decide_small<32, REFINE, MULTI><<<grid_for((uint64_t)cnt * 32, TB, 148u * 64u), TB, 0, st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 3) {
         const uint64_t warps = cnt;
-        k_decide_warp<REFINE><<<grid_for(warps * 32, 32 * WARPS_PER_BLOCK, 148u * 64u), 32 * WARPS_PER_BLOCK, 0,
+        k_decide_warp<REFINE, MULTI><<<grid_for(warps * 32, 32 * WARPS_PER_BLOCK, 148u * 64u), 32 * WARPS_PER_BLOCK, 0,
                                 st>>>(p, list, lbeg, ldeg, cnt);
     } else if (k == 4) {
         size_t sm = HCAP_SMEM * (sizeof(long long) + sizeof(uint32_t));
         unsigned grid = std::min<unsigned>(cnt, (unsigned)c.sm_count * 4);
-        k_decide_block<REFINE, false><<<grid, TB, sm, st>>>(p, list, lbeg, ldeg, cnt, nullptr, nullptr, 0);
+        k_decide_block<REFINE, false, MULTI><<<grid, TB, sm, st>>>(p, list, lbeg, ldeg, cnt, nullptr, nullptr, 0);
     } else {
         if (ws.nblk_large < 1 || ws.gcap == 0) fail(SC_E_INTERNAL, "hub scratch missing");
         unsigned grid = std::min<unsigned>(cnt, (unsigned)ws.nblk_large);
-        k_decide_block<REFINE, true><<<grid, TB, 0, st>>>(p, list, lbeg, ldeg, cnt, ws.gkeys.get(),
+        k_decide_block<REFINE, true, MULTI><<<grid, TB, 0, st>>>(p, list, lbeg, ldeg, cnt, ws.gkeys.get(),
                                                                ws.gvals.get(), ws.gcap);
     }
     SC_LAUNCH_CHECK();
@@ -1135,12 +1196,12 @@ void launch_decide(Ctx& c, Params& p, Workspace& ws, int k, uint32_t off, uint32
 Route route_of(const Ctx& c) { return Route{c.tuning.lanes8_max_degree, c.tuning.lanes16_max_degree,
                                              c.tuning.lanes32_max_degree}; }
 
-template <bool REFINE>
+template <bool REFINE, bool MULTI>
 void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs, int b) {
     const uint32_t* o = offs + b * NBUCKET;
     if (o[4] - o[0] <= c.tuning.small_batch) {
-        launch_decide<REFINE>(c, p, ws, 3, o[0], o[4] - o[0]);
-        for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+        launch_decide<REFINE, MULTI>(c, p, ws, 3, o[0], o[4] - o[0]);
+        for (int k = 4; k < NBUCKET; ++k) launch_decide<REFINE, MULTI>(c, p, ws, k, o[k], o[k + 1] - o[k]);
         return;
     }
     // Buckets of one batch read the same snapshot and write disjoint nodes: the
@@ -1149,7 +1210,7 @@ void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs,
     int nonempty = 0;
     for (int k = 0; k < NBUCKET; ++k) nonempty += o[k + 1] > o[k];
     if (nonempty < 2 || !c.side[0]) {
-        for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+        for (int k = 0; k < NBUCKET; ++k) launch_decide<REFINE, MULTI>(c, p, ws, k, o[k], o[k + 1] - o[k]);
         return;
     }
     SC_CUDA(cudaEventRecord(c.ev_fork, c.stream));
@@ -1158,13 +1219,13 @@ void launch_batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs,
     for (int k = 0; k < NBUCKET; ++k) {
         if (o[k + 1] == o[k]) continue;
         if (first) {  // the first non-empty bucket runs on the main stream
-            launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k]);
+            launch_decide<REFINE, MULTI>(c, p, ws, k, o[k], o[k + 1] - o[k]);
             first = false;
             continue;
         }
         cudaStream_t st = c.side[used % SIDE_STREAMS];
         if (used < SIDE_STREAMS) SC_CUDA(cudaStreamWaitEvent(st, c.ev_fork, 0));
-        launch_decide<REFINE>(c, p, ws, k, o[k], o[k + 1] - o[k], st);
+        launch_decide<REFINE, MULTI>(c, p, ws, k, o[k], o[k + 1] - o[k], st);
         ++used;
     }
     for (int t = 0; t < used && t < SIDE_STREAMS; ++t) {
@@ -1181,8 +1242,66 @@ struct MoveResult {
 
 // Parallel local moving over communities `memb` (ids < S0), extra ids
 // [S0, S0+n) are the fresh empty communities.
+// A level of a batched run: each node's instance, the instances' settings on
+// the device (InstCfg, one per instance) and their gain accumulators.
+struct MultiLevel {
+    const uint32_t* inst = nullptr;
+    const InstCfg* icfg = nullptr;
+    long long* gain_inst = nullptr;
+};
+
+template <bool REFINE>
+void batch_decide(Ctx& c, Params& p, Workspace& ws, const uint32_t* offs, int b) {
+    if (p.inst) launch_batch_decide<REFINE, true>(c, p, ws, offs, b);
+    else launch_batch_decide<REFINE, false>(c, p, ws, offs, b);
+}
+
+void launch_bucket_count(Ctx& c, const Params& p, const DevGraph& g, const uint32_t* alist, const uint32_t* acount,
+                         uint64_t seed, uint32_t sweep, int B, uint32_t* counts) {
+    const uint64_t n = g.n;
+    if (p.inst)
+        k_bucket_count<true><<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, alist, acount, n, seed, sweep, B,
+                                                                   route_of(c), counts, p.inst, p.icfg);
+    else
+        k_bucket_count<false><<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, alist, acount, n, seed, sweep, B,
+                                                                    route_of(c), counts, nullptr, nullptr);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+}
+
+void launch_bucket_scatter(Ctx& c, const Params& p, const DevGraph& g, const uint32_t* alist,
+                           const uint32_t* acount, uint64_t work, uint64_t seed, uint32_t sweep, int B,
+                           Workspace& ws) {
+    const uint64_t n = g.n;
+    if (p.inst)
+        k_bucket_scatter<true><<<grid_for(work, TB), TB, 0, c.stream>>>(g.ptr, alist, acount, n, seed, sweep, B,
+                                                                        route_of(c), ws.cursor.get(), ws.list.get(),
+                                                                        ws.lbeg.get(), ws.ldeg.get(), p.inst, p.icfg);
+    else
+        k_bucket_scatter<false><<<grid_for(work, TB), TB, 0, c.stream>>>(g.ptr, alist, acount, n, seed, sweep, B,
+                                                                         route_of(c), ws.cursor.get(), ws.list.get(),
+                                                                         ws.lbeg.get(), ws.ldeg.get(), nullptr, nullptr);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+}
+
+template <bool REFINE>
+void launch_claim_apply(Ctx& c, Params& p, const uint32_t* list, uint32_t cnt, bool claim_only) {
+    const unsigned grid = grid_for(cnt, TB);
+    if (claim_only) {
+        if (p.inst) k_claim<true><<<grid, TB, 0, c.stream>>>(p, list, cnt);
+        else k_claim<false><<<grid, TB, 0, c.stream>>>(p, list, cnt);
+    } else {
+        if (p.inst) k_apply<REFINE, true><<<grid, TB, 0, c.stream>>>(p, list, cnt);
+        else k_apply<REFINE, false><<<grid, TB, 0, c.stream>>>(p, list, cnt);
+    }
+    SC_LAUNCH_CHECK();
+    c.launches++;
+}
+
 MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, uint64_t S0,
-                      const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
+                      const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma,
+                      const MultiLevel* ml = nullptr) {
     MoveResult r;
     const uint64_t n = g.n;
     if (n == 0) return r;
@@ -1235,6 +1354,11 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
     p.gain_acc = ws.gain_acc.get();
     p.claim = claim.get();
     p.moved = ws.moved.get();
+    if (ml) {
+        p.inst = ml->inst;
+        p.icfg = ml->icfg;
+        p.gain_inst = ml->gain_inst;
+    }
     zero(c, ws.counters.get(), 4);
     zero(c, ws.gain_acc.get(), 1);
     zero(c, ws.epoch.get(), n);
@@ -1253,10 +1377,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         zero(c, ws.counts.get(), B * NBUCKET);
         zero(c, ws.ncount.get(), 1);
         const uint32_t* alist = all_active ? nullptr : ws.alist.get();
-        k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, alist, ws.acount.get(), n, seed, sweep, B,
-                                                             route_of(c), ws.counts.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
+        launch_bucket_count(c, p, g, alist, ws.acount.get(), seed, sweep, B, ws.counts.get());
         uint32_t counts[64];
         unsigned long long ctr[4];
         {
@@ -1283,11 +1404,8 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
         if (offs[B * NBUCKET] == 0) break;
         read_fresh = false;
         h2d(c, ws.cursor.get(), offs, B * NBUCKET);
-        k_bucket_scatter<<<grid_for(offs[B * NBUCKET], TB), TB, 0, c.stream>>>(
-            g.ptr, alist, ws.acount.get(), n, seed, sweep, B, route_of(c), ws.cursor.get(), ws.list.get(),
-            ws.lbeg.get(), ws.ldeg.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
+        launch_bucket_scatter(c, p, g, alist, ws.acount.get(), all_active ? n : offs[B * NBUCKET], seed, sweep, B,
+                              ws);
         // A batch's re-queue reads memberships and writes only the next sweep's
         // list, so with an auxiliary stream it runs while the next batch decides;
         // it must end before the next batch commits (which changes memberships).
@@ -1301,16 +1419,13 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
             p.seed = seed;
             uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
             if (lo == hi) continue;
-            launch_batch_decide<false>(c, p, ws, offs, b);
-            if (p.has_limit) {
-                k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
-                c.launches++;
-            }
+            batch_decide<false>(c, p, ws, offs, b);
+            if (p.has_limit) launch_claim_apply<false>(c, p, ws.list.get() + lo, hi - lo, true);
             if (act_pending) {
                 SC_CUDA(cudaStreamWaitEvent(c.stream, c.ev_aux_done, 0));
                 act_pending = false;
             }
-            k_apply<false><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
+            launch_claim_apply<false>(c, p, ws.list.get() + lo, hi - lo, false);
             cudaStream_t as = c.stream;
             if (overlap) {
                 SC_CUDA(cudaEventRecord(c.ev_aux_start, c.stream));
@@ -1324,7 +1439,7 @@ MoveResult local_move(Ctx& c, const DevGraph& g, Workspace& ws, uint32_t* memb, 
                 act_pending = true;
             }
             SC_LAUNCH_CHECK();
-            c.launches += 2;
+            c.launches++;
         }
         if (act_pending) SC_CUDA(cudaStreamWaitEvent(c.stream, c.ev_aux_done, 0));
         std::swap(ws.alist, ws.nlist);
@@ -1365,7 +1480,8 @@ double refine_alg_bytes(const unsigned long long* run) {
 }
 
 void refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint, uint32_t* refined,
-            const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma) {
+            const sc_leiden_config& cfg, uint64_t seed, const Scales& sc, double gamma,
+            const MultiLevel* ml = nullptr) {
     const uint64_t n = g.n;
     if (n == 0) return;
     const bool need_nc = cfg.objective == SC_OBJECTIVE_CPM || cfg.has_max_community_weight;
@@ -1418,14 +1534,16 @@ void refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint
     p.gain_acc = ws.gain_acc.get();
     p.claim = claim.get();
     p.moved = ws.moved.get();
+    if (ml) {
+        p.inst = ml->inst;
+        p.icfg = ml->icfg;
+        p.gain_inst = ml->gain_inst;
+    }
     zero(c, ws.counters.get(), 4);
     zero(c, ws.epoch.get(), n);
     const int B = RF_BATCHES;
     zero(c, ws.counts.get(), B * NBUCKET);
-    k_bucket_count<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
-                                                         ws.counts.get());
-    SC_LAUNCH_CHECK();
-    c.launches++;
+    launch_bucket_count(c, p, g, nullptr, nullptr, seed, 0xFFFFFFFFu, B, ws.counts.get());
     uint32_t counts[64];
     {
         Mailbox mb(c);
@@ -1437,23 +1555,14 @@ void refine(Ctx& c, const DevGraph& g, Workspace& ws, const uint32_t* constraint
     offs[0] = 0;
     for (int t = 0; t < B * NBUCKET; ++t) offs[t + 1] = offs[t] + counts[t];
     h2d(c, ws.cursor.get(), offs, B * NBUCKET);
-    k_bucket_scatter<<<grid_for(n, TB), TB, 0, c.stream>>>(g.ptr, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, route_of(c),
-                                                           ws.cursor.get(), ws.list.get(), ws.lbeg.get(),
-                                                           ws.ldeg.get());
-    SC_LAUNCH_CHECK();
-    c.launches++;
+    launch_bucket_scatter(c, p, g, nullptr, nullptr, n, seed, 0xFFFFFFFFu, B, ws);
     for (int b = 0; b < B; ++b) {
         p.cur = (uint32_t)(b + 1);
         uint32_t lo = offs[b * NBUCKET], hi = offs[(b + 1) * NBUCKET];
         if (lo == hi) continue;
-        launch_batch_decide<true>(c, p, ws, offs, b);
-        if (p.has_limit) {
-            k_claim<<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
-            c.launches++;
-        }
-        k_apply<true><<<grid_for(hi - lo, TB), TB, 0, c.stream>>>(p, ws.list.get() + lo, hi - lo);
-        SC_LAUNCH_CHECK();
-        c.launches++;
+        batch_decide<true>(c, p, ws, offs, b);
+        if (p.has_limit) launch_claim_apply<true>(c, p, ws.list.get() + lo, hi - lo, true);
+        launch_claim_apply<true>(c, p, ws.list.get() + lo, hi - lo, false);
     }
     // counters go to the run's totals on the device (read once, at the end of the run)
     k_add_refine_counters<<<1, 32, 0, c.stream>>>(ws.counters.get(), c.d_refine_ctr);
@@ -1560,6 +1669,306 @@ void run_pass(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, con
     out.improvement = improvement;
 }
 
+// ------------------------------------------------------------ batched runs over a disjoint union
+// Many leiden() runs at once: the instances' graphs form one disjoint union
+// (instance I's nodes are [bounds[I], bounds[I+1]) at every level) and every
+// kernel launch covers the nodes of all instances. Each node reads its
+// instance's settings (InstCfg) and hashes instance-local ids, community ids
+// keep their order inside an instance, and an instance freezes exactly where
+// its own run would stop (its graph stopped shrinking, max_levels, or its
+// passes are done), so every instance takes the decisions of its own run.
+
+__global__ void k_inst_of_nodes(const uint64_t* __restrict__ bounds, uint32_t* inst) {
+    const uint32_t I = blockIdx.y;
+    const uint64_t b = bounds[I], e = bounds[I + 1];
+    for (uint64_t v = b + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < e; v += (uint64_t)gridDim.x * blockDim.x)
+        inst[v] = I;
+}
+
+// Per instance (one block each): 2m = the Σ of its nodes' strengths (one warp;
+// any order inside the exact regime, the node order outside it) and its
+// edge_count, the entries with row <= neighbour.
+__global__ void k_inst_stats(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                             const uint32_t* __restrict__ erow, const double* __restrict__ strength,
+                             const uint64_t* __restrict__ bounds, int exact, double* two_m,
+                             unsigned long long* ecount) {
+    __shared__ unsigned long long s_cnt;
+    const uint32_t I = blockIdx.x;
+    const uint64_t b = bounds[I], e = bounds[I + 1];
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const double t = warp_fold(b, e, 0.0, exact != 0, [&](uint64_t v) { return strength[v]; });
+        if (threadIdx.x == 0) two_m[I] = t;
+    }
+    unsigned long long cnt = 0;
+    const uint64_t eb = ptr[b], ee = ptr[e];
+    for (uint64_t j = eb + threadIdx.x; j < ee; j += blockDim.x) cnt += nbr[j] >= erow[j];
+    for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xFFFFFFFFu, cnt, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(&s_cnt, cnt);
+    __syncthreads();
+    if (threadIdx.x == 0) ecount[I] = s_cnt;
+}
+
+__global__ void k_mark_ids(const uint32_t* __restrict__ ids, uint64_t n, uint32_t* used) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        used[ids[i]] = 1;
+}
+
+__global__ void k_rank_ids(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ rank, uint64_t n,
+                           uint32_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = rank[ids[i]];
+}
+
+__global__ void k_gather_at(const uint32_t* __restrict__ rank, const uint64_t* __restrict__ at, uint32_t count,
+                            uint32_t* out) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i <= count; i += gridDim.x * blockDim.x) out[i] = rank[at[i]];
+}
+
+__global__ void k_inst_keys(const uint32_t* __restrict__ ids, const uint32_t* __restrict__ inst, uint64_t n,
+                            uint64_t* keys, uint32_t* idx) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        keys[i] = ((uint64_t)inst[i] << 32) | ids[i];
+        idx[i] = (uint32_t)i;
+    }
+}
+
+__global__ void k_key_heads(const uint64_t* __restrict__ keys, uint64_t n, uint32_t* head, uint32_t* per_inst) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t h = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
+        head[i] = h;
+        if (h) atomicAdd(per_inst + (uint32_t)(keys[i] >> 32), 1u);
+    }
+}
+
+__global__ void k_scatter_key_rank(const uint32_t* __restrict__ order, const uint32_t* __restrict__ incl, uint64_t n,
+                                   uint32_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[order[i]] = incl[i] - 1;
+}
+
+__global__ void k_scatter_inst(const uint32_t* __restrict__ grp, const uint32_t* __restrict__ inst, uint64_t n,
+                               uint32_t* inst_c) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        inst_c[grp[v]] = inst[v];
+}
+
+__global__ void k_sub_base(uint32_t* x, const uint32_t* __restrict__ inst, const uint32_t* __restrict__ base,
+                           uint64_t n) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n; v += (uint64_t)gridDim.x * blockDim.x)
+        x[v] -= base[inst[v]];
+}
+
+// Ascending ranks of ids in [0, id_space) whose instance ranges are disjoint
+// and ordered (instance I's ids inside [bounds[I], bounds[I+1])): the ranks
+// keep each instance contiguous; counts[I] = its distinct ids.
+void renumber_ranged(Ctx& c, const uint32_t* ids, uint64_t n, uint64_t id_space, const uint64_t* d_bounds,
+                     uint32_t count, uint32_t* out, std::vector<uint32_t>& counts) {
+    DBuf<uint32_t> used(c, id_space + 1), rank(c, id_space + 1), at(c, count + 1);
+    zero(c, used.get(), id_space + 1);
+    k_mark_ids<<<grid_for(n, TB), TB, 0, c.stream>>>(ids, n, used.get());
+    exclusive_sum(c, used.get(), rank.get(), id_space + 1);
+    k_rank_ids<<<grid_for(n, TB), TB, 0, c.stream>>>(ids, rank.get(), n, out);
+    k_gather_at<<<grid_for(count + 1, TB), TB, 0, c.stream>>>(rank.get(), d_bounds, count, at.get());
+    SC_LAUNCH_CHECK();
+    c.launches += 3;
+    std::vector<uint32_t> r(count + 1);
+    d2h(c, r.data(), at.get(), count + 1);
+    sync(c);
+    counts.resize(count);
+    for (uint32_t i = 0; i < count; ++i) counts[i] = r[i + 1] - r[i];
+}
+
+// Ascending ranks of (instance, id): each instance's ids keep their order and
+// take a contiguous range of ranks; counts[I] = instance I's distinct ids.
+void renumber_by_instance(Ctx& c, const uint32_t* ids, const uint32_t* inst, uint64_t n, uint32_t count,
+                          uint32_t* out, std::vector<uint32_t>& counts) {
+    counts.assign(count, 0);
+    if (n == 0) return;
+    DBuf<uint64_t> keys(c, n), keys_s(c, n);
+    DBuf<uint32_t> idx(c, n), order(c, n), head(c, n), incl(c, n), per(c, count);
+    zero(c, per.get(), count);
+    k_inst_keys<<<grid_for(n, TB), TB, 0, c.stream>>>(ids, inst, n, keys.get(), idx.get());
+    SC_LAUNCH_CHECK();
+    sort_pairs(c, keys.get(), keys_s.get(), idx.get(), order.get(), n, 32 + bits_for(count));
+    k_key_heads<<<grid_for(n, TB), TB, 0, c.stream>>>(keys_s.get(), n, head.get(), per.get());
+    inclusive_sum(c, head.get(), incl.get(), n);
+    k_scatter_key_rank<<<grid_for(n, TB), TB, 0, c.stream>>>(order.get(), incl.get(), n, out);
+    SC_LAUNCH_CHECK();
+    c.launches += 3;
+    d2h(c, counts.data(), per.get(), count);
+    sync(c);
+}
+
+// Per-pass state of a batched run.
+struct MultiPass {
+    uint32_t count = 0;
+    const sc_leiden_config* cfgs = nullptr;
+    std::vector<uint64_t> pass_seed;   // per instance
+    std::vector<uint8_t> active;       // the instance runs this pass
+    std::vector<uint64_t> n0;          // nodes per instance at level 0
+    std::vector<double> improvement;   // out: per instance
+    std::vector<uint32_t> n_clusters;  // out: per instance
+    std::vector<double> total_weight0; // out: per instance, level 0
+};
+
+// run_once (mod.rs:214-289) for every active instance of the union g0 at once,
+// from the compact union ids `init` (< C0; each instance's ids a contiguous,
+// ordered range). Output labels are union ids, instance I's in a contiguous
+// range of n_clusters[I] starting after instance I-1's.
+void run_pass_multi(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C0, MultiPass& mp, PassOut& out,
+                    sc_run_stats& st, PhaseClock& clock, Workspace& ws) {
+    const uint32_t K = mp.count;
+    const uint64_t n0 = g0.n;
+    const sc_leiden_config& base_cfg = mp.cfgs[0];
+    std::unique_ptr<DevGraph> owned;
+    const DevGraph* gl = &g0;
+    DBuf<uint32_t> memb(c, n0), node_at(c, n0), inst(c, n0);
+    d2d(c, memb.get(), init, n0);
+    k_identity<<<grid_for(n0, TB), TB, 0, c.stream>>>(node_at.get(), n0);
+    c.launches++;
+    std::vector<uint64_t> nI = mp.n0;
+    std::vector<uint64_t> bounds(K + 1, 0);
+    auto set_bounds = [&]() {
+        bounds[0] = 0;
+        for (uint32_t i = 0; i < K; ++i) bounds[i + 1] = bounds[i] + nI[i];
+    };
+    set_bounds();
+    DBuf<uint64_t> d_bounds(c, K + 1);
+    h2d(c, d_bounds.get(), bounds.data(), K + 1);
+    if (n0) {
+        k_inst_of_nodes<<<dim3(grid_for(*std::max_element(nI.begin(), nI.end()), TB, 148u * 4u), K), TB, 0, c.stream>>>(
+            d_bounds.get(), inst.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    std::vector<uint8_t> frozen(K);
+    for (uint32_t i = 0; i < K; ++i) frozen[i] = mp.active[i] ? 0 : 1;
+    mp.improvement.assign(K, 0.0);
+    mp.total_weight0.assign(K, 0.0);
+    DBuf<InstCfg> icfg_lm(c, K), icfg_rf(c, K);
+    DBuf<long long> gain_inst(c, K);
+    DBuf<double> d_two_m(c, K);
+    DBuf<unsigned long long> d_ecount(c, K);
+    std::vector<InstCfg> h_lm(K), h_rf(K);
+    std::vector<double> two_m(K);
+    std::vector<unsigned long long> ecount(K);
+    std::vector<long long> gains(K);
+    std::vector<uint32_t> G(K);
+    uint64_t C = C0;
+    for (uint64_t level = 0;; ++level) {
+        for (uint32_t i = 0; i < K; ++i)
+            if (!frozen[i] && level >= mp.cfgs[i].max_levels) frozen[i] = 1;
+        if (std::all_of(frozen.begin(), frozen.end(), [](uint8_t f) { return f != 0; })) break;
+        const uint64_t nl = gl->n;
+        Scales sc = scales_for(*gl);
+        prepare_workspace(c, ws, *gl);
+        // the instances' level statistics
+        k_inst_stats<<<K, TB, 0, c.stream>>>(gl->ptr, gl->nbr, gl->erow, gl->strength, d_bounds.get(),
+                                            (int)gl->exact_w, d_two_m.get(), d_ecount.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        d2h(c, two_m.data(), d_two_m.get(), K);
+        d2h(c, ecount.data(), d_ecount.get(), K);
+        sync(c);
+        for (uint32_t i = 0; i < K; ++i) {
+            const sc_leiden_config& cf = mp.cfgs[i];
+            const double m = 0.5 * two_m[i];
+            if (level == 0) mp.total_weight0[i] = m;
+            const uint64_t lvl_seed = hash3(mp.pass_seed[i], level, 0x1eafull);
+            InstCfg a{};
+            a.gamma = cf.resolution;
+            a.four_m = 4.0 * m;
+            a.thr = 1e-12 * std::max(std::fabs(m), 1.0);  // local_move.rs:26-28
+            a.theta = 0.0;
+            a.seed = lvl_seed;
+            a.base = (uint32_t)bounds[i];
+            a.frozen = frozen[i];
+            h_lm[i] = a;
+            InstCfg r = a;
+            r.thr = 0.0;
+            r.theta = cf.refine_randomness * (ecount[i] > 0 ? m / (double)ecount[i] : 1.0);  // refine.rs:44-50
+            r.seed = hash3(lvl_seed, 0x7e71eull, 1);
+            h_rf[i] = r;
+        }
+        h2d(c, icfg_lm.get(), h_lm.data(), K);
+        h2d(c, icfg_rf.get(), h_rf.data(), K);
+        zero(c, gain_inst.get(), K);
+        MultiLevel ml_lm{inst.get(), icfg_lm.get(), gain_inst.get()};
+        MultiLevel ml_rf{inst.get(), icfg_rf.get(), gain_inst.get()};
+        {
+            const size_t t = clock.start();
+            MoveResult mr = local_move(c, *gl, ws, memb.get(), C, base_cfg, 0, sc, base_cfg.resolution, &ml_lm);
+            clock.stop(t, &st.ms_local_move);
+            st.local_move_sweeps += mr.sweeps;
+            st.moves += mr.moves;
+            st.alg_bytes_local_move += mr.alg_bytes;
+        }
+        d2h(c, gains.data(), gain_inst.get(), K);
+        DBuf<uint32_t> collapse(c, nl);
+        if (base_cfg.refine) {
+            const size_t t = clock.start();
+            refine(c, *gl, ws, memb.get(), collapse.get(), base_cfg, 0, sc, base_cfg.resolution, &ml_rf);
+            clock.stop(t, &st.ms_refine);
+        } else {
+            d2d(c, collapse.get(), memb.get(), nl);
+        }
+        sync(c);  // gains
+        for (uint32_t i = 0; i < K; ++i)
+            if (!frozen[i]) mp.improvement[i] += (double)gains[i] * sc.scale;
+        const size_t t_agg = clock.start();
+        DBuf<uint32_t> grp(c, nl);
+        if (base_cfg.refine) renumber_ranged(c, collapse.get(), nl, nl, d_bounds.get(), K, grp.get(), G);
+        else renumber_by_instance(c, collapse.get(), inst.get(), nl, K, grp.get(), G);
+        st.levels++;
+        uint64_t Gtot = 0;
+        bool any_shrinks = false;
+        for (uint32_t i = 0; i < K; ++i) {
+            Gtot += G[i];
+            if (!frozen[i] && G[i] >= nI[i]) frozen[i] = 1;  // the graph no longer shrinks (mod.rs:263-265)
+            if (!frozen[i]) any_shrinks = true;
+        }
+        if (!any_shrinks) {
+            clock.stop(t_agg, &st.ms_aggregate);
+            break;
+        }
+        std::unique_ptr<DevGraph> coarse(graph_aggregate(c, *gl, grp.get(), (uint32_t)Gtot));
+        coarse->stream = c.stream;
+        st.alg_bytes_aggregate += 12.0 * (double)gl->E + 12.0 * (double)nl + 8.0 * (double)coarse->E +
+                                  24.0 * (double)coarse->n;
+        DBuf<uint32_t> cm(c, Gtot), cm2(c, Gtot), inst_c(c, Gtot);
+        k_scatter_coarse<<<grid_for(nl, TB), TB, 0, c.stream>>>(grp.get(), memb.get(), nl, cm.get());
+        k_scatter_inst<<<grid_for(nl, TB), TB, 0, c.stream>>>(grp.get(), inst.get(), nl, inst_c.get());
+        k_gather<<<grid_for(n0, TB), TB, 0, c.stream>>>(grp.get(), node_at.get(), n0);
+        SC_LAUNCH_CHECK();
+        c.launches += 3;
+        C = renumber_ids(c, cm.get(), Gtot, C + nl, cm2.get());
+        memb = std::move(cm2);
+        inst = std::move(inst_c);
+        owned = std::move(coarse);
+        gl = owned.get();
+        for (uint32_t i = 0; i < K; ++i) nI[i] = G[i];
+        set_bounds();
+        h2d(c, d_bounds.get(), bounds.data(), K + 1);
+        clock.stop(t_agg, &st.ms_aggregate);
+    }
+    // final ascending renumber per instance (mod.rs:282-286)
+    const uint64_t nl = gl->n;
+    DBuf<uint32_t> fin(c, nl);
+    std::vector<uint32_t> Kc;
+    renumber_by_instance(c, memb.get(), inst.get(), nl, K, fin.get(), Kc);
+    out.labels.alloc(c, n0);
+    d2d(c, out.labels.get(), node_at.get(), n0);
+    k_gather<<<grid_for(n0, TB), TB, 0, c.stream>>>(fin.get(), out.labels.get(), n0);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    mp.n_clusters = Kc;
+    uint64_t tot = 0;
+    for (uint32_t k : Kc) tot += k;
+    out.n_clusters = tot;
+}
+
 // LeidenConfig::validate (mod.rs:117-153)
 void validate_config(const sc_leiden_config& cfg) {
     double r = cfg.resolution;
@@ -1642,6 +2051,151 @@ void leiden(Ctx& c, const DevGraph& g, const sc_leiden_config& cfg, const uint64
     c.stats.ms_other = c.stats.ms_total - c.stats.ms_local_move - c.stats.ms_refine - c.stats.ms_aggregate;
     c.stats.kernel_launches = c.launches;
     *n_clusters = clusters;
+}
+
+// Every instance's leiden() (mod.rs:168-204) over the disjoint union g of
+// their graphs (instance I owns nodes [offset_I, offset_I + n[I]), in order),
+// with instance I starting from initial[I] (host labels, nullable). Writes
+// each instance's labels (consecutive from 0 within the instance) to
+// d_labels_out in union node order and its cluster count to n_clusters.
+void leiden_union(Ctx& c, const DevGraph& g, uint32_t K, const uint64_t* n, const sc_leiden_config* cfgs,
+                  const uint64_t* const* initial, uint32_t* d_labels_out, uint64_t* n_clusters) {
+    if (K == 0) return;
+    for (uint32_t i = 0; i < K; ++i) validate_config(cfgs[i]);
+    for (uint32_t i = 1; i < K; ++i) {
+        if (cfgs[i].objective != cfgs[0].objective || (cfgs[i].refine != 0) != (cfgs[0].refine != 0) ||
+            cfgs[i].has_max_community_weight != cfgs[0].has_max_community_weight ||
+            (cfgs[i].has_max_community_weight && cfgs[i].max_community_weight != cfgs[0].max_community_weight))
+            fail(SC_E_INVALID_CONFIG,
+                 "invalid configuration: a batched run needs one objective kind, refine setting and "
+                 "max_community_weight for all instances");
+    }
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < K; ++i) total += n[i];
+    if (total != g.n) fail(SC_E_INTERNAL, "instance sizes do not add up to the union");
+    std::memset(&c.stats, 0, sizeof c.stats);
+    PhaseClock clock(c);
+    const size_t t_total = clock.start();
+    zero(c, c.d_refine_ctr, 3);
+    MultiPass mp;
+    mp.count = K;
+    mp.cfgs = cfgs;
+    mp.n0.assign(n, n + K);
+    std::vector<uint64_t> seed(K);
+    for (uint32_t i = 0; i < K; ++i)
+        seed[i] = cfgs[i].has_seed ? cfgs[i].seed : ((uint64_t)std::random_device{}() << 32 ^ std::random_device{}());
+    // initial union ids: each instance's compact ranks, offset past the instances before it
+    DBuf<uint32_t> labels(c, std::max<uint64_t>(total, 1));
+    std::vector<uint32_t> Ci(K);
+    {
+        uint64_t off = 0, cb = 0;
+        for (uint32_t i = 0; i < K; ++i) {
+            if (n[i] == 0) {
+                Ci[i] = 0;
+                continue;
+            }
+            if (initial && initial[i]) {
+                DBuf<uint64_t> ini(c, n[i]);
+                h2d(c, ini.get(), initial[i], n[i]);
+                Ci[i] = renumber_u64_labels(c, ini.get(), n[i], labels.get() + off, nullptr);
+            } else {
+                k_identity<<<grid_for(n[i], TB), TB, 0, c.stream>>>(labels.get() + off, n[i]);
+                c.launches++;
+                Ci[i] = (uint32_t)n[i];
+            }
+            off += n[i];
+        }
+        // shift instance I's ids by the ids of the instances before it
+        std::vector<uint32_t> shift(K);
+        DBuf<uint32_t> d_shift(c, K), inst0(c, std::max<uint64_t>(total, 1));
+        std::vector<uint64_t> b(K + 1, 0);
+        for (uint32_t i = 0; i < K; ++i) {
+            shift[i] = (uint32_t)(0u - (uint32_t)cb);  // k_sub_base subtracts: x - (-cb) = x + cb
+            cb += Ci[i];
+            b[i + 1] = b[i] + n[i];
+        }
+        DBuf<uint64_t> d_b(c, K + 1);
+        h2d(c, d_b.get(), b.data(), K + 1);
+        h2d(c, d_shift.get(), shift.data(), K);
+        if (total) {
+            k_inst_of_nodes<<<dim3(grid_for(*std::max_element(n, n + K), TB, 148u * 4u), K), TB, 0, c.stream>>>(
+                d_b.get(), inst0.get());
+            k_sub_base<<<grid_for(total, TB), TB, 0, c.stream>>>(labels.get(), inst0.get(), d_shift.get(), total);
+            SC_LAUNCH_CHECK();
+            c.launches += 2;
+        }
+    }
+    uint64_t C = 0;
+    for (uint32_t k : Ci) C += k;
+    std::vector<uint64_t> stagnant(K, 0);
+    std::vector<uint8_t> stopped(K, 0);
+    std::vector<uint32_t> clusters(Ci.begin(), Ci.end());
+    Workspace ws;
+    uint64_t max_it = 0;
+    for (uint32_t i = 0; i < K; ++i) max_it = std::max<uint64_t>(max_it, cfgs[i].n_iterations);
+    for (uint64_t it = 0; it < max_it; ++it) {
+        mp.active.assign(K, 0);
+        mp.pass_seed.resize(K);
+        bool any = false;
+        for (uint32_t i = 0; i < K; ++i) {
+            mp.active[i] = !stopped[i] && it < cfgs[i].n_iterations && n[i] > 0;
+            any = any || mp.active[i];
+            mp.pass_seed[i] = hash3(seed[i], it, 0x9a55ull);
+        }
+        if (!any) break;
+        PassOut po;
+        run_pass_multi(c, g, labels.get(), C, mp, po, c.stats, clock, ws);
+        labels = std::move(po.labels);
+        C = po.n_clusters;
+        for (uint32_t i = 0; i < K; ++i) {
+            clusters[i] = mp.n_clusters[i];
+            if (!mp.active[i]) continue;
+            const double scale = std::max(std::fabs(mp.total_weight0[i]), 1.0);
+            if (mp.improvement[i] <= cfgs[i].tolerance * scale) {
+                if (++stagnant[i] >= cfgs[i].patience) stopped[i] = 1;
+            } else {
+                stagnant[i] = 0;
+            }
+        }
+        c.stats.passes++;
+    }
+    // union ids -> instance-local labels
+    {
+        std::vector<uint32_t> base(K);
+        uint64_t cb = 0;
+        for (uint32_t i = 0; i < K; ++i) {
+            base[i] = (uint32_t)cb;
+            cb += clusters[i];
+        }
+        DBuf<uint32_t> d_base(c, K), inst0(c, std::max<uint64_t>(total, 1));
+        std::vector<uint64_t> b(K + 1, 0);
+        for (uint32_t i = 0; i < K; ++i) b[i + 1] = b[i] + n[i];
+        DBuf<uint64_t> d_b(c, K + 1);
+        h2d(c, d_b.get(), b.data(), K + 1);
+        h2d(c, d_base.get(), base.data(), K);
+        if (total) {
+            k_inst_of_nodes<<<dim3(grid_for(*std::max_element(n, n + K), TB, 148u * 4u), K), TB, 0, c.stream>>>(
+                d_b.get(), inst0.get());
+            k_sub_base<<<grid_for(total, TB), TB, 0, c.stream>>>(labels.get(), inst0.get(), d_base.get(), total);
+            SC_LAUNCH_CHECK();
+            c.launches += 2;
+            d2d(c, d_labels_out, labels.get(), total);
+        }
+    }
+    clock.stop(t_total, &c.stats.ms_total);
+    {
+        Mailbox mb(c);
+        const uint32_t* hs = mb.get(c.d_status, 1);
+        const unsigned long long* hr = mb.get(c.d_refine_ctr, 3);
+        mb.wait();
+        const uint32_t status = *hs;
+        c.stats.alg_bytes_refine = refine_alg_bytes(hr);
+        raise_device_status(c, status);
+    }
+    clock.collect();
+    c.stats.ms_other = c.stats.ms_total - c.stats.ms_local_move - c.stats.ms_refine - c.stats.ms_aggregate;
+    c.stats.kernel_launches = c.launches;
+    for (uint32_t i = 0; i < K; ++i) n_clusters[i] = clusters[i];
 }
 
 bool tuning_valid(const sc_tuning& t) {

@@ -446,8 +446,14 @@ def leiden_from(graph: CSRNetwork, config: LeidenConfig | None, initial) -> Clus
 
 
 def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig], warm_from=None,
-                 n_streams: int = 0) -> list:
-    """Many leiden() runs in one call, concurrently on `n_streams` worker streams.
+                 n_streams: int = 0, union: bool = False, max_union_entries: int = 0) -> list:
+    """Many leiden() runs in one call.
+
+    union=False: concurrently on `n_streams` worker streams (sc_leiden_batch_ex).
+    union=True: as batched device work over disjoint unions of the instances'
+    graphs (sc_leiden_batch_union): every launch covers all instances whose
+    warm start is done; labels equal the separate runs' inside the exact
+    summation regime.
 
     warm_from[i] = j (j < i) starts instance i from instance j's labels (leiden
     with `initial`); -1 starts from singletons."""
@@ -465,10 +471,14 @@ def leiden_batch(graphs: Sequence[CSRNetwork], configs: Sequence[LeidenConfig], 
     wf = None
     if warm_from is not None:
         wf = np.ascontiguousarray(warm_from, dtype=np.int64)
-    _check(lib().sc_leiden_batch_ex(ctx.h, harr, carr, count,
-                                    None if wf is None else wf.ctypes.data_as(C.POINTER(C.c_int64)),
-                                    _ptr(offs, _lib.u64p), _ptr(labels, _lib.u64p), _ptr(ncl, _lib.u64p),
-                                    int(n_streams)), ctx)
+    wfp = None if wf is None else wf.ctypes.data_as(C.POINTER(C.c_int64))
+    if union:
+        _check(lib().sc_leiden_batch_union(ctx.h, harr, carr, count, wfp, _ptr(offs, _lib.u64p),
+                                           _ptr(labels, _lib.u64p), _ptr(ncl, _lib.u64p),
+                                           int(max_union_entries)), ctx)
+    else:
+        _check(lib().sc_leiden_batch_ex(ctx.h, harr, carr, count, wfp, _ptr(offs, _lib.u64p),
+                                        _ptr(labels, _lib.u64p), _ptr(ncl, _lib.u64p), int(n_streams)), ctx)
     out = []
     for i in range(count):
         s0 = int(offs[i])
@@ -515,10 +525,11 @@ def sweep_plan(resolutions: Sequence[float], seeds: Sequence[int], objective=Rb,
 
 def leiden_sweep(graph: CSRNetwork, resolutions, seeds, objective=Rb, warm_start: bool = True,
                  n_streams: int = 0, base: LeidenConfig | None = None, split: int = 1,
-                 warm_passes: int | None = 1) -> dict:
+                 warm_passes: int | None = 1, union: bool = False, max_union_entries: int = 0) -> dict:
     """Resolution x seed sweep on one graph: {(resolution, seed): Clustering}."""
     configs, warm, keys = sweep_plan(resolutions, seeds, objective, warm_start, base, split, warm_passes)
-    res = leiden_batch([graph] * len(configs), configs, warm if warm_start else None, n_streams)
+    res = leiden_batch([graph] * len(configs), configs, warm if warm_start else None, n_streams, union,
+                       max_union_entries)
     return dict(zip(keys, res))
 
 

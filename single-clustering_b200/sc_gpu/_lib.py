@@ -131,6 +131,8 @@ SIGNATURES = [
                                   u64p]),
     ("sc_leiden_batch_ex", C.c_int, [vp, C.POINTER(vp), C.POINTER(LeidenConfigC), C.c_uint64,
                                      C.POINTER(C.c_int64), u64p, u64p, u64p, C.c_uint32]),
+    ("sc_leiden_batch_union", C.c_int, [vp, C.POINTER(vp), C.POINTER(LeidenConfigC), C.c_uint64,
+                                        C.POINTER(C.c_int64), u64p, u64p, u64p, C.c_uint64]),
     ("sc_knn_opts_default", None, [C.POINTER(KnnOpts)]),
     ("sc_knn_gaussian", C.c_int, [vp, f32p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(KnnOpts), u32p,
                                   f32p, u64p, u32p, f32p, C.c_uint64, u64p, vpp]),
