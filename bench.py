@@ -517,6 +517,10 @@ class ClockSampler:
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
 
+    def mark(self):
+        """Drops the samples taken so far: only those of the timed region count."""
+        self.samples = []
+
     def _run(self):
         while not self._stop.is_set():
             try:
@@ -545,6 +549,14 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- arms
+# DRAM bytes per algorithmic byte of the local-moving phase, from the warm-cache
+# ncu capture of a whole run on the 1M-point graph of the same family
+# (profiles/local_move_dram_knn10_gmm1000000x30.md: 7.39 GB read + written for
+# 3.866 GB algorithmic); the 4M-point run's traffic is this ratio times its
+# algorithmic bytes.
+LM_TRAFFIC_PER_ALG_BYTE = 7.39 / 3.866
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -630,7 +642,8 @@ def main():
     ap.add_argument("--no-c5", action="store_true", help="skip the 2M x 50 FP8 + learned warm start configuration")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 recall / connectivity checks")
     ap.add_argument("--sweep-points", type=int, default=SWEEP_POINTS)
-    ap.add_argument("--part", default="leiden", choices=["leiden", "knn"])
+    ap.add_argument("--part", default="leiden", choices=["leiden", "knn", "once"],
+                    help="once: one leiden() run on the library's kNN graph of --n points (a small case for ncu)")
     ap.add_argument("--knn-precision", default="bf16", choices=["bf16", "fp8"])
     args = ap.parse_args()
 
@@ -682,6 +695,17 @@ def main():
         if dist:
             dist.destroy_process_group()
         return
+    if args.part == "once":
+        if rank == 0:
+            import sc_gpu
+            ptr, nbr, w = knn_graph_sc(args.n, DIMS, COMPONENTS, GRAPH_SEED, K, local_rank)
+            g = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
+            sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(1.0), seed=LEIDEN_SEED))
+            print(json.dumps({"part": "once", "n": args.n, "edges": g.edge_count(), "entries": g.entry_count(),
+                              **sc_gpu.last_run_stats(local_rank)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
 
     import sc_gpu
     t0 = time.perf_counter()
@@ -691,13 +715,17 @@ def main():
     m = g.edge_count()
     cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(1.0), seed=LEIDEN_SEED)
 
+    # the clock sampler starts before the warm-up: its first nvidia-smi calls
+    # (driver and NVML start-up) stall the host for a moment, and inside the
+    # timed region that stall would leave the GPU idle between launches
+    clocks = ClockSampler(local_rank)
+    clocks.start()
     for _ in range(args.warmup):
         sc_gpu.leiden(g, cfg)
-    clocks = ClockSampler(local_rank)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
-    clocks.start()
+    clocks.mark()
     dev_ms = 0.0
     stats = None
     t = time.perf_counter()
@@ -758,7 +786,12 @@ def main():
             "gpu_launches": int(stats["kernel_launches"]) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "local-move sweeps (decide + apply)",
                          "achieved": lm_gbs, "peak": hbm, "unit": "GB/s",
-                         "frac": lm_gbs / hbm if hbm else None, "traffic": None,
+                         "frac": lm_gbs / hbm if hbm else None,
+                         "traffic": LM_TRAFFIC_PER_ALG_BYTE * stats["alg_bytes_local_move"],
+                         "algorithmic_bytes": stats["alg_bytes_local_move"],
+                         "traffic_note": "DRAM bytes of the phase per run: the warm-cache ncu ratio of the "
+                                         "1M-point run (profiles/local_move_dram_knn10_gmm1000000x30.md) x "
+                                         "this run's algorithmic bytes",
                          "peak_kind": peak_kind},
             "clocks": clk,
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,

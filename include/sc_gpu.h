@@ -365,6 +365,31 @@ typedef struct sc_knn_opts {
 void sc_knn_opts_default(sc_knn_opts* opts);
 
 /*
+ * Exact pruning of the kNN search (no counterpart in single-clustering, whose
+ * kd-tree prunes on the host). A search of n >= 65,536 points groups them
+ * with a deterministic k-means into `clusters` clusters (0: about sqrt(n)/8,
+ * 16..256) and skips, per group of 256 queries, the clusters a ball or slab
+ * bound proves farther than every query's (k+1)-th neighbour among its own
+ * clusters; the lists equal the full scan's. 1 scans every point tile.
+ * Applies to BF16 / FP8 searches of all rows (sc_knn_gaussian); row shards
+ * (sc_knn_search) and FP32 candidates scan every point.
+ */
+sc_status sc_set_knn_clusters(sc_ctx* ctx, uint32_t clusters);
+
+/* Counters of the last kNN search on a context. */
+typedef struct sc_knn_stats {
+    uint64_t clusters;       /* point clusters of the pruned search (0: full scan)     */
+    uint64_t tiles_scanned;  /* (query group, point tile) pairs the contraction ran    */
+    uint64_t tiles_full;     /* the pairs of a full scan                               */
+    uint64_t tiles_pass1;    /* of tiles_scanned: the own-cluster bounding pass        */
+    double ms_cluster;       /* device time: k-means, sort by cluster, cluster extents */
+    double ms_pass1;         /* the own-cluster pass (contraction and re-rank)         */
+    double ms_bounds;        /* the bounds deciding each group's clusters              */
+    double ms_pass2;         /* the final pass (contraction and re-rank)               */
+} sc_knn_stats;
+sc_status sc_knn_last_stats(const sc_ctx* ctx, sc_knn_stats* out);
+
+/*
  * knn_arrayd_kiddo_gaussian / knn_arrayd_hnswlib_gaussian
  * (src/neighborhood/mod.rs:51-202, :359-578), exact on the GPU. X is row-major
  * n x d float. Outputs (host):

@@ -6,6 +6,7 @@
 #include <mutex>
 #include <random>
 #include <thread>
+#include <chrono>
 
 #include "sc_prims.cuh"
 
@@ -235,6 +236,19 @@ sc_status sc_set_wait_limit(sc_ctx* ctx, uint32_t limit) {
 sc_status sc_get_wait_limit(const sc_ctx* ctx, uint32_t* out) {
     if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
     *out = ctx->c.wait_limit;
+    return SC_OK;
+}
+
+sc_status sc_set_knn_clusters(sc_ctx* ctx, uint32_t clusters) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        if (clusters > 256) sc::fail(SC_E_INVALID_ARGUMENT, "at most 256 kNN clusters, got %u", clusters);
+        c.knn_clusters = clusters;
+    });
+}
+
+sc_status sc_knn_last_stats(const sc_ctx* ctx, sc_knn_stats* out) {
+    if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
+    *out = ctx->c.knn_stats;
     return SC_OK;
 }
 
@@ -657,8 +671,17 @@ sc_status sc_leiden_batch_union(sc_ctx* ctx, const sc_graph* const* graphs, cons
                     n[t] = gs[t]->n;
                     if (warm_from && warm_from[i] >= 0) init[t] = labels_out + label_offsets[warm_from[i]];
                 }
+                static const bool trace = std::getenv("SC_TRACE") != nullptr;
+                const auto t0 = std::chrono::steady_clock::now();
                 std::unique_ptr<sc::DevGraph> u(sc::graph_union(c, gs.data(), K));
                 u->stream = c.stream;
+                if (trace) {
+                    sc::sync(c);
+                    std::fprintf(stderr, "[sc] union of %u instances: n=%llu E=%llu exact=%d built in %.3f ms\n", K,
+                                 (unsigned long long)u->n, (unsigned long long)u->E, (int)u->exact_w,
+                                 std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0)
+                                     .count());
+                }
                 sc::DBuf<uint32_t> lab(c, std::max<uint64_t>(u->n, 1));
                 sc::leiden_union(c, *u, K, n.data(), cf.data(), init.data(), lab.get(), ncl.data());
                 uint64_t off = 0;

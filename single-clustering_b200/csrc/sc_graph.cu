@@ -347,9 +347,11 @@ void finalize(Ctx& c, DevGraph& g, bool check_sum) {
 
     // approximate Σ strength (= 2m) decides the regime; exact inside it
     const double approx2m = n ? sums[0] : 0.0;
-    g.exact_w = (g.e0_w == 0x7FFFFFFF) || (approx2m < std::ldexp(1.0, 52 + g.e0_w));
+    const double regime2m = g.part_max_2m > 0.0 ? g.part_max_2m : approx2m;
+    g.exact_w = (g.e0_w == 0x7FFFFFFF) || (regime2m < std::ldexp(1.0, 52 + g.e0_w));
     const double approx_nw = n ? sums[1] : 0.0;
-    g.exact_nw = (g.e0_nw == 0x7FFFFFFF) || (approx_nw < std::ldexp(1.0, 52 + g.e0_nw));
+    const double regime_nw = g.part_max_nw > 0.0 ? g.part_max_nw : approx_nw;
+    g.exact_nw = (g.e0_nw == 0x7FFFFFFF) || (regime_nw < std::ldexp(1.0, 52 + g.e0_nw));
     // Rust-order Σ of the node weights (a fold from -0.0): in the exact regime any
     // order gives these bits, and n > 0 terms >= +0.0 never leave the -0.0 start
     if (n && !g.exact_w) {  // the strengths in the reference's order
@@ -1478,6 +1480,8 @@ namespace {
 DevGraph* contract_exact(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint64_t G, const uint64_t* gstart,
                          const uint32_t* members, const double* nw_new, const double* loops) {
     std::unique_ptr<DevGraph> out(new DevGraph());
+    out->part_max_2m = g.part_max_2m;  // aggregation keeps every instance's totals
+    out->part_max_nw = g.part_max_nw;
     DBuf<uint64_t> cap(c, G + 1), capstart(c, G + 1);
     zero(c, cap.get() + G, 1);
     if (G) {
@@ -1651,6 +1655,14 @@ DevGraph* graph_union(Ctx& c, const DevGraph* const* gs, uint64_t count) {
     if (n >= 0x7FFFFFFFull) fail(SC_E_TOO_MANY_NODES, "a union of %llu nodes exceeds 2^31 - 1", (unsigned long long)n);
     std::unique_ptr<DevGraph> u(new DevGraph());
     u->pooled = true;
+    // sums never cross instances: the heaviest instance decides the regime
+    for (uint64_t i = 0; i < count; ++i) {
+        const DevGraph& g = *gs[i];
+        u->part_max_2m = std::max(u->part_max_2m, std::max(g.part_max_2m, 2.0 * g.total_weight));
+        u->part_max_nw = std::max(u->part_max_nw, std::max(g.part_max_nw, g.total_node_weight));
+    }
+    if (u->part_max_2m == 0.0) u->part_max_2m = -1.0;  // no edges: the union's own (zero) totals decide
+    if (u->part_max_nw == 0.0) u->part_max_nw = -1.0;
     galloc(c, *u, n, E);
     DBuf<UnionPart> d_parts(c, count);
     h2d(c, d_parts.get(), parts.data(), count);
@@ -1686,6 +1698,8 @@ void finish_aggregate(Ctx& c, DevGraph& out) {
 DevGraph* graph_aggregate(Ctx& c, const DevGraph& g, const uint32_t* d_grp, uint32_t G) {
     const uint64_t n = g.n, E = g.E;
     std::unique_ptr<DevGraph> out(new DevGraph());
+    out->part_max_2m = g.part_max_2m;  // aggregation keeps every instance's totals
+    out->part_max_nw = g.part_max_nw;
     // members of each group in ascending node order
     DBuf<uint32_t> idx(c, n), grp_s(c, n), members(c, n);
     DBuf<uint64_t> gstart(c, (uint64_t)G + 1);

@@ -80,6 +80,10 @@ struct Ctx {
     // test hook (sc_test_knn_hold_tiles): the kNN producer issues no point
     // tiles, so the contraction's first wait runs out and the call times out
     uint32_t knn_hold_tiles = 0;
+    // kNN point clusters of the pruned search (sc_set_knn_clusters): 0 picks
+    // a count from n, 1 scans every tile
+    uint32_t knn_clusters = 0;
+    sc_knn_stats knn_stats{};  // the last kNN search on this context
     // side streams for kernels of one step that may run concurrently (fork / join by events)
     cudaStream_t side[3] = {nullptr, nullptr, nullptr};
     cudaEvent_t ev_fork = nullptr;
@@ -179,6 +183,12 @@ struct DevGraph {
     int e0_nw = 0;            // same over node weights
     bool exact_nw = true;
     double total_node_weight = 0.0;  // Σ node_w, Rust `sum()` order
+    // A disjoint union of instances (batched runs) sums nothing across
+    // instances, so its summation regime is that of its heaviest instance:
+    // the largest instance total of Σ strength and of Σ node weight (0: not a
+    // union, the graph's own totals decide).
+    double part_max_2m = 0.0;
+    double part_max_nw = 0.0;
     uint64_t n_hubs = 0;      // nodes whose degree exceeds the shared-memory hash
     // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
     // once, on first need; a benign race between contexts computes it twice)

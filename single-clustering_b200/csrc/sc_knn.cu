@@ -346,12 +346,36 @@ struct KnnSmem {
     static_assert(ROW_OFF % 16 == 0, "staged rows must be 16-byte aligned");
 };
 
+// The point tiles a query group scans, in order: every tile, or (a pruned
+// search) the group's ranges of (first tile, tile count), which never overlap.
+struct TileWalk {
+    const uint2* r;
+    uint32_t nr, ri, off, all;
+    __device__ TileWalk(const uint32_t* rptr, const uint2* rngs, uint32_t g, uint32_t ntiles)
+        : r(rptr ? rngs + rptr[g] : nullptr), nr(rptr ? rptr[g + 1] - rptr[g] : 0), ri(0), off(0), all(ntiles) {}
+    __device__ uint32_t count() const {
+        if (!r) return all;
+        uint32_t c = 0;
+        for (uint32_t i = 0; i < nr; ++i) c += r[i].y;
+        return c;
+    }
+    __device__ uint32_t next() {
+        if (!r) return off++;
+        while (off >= r[ri].y) {
+            ++ri;
+            off = 0;
+        }
+        return r[ri].x + off++;
+    }
+};
+
 // F8: the operands are e4m3 bytes with the row size of BF16 KA columns.
+// rptr / rngs (nullable): the tile ranges of each query group (pruned search).
 template <int KA, bool F8>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
              uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status,
-             uint32_t lim, uint32_t hold_tiles) {
+             uint32_t lim, uint32_t hold_tiles, const uint32_t* __restrict__ rptr, const uint2* __restrict__ rngs) {
     using L = KnnSmem<KA>;
     extern __shared__ __align__(1024) unsigned char raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
@@ -418,7 +442,10 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     ++gi;
                     break;
                 }
-                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                TileWalk walk(rptr, rngs, g, ntiles);
+                const uint32_t cnt = walk.count();
+                for (uint32_t t = 0; t < cnt; ++t, ++it) {
+                    const uint32_t tile = walk.next();
                     const uint32_t s = (uint32_t)(it % L::STAGES);
                     const uint64_t use = it / L::STAGES;
                     if (use > 0 && !mbar_wait(empty + s, (uint32_t)((use - 1) & 1), lim)) {
@@ -427,7 +454,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     }
                     if (*abort_flag) break;
                     mbar_expect_tx(full + s, L::TILE_BYTES);
-                    tma_load_2d(sB + s * L::TILE_BYTES, &tmB, full + s, 0, (int)(t * TILE));
+                    tma_load_2d(sB + s * L::TILE_BYTES, &tmB, full + s, 0, (int)(tile * TILE));
                 }
             }
             // drain: the copies issued last (one per stage, and the query tiles)
@@ -450,7 +477,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     break;
                 }
                 fence_after();
-                for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+                const uint32_t cnt = TileWalk(rptr, rngs, g, ntiles).count();
+                for (uint32_t t = 0; t < cnt; ++t, ++it) {
                     const uint32_t s = (uint32_t)(it % L::STAGES);
                     const uint32_t b = (uint32_t)(it & 1);
                     const uint64_t use_b = it >> 1;
@@ -511,7 +539,10 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 cs[s2 * S + owner] = INFINITY;
                 ci[s2 * S + owner] = 0xFFFFFFFFu;
             }
-            for (uint32_t t = 0; t < ntiles; ++t, ++it) {
+            TileWalk walk(rptr, rngs, g, ntiles);
+            const uint32_t cnt = walk.count();
+            for (uint32_t t = 0; t < cnt; ++t, ++it) {
+                const uint32_t tile = walk.next();
                 const uint32_t b = (uint32_t)(it & 1);
                 if (!mbar_wait(accfull + b, (uint32_t)((it >> 1) & 1), lim)) {
                     *abort_flag = 1;
@@ -532,7 +563,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                     for (int w2 = 8; w2 >= 1; w2 >>= 1)
 #pragma unroll
                         for (int j = 0; j < w2; ++j) m[j] = fminf(m[j], m[j + w2]);
-                    const uint32_t base_idx = t * TILE + h * (TILE / HALVES) + c0;
+                    const uint32_t base_idx = tile * TILE + h * (TILE / HALVES) + c0;
                     unsigned hits = __ballot_sync(0xFFFFFFFFu, m[0] < thr);
                     if (__popc(hits) > COOP_ROWS) {
                         // many rows have candidates: each lane scans its own row
@@ -890,16 +921,22 @@ CUtensorMap make_map(const void* base, uint64_t n, uint32_t row_bytes, bool byte
     return m;
 }
 
+// Tile ranges of each query group of a pruned search (device arrays).
+struct TileLists {
+    const uint32_t* rptr = nullptr;  // ngroups + 1
+    const uint2* rngs = nullptr;     // (first tile, tile count)
+};
+
 template <int KA, bool F8>
 void launch_tc(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, uint64_t n, uint64_t nq, float* cand_score,
-               uint32_t* cand_idx) {
+               uint32_t* cand_idx, const TileLists& tl = TileLists{}) {
     using L = KnnSmem<KA>;
     SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
     const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
     const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
     k_knn_tc<KA, F8><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
                                                                  cand_idx, c.d_status, c.wait_limit,
-                                                                 c.knn_hold_tiles);
+                                                                 c.knn_hold_tiles, tl.rptr, tl.rngs);
     SC_LAUNCH_CHECK();
     c.launches++;
 }
@@ -932,6 +969,196 @@ void candidates_f8(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0,
     launch_tc<32, true>(c, ta, tb, n, nq, cand_score, cand_idx);
 }
 
+// ------------------------------------------------------------ exact pruning
+// Points are grouped by a deterministic k-means (fixed-point sums, ties to the
+// lower centroid) and sorted by group, so every 128-row tile is spatially
+// coherent. A query group first scans the tiles of its own clusters; the exact
+// FP32 re-rank of those candidates bounds each query's (k+1)-th distance from
+// above. A cluster b can hold a closer point only if a lower bound on
+// |q - x| over x in b is at most that distance: the ball bound |q - c_b| - r_b
+// and the slab bound of the direction u from the query's cluster centre to
+// c_b (every x in b projects into [lo, hi] on u, so |q - x| >= the distance
+// from <q, u> to [lo, hi]). The second pass scans the own tiles and those of
+// every cluster some query of the group cannot exclude; skipped points are
+// provably farther than the query's (k+1)-th neighbour, so the result is the
+// full search's.
+constexpr int KM_ITERS = 8;
+
+// Nearest centroid of every point (squared FP32 distance, ties to the lower id).
+__global__ void k_km_assign(const float* __restrict__ X, uint64_t n, uint32_t d, const float* __restrict__ cent,
+                            uint32_t K, uint32_t* assign) {
+    extern __shared__ float s_cent[];
+    for (uint32_t i = threadIdx.x; i < K * d; i += blockDim.x) s_cent[i] = cent[i];
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* x = X + i * d;
+        float best = INFINITY;
+        uint32_t bc = 0;
+        for (uint32_t c = 0; c < K; ++c) {
+            const float* m = s_cent + c * d;
+            float acc = 0.0f;
+            for (uint32_t j = 0; j < d; ++j) {
+                const float df = __fsub_rn(x[j], m[j]);
+                acc = __fmaf_rn(df, df, acc);
+            }
+            if (acc < best) {
+                best = acc;
+                bc = c;
+            }
+        }
+        assign[i] = bc;
+    }
+}
+
+// Per-cluster coordinate sums in fixed point (x * 2^s rounded; integer adds are
+// associative, so the centroids do not depend on the order) and counts.
+__global__ void k_km_accum(const float* __restrict__ X, uint64_t n, uint32_t d, const uint32_t* __restrict__ assign,
+                           uint32_t K, double scale, unsigned long long* sum, unsigned* cnt) {
+    extern __shared__ unsigned long long s_sum[];
+    unsigned* s_cnt = (unsigned*)(s_sum + K * d);
+    for (uint32_t i = threadIdx.x; i < K * d; i += blockDim.x) s_sum[i] = 0;
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x) s_cnt[i] = 0;
+    __syncthreads();
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t c = assign[i];
+        const float* x = X + i * d;
+        for (uint32_t j = 0; j < d; ++j)
+            atomicAdd(s_sum + c * d + j, (unsigned long long)__double2ll_rn((double)x[j] * scale));
+        atomicAdd(s_cnt + c, 1u);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < K * d; i += blockDim.x)
+        if (s_sum[i]) atomicAdd(sum + i, s_sum[i]);
+    for (uint32_t i = threadIdx.x; i < K; i += blockDim.x)
+        if (s_cnt[i]) atomicAdd(cnt + i, s_cnt[i]);
+}
+
+// New centroids; an empty cluster keeps its centroid.
+__global__ void k_km_update(const unsigned long long* __restrict__ sum, const unsigned* __restrict__ cnt, uint32_t K,
+                            uint32_t d, double inv_scale, float* cent) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < K * d; i += gridDim.x * blockDim.x) {
+        const uint32_t c = i / d;
+        if (cnt[c]) cent[i] = (float)((double)(long long)sum[i] * inv_scale / (double)cnt[c]);
+    }
+}
+
+__global__ void k_gather_rows(const float* __restrict__ X, const uint32_t* __restrict__ rows, uint64_t m, uint32_t d,
+                              float* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m * d; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = X[(uint64_t)rows[i / d] * d + i % d];
+}
+
+__global__ void k_iota_u32(uint32_t* x, uint64_t n) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        x[i] = (uint32_t)i;
+}
+
+// Order-preserving map of doubles to unsigned integers (for atomic min / max).
+__device__ __forceinline__ unsigned long long ord64(double x) {
+    const unsigned long long b = (unsigned long long)__double_as_longlong(x);
+    return (b >> 63) ? ~b : (b | 0x8000000000000000ull);
+}
+
+// Radius of every cluster around its centroid (points sorted by cluster),
+// and the extent [lo, hi] of cluster b's points along every direction u_ab.
+// Sorted points make almost every warp one cluster's: its lanes reduce by
+// shuffles and one lane updates the global bound.
+__global__ void k_cluster_extent(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ cl,
+                                 const double* __restrict__ cent, const double* __restrict__ U, uint32_t K,
+                                 unsigned long long* rad, unsigned long long* lo, unsigned long long* hi) {
+    const unsigned FULL = 0xFFFFFFFFu;
+    const unsigned lane = threadIdx.x & 31u;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x - lane; base < n; base += stride) {
+        const uint64_t i = base + lane;
+        const bool ok = i < n;
+        const uint64_t ii = ok ? i : n - 1;  // idle lanes repeat the last point: min / max unchanged
+        const float* x = Xs + ii * d;
+        const uint32_t b = cl[ii];
+        const bool uniform = __all_sync(FULL, b == __shfl_sync(FULL, b, 0));
+        double r2 = 0.0;
+        for (uint32_t j = 0; j < d; ++j) {
+            const double df = (double)x[j] - cent[b * d + j];
+            r2 += df * df;
+        }
+        unsigned long long kr = ord64(sqrt(r2));
+        if (uniform) {
+            for (int o = 16; o; o >>= 1) kr = max(kr, __shfl_xor_sync(FULL, kr, o));
+            if (lane == 0) atomicMax(rad + b, kr);
+        } else {
+            atomicMax(rad + b, kr);
+        }
+        for (uint32_t a = 0; a < K; ++a) {
+            const double* u = U + ((uint64_t)a * K + b) * d;
+            double p = 0.0;
+            for (uint32_t j = 0; j < d; ++j) p += (double)x[j] * u[j];
+            unsigned long long kl = ord64(p), kh = kl;
+            if (uniform) {
+                for (int o = 16; o; o >>= 1) {
+                    kl = min(kl, __shfl_xor_sync(FULL, kl, o));
+                    kh = max(kh, __shfl_xor_sync(FULL, kh, o));
+                }
+                if (lane == 0) {
+                    atomicMin(lo + (uint64_t)a * K + b, kl);
+                    atomicMax(hi + (uint64_t)a * K + b, kh);
+                }
+            } else {
+                atomicMin(lo + (uint64_t)a * K + b, kl);
+                atomicMax(hi + (uint64_t)a * K + b, kh);
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ double unord64(unsigned long long k) {
+    const unsigned long long b = (k >> 63) ? (k & 0x7FFFFFFFFFFFFFFFull) : ~k;
+    return __longlong_as_double((long long)b);
+}
+
+// For every sorted query: the clusters whose lower bound does not exclude them
+// (given its current (k+1)-th distance), as bits of its group's mask.
+__global__ void k_cluster_needs(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ cl,
+                                const uint32_t* __restrict__ perm, const float* __restrict__ d2k, uint32_t k1,
+                                const double* __restrict__ cent, const unsigned long long* __restrict__ rad,
+                                const double* __restrict__ U, const unsigned long long* __restrict__ lo,
+                                const unsigned long long* __restrict__ hi, uint32_t K, uint32_t words,
+                                unsigned long long* mask) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float* x = Xs + i * d;
+        const uint32_t a = cl[i];
+        const float kd2 = d2k[(uint64_t)perm[i] * k1 + (k1 - 1)];
+        // no (k+1)-th neighbour among the own clusters: every cluster is needed
+        const double kth = isfinite(kd2) ? sqrt((double)kd2) * (1.0 + 1e-5) + 1e-6 : INFINITY;
+        unsigned long long* mk = mask + (i / (QT * TILE)) * words;
+        for (uint32_t b = 0; b < K; ++b) {
+            if (b == a) continue;
+            double dc = 0.0;
+            for (uint32_t j = 0; j < d; ++j) {
+                const double df = (double)x[j] - cent[b * d + j];
+                dc += df * df;
+            }
+            double lb = sqrt(dc) - unord64(rad[b]);
+            const double* u = U + ((uint64_t)a * K + b) * d;
+            double p = 0.0;
+            for (uint32_t j = 0; j < d; ++j) p += (double)x[j] * u[j];
+            const double l = unord64(lo[(uint64_t)a * K + b]), h = unord64(hi[(uint64_t)a * K + b]);
+            lb = fmax(lb, fmax(l - p, p - h));
+            if (lb <= kth) atomicOr(mk + b / 64, 1ull << (b % 64));
+        }
+    }
+}
+
+// Candidate rows of the sorted queries, re-indexed to the original points.
+__global__ void k_unsort_candidates(const uint32_t* __restrict__ cand, const uint32_t* __restrict__ perm, uint64_t n,
+                                    uint32_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n * RTOTAL;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t q = i / RTOTAL;
+        const uint32_t j = cand[i];
+        out[(uint64_t)perm[q] * RTOTAL + i % RTOTAL] = j < n ? perm[j] : 0xFFFFFFFFu;
+    }
+}
+
 void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
     if (d == 0 || d > 62) fail(SC_E_UNSUPPORTED, "kNN supports 1..62 dimensions, got %llu", (unsigned long long)d);
     if (k + 1 > 32) fail(SC_E_UNSUPPORTED, "kNN supports k <= 31");
@@ -942,6 +1169,277 @@ void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
         fail(SC_E_UNSUPPORTED, "the FP8 contraction supports 1..61 dimensions, got %llu", (unsigned long long)d);
 }
 
+constexpr uint64_t PRUNE_MIN_POINTS = 65536;
+
+uint32_t prune_clusters(const Ctx& c, uint64_t n) {
+    if (c.knn_clusters == 1 || n < PRUNE_MIN_POINTS) return 0;
+    if (c.knn_clusters) return std::min<uint32_t>(c.knn_clusters, 256);
+    const double k = std::round(std::sqrt((double)n) / 8.0);
+    return (uint32_t)std::min(256.0, std::max(16.0, k));
+}
+
+// BF16 or FP8 operands of the points X (rows = queries = candidates).
+struct TcOperands {
+    DBuf<uint8_t> A, B;
+    CUtensorMap ta{}, tb{};
+    int kind = 0;  // 0: BF16 KA = 32, 1: BF16 KA = 64, 2: e4m3
+};
+
+void prep_operands(Ctx& c, const float* dX, uint64_t n, uint32_t d, int precision, TcOperands& op) {
+    if (precision == SC_KNN_FP8) {
+        op.kind = 2;
+        op.A.alloc(c, n * 64);
+        op.B.alloc(c, n * 64);
+        DBuf<unsigned> mx(c, 2);
+        zero(c, mx.get(), 2);
+        k_knn_scales<<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, mx.get(), mx.get() + 1);
+        k_knn_prep_f8<<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, mx.get(), mx.get() + 1, op.A.get(),
+                                                              op.B.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+        op.ta = make_map(op.A.get(), n, 64, true);
+        op.tb = make_map(op.B.get(), n, 64, true);
+        return;
+    }
+    const uint32_t KA = d <= 30 ? 32 : 64;
+    op.kind = KA == 32 ? 0 : 1;
+    op.A.alloc(c, n * KA * 2);
+    op.B.alloc(c, n * KA * 2);
+    __nv_bfloat16* A = (__nv_bfloat16*)op.A.get();
+    __nv_bfloat16* B = (__nv_bfloat16*)op.B.get();
+    if (KA == 32) k_knn_prep<32><<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, A, B);
+    else k_knn_prep<64><<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, A, B);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    op.ta = make_map(A, n, KA * 2, false);
+    op.tb = make_map(B, n, KA * 2, false);
+}
+
+void launch_operands(Ctx& c, const TcOperands& op, uint64_t n, float* cscore, uint32_t* cidx, const TileLists& tl) {
+    if (op.kind == 2) launch_tc<32, true>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
+    else if (op.kind == 0) launch_tc<32, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
+    else launch_tc<64, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
+}
+
+// Merged tile ranges of the point ranges [b, e) given in ascending order of b.
+void tiles_of(const std::vector<std::pair<uint64_t, uint64_t>>& pts, std::vector<uint2>& out, uint64_t& total) {
+    const size_t first = out.size();
+    uint64_t cur_b = 0, cur_e = 0;
+    bool open = false;
+    for (const auto& pe : pts) {
+        if (pe.second <= pe.first) continue;
+        const uint64_t tb = pe.first / TILE, te = (pe.second + TILE - 1) / TILE;
+        if (open && tb <= cur_e) {
+            cur_e = std::max(cur_e, te);
+        } else {
+            if (open) out.push_back(make_uint2((uint32_t)cur_b, (uint32_t)(cur_e - cur_b)));
+            cur_b = tb;
+            cur_e = te;
+            open = true;
+        }
+    }
+    if (open) out.push_back(make_uint2((uint32_t)cur_b, (uint32_t)(cur_e - cur_b)));
+    for (size_t i = first; i < out.size(); ++i) total += out[i].y;
+}
+
+// The exact k+1 nearest points of every point by the pruned search (see
+// "exact pruning" above); the same lists as the full scan.
+// Device time between events recorded on the context's stream.
+struct StageTimer {
+    Ctx& c;
+    std::vector<cudaEvent_t> ev;
+    explicit StageTimer(Ctx& ctx) : c(ctx) {}
+    ~StageTimer() {
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
+    void mark() {
+        cudaEvent_t e;
+        SC_CUDA(cudaEventCreate(&e));
+        ev.push_back(e);
+        SC_CUDA(cudaEventRecord(e, c.stream));
+    }
+    double ms(size_t a, size_t b) {
+        SC_CUDA(cudaEventSynchronize(ev[b]));
+        float t = 0.0f;
+        SC_CUDA(cudaEventElapsedTime(&t, ev[a], ev[b]));
+        return t;
+    }
+};
+
+void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t k, int precision, uint32_t K,
+                       uint32_t* idx, float* d2) {
+    const uint32_t k1 = k + 1;
+    StageTimer tm(c);
+    tm.mark();
+    // 1. deterministic k-means: K centroids from evenly spaced points, KM_ITERS Lloyd steps
+    DBuf<unsigned> mx(c, 2);
+    zero(c, mx.get(), 2);
+    k_knn_scales<<<grid_for(n, 256), 256, 0, c.stream>>>(dX, n, d, mx.get(), mx.get() + 1);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    unsigned hmx[2];
+    d2h(c, hmx, mx.get(), 2);
+    std::vector<uint32_t> rows(K);
+    for (uint32_t i = 0; i < K; ++i) rows[i] = (uint32_t)((uint64_t)i * n / K);
+    DBuf<uint32_t> d_rows(c, K);
+    h2d(c, d_rows.get(), rows.data(), K);
+    DBuf<float> cent(c, (uint64_t)K * d);
+    k_gather_rows<<<grid_for((uint64_t)K * d, 256), 256, 0, c.stream>>>(dX, d_rows.get(), K, d, cent.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    sync(c);
+    float maxabs;
+    std::memcpy(&maxabs, &hmx[0], 4);
+    // sums of n coordinates of magnitude <= maxabs stay below 2^62 in fixed point
+    const double span = std::max(1e-30, (double)maxabs * (double)n);
+    const int e = std::min(40, (int)std::floor(62.0 - std::log2(span)) - 1);
+    const double scale = std::ldexp(1.0, e), inv_scale = std::ldexp(1.0, -e);
+    DBuf<uint32_t> assign(c, n);
+    DBuf<unsigned long long> sums(c, (uint64_t)K * d);
+    DBuf<unsigned> cnt(c, K);
+    const size_t sm_assign = (size_t)K * d * 4, sm_accum = (size_t)K * d * 8 + (size_t)K * 4;
+    SC_CUDA(cudaFuncSetAttribute(k_km_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_assign));
+    SC_CUDA(cudaFuncSetAttribute(k_km_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_accum));
+    const unsigned g_assign = grid_for(n, 256, (unsigned)c.sm_count * 4);
+    const unsigned g_accum = grid_for(n, 256, (unsigned)c.sm_count);
+    for (int it = 0; it <= KM_ITERS; ++it) {
+        k_km_assign<<<g_assign, 256, sm_assign, c.stream>>>(dX, n, d, cent.get(), K, assign.get());
+        c.launches++;
+        if (it == KM_ITERS) break;
+        zero(c, sums.get(), (uint64_t)K * d);
+        zero(c, cnt.get(), K);
+        k_km_accum<<<g_accum, 256, sm_accum, c.stream>>>(dX, n, d, assign.get(), K, scale, sums.get(), cnt.get());
+        k_km_update<<<grid_for((uint64_t)K * d, 256), 256, 0, c.stream>>>(sums.get(), cnt.get(), K, d, inv_scale,
+                                                                         cent.get());
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+    }
+    // 2. points sorted by cluster (stable: ascending point id inside a cluster)
+    DBuf<uint32_t> iota(c, n), cl_s(c, n), perm(c, n);
+    k_iota_u32<<<grid_for(n, 256), 256, 0, c.stream>>>(iota.get(), n);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    sort_pairs(c, assign.get(), cl_s.get(), iota.get(), perm.get(), n, bits_for(K - 1));
+    assign.release();
+    iota.release();
+    DBuf<float> Xs(c, n * d);
+    k_gather_rows<<<grid_for(n * d, 256), 256, 0, c.stream>>>(dX, perm.get(), n, d, Xs.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    std::vector<uint32_t> h_cl(n);
+    std::vector<float> h_cent((uint64_t)K * d);
+    d2h(c, h_cl.data(), cl_s.get(), n);
+    d2h(c, h_cent.data(), cent.get(), (uint64_t)K * d);
+    sync(c);
+    std::vector<uint64_t> start(K + 1, 0);
+    for (uint64_t i = 0; i < n; ++i) start[h_cl[i] + 1]++;
+    for (uint32_t b = 0; b < K; ++b) start[b + 1] += start[b];
+    // 3. cluster extents: radius, and [lo, hi] along each direction between centres
+    std::vector<double> cent64(h_cent.begin(), h_cent.end());
+    std::vector<double> U((uint64_t)K * K * d, 0.0);
+    for (uint32_t a = 0; a < K; ++a)
+        for (uint32_t b = 0; b < K; ++b) {
+            double nrm = 0.0;
+            for (uint32_t j = 0; j < d; ++j) {
+                const double t = cent64[b * d + j] - cent64[a * d + j];
+                nrm += t * t;
+            }
+            nrm = std::sqrt(nrm);
+            if (a == b || nrm == 0.0) continue;  // a zero direction bounds nothing (slab 0)
+            for (uint32_t j = 0; j < d; ++j) U[((uint64_t)a * K + b) * d + j] = (cent64[b * d + j] - cent64[a * d + j]) / nrm;
+        }
+    DBuf<double> d_cent(c, (uint64_t)K * d), d_U(c, (uint64_t)K * K * d);
+    h2d(c, d_cent.get(), cent64.data(), (uint64_t)K * d);
+    h2d(c, d_U.get(), U.data(), (uint64_t)K * K * d);
+    DBuf<unsigned long long> rad(c, K), lo(c, (uint64_t)K * K), hi(c, (uint64_t)K * K);
+    zero(c, rad.get(), K);
+    zero(c, hi.get(), (uint64_t)K * K);
+    SC_CUDA(cudaMemsetAsync(lo.get(), 0xFF, (uint64_t)K * K * 8, c.stream));
+    k_cluster_extent<<<grid_for(n, 256), 256, 0, c.stream>>>(Xs.get(), n, d, cl_s.get(), d_cent.get(), d_U.get(), K,
+                                                            rad.get(), lo.get(), hi.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    // 4. operands of the sorted points
+    TcOperands op;
+    prep_operands(c, Xs.get(), n, d, precision, op);
+    tm.mark();  // 1: clustering done
+    const uint64_t ngroups = (n + QT * TILE - 1) / (QT * TILE);
+    const uint64_t ntiles = (n + TILE - 1) / TILE;
+    auto own = [&](uint64_t g, std::vector<std::pair<uint64_t, uint64_t>>& pts) {
+        const uint32_t a0 = h_cl[g * QT * TILE], a1 = h_cl[std::min<uint64_t>(n, (g + 1) * QT * TILE) - 1];
+        pts.emplace_back(start[a0], start[a1 + 1]);
+        return std::make_pair(a0, a1);
+    };
+    DBuf<float> cscore(c, n * RTOTAL);
+    DBuf<uint32_t> cidx(c, n * RTOTAL), corig(c, n * RTOTAL);
+    auto run_pass = [&](const std::vector<uint32_t>& rptr, const std::vector<uint2>& rngs, uint32_t* out_idx,
+                        float* out_d2) {
+        DBuf<uint32_t> d_rptr(c, rptr.size());
+        DBuf<uint2> d_rngs(c, std::max<size_t>(rngs.size(), 1));
+        h2d(c, d_rptr.get(), rptr.data(), rptr.size());
+        h2d(c, d_rngs.get(), rngs.data(), rngs.size());
+        launch_operands(c, op, n, cscore.get(), cidx.get(), TileLists{d_rptr.get(), d_rngs.get()});
+        k_unsort_candidates<<<grid_for(n * RTOTAL, 256), 256, 0, c.stream>>>(cidx.get(), perm.get(), n, corig.get());
+        k_knn_rerank<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(dX, n, d, k, 0, n, corig.get(), out_idx, out_d2);
+        SC_LAUNCH_CHECK();
+        c.launches += 2;
+        sync(c);  // the host arrays above must outlive the copies
+    };
+    // 5. pass 1: every query group against its own clusters
+    std::vector<uint32_t> rptr(ngroups + 1, 0);
+    std::vector<uint2> rngs;
+    uint64_t tiles1 = 0;
+    for (uint64_t g = 0; g < ngroups; ++g) {
+        std::vector<std::pair<uint64_t, uint64_t>> pts;
+        own(g, pts);
+        tiles_of(pts, rngs, tiles1);
+        rptr[g + 1] = (uint32_t)rngs.size();
+    }
+    DBuf<uint32_t> idx1(c, n * k1);
+    DBuf<float> d21(c, n * k1);
+    run_pass(rptr, rngs, idx1.get(), d21.get());
+    tm.mark();  // 2: pass 1 done
+    // 6. the clusters every group still needs
+    const uint32_t words = (K + 63) / 64;
+    DBuf<unsigned long long> mask(c, ngroups * words);
+    zero(c, mask.get(), ngroups * words);
+    k_cluster_needs<<<grid_for(n, 128), 128, 0, c.stream>>>(Xs.get(), n, d, cl_s.get(), perm.get(), d21.get(), k1,
+                                                           d_cent.get(), rad.get(), d_U.get(), lo.get(), hi.get(), K,
+                                                           words, mask.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    std::vector<unsigned long long> h_mask(ngroups * words);
+    d2h(c, h_mask.data(), mask.get(), ngroups * words);
+    tm.mark();  // 3: bounds done
+    sync(c);
+    idx1.release();
+    d21.release();
+    // 7. pass 2: own clusters and every needed one
+    rngs.clear();
+    uint64_t tiles2 = 0;
+    for (uint64_t g = 0; g < ngroups; ++g) {
+        std::vector<std::pair<uint64_t, uint64_t>> pts;
+        const auto ar = own(g, pts);
+        for (uint32_t b = 0; b < K; ++b) {
+            if (b >= ar.first && b <= ar.second) continue;
+            if (h_mask[g * words + b / 64] >> (b % 64) & 1ull) pts.emplace_back(start[b], start[b + 1]);
+        }
+        std::sort(pts.begin(), pts.end());
+        tiles_of(pts, rngs, tiles2);
+        rptr[g + 1] = (uint32_t)rngs.size();
+    }
+    run_pass(rptr, rngs, idx, d2);
+    tm.mark();  // 4: pass 2 done
+    c.knn_stats.ms_cluster = tm.ms(0, 1);
+    c.knn_stats.ms_pass1 = tm.ms(1, 2);
+    c.knn_stats.ms_bounds = tm.ms(2, 3);
+    c.knn_stats.ms_pass2 = tm.ms(3, 4);
+    c.knn_stats.clusters = K;
+    c.knn_stats.tiles_scanned = tiles1 + tiles2;
+    c.knn_stats.tiles_pass1 = tiles1;
+    c.knn_stats.tiles_full = ngroups * ntiles;
+}
+
 // Exact (brute-force) k+1 nearest points of the queries q0 .. q0 + nq - 1
 // among all n points of the device array dX: 64 candidates per query (the 32
 // best of each half of the candidate columns) from the BF16 or FP8 tensor-core
@@ -950,7 +1448,20 @@ void knn_check(uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts) {
 // distance, ties by lower index.
 void knn_search_device(Ctx& c, const float* dX, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t nq,
                        int precision, uint32_t* idx, float* d2) {
+    c.knn_stats = sc_knn_stats{};
     if (!nq) return;
+    if (precision != SC_KNN_FP32 && q0 == 0 && nq == n) {
+        const uint32_t K = prune_clusters(c, n);
+        if (K) {
+            knn_search_pruned(c, dX, n, (uint32_t)d, (uint32_t)k, precision, K, idx, d2);
+            check_device_status(c);
+            return;
+        }
+    }
+    {
+        const uint64_t groups = (nq + QT * TILE - 1) / (QT * TILE), tiles = (n + TILE - 1) / TILE;
+        c.knn_stats.tiles_scanned = c.knn_stats.tiles_full = groups * tiles;
+    }
     DBuf<float> cscore(c, precision == SC_KNN_FP32 ? 0 : nq * RTOTAL);
     DBuf<uint32_t> cidx(c, nq * RTOTAL);
     if (precision == SC_KNN_FP32) {

@@ -1857,7 +1857,9 @@ void run_pass_multi(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C
     std::vector<long long> gains(K);
     std::vector<uint32_t> G(K);
     uint64_t C = C0;
+    static const bool trace = std::getenv("SC_TRACE") != nullptr;
     for (uint64_t level = 0;; ++level) {
+        const sc_run_stats before = st;
         for (uint32_t i = 0; i < K; ++i)
             if (!frozen[i] && level >= mp.cfgs[i].max_levels) frozen[i] = 1;
         if (std::all_of(frozen.begin(), frozen.end(), [](uint8_t f) { return f != 0; })) break;
@@ -1924,13 +1926,28 @@ void run_pass_multi(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C
         st.levels++;
         uint64_t Gtot = 0;
         bool any_shrinks = false;
+        uint32_t running = 0;
         for (uint32_t i = 0; i < K; ++i) {
             Gtot += G[i];
+            running += !frozen[i];
             if (!frozen[i] && G[i] >= nI[i]) frozen[i] = 1;  // the graph no longer shrinks (mod.rs:263-265)
             if (!frozen[i]) any_shrinks = true;
         }
+        auto trace_level = [&]() {
+            if (!trace) return;
+            clock.collect();
+            std::fprintf(stderr,
+                         "[sc] union level %llu instances=%u running=%u n=%llu E=%llu exact=%d groups=%llu sweeps=%llu "
+                         "moves=%llu lm=%.3fms ref=%.3fms agg=%.3fms\n",
+                         (unsigned long long)level, K, running, (unsigned long long)nl, (unsigned long long)gl->E,
+                         (int)gl->exact_w, (unsigned long long)Gtot,
+                         (unsigned long long)(st.local_move_sweeps - before.local_move_sweeps),
+                         (unsigned long long)(st.moves - before.moves), st.ms_local_move - before.ms_local_move,
+                         st.ms_refine - before.ms_refine, st.ms_aggregate - before.ms_aggregate);
+        };
         if (!any_shrinks) {
             clock.stop(t_agg, &st.ms_aggregate);
+            trace_level();
             break;
         }
         std::unique_ptr<DevGraph> coarse(graph_aggregate(c, *gl, grp.get(), (uint32_t)Gtot));
@@ -1952,6 +1969,7 @@ void run_pass_multi(Ctx& c, const DevGraph& g0, const uint32_t* init, uint64_t C
         set_bounds();
         h2d(c, d_bounds.get(), bounds.data(), K + 1);
         clock.stop(t_agg, &st.ms_aggregate);
+        trace_level();
     }
     // final ascending renumber per instance (mod.rs:282-286)
     const uint64_t nl = gl->n;

@@ -647,6 +647,22 @@ def knn_gaussian(X, k: int, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_I
     return NeighborResult(idx, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), graph)
 
 
+def set_knn_clusters(clusters: int, device: int | None = None) -> None:
+    """Point clusters of the exact pruned kNN search (sc_set_knn_clusters):
+    0 picks a count from n, 1 scans every point tile."""
+    ctx = context(device)
+    _check(lib().sc_set_knn_clusters(ctx.h, int(clusters)), ctx)
+
+
+def knn_last_stats(device: int | None = None) -> dict:
+    """Counters of the last kNN search on this thread's context: clusters,
+    (query group, point tile) pairs scanned and those of a full scan."""
+    ctx = context(device)
+    st = _lib.KnnStats()
+    _check(lib().sc_knn_last_stats(ctx.h, C.byref(st)), ctx)
+    return {name: getattr(st, name) for name, _ in _lib.KnnStats._fields_}
+
+
 def _knn_opts(sigma=SIGMA_MEDIAN, sym=SYM_LOWER_ID, precision=KNN_BF16, squared=False):
     opts = _lib.KnnOpts()
     lib().sc_knn_opts_default(C.byref(opts))

@@ -91,6 +91,19 @@ class KnnOpts(C.Structure):
     ]
 
 
+class KnnStats(C.Structure):
+    _fields_ = [
+        ("clusters", C.c_uint64),
+        ("tiles_scanned", C.c_uint64),
+        ("tiles_full", C.c_uint64),
+        ("tiles_pass1", C.c_uint64),
+        ("ms_cluster", C.c_double),
+        ("ms_pass1", C.c_double),
+        ("ms_bounds", C.c_double),
+        ("ms_pass2", C.c_double),
+    ]
+
+
 # (name, restype, argtypes) of every symbol include/sc_gpu.h declares
 SIGNATURES = [
     ("sc_abi_version", C.c_uint32, []),
@@ -106,6 +119,8 @@ SIGNATURES = [
     ("sc_set_wait_limit", C.c_int, [vp, C.c_uint32]),
     ("sc_get_wait_limit", C.c_int, [vp, C.POINTER(C.c_uint32)]),
     ("sc_test_knn_hold_tiles", C.c_int, [vp, C.c_int32]),
+    ("sc_set_knn_clusters", C.c_int, [vp, C.c_uint32]),
+    ("sc_knn_last_stats", C.c_int, [vp, C.POINTER(KnnStats)]),
     ("sc_autotune", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), C.POINTER(Tuning), f64p, f64p,
                               C.POINTER(C.c_uint32)]),
     ("sc_leiden_config_default", None, [C.POINTER(LeidenConfigC)]),

@@ -153,13 +153,17 @@ class WarmStartResult:
 
 
 def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
-                      verify: bool = True, tolerance: float = 1e-4, context=None) -> WarmStartResult:
+                      verify: bool = True, tolerance: float = 1e-4, context=None,
+                      warm_passes: int | None = 1) -> WarmStartResult:
     """leiden_from(model's proposal). With `verify`, the plain singleton start also
     runs and the proposal is kept only if its final modularity (for CPM: its CPM
     quality / total weight) is at least the plain one's minus `tolerance`;
     otherwise the plain result is returned.
     `context` is (coarse, fine), the partitions at the neighbouring lower and
-    higher resolutions the model was trained to read."""
+    higher resolutions the model was trained to read. The warm run makes
+    `warm_passes` passes (the proposal stands in for the first pass of a plain
+    run, which takes the singleton start to a converged partition); None keeps
+    config.n_iterations."""
     from . import leiden, leiden_from, modularity, quality, Rb
     is_rb = isinstance(config.objective, Rb)
     gamma = config.objective.resolution if is_rb else 1.0
@@ -174,7 +178,11 @@ def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, 
     t0 = time.perf_counter()
     prop, kprop = model.propose(graph, gamma, threshold, core_fraction, context=context)
     t_prop = (time.perf_counter() - t0) * 1e3
-    warm = leiden_from(graph, config, prop)
+    wcfg = config
+    if warm_passes is not None:
+        from dataclasses import replace
+        wcfg = replace(config, n_iterations=int(warm_passes))
+    warm = leiden_from(graph, wcfg, prop)
     sw = graph._ctx.run_stats()
     q_w = score(warm.labels())
     res = WarmStartResult(warm.labels(), warm.n_clusters(), True, q_w, None, sw["local_move_sweeps"], None,

@@ -236,3 +236,57 @@ def test_fp32_candidates_match_exact_fp64(n, d, k):
     b = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=sc_gpu.KNN_BF16)
     assert np.array_equal(b.index, r.index)
     assert np.array_equal(b.conn_w.view(np.uint32), r.conn_w.view(np.uint32))
+
+
+def _full_and_pruned(X, k, precision=sc_gpu.KNN_BF16, clusters=0):
+    try:
+        sc_gpu.set_knn_clusters(1)
+        full = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=precision)
+        st_full = sc_gpu.knn_last_stats()
+        sc_gpu.set_knn_clusters(clusters)
+        pr = sc_gpu.knn_gaussian(X, k, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=precision)
+        st = sc_gpu.knn_last_stats()
+    finally:
+        sc_gpu.set_knn_clusters(0)
+    return full, st_full, pr, st
+
+
+@pytest.mark.parametrize("n,d,comps,clusters", [(200_000, 30, 50, 0), (150_000, 50, 20, 0), (100_000, 30, 1, 0),
+                                                 (120_000, 20, 80, 16)])
+def test_pruned_search_equals_full_scan(n, d, comps, clusters):
+    """The exact pruned search (k-means clusters, ball and slab bounds) returns
+    the full scan's lists and connectivities bit for bit, scanning fewer tiles
+    where the points cluster; a single Gaussian (comps = 1) still comes out
+    exact, whatever it skips."""
+    X, _ = synth.gaussian_mixture(n, d, comps, seed=n + d, sigma=(0.7, 1.5))
+    full, st_full, pr, st = _full_and_pruned(X, 10, clusters=clusters)
+    assert st_full["clusters"] == 0 and st_full["tiles_scanned"] == st_full["tiles_full"]
+    assert st["clusters"] == (clusters or st["clusters"]) and st["clusters"] >= 16
+    assert np.array_equal(pr.index, full.index)
+    assert np.array_equal(pr.distances.view(np.uint32), full.distances.view(np.uint32))
+    assert np.array_equal(pr.conn_ptrs, full.conn_ptrs) and np.array_equal(pr.conn_nbrs, full.conn_nbrs)
+    assert np.array_equal(pr.conn_w.view(np.uint32), full.conn_w.view(np.uint32))
+    if comps >= 20:
+        assert st["tiles_scanned"] < 0.5 * st["tiles_full"], st
+
+
+def test_pruned_search_on_structureless_points():
+    """Uniform points in a cube: the bounds exclude little, the lists stay exact."""
+    rng = np.random.Generator(np.random.PCG64(3))
+    X = rng.uniform(-1.0, 1.0, size=(70_000, 8)).astype(np.float32)
+    full, _, pr, st = _full_and_pruned(X, 15)
+    assert np.array_equal(pr.index, full.index)
+    assert np.array_equal(pr.conn_w.view(np.uint32), full.conn_w.view(np.uint32))
+
+
+def test_pruned_fp8_search_keeps_its_recall():
+    n, d = 120_000, 50
+    X, _ = synth.gaussian_mixture(n, d, 60, seed=8, sigma=(0.5, 2.0))
+    full, _, pr, st = _full_and_pruned(X, 15, precision=sc_gpu.KNN_FP8)
+    sample = np.random.Generator(np.random.PCG64(2)).choice(n, 1500, replace=False)
+    # against the BF16 full scan, exact on this mixture (fewer competitors for a
+    # query's candidate slots can only keep more of its true neighbours)
+    ref = sc_gpu.knn_gaussian(X, 15, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
+    rec_full = K.recall(full.index[sample], ref.index[sample])
+    rec_pr = K.recall(pr.index[sample], ref.index[sample])
+    assert rec_pr >= rec_full - 1e-3, (rec_pr, rec_full)
