@@ -367,10 +367,11 @@ void sc_knn_opts_default(sc_knn_opts* opts);
 /*
  * Exact pruning of the kNN search (no counterpart in single-clustering, whose
  * kd-tree prunes on the host). A search of n >= 65,536 points groups them
- * with a deterministic k-means into `clusters` clusters (0: about sqrt(n)/8,
- * 16..256) and skips, per group of 256 queries, the clusters a ball or slab
- * bound proves farther than every query's (k+1)-th neighbour among its own
- * clusters; the lists equal the full scan's. 1 scans every point tile.
+ * with a deterministic k-means into `clusters` clusters (0: n / 8192, within
+ * 16..256), orders each cluster's points by fine cells of about 256 points,
+ * and skips, per group of 256 queries, every cell that a ball or slab bound
+ * proves farther than each query's (k+1)-th neighbour among its own cluster;
+ * the lists equal the full scan's. 1 scans every point tile.
  * Applies to BF16 / FP8 searches of all rows (sc_knn_gaussian); row shards
  * (sc_knn_search) and FP32 candidates scan every point.
  */

@@ -266,7 +266,7 @@ def test_pruned_search_equals_full_scan(n, d, comps, clusters):
     assert np.array_equal(pr.distances.view(np.uint32), full.distances.view(np.uint32))
     assert np.array_equal(pr.conn_ptrs, full.conn_ptrs) and np.array_equal(pr.conn_nbrs, full.conn_nbrs)
     assert np.array_equal(pr.conn_w.view(np.uint32), full.conn_w.view(np.uint32))
-    if comps >= 20:
+    if comps >= 20 and clusters == 0:
         assert st["tiles_scanned"] < 0.5 * st["tiles_full"], st
 
 
