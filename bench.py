@@ -352,7 +352,7 @@ def run_c2(device_index, cpu=True):
         t = time.perf_counter()
         r = sc_gpu.knn_gaussian(X, C2_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
                                 device=device_index)
-        arm = {"knn_build_s": time.perf_counter() - t,
+        arm = {"knn_build_s": time.perf_counter() - t, "pruning": sc_gpu.knn_last_stats(device_index),
                "accuracy": knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, C2_K,
                                         f"cuda:{device_index}")}
         csr[name] = (r.conn_ptrs, r.conn_nbrs, r.conn_w)
@@ -415,7 +415,7 @@ def run_c5(device_index):
         t = time.perf_counter()
         r = sc_gpu.knn_gaussian(X, C5_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, precision=prec,
                                 device=device_index)
-        out["knn"][name] = {"build_s": time.perf_counter() - t,
+        out["knn"][name] = {"build_s": time.perf_counter() - t, "pruning": sc_gpu.knn_last_stats(device_index),
                             "accuracy": knn_accuracy(X, r.index, r.conn_ptrs, r.conn_nbrs, r.conn_w, C5_K, dev)}
         if name == "fp8":
             keep = (r.conn_ptrs, r.conn_nbrs, r.conn_w)
@@ -487,7 +487,8 @@ def library_knn_leg(X, ptr, nbr, w, device_index, accuracy=True):
     sc_gpu.knn_gaussian(X[:65536], K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
     t = time.perf_counter()
     r = sc_gpu.knn_gaussian(X, K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
-    out = {"build_s": time.perf_counter() - t, "precision": "bf16", "points": int(X.shape[0])}
+    out = {"build_s": time.perf_counter() - t, "precision": "bf16", "points": int(X.shape[0]),
+           "pruning": sc_gpu.knn_last_stats(device_index)}
     same_ptr = np.array_equal(r.conn_ptrs, ptr)
     same_nbr = same_ptr and np.array_equal(r.conn_nbrs, nbr)
     out["same_edges_as_exact_graph"] = bool(same_nbr)
