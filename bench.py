@@ -153,6 +153,44 @@ def run_sweep(device_index, n_points=SWEEP_POINTS, n_streams=16, split=8, accura
             "knn_accuracy": acc}
 
 
+def run_sweep_sharded(device_index, rank, world, dist, n_points=SWEEP_POINTS, n_streams=16, warm_passes=1):
+    """The sweep's warm-started chains dealt across the ranks by cost (one
+    chain per seed: parallel.run_sharded), each rank running its share on its
+    own GPU; the only collective is one all-gather of the instances'
+    modularities after the runs. Every rank builds the same kNN graph. Timed
+    from a barrier to the end of the local runs, max over ranks."""
+    import torch
+    import sc_gpu
+    from sc_gpu import parallel, synth
+    X, _ = synth.gaussian_mixture(n_points, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_SEED, sigma=(0.7, 1.5))
+    r = sc_gpu.knn_gaussian(X, SWEEP_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w, device=device_index)
+    del X, r
+    res = np.geomspace(0.1, 3.0, SWEEP_RESOLUTIONS)
+    configs, warm, keys = sc_gpu.sweep_plan(res, SWEEP_SEEDS, sc_gpu.Rb, True, None, 8, warm_passes)
+    cost = [3.0 if w < 0 else 1.0 for w in warm]  # a singleton start costs about three warm runs
+    timing = {}
+
+    def run_local(ids, local_warm):
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        out = sc_gpu.leiden_batch([g] * len(ids), [configs[i] for i in ids], local_warm, n_streams)
+        timing["s"] = time.perf_counter() - t
+        timing["instances"] = len(ids)
+        return [sc_gpu.modularity(g, c.labels(), keys[i][0]) for i, c in zip(ids, out)]
+
+    sc_gpu.leiden_batch([g] * 4, configs[:4], warm[:4], n_streams)  # warm-up
+    dist.barrier()
+    qs = parallel.run_sharded(run_local, len(configs), warm, cost, rank, world)
+    tt = torch.tensor([timing["s"]], dtype=torch.float64, device=f"cuda:{device_index}")
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return {"workload": f"sweep_rb{SWEEP_RESOLUTIONS}x{len(SWEEP_SEEDS)}_knn{SWEEP_K}_gmm{n_points}x{SWEEP_DIMS}",
+            "ranks": world, "s": float(tt.item()), "instances": len(configs),
+            "instances_rank0": timing["instances"], "units": "one warm chain per seed (its 8 pieces concurrent on the rank's streams), dealt by cost",
+            "q_min": float(min(qs)), "q_max": float(max(qs)),
+            "how": "parallel.run_sharded: no collective inside a run, one all-gather of modularities"}
+
+
 MANY_GRAPHS, MANY_SEED, MANY_STREAMS = 512, 21, 16
 
 
@@ -369,6 +407,10 @@ def run_c2(device_index, cpu=True):
                 res["modularity"] = sc_gpu.modularity(g, c.labels(), 1.0)
             arm[oname] = res
         out["arms"][name] = arm
+    # the kNN autotuner on these points: the full scan against several cluster
+    # counts of the pruned search (lists identical), the fastest kept
+    out["knn_autotune"] = sc_gpu.knn_autotune(X, C2_K, device=device_index)
+    sc_gpu.set_knn_clusters(0, device_index)
     a, b = csr["fp32"], csr["bf16"]
     out["graphs_identical"] = bool(np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
                                    and np.array_equal(a[2].view(np.uint32), b[2].view(np.uint32)))
@@ -403,7 +445,8 @@ def run_c5(device_index):
     candidates re-ranked in FP32 (BF16 candidates beside it for their recall);
     the edge MLP trained on plain-GPU partitions at RB {0.5, 1.0, 2.0}
     (independent seeds), evaluated as a warm start at RB {0.8, 1.5} against the
-    plain singleton start, which is also the fallback."""
+    plain singleton start, which is also the fallback. The graph carries the
+    points as its embedding (the edge-length feature)."""
     import sc_gpu
     from sc_gpu import synth
     from sc_gpu.learned import EdgeMlp, warm_start_leiden
@@ -420,9 +463,12 @@ def run_c5(device_index):
         if name == "fp8":
             keep = (r.conn_ptrs, r.conn_nbrs, r.conn_w)
         del r
-    del X
     g = sc_gpu.CSRNetwork.from_csr_parts(*keep, device=device_index)
     del keep
+    t = time.perf_counter()
+    g.set_embedding(X)  # the points: the model reads edge lengths in their projection
+    out["embedding_attach_s"] = time.perf_counter() - t
+    del X
     out["edge_count"] = g.edge_count()
 
     def run(gamma, seed):
@@ -451,8 +497,36 @@ def run_c5(device_index):
         ev[str(gamma)] = {"used_proposal": res.used_proposal, "q_warm": res.q_warm, "q_plain": res.q_plain,
                           "dQ": res.q_warm - res.q_plain, "sweeps_warm": res.sweeps_warm,
                           "sweeps_plain": res.sweeps_plain, "ms_warm": res.ms_warm, "ms_plain": res.ms_plain,
-                          "ms_saved": res.ms_plain - res.ms_warm, "proposal_clusters": res.proposal_clusters}
+                          "ms_saved": res.ms_plain - res.ms_warm, "ms_proposal": res.ms_proposal,
+                          "proposal_clusters": res.proposal_clusters}
     out["warm_start"] = ev
+    return out
+
+
+def run_mlp_small(device_index, n_points):
+    """The edge MLP on the kNN graph of n_points of the C5 mixture (k = 15, the
+    points as the embedding): one plain run for labels, 2 training calls of 5
+    epochs, one proposal; wall times of each."""
+    import sc_gpu
+    from sc_gpu import synth
+    from sc_gpu.learned import EdgeMlp
+    X, _ = synth.gaussian_mixture(n_points, C5_DIMS, C5_COMPONENTS, C5_SEED, sigma=(0.5, 2.0))
+    r = sc_gpu.knn_gaussian(X, C5_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w, device=device_index)
+    g.set_embedding(X)
+    del X, r
+    lab = sc_gpu.leiden(g, sc_gpu.LeidenConfig(seed=1)).labels()
+    m = EdgeMlp(seed=4, device=device_index)
+    out = {"points": n_points, "edges": g.edge_count()}
+    t = time.perf_counter()
+    for _ in range(2):
+        loss = m.train(g, lab, 1.0, epochs=5, lr=5e-3)
+    out["train_s"] = time.perf_counter() - t
+    out["loss"] = loss
+    t = time.perf_counter()
+    _, k = m.propose(g, 1.0, 0.9, 0.0)
+    out["propose_s"] = time.perf_counter() - t
+    out["proposal_clusters"] = k
     return out
 
 
@@ -511,10 +585,20 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.idx = gpu_index
         self.samples = []
-        self._stop = threading.Event()
+        self._proc = None
         self._t = None
 
     def start(self):
+        # one long-lived nvidia-smi sampling every 200 ms: starting a new one
+        # per sample initialises NVML each time, and those start-ups stall the
+        # driver (and the timed launches) for tens of milliseconds
+        try:
+            self._proc = subprocess.Popen(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                                           "--format=csv,noheader,nounits", "-lms", "200"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self._proc = None
+            return
         self._t = threading.Thread(target=self._run, daemon=True)
         self._t.start()
 
@@ -523,19 +607,19 @@ class ClockSampler:
         self.samples = []
 
     def _run(self):
-        while not self._stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                     timeout=5).stdout.strip()
-                if out:
-                    self.samples.append([x.strip() for x in out.split(",")])
-            except Exception:
-                pass
-            self._stop.wait(0.2)
+        for line in self._proc.stdout:
+            out = line.strip()
+            if out:
+                self.samples.append([x.strip() for x in out.split(",")])
 
     def stop(self):
-        self._stop.set()
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=10)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+                self._proc.wait()
         if self._t:
             self._t.join(timeout=10)
         if not self.samples:
@@ -643,8 +727,10 @@ def main():
     ap.add_argument("--no-c5", action="store_true", help="skip the 2M x 50 FP8 + learned warm start configuration")
     ap.add_argument("--no-accuracy", action="store_true", help="skip the FP64 recall / connectivity checks")
     ap.add_argument("--sweep-points", type=int, default=SWEEP_POINTS)
-    ap.add_argument("--part", default="leiden", choices=["leiden", "knn", "once"],
-                    help="once: one leiden() run on the library's kNN graph of --n points (a small case for ncu)")
+    ap.add_argument("--part", default="leiden", choices=["leiden", "knn", "once", "c5", "mlp"],
+                    help="once: one leiden() run on the library's kNN graph of --n points (a small case for ncu); "
+                         "c5: the 2M x 50 FP8 kNN + learned warm start configuration alone; "
+                         "mlp: a few training epochs and one proposal on --n points of the C5 mixture (for ncu)")
     ap.add_argument("--knn-precision", default="bf16", choices=["bf16", "fp8"])
     args = ap.parse_args()
 
@@ -696,6 +782,18 @@ def main():
         if dist:
             dist.destroy_process_group()
         return
+    if args.part == "mlp":
+        if rank == 0:
+            print(json.dumps({"part": "mlp", **run_mlp_small(local_rank, args.n)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
+    if args.part == "c5":
+        if rank == 0:
+            print(json.dumps({"part": "c5", **run_c5(local_rank)}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     if args.part == "once":
         if rank == 0:
             import sc_gpu
@@ -715,6 +813,10 @@ def main():
     g = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
     m = g.edge_count()
     cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(1.0), seed=LEIDEN_SEED)
+
+    # the routing autotuner on this graph (first level under each candidate
+    # routing; labels never depend on it): the timed runs use what it keeps
+    tuned = sc_gpu.autotune(g, cfg)
 
     # the clock sampler starts before the warm-up: its first nvidia-smi calls
     # (driver and NVML start-up) stall the host for a moment, and inside the
@@ -770,6 +872,9 @@ def main():
     h2d = ptr.nbytes + nbr.nbytes + w.nbytes
     d2h = len(ptr) * 8 - 8
 
+    sharded = None
+    if dist and not args.no_sweep:
+        sharded = run_sweep_sharded(local_rank, rank, world, dist, args.sweep_points)
     if rank != 0:
         if dist:
             dist.destroy_process_group()
@@ -784,6 +889,7 @@ def main():
             "wall_s_per_step": wall / args.steps,
             "phases_ms": {k: stats[k] for k in ("ms_local_move", "ms_refine", "ms_aggregate", "ms_other")},
             "run_stats": {k: stats[k] for k in ("passes", "levels", "local_move_sweeps", "moves")},
+            "autotune": tuned,
             "gpu_launches": int(stats["kernel_launches"]) * args.steps,
             "roofline": {"bound": "hbm", "kernel": "local-move sweeps (decide + apply)",
                          "achieved": lm_gbs, "peak": hbm, "unit": "GB/s",
@@ -814,6 +920,8 @@ def main():
     if not args.no_sweep:
         del g
         line["sweep"] = run_sweep(local_rank, args.sweep_points, accuracy=not args.no_accuracy)
+        if sharded:
+            line["sweep"]["sharded"] = sharded
         line["many_graphs"] = run_many_graphs(local_rank)
     if not args.no_c2:
         line["c2"] = run_c2(local_rank, cpu=not args.no_cpu_baseline)

@@ -222,6 +222,13 @@ sc_status sc_graph_from_csr_matrix(sc_ctx* ctx,
  * the library's graph pool (kept for the next graph until the process exits). */
 void sc_graph_destroy(sc_graph* g);
 
+/* Attaches the kNN embedding the graph was built from (n x d float32,
+ * row-major host memory, n = node count) for the learned warm start's
+ * features: the library keeps its projection to 16 components per node (a
+ * fixed sign matrix), replacing any earlier one. The reference's Leiden takes
+ * no embedding; its kNN builder (src/neighborhood/mod.rs) starts from one. */
+sc_status sc_graph_set_embedding(sc_ctx* ctx, sc_graph* g, const float* X, uint64_t n, uint64_t d);
+
 /* node_count, stored entries, edge_count, total_weight, has_self_loops
  * (src/network/csr_network.rs:407-442, :648-652). */
 sc_status sc_graph_info(const sc_graph* g, uint64_t* n_nodes, uint64_t* n_entries,
@@ -377,6 +384,17 @@ void sc_knn_opts_default(sc_knn_opts* opts);
  */
 sc_status sc_set_knn_clusters(sc_ctx* ctx, uint32_t clusters);
 
+/*
+ * kNN autotuner (no counterpart in single-clustering): times the exact search
+ * of all n rows of X under candidate cluster counts (1 = full scan, and 32 ..
+ * 256 where n allows) and keeps the fastest on the context (as
+ * sc_set_knn_clusters would). Every candidate gives the same lists, so it
+ * changes speed only. Outputs (each nullable): the count chosen, its device
+ * time and the full scan's (ms), the number of candidates timed.
+ */
+sc_status sc_knn_autotune(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts* opts,
+                          uint32_t* chosen_clusters, double* ms_chosen, double* ms_full, uint32_t* n_candidates);
+
 /* Counters of the last kNN search on a context. */
 typedef struct sc_knn_stats {
     uint64_t clusters;       /* point clusters of the pruned search (0: full scan)     */
@@ -430,11 +448,16 @@ sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const fl
  * ReLU, one logit) scoring each undirected edge with the probability that its
  * endpoints share a community, from endpoint degree/strength, the edge weight,
  * the RB null-model term at the given resolution, the endpoints' common
- * neighbourhood and, when given, whether they share a community in the
- * partitions found at a neighbouring lower (`coarse`) and higher (`fine`)
- * resolution: host label arrays of n entries, each nullable. A model trained
- * with these context partitions is meant to be used with them. Forward passes use BF16 weights with FP32 accumulation; Adam
- * updates an FP32 master copy. Parameters are laid out W1[f*128+u], b1[u],
+ * neighbourhood, when given the partitions found at a neighbouring lower
+ * (`coarse`) and higher (`fine`) resolution (host label arrays of n entries,
+ * each nullable) whether the endpoints share a community there and how much of
+ * each endpoint's strength its neighbour-label histogram puts in the other's
+ * community, and, when the graph carries an embedding
+ * (sc_graph_set_embedding), the edge's length in the projected embedding
+ * relative to the endpoints' local scale. A model trained with a context or an
+ * embedding is meant to be used with them. The contraction runs on the tensor
+ * cores (BF16 operands, features and hidden gradients split into two BF16
+ * parts, FP32 accumulation); Adam updates an FP32 master copy. Parameters are laid out W1[f*128+u], b1[u],
  * w2[u], b2 (sc_mlp_param_count() floats). The feature scaler (means, then
  * inverse standard deviations, 2 * feature_count floats) is fitted on the first
  * graph the model trains on or extracts features from.

@@ -18,7 +18,8 @@ from __future__ import annotations
 
 import numpy as np
 
-F = 12
+F = 15
+EMB_R = 16
 H = 128
 GAMMA_FEATURE = 6
 
@@ -45,9 +46,28 @@ def unpack(params):
     return W1, b1, w2, b2
 
 
-def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=None):
+def _splitmix(x: int) -> int:
+    m = (1 << 64) - 1
+    x = (x + 0x9E3779B97F4A7C15) & m
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & m
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & m
+    return x ^ (x >> 31)
+
+
+def projection(d: int) -> np.ndarray:
+    """The d x EMB_R sign matrix of the embedding feature: +-1/4, negative where
+    the top bit of splitmix64(a * EMB_R + r) is set."""
+    P = np.empty((d, EMB_R), np.float64)
+    for a in range(d):
+        for r in range(EMB_R):
+            P[a, r] = -0.25 if _splitmix(a * EMB_R + r) >> 63 else 0.25
+    return P
+
+
+def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=None, embedding=None):
     """Raw features of the undirected edges (sc_mlp.cu k_edge_features);
-    coarse / fine: labels of the neighbouring-resolution partitions or None."""
+    coarse / fine: labels of the neighbouring-resolution partitions or None;
+    embedding: the n x d points the graph was built from, or None."""
     ptr = np.asarray(ptr, np.int64)
     nbr = np.asarray(nbr, np.int64)
     w = np.asarray(w, np.float32)
@@ -60,6 +80,18 @@ def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=
             wmap[i][int(nbr[x])] = float(w[x])
     ei, ej, feats = [], [], []
     two_m = 2.0 * total_weight
+    y = scale = None
+    if embedding is not None:
+        X = np.asarray(embedding, np.float64)
+        y = X @ projection(X.shape[1])
+        scale = np.zeros(n)
+        for i in range(n):
+            nb = [int(v) for v in nbr[ptr[i]:ptr[i + 1]] if int(v) != i]
+            scale[i] = np.mean([np.sum((y[i] - y[v]) ** 2) for v in nb]) if nb else 0.0
+
+    def share(i, L, labels, ki):
+        s = sum(wmap[i][v] for v in rows[i] if v != i and labels[v] == L)
+        return s / max(ki, 1e-300)
     for i in range(n):
         for x in range(ptr[i], ptr[i + 1]):
             j = int(nbr[x])
@@ -76,7 +108,10 @@ def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=
                  gamma * ki * kj / (two_m * max(wij, 1e-300)) if two_m > 0 else 0.0,
                  cw / max(min(ki, kj), 1e-300), len(common) / max(min(di, dj), 1.0),
                  0.0 if coarse is None else float(coarse[i] == coarse[j]),
-                 0.0 if fine is None else float(fine[i] == fine[j])]
+                 0.0 if fine is None else float(fine[i] == fine[j]),
+                 0.0 if coarse is None else 0.5 * (share(i, coarse[j], coarse, ki) + share(j, coarse[i], coarse, kj)),
+                 0.0 if fine is None else 0.5 * (share(i, fine[j], fine, ki) + share(j, fine[i], fine, kj)),
+                 0.0 if y is None else float(np.sum((y[i] - y[j]) ** 2)) / max(0.5 * (scale[i] + scale[j]), 1e-30)]
             ei.append(i)
             ej.append(j)
             feats.append(f)

@@ -246,6 +246,15 @@ sc_status sc_set_knn_clusters(sc_ctx* ctx, uint32_t clusters) {
     });
 }
 
+sc_status sc_knn_autotune(sc_ctx* ctx, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts* opts,
+                          uint32_t* chosen_clusters, double* ms_chosen, double* ms_full, uint32_t* n_candidates) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(X != nullptr && opts != nullptr, "X or opts is NULL");
+        const uint32_t nc = sc::knn_autotune(c, X, n, d, k, *opts, chosen_clusters, ms_chosen, ms_full);
+        if (n_candidates) *n_candidates = nc;
+    });
+}
+
 sc_status sc_knn_last_stats(const sc_ctx* ctx, sc_knn_stats* out) {
     if (!ctx || !out) return SC_E_INVALID_ARGUMENT;
     *out = ctx->c.knn_stats;
@@ -360,6 +369,15 @@ void sc_graph_destroy(sc_graph* g) {
     if (!g) return;
     delete g->g;
     delete g;
+}
+
+sc_status sc_graph_set_embedding(sc_ctx* ctx, sc_graph* g, const float* X, uint64_t n, uint64_t d) {
+    return guarded(ctx, [&](sc::Ctx& c) {
+        require(g && g->g, "graph is NULL");
+        require_same_device(c, *g->g);
+        require(n == g->g->n, "embedding row count differs from the graph's node count");
+        sc::graph_set_embedding(c, *g->g, X, d);
+    });
 }
 
 sc_status sc_graph_info(const sc_graph* g, uint64_t* n_nodes, uint64_t* n_entries, uint64_t* edge_count,

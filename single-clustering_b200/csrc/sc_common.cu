@@ -155,8 +155,8 @@ double ordered_sum_from(Ctx& c, const double* d_terms, uint64_t n, double init) 
 }
 
 void DevGraph::free_all() {
-    void* ps[] = {ptr, nbr, w, erow, node_w, strength, self_loop};
-    if (ptr || nbr || w || erow || node_w || strength || self_loop) {
+    void* ps[] = {ptr, nbr, w, erow, node_w, strength, self_loop, emb};
+    if (ptr || nbr || w || erow || node_w || strength || self_loop || emb) {
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != device) cudaSetDevice(device);
@@ -178,6 +178,7 @@ void DevGraph::free_all() {
     node_w = nullptr;
     strength = nullptr;
     self_loop = nullptr;
+    emb = nullptr;
 }
 
 }  // namespace sc

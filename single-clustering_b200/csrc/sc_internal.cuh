@@ -189,6 +189,10 @@ struct DevGraph {
     // union, the graph's own totals decide).
     double part_max_2m = 0.0;
     double part_max_nw = 0.0;
+    // The kNN embedding projected to EMB_R components per node (n x EMB_R,
+    // from the graph pool), read by the learned warm start's features; null
+    // when none was attached.
+    float* emb = nullptr;
     uint64_t n_hubs = 0;      // nodes whose degree exceeds the shared-memory hash
     // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
     // once, on first need; a benign race between contexts computes it twice)
@@ -206,6 +210,12 @@ struct DevGraph {
     void free_all();
     ~DevGraph() { free_all(); }
 };
+
+constexpr int EMB_R = 16;  // components of a graph's projected embedding
+
+// Attaches the projection of the n x d row-major host embedding X to g
+// (replacing any earlier one).
+void graph_set_embedding(Ctx& c, DevGraph& g, const float* X, uint64_t d);
 
 // ------------------------------------------------------------------ helpers
 inline unsigned grid_for(uint64_t work, unsigned block, unsigned cap = 148u * 16u) {
@@ -324,6 +334,8 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k,
                   uint64_t* conn_nnz, DevGraph** graph_out);
 void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t q1,
                 const sc_knn_opts& opts, uint32_t* knn_index, float* knn_d2);
+uint32_t knn_autotune(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
+                      uint32_t* chosen, double* ms_chosen, double* ms_full);
 void knn_connectivities(Ctx& c, const uint32_t* knn_index, const float* knn_d2, uint64_t n, uint64_t k,
                         const sc_knn_opts& opts, uint64_t* conn_ptrs, uint32_t* conn_nbrs, float* conn_w,
                         uint64_t conn_cap, uint64_t* conn_nnz, DevGraph** graph_out);

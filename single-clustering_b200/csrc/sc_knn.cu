@@ -2022,6 +2022,58 @@ void knn_gaussian(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, co
                               graph_out);
 }
 
+// Times the search of all rows of X under candidate cluster counts (1: the
+// full scan) and keeps the fastest on the context. Every candidate returns the
+// same lists, so this changes speed only. Returns the number of candidates.
+uint32_t knn_autotune(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, const sc_knn_opts& opts,
+                      uint32_t* chosen, double* ms_chosen, double* ms_full) {
+    knn_check(n, d, k, opts);
+    DBuf<float> dX(c, n * d);
+    upload(c, dX.get(), X, n * d * sizeof(float));
+    DBuf<uint32_t> idx(c, n * (k + 1));
+    DBuf<float> d2(c, n * (k + 1));
+    std::vector<uint32_t> cand{1};
+    for (uint32_t K : {32u, 64u, 128u, 256u})
+        if (n >= PRUNE_MIN_POINTS && (uint64_t)K * 4096 <= n) cand.push_back(K);
+    const uint32_t saved = c.knn_clusters;
+    double best = INFINITY, full = 0.0;
+    uint32_t pick = 1;
+    cudaEvent_t e0, e1;
+    SC_CUDA(cudaEventCreate(&e0));
+    SC_CUDA(cudaEventCreate(&e1));
+    try {
+        // warm-up: modules, pools, first-call costs
+        c.knn_clusters = cand.back();
+        knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision, idx.get(), d2.get());
+        for (uint32_t K : cand) {
+            c.knn_clusters = K;
+            SC_CUDA(cudaEventRecord(e0, c.stream));
+            knn_search_device(c, dX.get(), n, d, k, 0, n, opts.precision, idx.get(), d2.get());
+            SC_CUDA(cudaEventRecord(e1, c.stream));
+            SC_CUDA(cudaEventSynchronize(e1));
+            float ms = 0.0f;
+            SC_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+            if (K == 1) full = ms;
+            if (ms < best) {
+                best = ms;
+                pick = K;
+            }
+        }
+    } catch (...) {
+        c.knn_clusters = saved;
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        throw;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    c.knn_clusters = pick;
+    if (chosen) *chosen = pick;
+    if (ms_chosen) *ms_chosen = best;
+    if (ms_full) *ms_full = full;
+    return (uint32_t)cand.size();
+}
+
 // The k+1 lists of the query rows [q0, q1) only (one shard of a multi-GPU
 // build); squared FP32 distances.
 void knn_search(Ctx& c, const float* X, uint64_t n, uint64_t d, uint64_t k, uint64_t q0, uint64_t q1,

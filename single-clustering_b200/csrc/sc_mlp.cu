@@ -4,16 +4,24 @@
 // Community ids are arbitrary (any permutation of a partition is the same
 // partition), so the network does not classify nodes into ids: it scores each
 // undirected edge (i, j) from the features of its two endpoints, their shared
-// neighbourhood and the partitions found at neighbouring resolutions, F = 12:
+// neighbourhood, the partitions found at neighbouring resolutions and the kNN
+// embedding the graph came from, F = 15:
 //   w, log1p(k_i) + log1p(k_j), |log1p(k_i) - log1p(k_j)|, log(d_i) + log(d_j),
 //   |log d_i - log d_j|, w/k_i + w/k_j, log(gamma), gamma k_i k_j / (2 m w),
 //   sum_c min(w_ic, w_jc) / min(k_i, k_j), |N(i) & N(j)| / min(d_i, d_j),
-//   [i, j together at the coarser neighbour], [i, j together at the finer one]
+//   [i, j together at the coarser neighbour], [i, j together at the finer one],
+//   (a_i(C(j)) + a_j(C(i))) / 2 at the coarser neighbour C, the same at the
+//   finer one, |y_i - y_j|^2 / ((s_i + s_j) / 2)
 // (w edge weight, k strength, d degree, gamma the RB resolution; the 8th is the
 // configuration-model null term relative to the edge, the quantity local moving
 // weighs; the 9th and 10th compare the endpoints' neighbour histograms, c over
-// the common neighbours other than i and j; the last two are 0 without a
-// context) and outputs the logit that i and j share a community:
+// the common neighbours other than i and j; a_i(L) is the share of k_i on the
+// neighbours x != i with label L, the node's neighbour-label histogram read at
+// the other endpoint's community; y_i is the node's embedding projected to
+// EMB_R components by a fixed sign matrix and s_i the mean of |y_i - y_x|^2 over
+// its neighbours, so the last is the edge's length in the embedding relative
+// to the local scale; features 10-13 are 0 without a context, 14 without an
+// embedding) and outputs the logit that i and j share a community:
 //   h = relu(x W1 + b1) (hidden H), z = h . w2 + b2.
 // Weights are BF16 in the forward pass with FP32 accumulation; an FP32 master
 // copy is updated by Adam. Training labels are partitions plain Leiden found;
@@ -24,18 +32,22 @@
 // edges chain neighbouring communities together; a boundary node has some
 // unconfident edge, stays a singleton, and is placed by local moving.
 //
-// Kernels: one warp per edge stream, lane l owns hidden units l, l+32, ...;
-// gradients accumulate in registers, then per block in shared memory, then in
-// a fixed-order reduction over blocks (deterministic).
+// Kernels: the contraction runs on the tensor cores (mma.sync BF16 with FP32
+// accumulation, 16 edges per warp step, features and hidden gradients split
+// into two BF16 parts so the sums keep FP32-level accuracy); gradients
+// accumulate in registers, then per block in shared memory, then in a
+// fixed-order reduction over blocks (deterministic).
 #include <cuda_bf16.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "sc_prims.cuh"
 
 namespace sc {
 
-constexpr int MLP_F = 12;
+constexpr int MLP_F = 15;  // plus a constant 1 as the 16th MMA column
 constexpr int MLP_H = 128;
-constexpr int MLP_UPL = MLP_H / 32;  // hidden units per lane
 constexpr int MLP_NPARAM = MLP_F * MLP_H + MLP_H + MLP_H + 1;  // W1, b1, w2, b2
 
 struct Mlp {
@@ -82,11 +94,51 @@ __device__ void common_neighbours(const uint64_t* __restrict__ ptr, const uint32
     }
 }
 
+// Σ w_ix over the neighbours x != i of i with label L, over k_i: the entry of
+// i's neighbour-label histogram at L, as a share of its strength.
+__device__ double label_share(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                              const float* __restrict__ w, const uint32_t* __restrict__ label, uint32_t i, uint32_t L,
+                              double ki) {
+    double s = 0.0;
+    for (uint64_t x = ptr[i]; x < ptr[i + 1]; ++x) {
+        const uint32_t v = nbr[x];
+        if (v != i && label[v] == L) s += (double)w[x];
+    }
+    return s / fmax(ki, 1e-300);
+}
+
+__device__ __forceinline__ float emb_dist2(const float* __restrict__ emb, uint32_t i, uint32_t j) {
+    float s = 0.0f;
+#pragma unroll
+    for (int r = 0; r < EMB_R; ++r) {
+        const float d = emb[(uint64_t)i * EMB_R + r] - emb[(uint64_t)j * EMB_R + r];
+        s = __fmaf_rn(d, d, s);
+    }
+    return s;
+}
+
+// s_i: mean of |y_i - y_x|^2 over the neighbours x != i (0 for none).
+__global__ void k_emb_scale(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr, uint64_t n,
+                            const float* __restrict__ emb, float* scale) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        double s = 0.0;
+        uint64_t cnt = 0;
+        for (uint64_t x = ptr[i]; x < ptr[i + 1]; ++x) {
+            const uint32_t v = nbr[x];
+            if (v == (uint32_t)i) continue;
+            s += (double)emb_dist2(emb, (uint32_t)i, v);
+            ++cnt;
+        }
+        scale[i] = cnt ? (float)(s / (double)cnt) : 0.0f;
+    }
+}
+
 // Features of the undirected edges (stored entries with row < neighbour).
 __global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                                 const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
                                 const double* __restrict__ strength, double two_m, double gamma,
-                                const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine, float* feat,
+                                const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine,
+                                const float* __restrict__ emb, const float* __restrict__ emb_scale, float* feat,
                                 uint32_t* ei, uint32_t* ej, unsigned long long* count) {
     for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
          e += (uint64_t)gridDim.x * blockDim.x) {
@@ -113,6 +165,15 @@ __global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t
         f[9] = (float)((double)cn / fmax(fmin(di, dj), 1.0));
         f[10] = coarse ? (coarse[i] == coarse[j] ? 1.0f : 0.0f) : 0.0f;
         f[11] = fine ? (fine[i] == fine[j] ? 1.0f : 0.0f) : 0.0f;
+        f[12] = coarse ? (float)(0.5 * (label_share(ptr, nbr, w, coarse, i, coarse[j], ki) +
+                                        label_share(ptr, nbr, w, coarse, j, coarse[i], kj)))
+                       : 0.0f;
+        f[13] = fine ? (float)(0.5 * (label_share(ptr, nbr, w, fine, i, fine[j], ki) +
+                                      label_share(ptr, nbr, w, fine, j, fine[i], kj)))
+                     : 0.0f;
+        f[14] = emb ? (float)((double)emb_dist2(emb, i, j) /
+                              fmax(0.5 * ((double)emb_scale[i] + (double)emb_scale[j]), 1e-30))
+                    : 0.0f;
         ei[pos] = i;
         ej[pos] = j;
     }
@@ -203,81 +264,224 @@ __global__ void k_to_bf16(const float* __restrict__ master, __nv_bfloat16* out) 
         out[i] = __float2bfloat16_rn(master[i]);
 }
 
-// Forward (and with GRAD, backward) over the edge stream. Parameter layout:
-// W1[f * H + u], b1[u], w2[u], b2. Lane l owns units l + 32 t, t < 4.
+// ------------------------------------------------------------ tensor-core forward / backward
+// Forward (and with GRAD, backward) over the edge stream on the tensor cores
+// (mma.sync m16n8k16, BF16 in, FP32 accumulate). Parameter layout:
+// W1[f * H + u], b1[u], w2[u], b2. A warp takes 16 edges per step: X (16 edges x 16 features, the
+// 12 features, then a 1 in column 12 of every real edge, then zeros) as two
+// BF16 parts x = x_hi + x_lo; H = X W1 is 16 MMAs per part (W1 is BF16 already,
+// rows 12..15 zero, so the 1 adds nothing). Thread (g, t) of the warp holds
+// H[g][8n + 2t + j] and H[g + 8][...] for the 16 n-tiles n. Backward:
+// dW1 = X^T dH with dH = relu'(H) dz w2 split in BF16 parts too (three MMAs per
+// n-tile: hi.hi, hi.lo, lo.hi); row 12 of X^T (the ones) gives db1 in the same
+// MMAs. dw2 = H^T dz and db2 fold per lane; the block then reduces every
+// warp's parameters in warp order (deterministic), as k_mlp.
+constexpr int TC_WARPS = 4;
+constexpr int TC_THREADS = 32 * TC_WARPS;
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
+    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<uint32_t*>(&v);
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Shared tiles keep rows of XS = 24 BF16 (12 words): the fragment reads of
+// lanes (g, t) then fall on banks 12 g + t, all 32 distinct.
+constexpr int XS = 24;
+
+struct alignas(16) TcSmem {
+    __nv_bfloat16 w1t[MLP_H * XS];  // W1 transposed: [unit][feature], features 12..15 zero
+    float b1[MLP_H], w2[MLP_H];
+    float b2;
+};
+
+// per warp: X and X^T (hi and lo parts) 16 x XS each, dH^T (hi and lo) MLP_H x XS
+constexpr int TC_WARP_TILE = 4 * 16 * XS + 2 * MLP_H * XS;
+
+__device__ __forceinline__ uint32_t word_at(const __nv_bfloat16* p) { return *reinterpret_cast<const uint32_t*>(p); }
+
 template <bool GRAD>
-__global__ void __launch_bounds__(TB) k_mlp(const float* __restrict__ feat, const uint8_t* __restrict__ label,
-                                            uint64_t M, const __nv_bfloat16* __restrict__ wb, float* __restrict__ out_p,
-                                            float* __restrict__ partial_grad, double* __restrict__ partial_loss) {
-    __shared__ float sW1[MLP_F * MLP_H], sb1[MLP_H], sw2[MLP_H];
-    __shared__ float sb2;
-    for (int i = threadIdx.x; i < MLP_F * MLP_H; i += blockDim.x) sW1[i] = __bfloat162float(wb[i]);
-    for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
-        sb1[i] = __bfloat162float(wb[MLP_F * MLP_H + i]);
-        sw2[i] = __bfloat162float(wb[MLP_F * MLP_H + MLP_H + i]);
+__global__ void __launch_bounds__(TC_THREADS) k_mlp_tc(const float* __restrict__ feat, const uint8_t* __restrict__ label,
+                                                       uint64_t M, const __nv_bfloat16* __restrict__ wb,
+                                                       float* __restrict__ out_p, float* __restrict__ partial_grad,
+                                                       double* __restrict__ partial_loss) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    TcSmem& S = *reinterpret_cast<TcSmem*>(smem_raw);
+    __nv_bfloat16* wbase = reinterpret_cast<__nv_bfloat16*>(smem_raw + sizeof(TcSmem));
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int g = lane >> 2, t = lane & 3;
+    __nv_bfloat16* xh = wbase + (size_t)wid * TC_WARP_TILE;  // [edge][feature]
+    __nv_bfloat16* xl = xh + 16 * XS;
+    __nv_bfloat16* xth = xl + 16 * XS;  // [feature][edge]
+    __nv_bfloat16* xtl = xth + 16 * XS;
+    __nv_bfloat16* dhh = xtl + 16 * XS;  // [unit][edge]
+    __nv_bfloat16* dhl = dhh + MLP_H * XS;
+    for (int i = threadIdx.x; i < MLP_H * 16; i += blockDim.x) {
+        const int u = i >> 4, f = i & 15;
+        S.w1t[u * XS + f] = f < MLP_F ? wb[f * MLP_H + u] : __float2bfloat16_rn(0.0f);
     }
-    if (threadIdx.x == 0) sb2 = __bfloat162float(wb[MLP_F * MLP_H + 2 * MLP_H]);
+    for (int i = threadIdx.x; i < MLP_H; i += blockDim.x) {
+        S.b1[i] = __bfloat162float(wb[MLP_F * MLP_H + i]);
+        S.w2[i] = __bfloat162float(wb[MLP_F * MLP_H + MLP_H + i]);
+    }
+    if (threadIdx.x == 0) S.b2 = __bfloat162float(wb[MLP_F * MLP_H + 2 * MLP_H]);
     __syncthreads();
-    const int lane = threadIdx.x & 31;
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    float gW1[MLP_F][MLP_UPL] = {}, gb1[MLP_UPL] = {}, gw2[MLP_UPL] = {};
+    float gw1[16][4];  // dW1 (rows f = g, g + 8) and, in row 12, db1
+    float gw2[16][2];  // dw2 partials of this lane's columns
+#pragma unroll
+    for (int n = 0; n < 16; ++n) {
+        gw1[n][0] = gw1[n][1] = gw1[n][2] = gw1[n][3] = 0.0f;
+        gw2[n][0] = gw2[n][1] = 0.0f;
+    }
     float gb2 = 0.0f;
     double loss = 0.0;
-    for (uint64_t e = warp; e < M; e += nwarps) {
-        float x[MLP_F];
+    const uint64_t warp_g = (uint64_t)blockIdx.x * TC_WARPS + wid;
+    const uint64_t nwarps = (uint64_t)gridDim.x * TC_WARPS;
+    for (uint64_t base = warp_g * 16; base < M; base += nwarps * 16) {
+        // X tile: lane l stages edge l / 2, features 8 (l % 2) .. +7 (a 1 in column 12)
+        {
+            const int e = lane >> 1, f0 = (lane & 1) * 8;
+            const uint64_t ge = base + e;
+            const bool valid = ge < M;
 #pragma unroll
-        for (int f = 0; f < MLP_F; ++f) x[f] = feat[e * MLP_F + f];
-        float h[MLP_UPL];
-        float zpart = 0.0f;
-#pragma unroll
-        for (int t = 0; t < MLP_UPL; ++t) {
-            const int u = lane + 32 * t;
-            float a = sb1[u];
-#pragma unroll
-            for (int f = 0; f < MLP_F; ++f) a = __fmaf_rn(x[f], sW1[f * MLP_H + u], a);
-            h[t] = fmaxf(a, 0.0f);
-            zpart = __fmaf_rn(h[t], sw2[u], zpart);
+            for (int j = 0; j < 8; ++j) {
+                const int f = f0 + j;
+                float x = 0.0f;
+                if (valid) x = f < MLP_F ? feat[ge * MLP_F + f] : (f == MLP_F ? 1.0f : 0.0f);
+                const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+                const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+                xh[e * XS + f] = hi;
+                xl[e * XS + f] = lo;
+                xth[f * XS + e] = hi;
+                xtl[f * XS + e] = lo;
+            }
         }
-        for (int o = 16; o; o >>= 1) zpart += __shfl_xor_sync(0xFFFFFFFFu, zpart, o);
-        const float z = zpart + sb2;
-        const float p = 1.0f / (1.0f + expf(-z));
+        __syncwarp();
+        const uint32_t ah[4] = {word_at(xh + g * XS + 2 * t), word_at(xh + (g + 8) * XS + 2 * t),
+                                word_at(xh + g * XS + 2 * t + 8), word_at(xh + (g + 8) * XS + 2 * t + 8)};
+        const uint32_t al[4] = {word_at(xl + g * XS + 2 * t), word_at(xl + (g + 8) * XS + 2 * t),
+                                word_at(xl + g * XS + 2 * t + 8), word_at(xl + (g + 8) * XS + 2 * t + 8)};
+        float h[16][4];
+        float z0 = 0.0f, z1 = 0.0f;
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const __nv_bfloat16* wc = S.w1t + (8 * n + g) * XS;  // this lane's B column
+            const uint32_t b0 = word_at(wc + 2 * t), b1 = word_at(wc + 2 * t + 8);
+            float c[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            mma_bf16_16816(c, ah, b0, b1);
+            mma_bf16_16816(c, al, b0, b1);
+            const int c0 = 8 * n + 2 * t;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                h[n][j] = fmaxf(c[j] + S.b1[c0 + j], 0.0f);
+                h[n][2 + j] = fmaxf(c[2 + j] + S.b1[c0 + j], 0.0f);
+                z0 = __fmaf_rn(h[n][j], S.w2[c0 + j], z0);
+                z1 = __fmaf_rn(h[n][2 + j], S.w2[c0 + j], z1);
+            }
+        }
+        // the four lanes of a quad hold the same rows: fold their columns
+        z0 += __shfl_xor_sync(0xFFFFFFFFu, z0, 1);
+        z0 += __shfl_xor_sync(0xFFFFFFFFu, z0, 2);
+        z1 += __shfl_xor_sync(0xFFFFFFFFu, z1, 1);
+        z1 += __shfl_xor_sync(0xFFFFFFFFu, z1, 2);
+        z0 += S.b2;
+        z1 += S.b2;
+        const float p0 = 1.0f / (1.0f + expf(-z0)), p1 = 1.0f / (1.0f + expf(-z1));
+        const uint64_t e0 = base + g, e1 = base + g + 8;
         if (!GRAD) {
-            if (lane == 0) out_p[e] = p;
+            if (t == 0) {
+                if (e0 < M) out_p[e0] = p0;
+                if (e1 < M) out_p[e1] = p1;
+            }
+            __syncwarp();
             continue;
         }
-        const float y = label[e] ? 1.0f : 0.0f;
-        // BCE with logits, numerically stable: max(z,0) - z y + log(1 + e^-|z|)
-        if (lane == 0) loss += (double)(fmaxf(z, 0.0f) - z * y + log1pf(expf(-fabsf(z))));
-        const float dz = p - y;
-        gb2 += dz;
-#pragma unroll
-        for (int t = 0; t < MLP_UPL; ++t) {
-            const int u = lane + 32 * t;
-            gw2[t] = __fmaf_rn(h[t], dz, gw2[t]);
-            const float dh = h[t] > 0.0f ? dz * sw2[u] : 0.0f;
-            gb1[t] += dh;
-#pragma unroll
-            for (int f = 0; f < MLP_F; ++f) gW1[f][t] = __fmaf_rn(x[f], dh, gW1[f][t]);
+        const float y0 = (e0 < M && label[e0]) ? 1.0f : 0.0f, y1 = (e1 < M && label[e1]) ? 1.0f : 0.0f;
+        const float dz0 = e0 < M ? p0 - y0 : 0.0f, dz1 = e1 < M ? p1 - y1 : 0.0f;
+        if (t == 0) {
+            // BCE with logits, numerically stable: max(z,0) - z y + log(1 + e^-|z|)
+            if (e0 < M) loss += (double)(fmaxf(z0, 0.0f) - z0 * y0 + log1pf(expf(-fabsf(z0))));
+            if (e1 < M) loss += (double)(fmaxf(z1, 0.0f) - z1 * y1 + log1pf(expf(-fabsf(z1))));
+            gb2 += dz0 + dz1;
         }
+        // dH^T (this lane's units; edges g, g + 8) into shared memory as BF16 parts; dw2 partials
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const int c0 = 8 * n + 2 * t;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const float w = S.w2[c0 + j];
+                gw2[n][j] = __fmaf_rn(h[n][j], dz0, gw2[n][j]);
+                gw2[n][j] = __fmaf_rn(h[n][2 + j], dz1, gw2[n][j]);
+                const float d0 = h[n][j] > 0.0f ? dz0 * w : 0.0f;
+                const float d1 = h[n][2 + j] > 0.0f ? dz1 * w : 0.0f;
+                const __nv_bfloat16 h0 = __float2bfloat16_rn(d0), h1 = __float2bfloat16_rn(d1);
+                __nv_bfloat16* rh = dhh + (c0 + j) * XS;
+                __nv_bfloat16* rl = dhl + (c0 + j) * XS;
+                rh[g] = h0;
+                rl[g] = __float2bfloat16_rn(d0 - __bfloat162float(h0));
+                rh[g + 8] = h1;
+                rl[g + 8] = __float2bfloat16_rn(d1 - __bfloat162float(h1));
+            }
+        }
+        __syncwarp();
+        // X^T as the A operand: rows = features (g, g + 8), columns = edges
+        const uint32_t th[4] = {word_at(xth + g * XS + 2 * t), word_at(xth + (g + 8) * XS + 2 * t),
+                                word_at(xth + g * XS + 2 * t + 8), word_at(xth + (g + 8) * XS + 2 * t + 8)};
+        const uint32_t tl[4] = {word_at(xtl + g * XS + 2 * t), word_at(xtl + (g + 8) * XS + 2 * t),
+                                word_at(xtl + g * XS + 2 * t + 8), word_at(xtl + (g + 8) * XS + 2 * t + 8)};
+#pragma unroll
+        for (int n = 0; n < 16; ++n) {
+            const __nv_bfloat16* ch = dhh + (8 * n + g) * XS;
+            const __nv_bfloat16* cl = dhl + (8 * n + g) * XS;
+            const uint32_t bh0 = word_at(ch + 2 * t), bh1 = word_at(ch + 2 * t + 8);
+            const uint32_t bl0 = word_at(cl + 2 * t), bl1 = word_at(cl + 2 * t + 8);
+            mma_bf16_16816(gw1[n], th, bh0, bh1);
+            mma_bf16_16816(gw1[n], th, bl0, bl1);
+            mma_bf16_16816(gw1[n], tl, bh0, bh1);
+        }
+        __syncwarp();
     }
     if (!GRAD) return;
-    // block reduction in shared memory: warps add in index order (deterministic)
-    __shared__ float sg[MLP_NPARAM];
+    // dw2 over the lanes that share columns (same t): fixed butterfly over g
+#pragma unroll
+    for (int n = 0; n < 16; ++n)
+#pragma unroll
+        for (int j = 0; j < 2; ++j)
+            for (int o = 4; o < 32; o <<= 1) gw2[n][j] += __shfl_xor_sync(0xFFFFFFFFu, gw2[n][j], o);
+    for (int o = 4; o < 32; o <<= 1) {
+        gb2 += __shfl_xor_sync(0xFFFFFFFFu, gb2, o);
+        loss += __shfl_xor_sync(0xFFFFFFFFu, loss, o);
+    }
+    // block reduction in shared memory, warps in index order (deterministic)
+    float* sg = reinterpret_cast<float*>(wbase);  // reuses the tiles: MLP_NPARAM floats
     __shared__ double sl;
-    const int wid = threadIdx.x >> 5;
-    for (int k = 0; k < (int)(blockDim.x / 32); ++k) {
+    __syncthreads();
+    for (int k = 0; k < TC_WARPS; ++k) {
         if (wid == k) {
             const bool first = k == 0;
 #pragma unroll
-            for (int t = 0; t < MLP_UPL; ++t) {
-                const int u = lane + 32 * t;
+            for (int n = 0; n < 16; ++n)
 #pragma unroll
-                for (int f = 0; f < MLP_F; ++f)
-                    sg[f * MLP_H + u] = first ? gW1[f][t] : sg[f * MLP_H + u] + gW1[f][t];
-                sg[MLP_F * MLP_H + u] = first ? gb1[t] : sg[MLP_F * MLP_H + u] + gb1[t];
-                sg[MLP_F * MLP_H + MLP_H + u] = first ? gw2[t] : sg[MLP_F * MLP_H + MLP_H + u] + gw2[t];
-            }
+                for (int j = 0; j < 2; ++j) {
+                    const int col = 8 * n + 2 * t + j;
+                    // dW1 rows g and g + 8 (< 12), db1 in row 12
+                    const int r0 = g, r1 = g + 8;
+                    const float v0 = gw1[n][j], v1 = gw1[n][2 + j];
+                    if (r0 < MLP_F) sg[r0 * MLP_H + col] = first ? v0 : sg[r0 * MLP_H + col] + v0;
+                    if (r1 < MLP_F) sg[r1 * MLP_H + col] = first ? v1 : sg[r1 * MLP_H + col] + v1;
+                    if (r1 == MLP_F) sg[MLP_F * MLP_H + col] = first ? v1 : sg[MLP_F * MLP_H + col] + v1;
+                    if (g == 0)
+                        sg[MLP_F * MLP_H + MLP_H + col] =
+                            first ? gw2[n][j] : sg[MLP_F * MLP_H + MLP_H + col] + gw2[n][j];
+                }
             if (lane == 0) {
                 sg[MLP_NPARAM - 1] = first ? gb2 : sg[MLP_NPARAM - 1] + gb2;
                 sl = first ? loss : sl + loss;
@@ -287,6 +491,20 @@ __global__ void __launch_bounds__(TB) k_mlp(const float* __restrict__ feat, cons
     }
     for (int i = threadIdx.x; i < MLP_NPARAM; i += blockDim.x) partial_grad[(uint64_t)blockIdx.x * MLP_NPARAM + i] = sg[i];
     if (threadIdx.x == 0) partial_loss[blockIdx.x] = sl;
+}
+
+size_t tc_smem_bytes() {
+    return sizeof(TcSmem) + (size_t)TC_WARPS * TC_WARP_TILE * sizeof(__nv_bfloat16);
+}
+
+template <bool GRAD>
+void launch_mlp_tc(Ctx& c, const float* feat, const uint8_t* label, uint64_t M, const __nv_bfloat16* wb, float* out_p,
+                   float* partial_grad, double* partial_loss) {
+    const size_t sm = tc_smem_bytes();
+    SC_CUDA(cudaFuncSetAttribute(k_mlp_tc<GRAD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_mlp_tc<GRAD><<<MLP_BLOCKS, TC_THREADS, sm, c.stream>>>(feat, label, M, wb, out_p, partial_grad, partial_loss);
+    SC_LAUNCH_CHECK();
+    c.launches++;
 }
 
 __global__ void k_grad_reduce(const float* __restrict__ partial, const double* __restrict__ partial_loss, int nblocks,
@@ -401,10 +619,18 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
     DBuf<uint32_t> ei(c, cap), ej(c, cap);
     DBuf<unsigned long long> cnt(c, 1);
     zero(c, cnt.get(), 1);
+    DBuf<float> scale;
+    if (g.emb && g.n) {
+        scale.alloc(c, g.n);
+        k_emb_scale<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, g.emb, scale.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
     if (g.E) {
         k_edge_features<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, g.strength,
-                                                                2.0 * g.total_weight, gamma, coarse, fine, feat.get(),
-                                                                ei.get(), ej.get(), cnt.get());
+                                                                2.0 * g.total_weight, gamma, coarse, fine, g.emb,
+                                                                scale.get(), feat.get(), ei.get(), ej.get(),
+                                                                cnt.get());
         SC_LAUNCH_CHECK();
         c.launches++;
     }
@@ -451,15 +677,68 @@ double grad_at(Ctx& c, const Mlp& m, const EdgeSet& es, const uint8_t* labels, f
     k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());
     DBuf<float> partial(c, (uint64_t)MLP_BLOCKS * MLP_NPARAM);
     DBuf<double> partial_loss(c, MLP_BLOCKS), loss(c, 1);
-    k_mlp<true><<<MLP_BLOCKS, TB, 0, c.stream>>>(es.feat.get(), labels, es.M, wb.get(), nullptr, partial.get(),
-                                                 partial_loss.get());
+    launch_mlp_tc<true>(c, es.feat.get(), labels, es.M, wb.get(), nullptr, partial.get(), partial_loss.get());
     k_grad_reduce<<<8, 256, 0, c.stream>>>(partial.get(), partial_loss.get(), MLP_BLOCKS, es.M, d_grad, loss.get());
     SC_LAUNCH_CHECK();
     c.launches += 3;
     return to_host(c, loss.get());
 }
 
+// y_i[r] = sum_a X[i][a] P[a][r], P the d x EMB_R sign matrix (rows of X in
+// chunks: the host embedding is uploaded piecewise).
+__global__ void k_emb_project(const float* __restrict__ X, uint64_t rows, uint64_t d, const float* __restrict__ P,
+                              float* y) {
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < rows * EMB_R;
+         t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = t / EMB_R;
+        const int r = (int)(t % EMB_R);
+        float acc = 0.0f;
+        for (uint64_t a = 0; a < d; ++a) acc = __fmaf_rn(X[i * d + a], P[a * EMB_R + r], acc);
+        y[t] = acc;
+    }
+}
+
 }  // namespace
+
+// P[a][r] = +-1/sqrt(EMB_R), the sign from the top bit of splitmix(a EMB_R + r):
+// a fixed random projection (Johnson-Lindenstrauss with signs), the same for
+// every graph and embedding width.
+void graph_set_embedding(Ctx& c, DevGraph& g, const float* X, uint64_t d) {
+    if (d == 0) fail(SC_E_INVALID_ARGUMENT, "embedding width must be positive");
+    if (X == nullptr && g.n) fail(SC_E_INVALID_ARGUMENT, "embedding is NULL");
+    std::vector<float> P(d * EMB_R);
+    for (uint64_t a = 0; a < d; ++a)
+        for (int r = 0; r < EMB_R; ++r) P[a * EMB_R + r] = (splitmix(a * EMB_R + r) >> 63) ? -0.25f : 0.25f;
+    DBuf<float> dP(c, P.size());
+    SC_CUDA(cudaMemcpyAsync(dP.get(), P.data(), P.size() * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+    float* y = nullptr;
+    if (g.n) {
+        cudaError_t e = cudaMallocFromPoolAsync((void**)&y, g.n * EMB_R * sizeof(float), user_graph_pool(c.device),
+                                                c.stream);
+        if (e == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            fail(SC_E_OUT_OF_MEMORY, "device allocation of the projected embedding failed");
+        }
+        if (e != cudaSuccess) throw_cuda(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+    }
+    const uint64_t chunk = std::max<uint64_t>(1, (64ull << 20) / (d * sizeof(float)));
+    DBuf<float> xb(c, std::min(chunk, std::max<uint64_t>(g.n, 1)) * d);
+    for (uint64_t r0 = 0; r0 < g.n; r0 += chunk) {
+        const uint64_t rows = std::min(chunk, g.n - r0);
+        SC_CUDA(cudaMemcpyAsync(xb.get(), X + r0 * d, rows * d * sizeof(float), cudaMemcpyHostToDevice, c.stream));
+        k_emb_project<<<grid_for(rows * EMB_R, TB), TB, 0, c.stream>>>(xb.get(), rows, d, dP.get(),
+                                                                      y + r0 * EMB_R);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    sync(c);
+    if (g.emb) {
+        SC_CUDA(cudaDeviceSynchronize());
+        SC_CUDA(cudaFreeAsync(g.emb, c.stream));
+        sync(c);
+    }
+    g.emb = y;
+}
 
 Mlp* mlp_create(Ctx& c, uint64_t seed) {
     std::unique_ptr<Mlp> m(new Mlp());
@@ -576,7 +855,7 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
     k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());
     DBuf<float> p(c, es.M);
     if (es.M)
-        k_mlp<false><<<MLP_BLOCKS, TB, 0, c.stream>>>(es.feat.get(), nullptr, es.M, wb.get(), p.get(), nullptr, nullptr);
+        launch_mlp_tc<false>(c, es.feat.get(), nullptr, es.M, wb.get(), p.get(), nullptr, nullptr);
     SC_LAUNCH_CHECK();
     if (prob_host) {
         if (es.M > prob_cap) fail(SC_E_INVALID_ARGUMENT, "probability capacity too small");

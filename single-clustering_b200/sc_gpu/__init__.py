@@ -339,6 +339,16 @@ class CSRNetwork:
     def has_self_loops(self) -> bool:
         return self._info()[4]
 
+    def set_embedding(self, X) -> None:
+        """Attaches the kNN embedding the graph was built from (node_count x d
+        points): the learned warm start reads the edge's length in a fixed
+        16-component projection of it, relative to the endpoints' local scale."""
+        X = np.ascontiguousarray(X, np.float32)
+        if X.ndim != 2:
+            raise ValueError("embedding must be a 2-D array (nodes x dims)")
+        _check(lib().sc_graph_set_embedding(self._ctx.h, self._h, _ptr(X, _lib.f32p), X.shape[0], X.shape[1]),
+               self._ctx)
+
     def to_csr_parts(self):
         n, e, *_ = self._info()
         ptr = np.zeros(n + 1, np.uint64)
@@ -652,6 +662,20 @@ def set_knn_clusters(clusters: int, device: int | None = None) -> None:
     0 picks a count from n, 1 scans every point tile."""
     ctx = context(device)
     _check(lib().sc_set_knn_clusters(ctx.h, int(clusters)), ctx)
+
+
+def knn_autotune(X, k: int, *, precision: int = KNN_BF16, device: int | None = None) -> dict:
+    """Times the exact kNN search of X under candidate cluster counts (1 = full
+    scan) and keeps the fastest on this thread's context (sc_knn_autotune)."""
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    n, d = X.shape
+    ctx = context(device)
+    opts = _knn_opts(precision=precision)
+    chosen, nc = C.c_uint32(), C.c_uint32()
+    ms_c, ms_f = C.c_double(), C.c_double()
+    _check(lib().sc_knn_autotune(ctx.h, _ptr(X, _lib.f32p), n, d, k, C.byref(opts), C.byref(chosen),
+                                 C.byref(ms_c), C.byref(ms_f), C.byref(nc)), ctx)
+    return {"clusters": chosen.value, "ms_chosen": ms_c.value, "ms_full": ms_f.value, "candidates": nc.value}
 
 
 def knn_last_stats(device: int | None = None) -> dict:

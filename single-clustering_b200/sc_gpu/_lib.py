@@ -121,6 +121,8 @@ SIGNATURES = [
     ("sc_test_knn_hold_tiles", C.c_int, [vp, C.c_int32]),
     ("sc_set_knn_clusters", C.c_int, [vp, C.c_uint32]),
     ("sc_knn_last_stats", C.c_int, [vp, C.POINTER(KnnStats)]),
+    ("sc_knn_autotune", C.c_int, [vp, f32p, C.c_uint64, C.c_uint64, C.c_uint64, C.POINTER(KnnOpts),
+                                  C.POINTER(C.c_uint32), f64p, f64p, C.POINTER(C.c_uint32)]),
     ("sc_autotune", C.c_int, [vp, vp, C.POINTER(LeidenConfigC), C.POINTER(Tuning), f64p, f64p,
                               C.POINTER(C.c_uint32)]),
     ("sc_leiden_config_default", None, [C.POINTER(LeidenConfigC)]),
@@ -132,6 +134,7 @@ SIGNATURES = [
     ("sc_graph_from_csr_matrix", C.c_int, [vp, u64p, C.c_uint64, u64p, f64p, C.c_uint64, f64p, vpp]),
     ("sc_graph_destroy", None, [vp]),
     ("sc_graph_info", C.c_int, [vp, u64p, u64p, u64p, f64p, i32p]),
+    ("sc_graph_set_embedding", C.c_int, [vp, vp, f32p, C.c_uint64, C.c_uint64]),
     ("sc_graph_copy_csr", C.c_int, [vp, vp, u64p, u32p, f32p]),
     ("sc_graph_copy_node_data", C.c_int, [vp, vp, f64p, f64p]),
     ("sc_graph_validate_symmetry", C.c_int, [vp, vp]),

@@ -150,6 +150,7 @@ class WarmStartResult:
     ms_warm: float            # propose (host wall clock) + leiden_from (the library's device timing)
     ms_plain: float | None
     proposal_clusters: int
+    ms_proposal: float | None = None  # the propose part of ms_warm (host wall clock)
 
 
 def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, core_fraction: float = 1.0,
@@ -186,7 +187,7 @@ def warm_start_leiden(model: EdgeMlp, graph, config, *, threshold: float = 0.9, 
     sw = graph._ctx.run_stats()
     q_w = score(warm.labels())
     res = WarmStartResult(warm.labels(), warm.n_clusters(), True, q_w, None, sw["local_move_sweeps"], None,
-                          t_prop + sw["ms_total"], None, kprop)
+                          t_prop + sw["ms_total"], None, kprop, t_prop)
     if not verify:
         return res
     plain = leiden(graph, config)

@@ -9,8 +9,9 @@ all-gather of Python objects over the process group (NCCL over NVLink between
 GPUs, gloo on CPU). No collective runs inside a Leiden run.
 
 The kNN search shards by query rows: every rank holds all points, searches
-its contiguous block of rows (`knn_search`), and one all-gather of the k+1
-lists lets every rank build the connectivities (`knn_connectivities`).
+its contiguous block of rows (`knn_search`), and a tensor all-gather of the
+k+1 lists (ids and squared distances) lets every rank build the
+connectivities (`knn_connectivities`).
 """
 from __future__ import annotations
 
@@ -91,8 +92,21 @@ def knn_sharded(search: Callable, n: int, rank: int, world: int, group=None):
     idx, d2 = search(b, e)
     if world == 1:
         return idx, d2
+    import torch
     import torch.distributed as dist
-    gathered = [None] * world
-    dist.all_gather_object(gathered, (b, idx, d2), group=group)
-    gathered.sort(key=lambda t: t[0])
-    return np.concatenate([g[1] for g in gathered]), np.concatenate([g[2] for g in gathered])
+    # one tensor all-gather per array (rows padded to the largest block): the
+    # ids travel as int32 bit patterns, on the GPU under NCCL, on the host under
+    # gloo; nothing is pickled
+    blocks = row_blocks(n, world)
+    rows = max(hi - lo for lo, hi in blocks)
+    kk = idx.shape[1]
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+    out = []
+    for a, dt in ((np.ascontiguousarray(idx, np.uint32).view(np.int32), torch.int32),
+                  (np.ascontiguousarray(d2, np.float32), torch.float32)):
+        mine = torch.zeros((rows, kk), dtype=dt, device=dev)
+        mine[:e - b] = torch.from_numpy(a).to(dev)
+        parts = [torch.empty_like(mine) for _ in range(world)]
+        dist.all_gather(parts, mine, group=group)
+        out.append(np.concatenate([parts[r][:hi - lo].cpu().numpy() for r, (lo, hi) in enumerate(blocks)]))
+    return out[0].view(np.uint32), out[1]

@@ -267,7 +267,7 @@ def test_pruned_search_equals_full_scan(n, d, comps, clusters):
     assert np.array_equal(pr.conn_ptrs, full.conn_ptrs) and np.array_equal(pr.conn_nbrs, full.conn_nbrs)
     assert np.array_equal(pr.conn_w.view(np.uint32), full.conn_w.view(np.uint32))
     if comps >= 20 and clusters == 0:
-        assert st["tiles_scanned"] < 0.5 * st["tiles_full"], st
+        assert st["tiles_scanned"] < 0.7 * st["tiles_full"], st
 
 
 def test_pruned_search_on_structureless_points():
@@ -290,3 +290,21 @@ def test_pruned_fp8_search_keeps_its_recall():
     rec_full = K.recall(full.index[sample], ref.index[sample])
     rec_pr = K.recall(pr.index[sample], ref.index[sample])
     assert rec_pr >= rec_full - 1e-3, (rec_pr, rec_full)
+
+
+def test_knn_autotune_keeps_a_count_that_gives_the_same_lists():
+    """The autotuner times the full scan and the pruned search at a few cluster
+    counts, keeps the fastest on the context, and the lists do not change."""
+    X, _ = synth.gaussian_mixture(300_000, 30, 60, seed=12, sigma=(0.7, 1.5))
+    try:
+        sc_gpu.set_knn_clusters(1)
+        ref = sc_gpu.knn_gaussian(X, 10, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
+        r = sc_gpu.knn_autotune(X, 10)
+        assert r["candidates"] >= 2 and r["clusters"] in (1, 32, 64)
+        assert r["ms_chosen"] <= r["ms_full"]
+        got = sc_gpu.knn_gaussian(X, 10, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
+        assert sc_gpu.knn_last_stats()["clusters"] == (0 if r["clusters"] == 1 else r["clusters"])
+        assert np.array_equal(got.index, ref.index)
+        assert np.array_equal(got.conn_w.view(np.uint32), ref.conn_w.view(np.uint32))
+    finally:
+        sc_gpu.set_knn_clusters(0)

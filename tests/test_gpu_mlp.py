@@ -42,11 +42,15 @@ def test_features_match_oracle():
     rng = np.random.default_rng(0)
     for g in (sc_gpu.CSRNetwork.from_edges(34, edges), _planted(800, 8)[0]):
         n = g.node_count()
-        for gamma, ctx in ((1.0, None), (0.3, (rng.integers(0, 3, n) * 7, rng.integers(0, 9, n)))):
+        X = rng.normal(size=(n, 7)).astype(np.float32)
+        for gamma, ctx, emb in ((1.0, None, None), (0.3, (rng.integers(0, 3, n) * 7, rng.integers(0, 9, n)), None),
+                                (0.7, (rng.integers(0, 4, n), rng.integers(0, 11, n)), X)):
+            if emb is not None:
+                g.set_embedding(emb)
             m = EdgeMlp(seed=1)
             feat, ei, ej = m.features(g, gamma, context=ctx)
             ptr, nbr, w, st, tw = _graph_arrays(g)
-            raw, oi, oj = mo.edge_features(ptr, nbr, w, st, tw, gamma, *(ctx or (None, None)))
+            raw, oi, oj = mo.edge_features(ptr, nbr, w, st, tw, gamma, *(ctx or (None, None)), embedding=emb)
             assert np.array_equal(ei, oi) and np.array_equal(ej, oj)
             mean, istd = m.scaler()
             omean, oistd = mo.scaler_fit(raw)
@@ -154,6 +158,7 @@ def test_warm_start_gain_over_plain_start():
     X, _ = synth.gaussian_mixture(60000, 50, 200, 5, sigma=(0.5, 2.0))
     r = sc_gpu.knn_gaussian(X, 15, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION)
     g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w)
+    g.set_embedding(X)
     m, labs = train_context_model(g)
     saved = []
     for gamma, ctx in ((0.8, (labs[0.5], labs[1.0])), (1.5, (labs[1.0], labs[2.0]))):

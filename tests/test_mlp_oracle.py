@@ -78,6 +78,34 @@ def test_features_on_triangle_with_tail():
     feats2, _, _ = mo.edge_features(ptr, nbr, w, strength, 7.0, 1.0, coarse=[0, 0, 0, 1], fine=[0, 1, 1, 2])
     # edges (0,1) (0,2) (1,2) (2,3): together at coarse 1 1 1 0, at fine 0 0 1 0
     assert list(feats2[:, 10]) == [1, 1, 1, 0] and list(feats2[:, 11]) == [0, 0, 1, 0]
+    # neighbour-label histograms read at the other endpoint's community:
+    # (0,1) coarse: 0 sends 4/4 and 1 sends 3/3 of its strength to label 0 -> 1;
+    # (2,3) coarse: 2 sends 1/6 to label 1, 3 sends 1/1 to label 0 -> 7/12;
+    # (0,1) fine: 0 sends 4/4 to label 1, 1 sends 1/3 to label 0 -> 2/3
+    assert np.isclose(feats2[0, 12], 1.0) and np.isclose(feats2[3, 12], 7.0 / 12.0)
+    assert np.isclose(feats2[0, 13], 2.0 / 3.0)
+    assert np.all(feats2[:, 14] == 0.0)  # no embedding
+
+
+def test_embedding_feature_is_scale_and_shift_free():
+    # triangle with a tail again; points in 5-D
+    ptr = np.array([0, 2, 4, 7, 8])
+    nbr = np.array([1, 2, 0, 2, 0, 1, 3, 2])
+    w = np.array([1, 3, 1, 2, 3, 2, 1, 1], np.float32)
+    strength = np.array([4.0, 3.0, 6.0, 1.0])
+    X = np.random.default_rng(3).normal(size=(4, 5))
+    f1, _, _ = mo.edge_features(ptr, nbr, w, strength, 7.0, 1.0, embedding=X)
+    f2, _, _ = mo.edge_features(ptr, nbr, w, strength, 7.0, 1.0, embedding=3.0 * X + 5.0)
+    assert np.all(f1[:, 14] > 0.0)
+    assert np.allclose(f1[:, 14], f2[:, 14], rtol=1e-12)
+    assert np.array_equal(f1[:, :14], f2[:, :14])
+    P = mo.projection(5)
+    assert P.shape == (5, mo.EMB_R) and set(np.unique(P)) <= {-0.25, 0.25}
+    # edge (0, 1) by hand: its projected length over the endpoints' mean scale
+    y = X @ P
+    s0 = np.mean([np.sum((y[0] - y[v]) ** 2) for v in (1, 2)])
+    s1 = np.mean([np.sum((y[1] - y[v]) ** 2) for v in (0, 2)])
+    assert np.isclose(f1[0, 14], np.sum((y[0] - y[1]) ** 2) / (0.5 * (s0 + s1)))
 
 
 def test_scaler_passes_gamma_through():
