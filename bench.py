@@ -255,7 +255,7 @@ def run_knn_part(args, device_index):
             "ms_per_step": dt * 1e3, "higher_is_better": True, "dtype": args.knn_precision, "data": "synthetic",
             "config": {"workload": f"knn{K}_gmm{args.n}x{DIMS}", "n_points": args.n, "dims": DIMS, "k": K},
             "timing": "host wall clock around the C ABI call (host input, host CSR output)",
-            "conn_nnz": int(len(r.conn_w))}
+            "conn_nnz": int(len(r.conn_w)), "pruning": sc_gpu.knn_last_stats(device_index)}
     if not args.no_cpu_baseline:
         line["cpu_baseline"], line["recall_at_k"] = knn_cpu_baseline(X, r.index)
     print(json.dumps(line), flush=True)

@@ -371,11 +371,15 @@ struct TileWalk {
 
 // F8: the operands are e4m3 bytes with the row size of BF16 KA columns.
 // rptr / rngs (nullable): the tile ranges of each query group (pruned search).
+// qcap (nullable): per query, a score no kept candidate reaches (a proven
+// bound of the pruned search's second pass); the rows start from it instead
+// of +inf, so far points never enter the insertion path.
 template <int KA, bool F8>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
              uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status,
-             uint32_t lim, uint32_t hold_tiles, const uint32_t* __restrict__ rptr, const uint2* __restrict__ rngs) {
+             uint32_t lim, uint32_t hold_tiles, const uint32_t* __restrict__ rptr, const uint2* __restrict__ rngs,
+             const float* __restrict__ qcap) {
     using L = KnnSmem<KA>;
     extern __shared__ __align__(1024) unsigned char raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
@@ -533,7 +537,9 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
         float* srow = (float*)(smem + L::ROW_OFF) + ew * 32;  // this warp's staged row chunk
         uint64_t it = 0;
         for (uint32_t g = blockIdx.x; g < ngroups && !*abort_flag; g += gridDim.x) {
-            float thr = INFINITY;
+            const uint64_t qrow = (uint64_t)g * QT * TILE + q * TILE + row;
+            const float capv = (qcap && qrow < nq) ? qcap[qrow] : INFINITY;
+            float thr = capv;
             int thr_slot = 0;
             for (int s2 = 0; s2 < RCAND; ++s2) {
                 cs[s2 * S + owner] = INFINITY;
@@ -572,7 +578,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                             for (int j = 0; j < 32; ++j) {
                                 if (r[j] < thr && base_idx + j < n) {
                                     const Worst w = cand_insert(cs, ci, owner, thr_slot, r[j], base_idx + j);
-                                    thr = w.thr;
+                                    thr = fminf(w.thr, capv);
                                     thr_slot = w.slot;
                                 }
                             }
@@ -595,6 +601,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                             const int ownerL = owner - lane + L;
                             float thrL = __shfl_sync(0xFFFFFFFFu, thr, L);
                             int slotL = __shfl_sync(0xFFFFFFFFu, thr_slot, L);
+                            const float capL = __shfl_sync(0xFFFFFFFFu, capv, L);
                             const bool inrange = base_idx + lane < n;
                             unsigned cand = __ballot_sync(0xFFFFFFFFu, inrange && v < thrL);
                             while (cand) {
@@ -616,7 +623,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                                         ws = os;
                                     }
                                 }
-                                thrL = wv;
+                                thrL = fminf(wv, capL);
                                 slotL = ws;
                                 // later columns of this row that still beat the new worst
                                 cand &= ~((2u << jc) - 1u);
@@ -634,11 +641,10 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                 if (lane == 0) mbar_arrive(accempty + b);
             }
             if (*abort_flag) break;
-            const uint64_t qg = (uint64_t)g * QT * TILE + q * TILE + row;
-            if (qg < nq) {
+            if (qrow < nq) {
                 for (int s2 = 0; s2 < RCAND; ++s2) {
-                    cand_score[qg * RTOTAL + h * RCAND + s2] = cs[s2 * S + owner];
-                    cand_idx[qg * RTOTAL + h * RCAND + s2] = ci[s2 * S + owner];
+                    cand_score[qrow * RTOTAL + h * RCAND + s2] = cs[s2 * S + owner];
+                    cand_idx[qrow * RTOTAL + h * RCAND + s2] = ci[s2 * S + owner];
                 }
             }
         }
@@ -925,6 +931,7 @@ CUtensorMap make_map(const void* base, uint64_t n, uint32_t row_bytes, bool byte
 struct TileLists {
     const uint32_t* rptr = nullptr;  // ngroups + 1
     const uint2* rngs = nullptr;     // (first tile, tile count)
+    const float* cap = nullptr;      // per query (launch order): the score bound of k_knn_tc's qcap
 };
 
 template <int KA, bool F8>
@@ -936,7 +943,7 @@ void launch_tc(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, uint64_t n,
     const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
     k_knn_tc<KA, F8><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
                                                                  cand_idx, c.d_status, c.wait_limit,
-                                                                 c.knn_hold_tiles, tl.rptr, tl.rngs);
+                                                                 c.knn_hold_tiles, tl.rptr, tl.rngs, tl.cap);
     SC_LAUNCH_CHECK();
     c.launches++;
 }
@@ -1402,6 +1409,35 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
     for (uint32_t w = threadIdx.x; w < cwords; w += blockDim.x) gcell[g * cwords + w] = s_bits[w];
 }
 
+// The pass-2 score bound of every query (row r of the pass-2 order is the
+// sorted query ord[r]). Scores are |y|^2 - 2 x.y from BF16 operands with FP32
+// accumulation. A point that can reach the final list has an FP32 distance of
+// at most d21 (the query's (k+1)-th FP32 distance from pass 1), so |y| <= Y =
+// |x| + sqrt(d21), and its score lies within 2^-5 |x| Y + 2^-12 Y^2 of
+// d^2 - |x|^2: the BF16 roundings of x and y (unit roundoff 2^-8 each, so
+// 2 x.y moves by at most about 2^-6 |x| |y| by Cauchy-Schwarz over the
+// products), the two-term norm and up to 64 FP32 accumulations, with a factor
+// of two to spare. 2^-16 (d21 + |x|^2) covers the FP32 distances and norm; the
+// sum is rounded up.
+__global__ void k_pass2_cap(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ ord,
+                            const uint32_t* __restrict__ perm, const float* __restrict__ d21, uint32_t k1,
+                            float* __restrict__ cap) {
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < n; r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t sq = ord[r];
+        const float* x = Xs + sq * d;
+        float nx2 = 0.0f;
+        for (uint32_t t = 0; t < d; ++t) nx2 = __fmaf_rn(x[t], x[t], nx2);
+        const float dk = d21[(uint64_t)perm[sq] * k1 + k1 - 1];
+        if (!(dk < INFINITY)) {
+            cap[r] = INFINITY;
+            continue;
+        }
+        const double nx = sqrt((double)nx2), Y = nx + sqrt((double)dk);
+        const double margin = ldexp(nx * Y, -5) + ldexp(Y * Y, -12) + ldexp((double)dk + (double)nx2, -16);
+        cap[r] = __double2float_ru((double)dk - (double)nx2 + 1.01 * margin);
+    }
+}
+
 // The exact re-rank on the cluster-sorted copy Xs (the same FP32 values as X,
 // so the same distances): row r is the sorted query ord[r] (ord nullable:
 // r itself), candidates are sorted positions, ties are broken on original ids
@@ -1773,31 +1809,41 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     DBuf<uint32_t> cidx(c, n * RTOTAL);
     // queries in the order `ord` (nullable: the sorted order), operand `o`
     auto run_pass = [&](const TcOperands& o, const uint32_t* ord, const std::vector<uint32_t>& rptr,
-                        const std::vector<uint2>& rngs, uint32_t* out_idx, float* out_d2) {
+                        const std::vector<uint2>& rngs, uint32_t* out_idx, float* out_d2, const float* qcap) {
         DBuf<uint32_t> d_rptr(c, rptr.size());
         DBuf<uint2> d_rngs(c, std::max<size_t>(rngs.size(), 1));
         h2d(c, d_rptr.get(), rptr.data(), rptr.size());
         h2d(c, d_rngs.get(), rngs.data(), rngs.size());
-        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr.get(), d_rngs.get()});
+        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr.get(), d_rngs.get(), qcap});
         k_knn_rerank_sorted<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(Xs.get(), n, d, k, ord, perm.get(),
                                                                         cidx.get(), out_idx, out_d2);
         SC_LAUNCH_CHECK();
         c.launches++;
         sync(c);  // the host arrays above must outlive the copies
     };
-    // 6. pass 1: every query group against its own clusters
+    // 6. pass 1: every query group against its own clusters, starting at its own
+    // tile (the nearest points come first, so the rows' thresholds tighten early
+    // and fewer later scores take the insertion path; pass 1 only yields the
+    // bounds of pass 2, which scans in point order)
     std::vector<uint32_t> rptr(ngroups + 1, 0);
     std::vector<uint2> rngs;
     uint64_t tiles1 = 0;
     for (uint64_t g = 0; g < ngroups; ++g) {
         std::vector<std::pair<uint64_t, uint64_t>> pts;
         own(g, pts);
+        const size_t first = rngs.size();
         tiles_of(pts, rngs, tiles1);
+        const uint32_t gt = (uint32_t)(g * QT * TILE / TILE);
+        if (rngs.size() == first + 1 && gt > rngs[first].x && gt < rngs[first].x + rngs[first].y) {
+            const uint2 r0 = rngs[first];
+            rngs[first] = make_uint2(gt, r0.x + r0.y - gt);
+            rngs.push_back(make_uint2(r0.x, gt - r0.x));
+        }
         rptr[g + 1] = (uint32_t)rngs.size();
     }
     DBuf<uint32_t> idx1(c, n * k1);
     DBuf<float> d21(c, n * k1);
-    run_pass(op, nullptr, rptr, rngs, idx1.get(), d21.get());
+    run_pass(op, nullptr, rptr, rngs, idx1.get(), d21.get(), nullptr);
     tm.mark();  // 4: pass 1
     // 7. the clusters every group still needs
     const uint32_t words = (K + 63) / 64;
@@ -1858,6 +1904,16 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
         op2.ta = make_map(op2.A.get(), n, row_bytes, op.kind == 2);
         op2.tb = op.tb;
     }
+    // score bounds of the BF16 search from the pass-1 distances (FP8 scores
+    // carry too coarse an error for a useful bound: none)
+    DBuf<float> qcap;
+    if (op.kind != 2) {
+        qcap.alloc(c, n);
+        k_pass2_cap<<<grid_for(n, 256), 256, 0, c.stream>>>(Xs.get(), n, d, ord.get(), perm.get(), d21.get(), k1,
+                                                            qcap.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
     sync(c);
     tm.mark();  // 9: bounds
     idx1.release();
@@ -1876,7 +1932,7 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
         rptr[g + 1] = (uint32_t)rngs.size();
     }
     tm.mark();  // 10: lists built
-    run_pass(op2, ord.get(), rptr, rngs, idx, d2);
+    run_pass(op2, ord.get(), rptr, rngs, idx, d2, qcap.get());
     tm.mark();  // 11: pass 2
     c.knn_stats.ms_cluster = tm.ms(0, 3);
     c.knn_stats.ms_pass1 = tm.ms(3, 4);
