@@ -40,6 +40,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <vector>
 
 #include "sc_prims.cuh"
@@ -65,46 +66,58 @@ namespace {
 constexpr unsigned TB = 256;
 constexpr int MLP_BLOCKS = 148 * 4;
 
-// Σ_c min(w_ic, w_jc) and the count over common neighbours c ∉ {i, j}: walk the
-// shorter row and binary-search the longer (rows are strictly increasing), so a
-// hub endpoint costs O(d_small log d_large).
-__device__ void common_neighbours(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
-                                  const float* __restrict__ w, uint32_t i, uint32_t j, double& wsum,
-                                  uint32_t& count) {
-    uint64_t a0 = ptr[i], a1 = ptr[i + 1], b0 = ptr[j], b1 = ptr[j + 1];
-    if (a1 - a0 > b1 - b0) {
-        uint64_t t = a0; a0 = b0; b0 = t;
-        t = a1; a1 = b1; b1 = t;
-    }
-    wsum = 0.0;
-    count = 0;
-    for (uint64_t x = a0; x < a1; ++x) {
-        const uint32_t c = nbr[x];
-        if (c == i || c == j) continue;
-        uint64_t lo = b0, hi = b1;
-        while (lo < hi) {
-            const uint64_t mid = (lo + hi) >> 1;
-            if (nbr[mid] < c) lo = mid + 1;
-            else hi = mid;
-        }
-        if (lo < b1 && nbr[lo] == c) {
-            wsum += (double)fminf(w[x], w[lo]);
-            ++count;
+// For every stored entry e = (i, j): Σ w_ix over the neighbours x != i of i
+// with label(x) = label(j), over k_i — the entry of i's neighbour-label
+// histogram at j's community, as a share of i's strength. A warp per row: each
+// lane owns an entry, the row's (label, weight) pairs are broadcast 32 at a
+// time by shuffles, and every sum runs over x in ascending order.
+__global__ void k_label_share(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                              const float* __restrict__ w, const uint32_t* __restrict__ label,
+                              const double* __restrict__ strength, uint64_t n, float* __restrict__ share) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < n; i += nwarps) {
+        const uint64_t a = ptr[i], b = ptr[i + 1];
+        const double ki = fmax(strength[i], 1e-300);
+        for (uint64_t e0 = a; e0 < b; e0 += 32) {
+            const uint64_t e = e0 + lane;
+            const uint32_t L = e < b ? label[nbr[e]] : 0u;
+            double acc = 0.0;
+            for (uint64_t x0 = a; x0 < b; x0 += 32) {
+                const uint64_t x = x0 + lane;
+                uint32_t lx = 0u;
+                float wx = 0.0f;
+                int vx = 0;
+                if (x < b) {
+                    const uint32_t v = nbr[x];
+                    vx = v != (uint32_t)i;
+                    lx = label[v];
+                    wx = w[x];
+                }
+                const int cnt = (int)(b - x0 < 32 ? b - x0 : 32);
+                for (int t = 0; t < cnt; ++t) {
+                    const uint32_t lt = __shfl_sync(0xFFFFFFFFu, lx, t);
+                    const float wt = __shfl_sync(0xFFFFFFFFu, wx, t);
+                    const int vt = __shfl_sync(0xFFFFFFFFu, vx, t);
+                    if (vt && lt == L) acc += (double)wt;
+                }
+            }
+            if (e < b) share[e] = (float)(acc / ki);
         }
     }
 }
 
-// Σ w_ix over the neighbours x != i of i with label L, over k_i: the entry of
-// i's neighbour-label histogram at L, as a share of its strength.
-__device__ double label_share(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
-                              const float* __restrict__ w, const uint32_t* __restrict__ label, uint32_t i, uint32_t L,
-                              double ki) {
-    double s = 0.0;
-    for (uint64_t x = ptr[i]; x < ptr[i + 1]; ++x) {
-        const uint32_t v = nbr[x];
-        if (v != i && label[v] == L) s += (double)w[x];
+// The stored entry (j, i): rows are strictly increasing, the graph symmetric.
+__device__ __forceinline__ uint64_t entry_of(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                             uint32_t j, uint32_t i) {
+    uint64_t lo = ptr[j], hi = ptr[j + 1];
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (nbr[mid] < i) lo = mid + 1;
+        else hi = mid;
     }
-    return s / fmax(ki, 1e-300);
+    return lo;
 }
 
 __device__ __forceinline__ float emb_dist2(const float* __restrict__ emb, uint32_t i, uint32_t j) {
@@ -133,72 +146,158 @@ __global__ void k_emb_scale(const uint64_t* __restrict__ ptr, const uint32_t* __
     }
 }
 
-// Features of the undirected edges (stored entries with row < neighbour).
-__global__ void k_edge_features(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
-                                const float* __restrict__ w, const uint32_t* __restrict__ erow, uint64_t E,
-                                const double* __restrict__ strength, double two_m, double gamma,
-                                const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine,
-                                const float* __restrict__ emb, const float* __restrict__ emb_scale, float* feat,
-                                uint32_t* ei, uint32_t* ej, unsigned long long* count) {
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < E;
-         e += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t i = erow[e], j = nbr[e];
-        if (!(i < j)) continue;
-        const unsigned long long pos = atomicAdd(count, 1ull);
-        const double wij = (double)w[e];
-        const double ki = strength[i], kj = strength[j];
-        const double di = (double)(ptr[i + 1] - ptr[i]), dj = (double)(ptr[j + 1] - ptr[j]);
-        const double lki = log1p(ki), lkj = log1p(kj), ldi = log(di), ldj = log(dj);
-        double cw;
-        uint32_t cn;
-        common_neighbours(ptr, nbr, w, i, j, cw, cn);
-        float* f = feat + pos * MLP_F;
-        f[0] = (float)wij;
-        f[1] = (float)(lki + lkj);
-        f[2] = (float)fabs(lki - lkj);
-        f[3] = (float)(ldi + ldj);
-        f[4] = (float)fabs(ldi - ldj);
-        f[5] = (float)(wij / fmax(ki, 1e-300) + wij / fmax(kj, 1e-300));
-        f[6] = (float)log(gamma);
-        f[7] = (float)(two_m > 0.0 ? gamma * ki * kj / (two_m * fmax(wij, 1e-300)) : 0.0);
-        f[8] = (float)(cw / fmax(fmin(ki, kj), 1e-300));
-        f[9] = (float)((double)cn / fmax(fmin(di, dj), 1.0));
-        f[10] = coarse ? (coarse[i] == coarse[j] ? 1.0f : 0.0f) : 0.0f;
-        f[11] = fine ? (fine[i] == fine[j] ? 1.0f : 0.0f) : 0.0f;
-        f[12] = coarse ? (float)(0.5 * (label_share(ptr, nbr, w, coarse, i, coarse[j], ki) +
-                                        label_share(ptr, nbr, w, coarse, j, coarse[i], kj)))
-                       : 0.0f;
-        f[13] = fine ? (float)(0.5 * (label_share(ptr, nbr, w, fine, i, fine[j], ki) +
-                                      label_share(ptr, nbr, w, fine, j, fine[i], kj)))
-                     : 0.0f;
-        f[14] = emb ? (float)((double)emb_dist2(emb, i, j) /
-                              fmax(0.5 * ((double)emb_scale[i] + (double)emb_scale[j]), 1e-30))
-                    : 0.0f;
-        ei[pos] = i;
-        ej[pos] = j;
-    }
+// Upper entries (neighbour > row) per row: the undirected edges i < j that
+// row i owns. cnt[n] = 0, so the exclusive sum ends with the edge count.
+__global__ void k_upper_counts(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr, uint64_t n,
+                               uint64_t* cnt) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i <= n; i += (uint64_t)gridDim.x * blockDim.x)
+        cnt[i] = i < n ? ptr[i + 1] - entry_of(ptr, nbr, (uint32_t)i, (uint32_t)i + 1u) : 0;
 }
 
-// Edges are written in atomic order above; sort by (i, j) so the edge stream
-// (and with it every fixed-order reduction) is the same on every run.
-__global__ void k_edge_keys(const uint32_t* __restrict__ ei, const uint32_t* __restrict__ ej, uint64_t M,
-                            uint64_t* keys, uint32_t* idx) {
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
-         e += (uint64_t)gridDim.x * blockDim.x) {
-        keys[e] = ((uint64_t)ei[e] << 32) | ej[e];
-        idx[e] = (uint32_t)e;
-    }
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
+    return v;
 }
 
-__global__ void k_gather_edges(const uint32_t* __restrict__ order, uint64_t M, const float* __restrict__ feat,
-                               const uint64_t* __restrict__ keys_sorted, float* feat_out, uint32_t* ei,
-                               uint32_t* ej) {
-    for (uint64_t e = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; e < M;
-         e += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t src = order[e];
-        for (int f = 0; f < MLP_F; ++f) feat_out[e * MLP_F + f] = feat[(uint64_t)src * MLP_F + f];
-        ei[e] = (uint32_t)(keys_sorted[e] >> 32);
-        ej[e] = (uint32_t)keys_sorted[e];
+constexpr int ROW_STAGE = 256;  // row entries a warp keeps in shared memory for the searches
+
+// Features of the undirected edges i < j, a warp per row i. Edge (i, j) lands
+// at base[i] + its rank among i's upper entries, i.e. in ascending (i, j)
+// order, the same on every run. Per edge the warp walks one endpoint's row in
+// 32-entry chunks (lane l takes entry l of a chunk) and every lane looks its
+// entry up in the other row by binary search: row i from shared memory (when
+// it fits) unless row j is much the shorter one. The common-neighbour sums
+// and the embedding length are warp reductions in a fixed tree; lane f writes
+// feature f.
+__global__ void __launch_bounds__(TB) k_edge_rows(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                                  const float* __restrict__ w, uint64_t n,
+                                                  const double* __restrict__ strength, double two_m, double gamma,
+                                                  const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine,
+                                                  const float* __restrict__ share_c, const float* __restrict__ share_f,
+                                                  const float* __restrict__ emb, const float* __restrict__ emb_scale,
+                                                  const uint64_t* __restrict__ base, float* __restrict__ feat,
+                                                  uint32_t* __restrict__ ei, uint32_t* __restrict__ ej) {
+    __shared__ uint32_t s_id[TB / 32][ROW_STAGE];
+    __shared__ float s_w[TB / 32][ROW_STAGE];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint32_t* sid = s_id[wib];
+    float* sw = s_w[wib];
+    for (uint64_t iw = warp; iw < n; iw += nwarps) {
+        const uint32_t i = (uint32_t)iw;
+        const uint64_t a = ptr[i], b = ptr[i + 1];
+        const uint64_t us = entry_of(ptr, nbr, i, i + 1u);
+        if (us == b) continue;  // no upper entries
+        const uint64_t di_n = b - a;
+        const bool staged = di_n <= (uint64_t)ROW_STAGE;
+        __syncwarp();
+        if (staged)
+            for (uint64_t x = lane; x < di_n; x += 32) {
+                sid[x] = nbr[a + x];
+                sw[x] = w[a + x];
+            }
+        __syncwarp();
+        const double ki = strength[i], di = (double)di_n;
+        const double lki = log1p(ki), ldi = log(di);
+        uint64_t pos = base[i];
+        for (uint64_t e = us; e < b; ++e, ++pos) {
+            const uint32_t j = nbr[e];
+            const double wij = (double)w[e];
+            const uint64_t ja = ptr[j], jb = ptr[j + 1];
+            const uint64_t dj_n = jb - ja;
+            const double kj = strength[j], dj = (double)dj_n;
+            // common neighbours c != i, j: walk one row, search the other
+            const bool walk_j = staged ? dj_n <= 8 * di_n : dj_n <= di_n;
+            double cw = 0.0;
+            uint32_t cn = 0;
+            uint64_t rev = ~0ull;  // the entry (j, i), found while walking row j
+            const uint64_t wa = walk_j ? ja : a, wb = walk_j ? jb : b;
+            for (uint64_t x0 = wa; x0 < wb; x0 += 32) {
+                const uint64_t x = x0 + lane;
+                if (x < wb) {
+                    const uint32_t cc = nbr[x];
+                    const float wc = w[x];
+                    if (walk_j && cc == i) rev = x;
+                    if (cc != i && cc != j) {
+                        float wo = 0.0f;
+                        bool found = false;
+                        if (walk_j && staged) {
+                            uint32_t lo = 0, hi = (uint32_t)di_n;
+                            while (lo < hi) {
+                                const uint32_t mid = (lo + hi) >> 1;
+                                if (sid[mid] < cc) lo = mid + 1;
+                                else hi = mid;
+                            }
+                            if (lo < di_n && sid[lo] == cc) {
+                                found = true;
+                                wo = sw[lo];
+                            }
+                        } else {
+                            const uint64_t oa = walk_j ? a : ja, ob = walk_j ? b : jb;
+                            uint64_t lo = oa, hi = ob;
+                            while (lo < hi) {
+                                const uint64_t mid = (lo + hi) >> 1;
+                                if (nbr[mid] < cc) lo = mid + 1;
+                                else hi = mid;
+                            }
+                            if (lo < ob && nbr[lo] == cc) {
+                                found = true;
+                                wo = w[lo];
+                            }
+                        }
+                        if (found) {
+                            cw += (double)fminf(wc, wo);
+                            ++cn;
+                        }
+                    }
+                }
+            }
+            cw = warp_sum_d(cw);
+            for (int o = 16; o; o >>= 1) cn += __shfl_xor_sync(0xFFFFFFFFu, cn, o);
+            if (coarse || fine) {
+                unsigned long long r = rev;
+                for (int o = 16; o; o >>= 1) r = min(r, (unsigned long long)__shfl_xor_sync(0xFFFFFFFFu, r, o));
+                rev = r != ~0ull ? r : entry_of(ptr, nbr, j, i);
+            }
+            double ed2 = 0.0;
+            if (emb) {
+                float t = 0.0f;
+                if (lane < EMB_R) {
+                    const float dd = emb[(uint64_t)i * EMB_R + lane] - emb[(uint64_t)j * EMB_R + lane];
+                    t = dd * dd;
+                }
+                for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+                ed2 = (double)t;
+            }
+            if (lane < MLP_F) {
+                const double lkj = log1p(kj), ldj = log(dj);
+                double v = 0.0;
+                switch (lane) {
+                    case 0: v = wij; break;
+                    case 1: v = lki + lkj; break;
+                    case 2: v = fabs(lki - lkj); break;
+                    case 3: v = ldi + ldj; break;
+                    case 4: v = fabs(ldi - ldj); break;
+                    case 5: v = wij / fmax(ki, 1e-300) + wij / fmax(kj, 1e-300); break;
+                    case 6: v = log(gamma); break;
+                    case 7: v = two_m > 0.0 ? gamma * ki * kj / (two_m * fmax(wij, 1e-300)) : 0.0; break;
+                    case 8: v = cw / fmax(fmin(ki, kj), 1e-300); break;
+                    case 9: v = (double)cn / fmax(fmin(di, dj), 1.0); break;
+                    case 10: v = coarse ? (coarse[i] == coarse[j] ? 1.0 : 0.0) : 0.0; break;
+                    case 11: v = fine ? (fine[i] == fine[j] ? 1.0 : 0.0) : 0.0; break;
+                    case 12: v = coarse ? 0.5 * ((double)share_c[e] + (double)share_c[rev]) : 0.0; break;
+                    case 13: v = fine ? 0.5 * ((double)share_f[e] + (double)share_f[rev]) : 0.0; break;
+                    default:
+                        v = emb ? ed2 / fmax(0.5 * ((double)emb_scale[i] + (double)emb_scale[j]), 1e-30) : 0.0;
+                }
+                feat[pos * MLP_F + lane] = (float)v;
+            }
+            if (lane == 0) {
+                ei[pos] = i;
+                ej[pos] = j;
+            }
+        }
     }
 }
 
@@ -267,22 +366,18 @@ __global__ void k_to_bf16(const float* __restrict__ master, __nv_bfloat16* out) 
 // ------------------------------------------------------------ tensor-core forward / backward
 // Forward (and with GRAD, backward) over the edge stream on the tensor cores
 // (mma.sync m16n8k16, BF16 in, FP32 accumulate). Parameter layout:
-// W1[f * H + u], b1[u], w2[u], b2. A warp takes 16 edges per step: X (16 edges x 16 features, the
-// 12 features, then a 1 in column 12 of every real edge, then zeros) as two
-// BF16 parts x = x_hi + x_lo; H = X W1 is 16 MMAs per part (W1 is BF16 already,
-// rows 12..15 zero, so the 1 adds nothing). Thread (g, t) of the warp holds
-// H[g][8n + 2t + j] and H[g + 8][...] for the 16 n-tiles n. Backward:
-// dW1 = X^T dH with dH = relu'(H) dz w2 split in BF16 parts too (three MMAs per
-// n-tile: hi.hi, hi.lo, lo.hi); row 12 of X^T (the ones) gives db1 in the same
-// MMAs. dw2 = H^T dz and db2 fold per lane; the block then reduces every
-// warp's parameters in warp order (deterministic), as k_mlp.
+// W1[f * H + u], b1[u], w2[u], b2. A warp takes 16 edges per step: X (16
+// edges x 16 columns: the MLP_F = 15 features, then a 1 in the last column of
+// every real edge) as two BF16 parts x = x_hi + x_lo; H = X W1 is 16 MMAs per
+// part (W1 is BF16 already, its row 15 zero, so the 1 adds nothing). Thread
+// (g, t) of the warp holds H[g][8n + 2t + j] and H[g + 8][...] for the 16
+// n-tiles n. Backward: dW1 = X^T dH with dH = relu'(H) dz w2 split in BF16
+// parts too (three MMAs per n-tile: hi.hi, hi.lo, lo.hi); row 15 of X^T (the
+// ones) gives db1 in the same MMAs. dw2 = H^T dz and db2 fold per lane; the
+// block then reduces every warp's parameters in warp order and the grid in
+// block order (deterministic).
 constexpr int TC_WARPS = 4;
 constexpr int TC_THREADS = 32 * TC_WARPS;
-
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi) {
-    __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
-    return *reinterpret_cast<uint32_t*>(&v);
-}
 
 __device__ __forceinline__ void mma_bf16_16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
     asm volatile(
@@ -614,40 +709,42 @@ struct EdgeSet {
 
 void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
                  EdgeSet& es) {
-    const uint64_t cap = g.E;
-    DBuf<float> feat(c, cap * MLP_F);
-    DBuf<uint32_t> ei(c, cap), ej(c, cap);
-    DBuf<unsigned long long> cnt(c, 1);
-    zero(c, cnt.get(), 1);
-    DBuf<float> scale;
-    if (g.emb && g.n) {
-        scale.alloc(c, g.n);
-        k_emb_scale<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, g.emb, scale.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
-    }
-    if (g.E) {
-        k_edge_features<<<grid_for(g.E, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.erow, g.E, g.strength,
-                                                                2.0 * g.total_weight, gamma, coarse, fine, g.emb,
-                                                                scale.get(), feat.get(), ei.get(), ej.get(),
-                                                                cnt.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
-    }
-    const uint64_t M = to_host(c, cnt.get());
+    // edge positions: upper entries per row, exclusive sum
+    DBuf<uint64_t> cnt(c, g.n + 1), base(c, g.n + 1);
+    k_upper_counts<<<grid_for(g.n + 1, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, cnt.get());
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    exclusive_sum(c, cnt.get(), base.get(), g.n + 1);
+    const uint64_t M = to_host(c, base.get() + g.n);
     es.M = M;
     es.feat.alloc(c, M * MLP_F);
     es.ei.alloc(c, M);
     es.ej.alloc(c, M);
     if (!M) return;
-    DBuf<uint64_t> keys(c, M), keys_s(c, M);
-    DBuf<uint32_t> idx(c, M), order(c, M);
-    k_edge_keys<<<grid_for(M, TB), TB, 0, c.stream>>>(ei.get(), ej.get(), M, keys.get(), idx.get());
-    sort_pairs(c, keys.get(), keys_s.get(), idx.get(), order.get(), M, 64);
-    k_gather_edges<<<grid_for(M, TB), TB, 0, c.stream>>>(order.get(), M, feat.get(), keys_s.get(), es.feat.get(),
-                                                         es.ei.get(), es.ej.get());
+    DBuf<float> share_c, share_f;
+    for (int t = 0; t < 2; ++t) {
+        const uint32_t* lab = t == 0 ? coarse : fine;
+        DBuf<float>& sh = t == 0 ? share_c : share_f;
+        if (!lab) continue;
+        sh.alloc(c, g.E);
+        k_label_share<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, lab, g.strength, g.n,
+                                                                   sh.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    DBuf<float> scale;
+    if (g.emb) {
+        scale.alloc(c, g.n);
+        k_emb_scale<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, g.emb, scale.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    k_edge_rows<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.n, g.strength, 2.0 * g.total_weight,
+                                                             gamma, coarse, fine, share_c.get(), share_f.get(), g.emb,
+                                                             scale.get(), base.get(), es.feat.get(), es.ei.get(),
+                                                             es.ej.get());
     SC_LAUNCH_CHECK();
-    c.launches += 2;
+    c.launches++;
 }
 
 // Standardise es's features with the model's scaler, fitting it first if the
@@ -848,8 +945,20 @@ double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, doub
 // Proposal: components of the edges whose predicted probability exceeds thr.
 uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
                      double thr, double core_fraction, uint32_t* d_labels, float* prob_host, uint64_t prob_cap) {
+    // SC_TRACE: device time of the stages (events on the context's stream)
+    static const bool trace = std::getenv("SC_TRACE") != nullptr;
+    std::vector<cudaEvent_t> ev;
+    auto mark = [&]() {
+        if (!trace) return;
+        cudaEvent_t e;
+        SC_CUDA(cudaEventCreate(&e));
+        SC_CUDA(cudaEventRecord(e, c.stream));
+        ev.push_back(e);
+    };
+    mark();
     EdgeSet es;
     build_edges(c, g, gamma, coarse, fine, es);
+    mark();
     scale_edges(c, m, es, false);
     DBuf<__nv_bfloat16> wb(c, MLP_NPARAM);
     k_to_bf16<<<4, 256, 0, c.stream>>>(m.master, wb.get());
@@ -857,6 +966,7 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
     if (es.M)
         launch_mlp_tc<false>(c, es.feat.get(), nullptr, es.M, wb.get(), p.get(), nullptr, nullptr);
     SC_LAUNCH_CHECK();
+    mark();
     if (prob_host) {
         if (es.M > prob_cap) fail(SC_E_INVALID_ARGUMENT, "probability capacity too small");
         d2h(c, prob_host, p.get(), es.M);
@@ -890,10 +1000,19 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
         done = !to_host(c, changed.get());
     }
     if (!done) fail(SC_E_INTERNAL, "proposal components did not converge");
+    mark();
     DBuf<uint32_t> compact(c, n);
     const uint32_t K = renumber_ids(c, d_labels, n, n, compact.get());
     d2d(c, d_labels, compact.get(), n);
+    mark();
     sync(c);
+    if (trace) {
+        float t[4] = {};
+        for (int k = 0; k < 4; ++k) SC_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+        std::fprintf(stderr, "[sc] mlp propose M=%llu: features %.2f ms, scale + infer %.2f ms, components %.2f ms, "
+                     "renumber %.2f ms\n", (unsigned long long)es.M, t[0], t[1], t[2], t[3]);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
     return K;
 }
 
