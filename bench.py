@@ -505,8 +505,9 @@ def run_c5(device_index):
 
 def run_mlp_small(device_index, n_points):
     """The edge MLP on the kNN graph of n_points of the C5 mixture (k = 15, the
-    points as the embedding): one plain run for labels, 2 training calls of 5
-    epochs, one proposal; wall times of each."""
+    points as the embedding): plain runs for the labels (RB 1) and the context
+    (RB 0.5 and 2), 2 training calls of 5 epochs, one proposal; wall times of
+    each."""
     import sc_gpu
     from sc_gpu import synth
     from sc_gpu.learned import EdgeMlp
@@ -516,15 +517,17 @@ def run_mlp_small(device_index, n_points):
     g.set_embedding(X)
     del X, r
     lab = sc_gpu.leiden(g, sc_gpu.LeidenConfig(seed=1)).labels()
+    ctx = (sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(0.5), seed=2)).labels(),
+           sc_gpu.leiden(g, sc_gpu.LeidenConfig(objective=sc_gpu.Rb(2.0), seed=3)).labels())
     m = EdgeMlp(seed=4, device=device_index)
     out = {"points": n_points, "edges": g.edge_count()}
     t = time.perf_counter()
     for _ in range(2):
-        loss = m.train(g, lab, 1.0, epochs=5, lr=5e-3)
+        loss = m.train(g, lab, 1.0, epochs=5, lr=5e-3, context=ctx)
     out["train_s"] = time.perf_counter() - t
     out["loss"] = loss
     t = time.perf_counter()
-    _, k = m.propose(g, 1.0, 0.9, 0.0)
+    _, k = m.propose(g, 1.0, 0.9, 0.0, context=ctx)
     out["propose_s"] = time.perf_counter() - t
     out["proposal_clusters"] = k
     return out

@@ -89,9 +89,20 @@ def edge_features(ptr, nbr, w, strength, total_weight, gamma, coarse=None, fine=
             nb = [int(v) for v in nbr[ptr[i]:ptr[i + 1]] if int(v) != i]
             scale[i] = np.mean([np.sum((y[i] - y[v]) ** 2) for v in nb]) if nb else 0.0
 
+    memo = {}
+
     def share(i, L, labels, ki):
-        s = sum(wmap[i][v] for v in rows[i] if v != i and labels[v] == L)
-        return s / max(ki, 1e-300)
+        # Σ over the row in ascending neighbour order (the kernel's order);
+        # memoised per (partition, node, label): hub rows are long
+        key = (id(labels), i, int(L))
+        if key not in memo:
+            s = 0.0
+            for x in range(ptr[i], ptr[i + 1]):
+                v = int(nbr[x])
+                if v != i and labels[v] == L:
+                    s += float(w[x])
+            memo[key] = s / max(ki, 1e-300)
+        return memo[key]
     for i in range(n):
         for x in range(ptr[i], ptr[i + 1]):
             j = int(nbr[x])

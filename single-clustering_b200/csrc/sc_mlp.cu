@@ -68,43 +68,78 @@ constexpr int MLP_BLOCKS = 148 * 4;
 
 // For every stored entry e = (i, j): Σ w_ix over the neighbours x != i of i
 // with label(x) = label(j), over k_i — the entry of i's neighbour-label
-// histogram at j's community, as a share of i's strength. A warp per row: each
-// lane owns an entry, the row's (label, weight) pairs are broadcast 32 at a
-// time by shuffles, and every sum runs over x in ascending order.
+// histogram at j's community, as a share of i's strength. A warp takes a run
+// of the row's 32-entry chunks (the e-chunks) and walks all its chunks (the
+// x-chunks): in each x-chunk the lanes of one label find each other with
+// __match_any_sync, the lowest of them sums the group's weights in lane order,
+// and the warp broadcasts (label, sum) once per distinct label; a lane adds
+// the sums of its entry's label. Per entry the order is fixed (chunks
+// ascending, lanes ascending inside a chunk), so the result is the same on
+// every run.
+__device__ void label_share_chunks(const uint32_t* __restrict__ nbr,
+                                   const float* __restrict__ w, const uint32_t* __restrict__ label, uint32_t i,
+                                   uint64_t a, uint64_t b, uint64_t ce_begin, uint64_t ce_step, double ki,
+                                   float* __restrict__ share) {
+    const int lane = threadIdx.x & 31;
+    for (uint64_t e0 = a + ce_begin * 32; e0 < b; e0 += ce_step * 32) {
+        const uint64_t e = e0 + lane;
+        const uint32_t L = e < b ? label[nbr[e]] : 0u;
+        double acc = 0.0;
+        for (uint64_t x0 = a; x0 < b; x0 += 32) {
+            const uint64_t x = x0 + lane;
+            bool valid = false;
+            uint32_t lx = 0u;
+            float wx = 0.0f;
+            if (x < b) {
+                const uint32_t v = nbr[x];
+                valid = v != i;
+                lx = label[v];
+                wx = w[x];
+            }
+            const unsigned long long key = valid ? (unsigned long long)lx : ((1ull << 32) | (unsigned)lane);
+            const unsigned peers = __match_any_sync(0xFFFFFFFFu, key);
+            double sum = 0.0;
+            for (int t = 0; t < 32; ++t) {
+                const float wt = __shfl_sync(0xFFFFFFFFu, wx, t);
+                if ((peers >> t) & 1u) sum += (double)wt;
+            }
+            unsigned leaders = __ballot_sync(0xFFFFFFFFu, valid && (__ffs(peers) - 1) == lane);
+            while (leaders) {
+                const int l = __ffs(leaders) - 1;
+                leaders &= leaders - 1;
+                const uint32_t Ll = __shfl_sync(0xFFFFFFFFu, lx, l);
+                const double Sl = __shfl_sync(0xFFFFFFFFu, sum, l);
+                if (Ll == L) acc += Sl;
+            }
+        }
+        if (e < b) share[e] = (float)(acc / ki);
+    }
+}
+
+// Rows of at most 32 chunks: a warp per row. Longer rows are left to
+// k_label_share_big.
 __global__ void k_label_share(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
                               const float* __restrict__ w, const uint32_t* __restrict__ label,
                               const double* __restrict__ strength, uint64_t n, float* __restrict__ share) {
-    const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     for (uint64_t i = warp; i < n; i += nwarps) {
         const uint64_t a = ptr[i], b = ptr[i + 1];
-        const double ki = fmax(strength[i], 1e-300);
-        for (uint64_t e0 = a; e0 < b; e0 += 32) {
-            const uint64_t e = e0 + lane;
-            const uint32_t L = e < b ? label[nbr[e]] : 0u;
-            double acc = 0.0;
-            for (uint64_t x0 = a; x0 < b; x0 += 32) {
-                const uint64_t x = x0 + lane;
-                uint32_t lx = 0u;
-                float wx = 0.0f;
-                int vx = 0;
-                if (x < b) {
-                    const uint32_t v = nbr[x];
-                    vx = v != (uint32_t)i;
-                    lx = label[v];
-                    wx = w[x];
-                }
-                const int cnt = (int)(b - x0 < 32 ? b - x0 : 32);
-                for (int t = 0; t < cnt; ++t) {
-                    const uint32_t lt = __shfl_sync(0xFFFFFFFFu, lx, t);
-                    const float wt = __shfl_sync(0xFFFFFFFFu, wx, t);
-                    const int vt = __shfl_sync(0xFFFFFFFFu, vx, t);
-                    if (vt && lt == L) acc += (double)wt;
-                }
-            }
-            if (e < b) share[e] = (float)(acc / ki);
-        }
+        if (b - a > 32 * 32) continue;
+        label_share_chunks(nbr, w, label, (uint32_t)i, a, b, 0, 1, fmax(strength[i], 1e-300), share);
+    }
+}
+
+// Rows of more than 32 chunks (listed in big[0, nbig)): a block per row, its
+// warps on alternate e-chunks.
+__global__ void k_label_share_big(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
+                                  const float* __restrict__ w, const uint32_t* __restrict__ label,
+                                  const double* __restrict__ strength, const uint32_t* __restrict__ big,
+                                  uint32_t nbig, float* __restrict__ share) {
+    const uint64_t wib = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t k = blockIdx.x; k < nbig; k += gridDim.x) {
+        const uint32_t i = big[k];
+        label_share_chunks(nbr, w, label, i, ptr[i], ptr[i + 1], wib, nw, fmax(strength[i], 1e-300), share);
     }
 }
 
@@ -120,30 +155,39 @@ __device__ __forceinline__ uint64_t entry_of(const uint64_t* __restrict__ ptr, c
     return lo;
 }
 
-__device__ __forceinline__ float emb_dist2(const float* __restrict__ emb, uint32_t i, uint32_t j) {
-    float s = 0.0f;
-#pragma unroll
-    for (int r = 0; r < EMB_R; ++r) {
-        const float d = emb[(uint64_t)i * EMB_R + r] - emb[(uint64_t)j * EMB_R + r];
-        s = __fmaf_rn(d, d, s);
-    }
-    return s;
-}
-
 // s_i: mean of |y_i - y_x|^2 over the neighbours x != i (0 for none).
 __global__ void k_emb_scale(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr, uint64_t n,
                             const float* __restrict__ emb, float* scale) {
+    static_assert(EMB_R == 16, "four float4 loads per projected point");
+    const float4* e4 = reinterpret_cast<const float4*>(emb);
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        float4 yi[4];
+        for (int q = 0; q < 4; ++q) yi[q] = e4[i * 4 + q];
         double s = 0.0;
         uint64_t cnt = 0;
         for (uint64_t x = ptr[i]; x < ptr[i + 1]; ++x) {
             const uint32_t v = nbr[x];
             if (v == (uint32_t)i) continue;
-            s += (double)emb_dist2(emb, (uint32_t)i, v);
+            float t = 0.0f;
+            for (int q = 0; q < 4; ++q) {
+                const float4 yv = e4[(uint64_t)v * 4 + q];
+                const float d0 = yi[q].x - yv.x, d1 = yi[q].y - yv.y, d2 = yi[q].z - yv.z, d3 = yi[q].w - yv.w;
+                t = __fmaf_rn(d0, d0, t);
+                t = __fmaf_rn(d1, d1, t);
+                t = __fmaf_rn(d2, d2, t);
+                t = __fmaf_rn(d3, d3, t);
+            }
+            s += (double)t;
             ++cnt;
         }
         scale[i] = cnt ? (float)(s / (double)cnt) : 0.0f;
     }
+}
+
+__global__ void k_node_logs(const uint64_t* __restrict__ ptr, const double* __restrict__ strength, uint64_t n,
+                            float2* nlog) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        nlog[i] = make_float2((float)log1p(strength[i]), (float)log((double)(ptr[i + 1] - ptr[i])));
 }
 
 // Upper entries (neighbour > row) per row: the undirected edges i < j that
@@ -154,151 +198,234 @@ __global__ void k_upper_counts(const uint64_t* __restrict__ ptr, const uint32_t*
         cnt[i] = i < n ? ptr[i + 1] - entry_of(ptr, nbr, (uint32_t)i, (uint32_t)i + 1u) : 0;
 }
 
-__device__ __forceinline__ double warp_sum_d(double v) {
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xFFFFFFFFu, v, o);
-    return v;
+constexpr int ROW_STAGE = 256;   // row entries a warp keeps in shared memory (rows up to this size)
+constexpr int BIG_STAGE = 8192;  // row entries a block keeps in shared memory for a larger row
+constexpr int EDGE_LANES = 8;    // lanes per edge: a warp works on 4 edges of a row at once
+
+struct FeatArgs {
+    const uint64_t* ptr;
+    const uint32_t* nbr;
+    const float* w;
+    const double* strength;
+    const float2* nlog;  // per node: log1p(strength), log(degree)
+    double two_m, gamma;
+    const uint32_t* coarse;
+    const uint32_t* fine;
+    const float* share_c;
+    const float* share_f;
+    const float* emb;
+    const float* emb_scale;
+    const uint64_t* base;
+    float* feat;
+    uint32_t* ei;
+    uint32_t* ej;
+};
+
+// Row i's entries [a, b), staged (ids and weights at x - a in shared memory)
+// or not (read from the graph).
+struct RowView {
+    uint32_t i;
+    uint64_t a, b, us;  // us: first entry with neighbour > i
+    const uint32_t* sid;
+    const float* sw;
+    bool staged;
+};
+
+// The features of edge (i, nbr[e]) by the 8 lanes of a group (gl = lane in
+// the group). Called by all 32 lanes of the warp together (the reductions
+// shuffle across the full warp, each group within itself); inactive groups
+// take part with nothing to do. The 8 lanes walk one endpoint's row (lane l
+// takes entries l, l + 8, ...) and look each entry up in the other row by
+// binary search: row i from shared memory when staged, unless row j is much
+// the shorter one. Sums are reductions over the 8 lanes in a fixed tree; lane
+// l writes features l and l + 8. Edge (i, j) lands at base[i] + its rank among
+// i's upper entries, i.e. in ascending (i, j) order.
+__device__ __forceinline__ void edge_group(const FeatArgs& A, const RowView& R, uint64_t e, bool active, int gl) {
+    const uint64_t* __restrict__ ptr = A.ptr;
+    const uint32_t* __restrict__ nbr = A.nbr;
+    const float* __restrict__ w = A.w;
+    const uint32_t i = R.i;
+    const uint64_t di_n = R.b - R.a;
+    const uint32_t j = active ? (R.staged ? R.sid[e - R.a] : nbr[e]) : i;
+    const uint64_t ja = ptr[j], jb = ptr[j + 1];
+    const uint64_t dj_n = jb - ja;
+    // common neighbours c != i, j: walk one row, search the other
+    const bool walk_j = R.staged ? dj_n <= 8 * di_n : dj_n <= di_n;
+    double cw = 0.0;
+    uint32_t cn = 0;
+    unsigned long long rev = ~0ull;  // the entry (j, i), found while walking row j
+    const uint64_t wa = active ? (walk_j ? ja : R.a) : 0, wb = active ? (walk_j ? jb : R.b) : 0;
+    for (uint64_t x = wa + gl; x < wb; x += EDGE_LANES) {
+        const bool from_smem = !walk_j && R.staged;
+        const uint32_t cc = from_smem ? R.sid[x - R.a] : nbr[x];
+        const float wc = from_smem ? R.sw[x - R.a] : w[x];
+        if (walk_j && cc == i) rev = x;
+        if (cc == i || cc == j) continue;
+        float wo = 0.0f;
+        bool found = false;
+        if (walk_j && R.staged) {
+            uint32_t lo = 0, hi = (uint32_t)di_n;
+            while (lo < hi) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (R.sid[mid] < cc) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < di_n && R.sid[lo] == cc) {
+                found = true;
+                wo = R.sw[lo];
+            }
+        } else {
+            const uint64_t oa = walk_j ? R.a : ja, ob = walk_j ? R.b : jb;
+            uint64_t lo = oa, hi = ob;
+            while (lo < hi) {
+                const uint64_t mid = (lo + hi) >> 1;
+                if (nbr[mid] < cc) lo = mid + 1;
+                else hi = mid;
+            }
+            if (lo < ob && nbr[lo] == cc) {
+                found = true;
+                wo = w[lo];
+            }
+        }
+        if (found) {
+            cw += (double)fminf(wc, wo);
+            ++cn;
+        }
+    }
+    for (int o = EDGE_LANES / 2; o; o >>= 1) {
+        cw += __shfl_xor_sync(0xFFFFFFFFu, cw, o);
+        cn += __shfl_xor_sync(0xFFFFFFFFu, cn, o);
+        rev = min(rev, (unsigned long long)__shfl_xor_sync(0xFFFFFFFFu, rev, o));
+    }
+    if ((A.coarse || A.fine) && active && rev == ~0ull) rev = entry_of(ptr, nbr, j, i);
+    float ed2 = 0.0f;
+    if (A.emb) {
+        float t = 0.0f;
+        if (active)
+            for (int r = gl; r < EMB_R; r += EDGE_LANES) {
+                const float dd = A.emb[(uint64_t)i * EMB_R + r] - A.emb[(uint64_t)j * EMB_R + r];
+                t = __fmaf_rn(dd, dd, t);
+            }
+        for (int o = EDGE_LANES / 2; o; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
+        ed2 = t;
+    }
+    if (!active) return;
+    const uint64_t pos = A.base[i] + (e - R.us);
+    // every lane of the group forms all 15 features (same addresses: one
+    // transaction per load), then writes features gl and gl + 8
+    const float wij = R.staged ? R.sw[e - R.a] : w[e];
+    const double kid = A.strength[i], kjd = A.strength[j];
+    const float ki = (float)kid, kj = (float)kjd, di = (float)di_n, dj = (float)dj_n;
+    const float2 li = A.nlog[i], lj = A.nlog[j];
+    static_assert(MLP_F == 15 && EDGE_LANES == 8, "lane gl writes features gl and gl + 8");
+    const float v0 = wij, v1 = li.x + lj.x, v2 = fabsf(li.x - lj.x), v3 = li.y + lj.y, v4 = fabsf(li.y - lj.y);
+    const float v5 = wij / fmaxf(ki, 1e-30f) + wij / fmaxf(kj, 1e-30f);
+    const float v6 = (float)log(A.gamma);
+    const float v7 = A.two_m > 0.0 ? (float)(A.gamma * kid * kjd / (A.two_m * fmax((double)wij, 1e-300))) : 0.0f;
+    const float v8 = (float)(cw / fmax(fmin(kid, kjd), 1e-300));
+    const float v9 = (float)cn / fmaxf(fminf(di, dj), 1.0f);
+    const float v10 = A.coarse ? (A.coarse[i] == A.coarse[j] ? 1.0f : 0.0f) : 0.0f;
+    const float v11 = A.fine ? (A.fine[i] == A.fine[j] ? 1.0f : 0.0f) : 0.0f;
+    const float v12 = A.coarse ? 0.5f * (A.share_c[e] + A.share_c[rev]) : 0.0f;
+    const float v13 = A.fine ? 0.5f * (A.share_f[e] + A.share_f[rev]) : 0.0f;
+    const float v14 = A.emb ? ed2 / fmaxf(0.5f * (A.emb_scale[i] + A.emb_scale[j]), 1e-30f) : 0.0f;
+    const float o0 = gl == 0 ? v0 : gl == 1 ? v1 : gl == 2 ? v2 : gl == 3 ? v3 : gl == 4 ? v4 : gl == 5 ? v5
+                   : gl == 6 ? v6 : v7;
+    const float o1 = gl == 0 ? v8 : gl == 1 ? v9 : gl == 2 ? v10 : gl == 3 ? v11 : gl == 4 ? v12 : gl == 5 ? v13
+                   : v14;
+    A.feat[pos * MLP_F + gl] = o0;
+    if (gl < MLP_F - 8) A.feat[pos * MLP_F + gl + 8] = o1;
+    if (gl == 0) {
+        A.ei[pos] = i;
+        A.ej[pos] = j;
+    }
 }
 
-constexpr int ROW_STAGE = 256;  // row entries a warp keeps in shared memory for the searches
-
-// Features of the undirected edges i < j, a warp per row i. Edge (i, j) lands
-// at base[i] + its rank among i's upper entries, i.e. in ascending (i, j)
-// order, the same on every run. Per edge the warp walks one endpoint's row in
-// 32-entry chunks (lane l takes entry l of a chunk) and every lane looks its
-// entry up in the other row by binary search: row i from shared memory (when
-// it fits) unless row j is much the shorter one. The common-neighbour sums
-// and the embedding length are warp reductions in a fixed tree; lane f writes
-// feature f.
-__global__ void __launch_bounds__(TB) k_edge_rows(const uint64_t* __restrict__ ptr, const uint32_t* __restrict__ nbr,
-                                                  const float* __restrict__ w, uint64_t n,
-                                                  const double* __restrict__ strength, double two_m, double gamma,
-                                                  const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine,
-                                                  const float* __restrict__ share_c, const float* __restrict__ share_f,
-                                                  const float* __restrict__ emb, const float* __restrict__ emb_scale,
-                                                  const uint64_t* __restrict__ base, float* __restrict__ feat,
-                                                  uint32_t* __restrict__ ei, uint32_t* __restrict__ ej) {
+// Rows of at most ROW_STAGE entries: a warp per row, 4 edges at a time.
+// Larger rows are left to k_edge_big_rows.
+__global__ void __launch_bounds__(TB, 4) k_edge_rows(FeatArgs A, uint64_t n) {
     __shared__ uint32_t s_id[TB / 32][ROW_STAGE];
     __shared__ float s_w[TB / 32][ROW_STAGE];
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int grp = lane / EDGE_LANES, gl = lane % EDGE_LANES;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    uint32_t* sid = s_id[wib];
-    float* sw = s_w[wib];
     for (uint64_t iw = warp; iw < n; iw += nwarps) {
-        const uint32_t i = (uint32_t)iw;
-        const uint64_t a = ptr[i], b = ptr[i + 1];
-        const uint64_t us = entry_of(ptr, nbr, i, i + 1u);
-        if (us == b) continue;  // no upper entries
-        const uint64_t di_n = b - a;
-        const bool staged = di_n <= (uint64_t)ROW_STAGE;
+        RowView R;
+        R.i = (uint32_t)iw;
+        R.a = A.ptr[R.i];
+        R.b = A.ptr[R.i + 1];
+        if (R.b - R.a > (uint64_t)ROW_STAGE) continue;
+        R.sid = s_id[wib];
+        R.sw = s_w[wib];
+        R.staged = true;
         __syncwarp();
-        if (staged)
-            for (uint64_t x = lane; x < di_n; x += 32) {
-                sid[x] = nbr[a + x];
-                sw[x] = w[a + x];
-            }
+        uint32_t below = 0;  // entries with neighbour <= i
+        for (uint64_t x = lane; x < R.b - R.a; x += 32) {
+            const uint32_t v = A.nbr[R.a + x];
+            s_id[wib][x] = v;
+            s_w[wib][x] = A.w[R.a + x];
+            below += v <= R.i;
+        }
+        for (int o = 16; o; o >>= 1) below += __shfl_xor_sync(0xFFFFFFFFu, below, o);
         __syncwarp();
-        const double ki = strength[i], di = (double)di_n;
-        const double lki = log1p(ki), ldi = log(di);
-        uint64_t pos = base[i];
-        for (uint64_t e = us; e < b; ++e, ++pos) {
-            const uint32_t j = nbr[e];
-            const double wij = (double)w[e];
-            const uint64_t ja = ptr[j], jb = ptr[j + 1];
-            const uint64_t dj_n = jb - ja;
-            const double kj = strength[j], dj = (double)dj_n;
-            // common neighbours c != i, j: walk one row, search the other
-            const bool walk_j = staged ? dj_n <= 8 * di_n : dj_n <= di_n;
-            double cw = 0.0;
-            uint32_t cn = 0;
-            uint64_t rev = ~0ull;  // the entry (j, i), found while walking row j
-            const uint64_t wa = walk_j ? ja : a, wb = walk_j ? jb : b;
-            for (uint64_t x0 = wa; x0 < wb; x0 += 32) {
-                const uint64_t x = x0 + lane;
-                if (x < wb) {
-                    const uint32_t cc = nbr[x];
-                    const float wc = w[x];
-                    if (walk_j && cc == i) rev = x;
-                    if (cc != i && cc != j) {
-                        float wo = 0.0f;
-                        bool found = false;
-                        if (walk_j && staged) {
-                            uint32_t lo = 0, hi = (uint32_t)di_n;
-                            while (lo < hi) {
-                                const uint32_t mid = (lo + hi) >> 1;
-                                if (sid[mid] < cc) lo = mid + 1;
-                                else hi = mid;
-                            }
-                            if (lo < di_n && sid[lo] == cc) {
-                                found = true;
-                                wo = sw[lo];
-                            }
-                        } else {
-                            const uint64_t oa = walk_j ? a : ja, ob = walk_j ? b : jb;
-                            uint64_t lo = oa, hi = ob;
-                            while (lo < hi) {
-                                const uint64_t mid = (lo + hi) >> 1;
-                                if (nbr[mid] < cc) lo = mid + 1;
-                                else hi = mid;
-                            }
-                            if (lo < ob && nbr[lo] == cc) {
-                                found = true;
-                                wo = w[lo];
-                            }
-                        }
-                        if (found) {
-                            cw += (double)fminf(wc, wo);
-                            ++cn;
-                        }
-                    }
-                }
-            }
-            cw = warp_sum_d(cw);
-            for (int o = 16; o; o >>= 1) cn += __shfl_xor_sync(0xFFFFFFFFu, cn, o);
-            if (coarse || fine) {
-                unsigned long long r = rev;
-                for (int o = 16; o; o >>= 1) r = min(r, (unsigned long long)__shfl_xor_sync(0xFFFFFFFFu, r, o));
-                rev = r != ~0ull ? r : entry_of(ptr, nbr, j, i);
-            }
-            double ed2 = 0.0;
-            if (emb) {
-                float t = 0.0f;
-                if (lane < EMB_R) {
-                    const float dd = emb[(uint64_t)i * EMB_R + lane] - emb[(uint64_t)j * EMB_R + lane];
-                    t = dd * dd;
-                }
-                for (int o = 16; o; o >>= 1) t += __shfl_xor_sync(0xFFFFFFFFu, t, o);
-                ed2 = (double)t;
-            }
-            if (lane < MLP_F) {
-                const double lkj = log1p(kj), ldj = log(dj);
-                double v = 0.0;
-                switch (lane) {
-                    case 0: v = wij; break;
-                    case 1: v = lki + lkj; break;
-                    case 2: v = fabs(lki - lkj); break;
-                    case 3: v = ldi + ldj; break;
-                    case 4: v = fabs(ldi - ldj); break;
-                    case 5: v = wij / fmax(ki, 1e-300) + wij / fmax(kj, 1e-300); break;
-                    case 6: v = log(gamma); break;
-                    case 7: v = two_m > 0.0 ? gamma * ki * kj / (two_m * fmax(wij, 1e-300)) : 0.0; break;
-                    case 8: v = cw / fmax(fmin(ki, kj), 1e-300); break;
-                    case 9: v = (double)cn / fmax(fmin(di, dj), 1.0); break;
-                    case 10: v = coarse ? (coarse[i] == coarse[j] ? 1.0 : 0.0) : 0.0; break;
-                    case 11: v = fine ? (fine[i] == fine[j] ? 1.0 : 0.0) : 0.0; break;
-                    case 12: v = coarse ? 0.5 * ((double)share_c[e] + (double)share_c[rev]) : 0.0; break;
-                    case 13: v = fine ? 0.5 * ((double)share_f[e] + (double)share_f[rev]) : 0.0; break;
-                    default:
-                        v = emb ? ed2 / fmax(0.5 * ((double)emb_scale[i] + (double)emb_scale[j]), 1e-30) : 0.0;
-                }
-                feat[pos * MLP_F + lane] = (float)v;
-            }
-            if (lane == 0) {
-                ei[pos] = i;
-                ej[pos] = j;
-            }
+        R.us = R.a + below;
+        for (uint64_t e0 = R.us; e0 < R.b; e0 += 32 / EDGE_LANES) {
+            const uint64_t e = e0 + grp;
+            edge_group(A, R, e, e < R.b, gl);
         }
     }
+}
+
+// Rows of more than ROW_STAGE entries (hubs of the kNN graph: a point in many
+// other points' lists), listed in big[0, nbig): a block per row, its 32 lane
+// groups on 32 edges at a time, the row staged in shared memory up to
+// BIG_STAGE entries (beyond that the searches read the graph).
+__global__ void __launch_bounds__(TB) k_edge_big_rows(FeatArgs A, const uint32_t* __restrict__ big, uint32_t nbig) {
+    extern __shared__ __align__(16) unsigned char big_smem[];
+    uint32_t* sid = reinterpret_cast<uint32_t*>(big_smem);
+    float* sw = reinterpret_cast<float*>(big_smem + BIG_STAGE * sizeof(uint32_t));
+    __shared__ uint32_t s_below;
+    const int lane = threadIdx.x & 31;
+    const int grp = threadIdx.x / EDGE_LANES, gl = lane % EDGE_LANES;
+    constexpr int GROUPS = TB / EDGE_LANES;
+    for (uint32_t k = blockIdx.x; k < nbig; k += gridDim.x) {
+        RowView R;
+        R.i = big[k];
+        R.a = A.ptr[R.i];
+        R.b = A.ptr[R.i + 1];
+        R.staged = R.b - R.a <= (uint64_t)BIG_STAGE;
+        R.sid = sid;
+        R.sw = sw;
+        __syncthreads();
+        if (threadIdx.x == 0) s_below = 0;
+        __syncthreads();
+        uint32_t below = 0;
+        for (uint64_t x = threadIdx.x; x < R.b - R.a; x += blockDim.x) {
+            const uint32_t v = A.nbr[R.a + x];
+            if (R.staged) {
+                sid[x] = v;
+                sw[x] = A.w[R.a + x];
+            }
+            below += v <= R.i;
+        }
+        for (int o = 16; o; o >>= 1) below += __shfl_xor_sync(0xFFFFFFFFu, below, o);
+        if (lane == 0) atomicAdd(&s_below, below);
+        __syncthreads();
+        R.us = R.a + s_below;
+        for (uint64_t e0 = R.us; e0 < R.b; e0 += GROUPS) {
+            const uint64_t e = e0 + grp;
+            edge_group(A, R, e, e < R.b, gl);
+        }
+    }
+}
+
+// Rows of more than `limit` entries (in no particular order: each row's
+// results have fixed places).
+__global__ void k_big_rows(const uint64_t* __restrict__ ptr, uint64_t n, uint64_t limit, uint32_t* big,
+                           unsigned* nbig) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        if (ptr[i + 1] - ptr[i] > limit) big[atomicAdd(nbig, 1u)] = (uint32_t)i;
 }
 
 // Per-feature mean / inverse std over the edges (fixed-order block partials).
@@ -709,6 +836,16 @@ struct EdgeSet {
 
 void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
                  EdgeSet& es) {
+    static const bool trace = std::getenv("SC_TRACE") != nullptr;
+    std::vector<cudaEvent_t> ev;
+    auto mark = [&]() {
+        if (!trace) return;
+        cudaEvent_t e;
+        SC_CUDA(cudaEventCreate(&e));
+        SC_CUDA(cudaEventRecord(e, c.stream));
+        ev.push_back(e);
+    };
+    mark();
     // edge positions: upper entries per row, exclusive sum
     DBuf<uint64_t> cnt(c, g.n + 1), base(c, g.n + 1);
     k_upper_counts<<<grid_for(g.n + 1, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, cnt.get());
@@ -721,7 +858,21 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
     es.ei.alloc(c, M);
     es.ej.alloc(c, M);
     if (!M) return;
+    mark();
+    // rows past what a warp handles, for the block-per-row kernels
+    auto big_rows = [&](uint64_t limit, DBuf<uint32_t>& list) -> unsigned {
+        if (g.max_degree <= limit) return 0;
+        list.alloc(c, g.n);
+        DBuf<unsigned> nb(c, 1);
+        zero(c, nb.get(), 1);
+        k_big_rows<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.n, limit, list.get(), nb.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        return to_host(c, nb.get());
+    };
     DBuf<float> share_c, share_f;
+    DBuf<uint32_t> big_share;
+    const unsigned nb_share = (coarse || fine) ? big_rows(32 * 32, big_share) : 0;
     for (int t = 0; t < 2; ++t) {
         const uint32_t* lab = t == 0 ? coarse : fine;
         DBuf<float>& sh = t == 0 ? share_c : share_f;
@@ -731,7 +882,14 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
                                                                    sh.get());
         SC_LAUNCH_CHECK();
         c.launches++;
+        if (nb_share) {
+            k_label_share_big<<<std::min<unsigned>(nb_share, 148u * 8u), TB, 0, c.stream>>>(
+                g.ptr, g.nbr, g.w, lab, g.strength, big_share.get(), nb_share, sh.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+        }
     }
+    mark();
     DBuf<float> scale;
     if (g.emb) {
         scale.alloc(c, g.n);
@@ -739,12 +897,37 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
         SC_LAUNCH_CHECK();
         c.launches++;
     }
-    k_edge_rows<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, g.n, g.strength, 2.0 * g.total_weight,
-                                                             gamma, coarse, fine, share_c.get(), share_f.get(), g.emb,
-                                                             scale.get(), base.get(), es.feat.get(), es.ei.get(),
-                                                             es.ej.get());
+    mark();
+    DBuf<float2> nlog(c, g.n);
+    k_node_logs<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.strength, g.n, nlog.get());
     SC_LAUNCH_CHECK();
     c.launches++;
+    const FeatArgs A{g.ptr, g.nbr, g.w, g.strength, nlog.get(), 2.0 * g.total_weight, gamma, coarse, fine,
+                     share_c.get(), share_f.get(), g.emb, scale.get(), base.get(), es.feat.get(), es.ei.get(),
+                     es.ej.get()};
+    k_edge_rows<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(A, g.n);
+    SC_LAUNCH_CHECK();
+    c.launches++;
+    mark();
+    DBuf<uint32_t> big_edge;
+    const unsigned nb = big_rows(ROW_STAGE, big_edge);
+    if (nb) {
+        const size_t sm = (size_t)BIG_STAGE * (sizeof(uint32_t) + sizeof(float));
+        SC_CUDA(cudaFuncSetAttribute(k_edge_big_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+        k_edge_big_rows<<<std::min<unsigned>(nb, 148u * 8u), TB, sm, c.stream>>>(A, big_edge.get(), nb);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    }
+    if (trace) std::fprintf(stderr, "[sc] edge features: %u rows past %d entries\n", nb, ROW_STAGE);
+    mark();
+    if (trace) {
+        SC_CUDA(cudaEventSynchronize(ev.back()));
+        float t[5] = {};
+        for (int k = 0; k < 5; ++k) SC_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+        std::fprintf(stderr, "[sc] edge features M=%llu: positions %.2f ms, label shares %.2f ms, embedding scale "
+                     "%.2f ms, rows %.2f ms, big rows %.2f ms\n", (unsigned long long)M, t[0], t[1], t[2], t[3], t[4]);
+        for (cudaEvent_t e : ev) cudaEventDestroy(e);
+    }
 }
 
 // Standardise es's features with the model's scaler, fitting it first if the

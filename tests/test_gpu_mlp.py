@@ -34,13 +34,28 @@ def _planted(n=3000, blocks=30, seed=2):
     return sc_gpu.CSRNetwork.from_edge_arrays(n, src, dst, w), truth
 
 
+def _hub_graph(n):
+    """A ring with chords (i, i+1), (i, i+3) plus node 0 joined to every node
+    and node 1 to every 20th: rows far longer than a warp stages (node 0 also
+    past what a block stages), the shapes of kNN hubs."""
+    import sc_gpu
+    rng = np.random.default_rng(4)
+    src = np.concatenate([np.arange(n), np.arange(n), np.zeros(n - 1, np.int64), np.ones(n // 20, np.int64)])
+    dst = np.concatenate([(np.arange(n) + 1) % n, (np.arange(n) + 3) % n, np.arange(1, n),
+                          np.arange(0, n, 20) + 2])
+    keep = src != dst
+    src, dst = src[keep], dst[keep]
+    w = rng.uniform(0.5, 1.5, len(src))
+    return sc_gpu.CSRNetwork.from_edge_arrays(n, src.astype(np.uint64), dst.astype(np.uint64), w)
+
+
 def test_features_match_oracle():
     import sc_gpu
     from sc_gpu.learned import EdgeMlp
     from helpers import karate
     edges, _ = karate()
     rng = np.random.default_rng(0)
-    for g in (sc_gpu.CSRNetwork.from_edges(34, edges), _planted(800, 8)[0]):
+    for g in (sc_gpu.CSRNetwork.from_edges(34, edges), _planted(800, 8)[0], _hub_graph(9000)):
         n = g.node_count()
         X = rng.normal(size=(n, 7)).astype(np.float32)
         for gamma, ctx, emb in ((1.0, None, None), (0.3, (rng.integers(0, 3, n) * 7, rng.integers(0, 9, n)), None),
