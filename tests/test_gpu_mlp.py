@@ -11,8 +11,8 @@
 * gain: trained on plain-GPU Leiden partitions at RB {0.5, 1, 2} (each with the
   partitions of its neighbouring resolutions as context), the proposal used as
   a warm start at RB {0.8, 1.5} needs fewer local-moving sweeps than the plain
-  singleton start, with final modularity >= plain - 1e-4 or the check falling
-  back to the plain result.
+  singleton start and less wall time (proposal included, best of three, at
+  least 10% less), with final modularity >= plain - 1e-4.
 """
 import numpy as np
 import pytest
@@ -178,11 +178,18 @@ def test_warm_start_gain_over_plain_start():
     saved = []
     for gamma, ctx in ((0.8, (labs[0.5], labs[1.0])), (1.5, (labs[1.0], labs[2.0]))):
         cfg = sc_gpu.LeidenConfig(objective=sc_gpu.Rb(gamma), seed=9)
-        res = warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=0.0, context=ctx)
+        runs = [warm_start_leiden(m, g, cfg, threshold=0.9, core_fraction=0.0, context=ctx) for _ in range(3)]
+        res = runs[-1]
         assert res.q_warm >= res.q_plain - 1e-4 or not res.used_proposal
         final_q = sc_gpu.modularity(g, res.labels, gamma)
         assert final_q >= res.q_plain - 1e-4
         saved.append(res.sweeps_plain - res.sweeps_warm)
+        # wall time: the proposal (host clock) plus the warm run against the
+        # plain run, best of three each (measured ~6.7 vs ~10.8 ms here)
+        assert res.used_proposal
+        best_warm = min(r.ms_warm for r in runs)
+        best_plain = min(r.ms_plain for r in runs)
+        assert best_warm < 0.9 * best_plain, (gamma, best_warm, best_plain)
     assert sum(saved) > 0, saved
 
 
