@@ -457,7 +457,11 @@ sc_status sc_knn_connectivities(sc_ctx* ctx, const uint32_t* knn_index, const fl
  * relative to the endpoints' local scale. A model trained with a context or an
  * embedding is meant to be used with them. The contraction runs on the tensor
  * cores (BF16 operands, features and hidden gradients split into two BF16
- * parts, FP32 accumulation); Adam updates an FP32 master copy. Parameters are laid out W1[f*128+u], b1[u],
+ * parts, FP32 accumulation); Adam updates an FP32 master copy. The features
+ * that depend on neither the resolution nor a context (40 bytes per undirected
+ * edge, plus the edge list: 64 bytes per edge) are computed on a graph's first
+ * use and kept with the graph until sc_graph_destroy or a new
+ * sc_graph_set_embedding. Parameters are laid out W1[f*128+u], b1[u],
  * w2[u], b2 (sc_mlp_param_count() floats). The feature scaler (means, then
  * inverse standard deviations, 2 * feature_count floats) is fitted on the first
  * graph the model trains on or extracts features from.

@@ -155,8 +155,8 @@ double ordered_sum_from(Ctx& c, const double* d_terms, uint64_t n, double init) 
 }
 
 void DevGraph::free_all() {
-    void* ps[] = {ptr, nbr, w, erow, node_w, strength, self_loop, emb};
-    if (ptr || nbr || w || erow || node_w || strength || self_loop || emb) {
+    void* ps[] = {ptr, nbr, w, erow, node_w, strength, self_loop, emb, edge_sf, edge_i, edge_j, edge_e};
+    if (ptr || nbr || w || erow || node_w || strength || self_loop || emb || edge_sf || edge_i || edge_j || edge_e) {
         int prev = 0;
         cudaGetDevice(&prev);
         if (prev != device) cudaSetDevice(device);
@@ -179,6 +179,12 @@ void DevGraph::free_all() {
     strength = nullptr;
     self_loop = nullptr;
     emb = nullptr;
+    edge_sf = nullptr;
+    edge_i = nullptr;
+    edge_j = nullptr;
+    edge_e = nullptr;
+    edge_m = 0;
+    edge_ready = false;
 }
 
 }  // namespace sc

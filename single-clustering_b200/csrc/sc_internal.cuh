@@ -13,6 +13,7 @@
 #include <cmath>
 #include <cstdio>
 #include <memory>
+#include <mutex>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -193,6 +194,18 @@ struct DevGraph {
     // from the graph pool), read by the learned warm start's features; null
     // when none was attached.
     float* emb = nullptr;
+    // The learned warm start's structural edge features (those that depend on
+    // neither the resolution nor a context partition), computed on first use
+    // and kept until the graph is freed or its embedding replaced, all from
+    // the graph pool: per undirected edge i < j in ascending order, its
+    // EDGE_SF features, endpoints and stored entries (i, j), (j, i).
+    mutable std::mutex edge_mu;
+    mutable float* edge_sf = nullptr;
+    mutable uint32_t* edge_i = nullptr;
+    mutable uint32_t* edge_j = nullptr;
+    mutable uint64_t* edge_e = nullptr;  // 2 per edge
+    mutable uint64_t edge_m = 0;
+    mutable bool edge_ready = false;
     uint64_t n_hubs = 0;      // nodes whose degree exceeds the shared-memory hash
     // stored weights bitwise symmetric: 0 not yet known, 1 yes, 2 no (computed
     // once, on first need; a benign race between contexts computes it twice)

@@ -40,6 +40,7 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cstdlib>
 #include <vector>
 
@@ -202,23 +203,25 @@ constexpr int ROW_STAGE = 256;   // row entries a warp keeps in shared memory (r
 constexpr int BIG_STAGE = 8192;  // row entries a block keeps in shared memory for a larger row
 constexpr int EDGE_LANES = 8;    // lanes per edge: a warp works on 4 edges of a row at once
 
+// The structural features of an edge, stored with the graph (EDGE_SF per
+// edge): features 0-5 of the MLP, k_i k_j / (2 m w) (feature 7 over gamma),
+// features 8 and 9, and feature 14.
+constexpr int EDGE_SF = 10;
+
 struct FeatArgs {
     const uint64_t* ptr;
     const uint32_t* nbr;
     const float* w;
     const double* strength;
     const float2* nlog;  // per node: log1p(strength), log(degree)
-    double two_m, gamma;
-    const uint32_t* coarse;
-    const uint32_t* fine;
-    const float* share_c;
-    const float* share_f;
+    double two_m;
     const float* emb;
     const float* emb_scale;
     const uint64_t* base;
-    float* feat;
+    float* sf;
     uint32_t* ei;
     uint32_t* ej;
+    uint64_t* ee;
 };
 
 // Row i's entries [a, b), staged (ids and weights at x - a in shared memory)
@@ -231,7 +234,7 @@ struct RowView {
     bool staged;
 };
 
-// The features of edge (i, nbr[e]) by the 8 lanes of a group (gl = lane in
+// The structural features of edge (i, nbr[e]) by the 8 lanes of a group (gl = lane in
 // the group). Called by all 32 lanes of the warp together (the reductions
 // shuffle across the full warp, each group within itself); inactive groups
 // take part with nothing to do. The 8 lanes walk one endpoint's row (lane l
@@ -239,7 +242,8 @@ struct RowView {
 // binary search: row i from shared memory when staged, unless row j is much
 // the shorter one. Sums are reductions over the 8 lanes in a fixed tree; lane
 // l writes features l and l + 8. Edge (i, j) lands at base[i] + its rank among
-// i's upper entries, i.e. in ascending (i, j) order.
+// i's upper entries, i.e. in ascending (i, j) order, with its endpoints and
+// its entries (i, j) and (j, i).
 __device__ __forceinline__ void edge_group(const FeatArgs& A, const RowView& R, uint64_t e, bool active, int gl) {
     const uint64_t* __restrict__ ptr = A.ptr;
     const uint32_t* __restrict__ nbr = A.nbr;
@@ -297,7 +301,7 @@ __device__ __forceinline__ void edge_group(const FeatArgs& A, const RowView& R, 
         cn += __shfl_xor_sync(0xFFFFFFFFu, cn, o);
         rev = min(rev, (unsigned long long)__shfl_xor_sync(0xFFFFFFFFu, rev, o));
     }
-    if ((A.coarse || A.fine) && active && rev == ~0ull) rev = entry_of(ptr, nbr, j, i);
+    if (active && rev == ~0ull) rev = entry_of(ptr, nbr, j, i);
     float ed2 = 0.0f;
     if (A.emb) {
         float t = 0.0f;
@@ -311,33 +315,55 @@ __device__ __forceinline__ void edge_group(const FeatArgs& A, const RowView& R, 
     }
     if (!active) return;
     const uint64_t pos = A.base[i] + (e - R.us);
-    // every lane of the group forms all 15 features (same addresses: one
-    // transaction per load), then writes features gl and gl + 8
+    // every lane of the group forms all EDGE_SF values (same addresses: one
+    // transaction per load), then writes values gl and gl + 8
     const float wij = R.staged ? R.sw[e - R.a] : w[e];
     const double kid = A.strength[i], kjd = A.strength[j];
     const float ki = (float)kid, kj = (float)kjd, di = (float)di_n, dj = (float)dj_n;
     const float2 li = A.nlog[i], lj = A.nlog[j];
-    static_assert(MLP_F == 15 && EDGE_LANES == 8, "lane gl writes features gl and gl + 8");
+    static_assert(EDGE_SF == 10 && EDGE_LANES == 8, "lane gl writes values gl and gl + 8");
     const float v0 = wij, v1 = li.x + lj.x, v2 = fabsf(li.x - lj.x), v3 = li.y + lj.y, v4 = fabsf(li.y - lj.y);
     const float v5 = wij / fmaxf(ki, 1e-30f) + wij / fmaxf(kj, 1e-30f);
-    const float v6 = (float)log(A.gamma);
-    const float v7 = A.two_m > 0.0 ? (float)(A.gamma * kid * kjd / (A.two_m * fmax((double)wij, 1e-300))) : 0.0f;
-    const float v8 = (float)(cw / fmax(fmin(kid, kjd), 1e-300));
-    const float v9 = (float)cn / fmaxf(fminf(di, dj), 1.0f);
-    const float v10 = A.coarse ? (A.coarse[i] == A.coarse[j] ? 1.0f : 0.0f) : 0.0f;
-    const float v11 = A.fine ? (A.fine[i] == A.fine[j] ? 1.0f : 0.0f) : 0.0f;
-    const float v12 = A.coarse ? 0.5f * (A.share_c[e] + A.share_c[rev]) : 0.0f;
-    const float v13 = A.fine ? 0.5f * (A.share_f[e] + A.share_f[rev]) : 0.0f;
-    const float v14 = A.emb ? ed2 / fmaxf(0.5f * (A.emb_scale[i] + A.emb_scale[j]), 1e-30f) : 0.0f;
+    const float v6 = A.two_m > 0.0 ? (float)(kid * kjd / (A.two_m * fmax((double)wij, 1e-300))) : 0.0f;
+    const float v7 = (float)(cw / fmax(fmin(kid, kjd), 1e-300));
+    const float v8 = (float)cn / fmaxf(fminf(di, dj), 1.0f);
+    const float v9 = A.emb ? ed2 / fmaxf(0.5f * (A.emb_scale[i] + A.emb_scale[j]), 1e-30f) : 0.0f;
     const float o0 = gl == 0 ? v0 : gl == 1 ? v1 : gl == 2 ? v2 : gl == 3 ? v3 : gl == 4 ? v4 : gl == 5 ? v5
                    : gl == 6 ? v6 : v7;
-    const float o1 = gl == 0 ? v8 : gl == 1 ? v9 : gl == 2 ? v10 : gl == 3 ? v11 : gl == 4 ? v12 : gl == 5 ? v13
-                   : v14;
-    A.feat[pos * MLP_F + gl] = o0;
-    if (gl < MLP_F - 8) A.feat[pos * MLP_F + gl + 8] = o1;
+    const float o1 = gl == 0 ? v8 : v9;
+    A.sf[pos * EDGE_SF + gl] = o0;
+    if (gl < EDGE_SF - 8) A.sf[pos * EDGE_SF + gl + 8] = o1;
     if (gl == 0) {
         A.ei[pos] = i;
         A.ej[pos] = j;
+        A.ee[2 * pos] = e;
+        A.ee[2 * pos + 1] = rev;
+    }
+}
+
+// The MLP's input of every edge: the structural values, log(gamma), gamma
+// times the null-term ratio, and the context features (co-membership at the
+// coarser and finer partitions, the two endpoints' label shares).
+__global__ void k_assemble(uint64_t M, const float* __restrict__ sf, const uint32_t* __restrict__ ei,
+                           const uint32_t* __restrict__ ej, const uint64_t* __restrict__ ee, float lgam,
+                           double gamma, const uint32_t* __restrict__ coarse, const uint32_t* __restrict__ fine,
+                           const float* __restrict__ share_c, const float* __restrict__ share_f,
+                           float* __restrict__ feat) {
+    for (uint64_t m = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; m < M; m += (uint64_t)gridDim.x * blockDim.x) {
+        const float* s = sf + m * EDGE_SF;
+        float* f = feat + m * MLP_F;
+        for (int k = 0; k < 6; ++k) f[k] = s[k];
+        f[6] = lgam;
+        f[7] = (float)(gamma * (double)s[6]);
+        f[8] = s[7];
+        f[9] = s[8];
+        const uint32_t i = ei[m], j = ej[m];
+        const uint64_t e = ee[2 * m], rev = ee[2 * m + 1];
+        f[10] = coarse ? (coarse[i] == coarse[j] ? 1.0f : 0.0f) : 0.0f;
+        f[11] = fine ? (fine[i] == fine[j] ? 1.0f : 0.0f) : 0.0f;
+        f[12] = coarse ? 0.5f * (share_c[e] + share_c[rev]) : 0.0f;
+        f[13] = fine ? 0.5f * (share_f[e] + share_f[rev]) : 0.0f;
+        f[14] = s[9];
     }
 }
 
@@ -831,21 +857,48 @@ __global__ void k_init_params(float* p, uint64_t seed) {
 struct EdgeSet {
     uint64_t M = 0;
     DBuf<float> feat;
-    DBuf<uint32_t> ei, ej;
+    const uint32_t* ei = nullptr;  // the graph's edge list (kept with the graph)
+    const uint32_t* ej = nullptr;
 };
 
-void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
-                 EdgeSet& es) {
+template <class T>
+T* graph_pool_alloc(Ctx& c, uint64_t count) {
+    T* p = nullptr;
+    if (!count) return p;
+    const cudaError_t e = cudaMallocFromPoolAsync((void**)&p, count * sizeof(T), user_graph_pool(c.device), c.stream);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        fail(SC_E_OUT_OF_MEMORY, "device allocation of %llu bytes failed", (unsigned long long)(count * sizeof(T)));
+    }
+    if (e != cudaSuccess) throw_cuda(e, "cudaMallocFromPoolAsync", __FILE__, __LINE__);
+    return p;
+}
+
+// Frees the graph's cached edge features (caller holds edge_mu).
+void drop_edge_cache(const DevGraph& g) {
+    if (!g.edge_sf && !g.edge_i && !g.edge_j && !g.edge_e) {
+        g.edge_ready = false;
+        return;
+    }
+    SC_CUDA(cudaDeviceSynchronize());  // any context's stream may still read them
+    for (void* p : {(void*)g.edge_sf, (void*)g.edge_i, (void*)g.edge_j, (void*)g.edge_e})
+        if (p) SC_CUDA(cudaFreeAsync(p, (cudaStream_t)0));
+    SC_CUDA(cudaStreamSynchronize((cudaStream_t)0));
+    g.edge_sf = nullptr;
+    g.edge_i = g.edge_j = nullptr;
+    g.edge_e = nullptr;
+    g.edge_m = 0;
+    g.edge_ready = false;
+}
+
+// The graph's structural edge features, computed once per graph (and again
+// after a new embedding): they depend on neither the resolution nor a context.
+void build_structural(Ctx& c, const DevGraph& g) {
+    std::lock_guard<std::mutex> lock(g.edge_mu);
+    if (g.edge_ready) return;
+    drop_edge_cache(g);  // the leftovers of a build that failed
     static const bool trace = std::getenv("SC_TRACE") != nullptr;
-    std::vector<cudaEvent_t> ev;
-    auto mark = [&]() {
-        if (!trace) return;
-        cudaEvent_t e;
-        SC_CUDA(cudaEventCreate(&e));
-        SC_CUDA(cudaEventRecord(e, c.stream));
-        ev.push_back(e);
-    };
-    mark();
+    const auto t0 = std::chrono::steady_clock::now();
     // edge positions: upper entries per row, exclusive sum
     DBuf<uint64_t> cnt(c, g.n + 1), base(c, g.n + 1);
     k_upper_counts<<<grid_for(g.n + 1, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, cnt.get());
@@ -853,26 +906,78 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
     c.launches++;
     exclusive_sum(c, cnt.get(), base.get(), g.n + 1);
     const uint64_t M = to_host(c, base.get() + g.n);
-    es.M = M;
-    es.feat.alloc(c, M * MLP_F);
-    es.ei.alloc(c, M);
-    es.ej.alloc(c, M);
-    if (!M) return;
-    mark();
-    // rows past what a warp handles, for the block-per-row kernels
-    auto big_rows = [&](uint64_t limit, DBuf<uint32_t>& list) -> unsigned {
-        if (g.max_degree <= limit) return 0;
-        list.alloc(c, g.n);
-        DBuf<unsigned> nb(c, 1);
-        zero(c, nb.get(), 1);
-        k_big_rows<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.n, limit, list.get(), nb.get());
+    g.edge_sf = graph_pool_alloc<float>(c, M * EDGE_SF);
+    g.edge_i = graph_pool_alloc<uint32_t>(c, M);
+    g.edge_j = graph_pool_alloc<uint32_t>(c, M);
+    g.edge_e = graph_pool_alloc<uint64_t>(c, 2 * M);
+    g.edge_m = M;
+    if (M) {
+        DBuf<float> scale;
+        if (g.emb) {
+            scale.alloc(c, g.n);
+            k_emb_scale<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, g.emb, scale.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+        }
+        DBuf<float2> nlog(c, g.n);
+        k_node_logs<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.strength, g.n, nlog.get());
         SC_LAUNCH_CHECK();
         c.launches++;
-        return to_host(c, nb.get());
-    };
+        const FeatArgs A{g.ptr,  g.nbr,       g.w,       g.strength, nlog.get(), 2.0 * g.total_weight, g.emb,
+                         scale.get(), base.get(), g.edge_sf, g.edge_i,   g.edge_j,   g.edge_e};
+        k_edge_rows<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(A, g.n);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        if (g.max_degree > (uint32_t)ROW_STAGE) {
+            // rows a warp cannot stage: a block each
+            DBuf<uint32_t> big(c, g.n);
+            DBuf<unsigned> nbig(c, 1);
+            zero(c, nbig.get(), 1);
+            k_big_rows<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.n, ROW_STAGE, big.get(), nbig.get());
+            SC_LAUNCH_CHECK();
+            c.launches++;
+            const unsigned nb = to_host(c, nbig.get());
+            if (nb) {
+                const size_t sm = (size_t)BIG_STAGE * (sizeof(uint32_t) + sizeof(float));
+                SC_CUDA(cudaFuncSetAttribute(k_edge_big_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_edge_big_rows<<<std::min<unsigned>(nb, 148u * 8u), TB, sm, c.stream>>>(A, big.get(), nb);
+                SC_LAUNCH_CHECK();
+                c.launches++;
+            }
+        }
+    }
+    sync(c);
+    g.edge_ready = true;
+    if (trace)
+        std::fprintf(stderr, "[sc] structural edge features M=%llu: %.2f ms (once per graph)\n", (unsigned long long)M,
+                     std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+}
+
+// The MLP input of every undirected edge of g at gamma with the context
+// partitions (nullable): the graph's structural values plus the
+// resolution and context features.
+void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse, const uint32_t* fine,
+                 EdgeSet& es) {
+    build_structural(c, g);
+    const uint64_t M = g.edge_m;
+    es.M = M;
+    es.ei = g.edge_i;
+    es.ej = g.edge_j;
+    es.feat.alloc(c, M * MLP_F);
+    if (!M) return;
     DBuf<float> share_c, share_f;
-    DBuf<uint32_t> big_share;
-    const unsigned nb_share = (coarse || fine) ? big_rows(32 * 32, big_share) : 0;
+    DBuf<uint32_t> big;
+    unsigned nb = 0;
+    if ((coarse || fine) && g.max_degree > 32u * 32u) {
+        // rows past 32 chunks: a block each
+        big.alloc(c, g.n);
+        DBuf<unsigned> nbig(c, 1);
+        zero(c, nbig.get(), 1);
+        k_big_rows<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.n, 32 * 32, big.get(), nbig.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        nb = to_host(c, nbig.get());
+    }
     for (int t = 0; t < 2; ++t) {
         const uint32_t* lab = t == 0 ? coarse : fine;
         DBuf<float>& sh = t == 0 ? share_c : share_f;
@@ -882,52 +987,18 @@ void build_edges(Ctx& c, const DevGraph& g, double gamma, const uint32_t* coarse
                                                                    sh.get());
         SC_LAUNCH_CHECK();
         c.launches++;
-        if (nb_share) {
-            k_label_share_big<<<std::min<unsigned>(nb_share, 148u * 8u), TB, 0, c.stream>>>(
-                g.ptr, g.nbr, g.w, lab, g.strength, big_share.get(), nb_share, sh.get());
+        if (nb) {
+            k_label_share_big<<<std::min<unsigned>(nb, 148u * 8u), TB, 0, c.stream>>>(g.ptr, g.nbr, g.w, lab,
+                                                                                    g.strength, big.get(), nb,
+                                                                                    sh.get());
             SC_LAUNCH_CHECK();
             c.launches++;
         }
     }
-    mark();
-    DBuf<float> scale;
-    if (g.emb) {
-        scale.alloc(c, g.n);
-        k_emb_scale<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.nbr, g.n, g.emb, scale.get());
-        SC_LAUNCH_CHECK();
-        c.launches++;
-    }
-    mark();
-    DBuf<float2> nlog(c, g.n);
-    k_node_logs<<<grid_for(g.n, TB), TB, 0, c.stream>>>(g.ptr, g.strength, g.n, nlog.get());
+    k_assemble<<<grid_for(M, TB), TB, 0, c.stream>>>(M, g.edge_sf, g.edge_i, g.edge_j, g.edge_e, (float)log(gamma),
+                                                     gamma, coarse, fine, share_c.get(), share_f.get(), es.feat.get());
     SC_LAUNCH_CHECK();
     c.launches++;
-    const FeatArgs A{g.ptr, g.nbr, g.w, g.strength, nlog.get(), 2.0 * g.total_weight, gamma, coarse, fine,
-                     share_c.get(), share_f.get(), g.emb, scale.get(), base.get(), es.feat.get(), es.ei.get(),
-                     es.ej.get()};
-    k_edge_rows<<<grid_for(g.n * 32, TB), TB, 0, c.stream>>>(A, g.n);
-    SC_LAUNCH_CHECK();
-    c.launches++;
-    mark();
-    DBuf<uint32_t> big_edge;
-    const unsigned nb = big_rows(ROW_STAGE, big_edge);
-    if (nb) {
-        const size_t sm = (size_t)BIG_STAGE * (sizeof(uint32_t) + sizeof(float));
-        SC_CUDA(cudaFuncSetAttribute(k_edge_big_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_edge_big_rows<<<std::min<unsigned>(nb, 148u * 8u), TB, sm, c.stream>>>(A, big_edge.get(), nb);
-        SC_LAUNCH_CHECK();
-        c.launches++;
-    }
-    if (trace) std::fprintf(stderr, "[sc] edge features: %u rows past %d entries\n", nb, ROW_STAGE);
-    mark();
-    if (trace) {
-        SC_CUDA(cudaEventSynchronize(ev.back()));
-        float t[5] = {};
-        for (int k = 0; k < 5; ++k) SC_CUDA(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
-        std::fprintf(stderr, "[sc] edge features M=%llu: positions %.2f ms, label shares %.2f ms, embedding scale "
-                     "%.2f ms, rows %.2f ms, big rows %.2f ms\n", (unsigned long long)M, t[0], t[1], t[2], t[3], t[4]);
-        for (cudaEvent_t e : ev) cudaEventDestroy(e);
-    }
 }
 
 // Standardise es's features with the model's scaler, fitting it first if the
@@ -1012,6 +1083,8 @@ void graph_set_embedding(Ctx& c, DevGraph& g, const float* X, uint64_t d) {
         c.launches++;
     }
     sync(c);
+    std::lock_guard<std::mutex> lock(g.edge_mu);
+    drop_edge_cache(g);  // the structural features read the embedding
     if (g.emb) {
         SC_CUDA(cudaDeviceSynchronize());
         SC_CUDA(cudaFreeAsync(g.emb, c.stream));
@@ -1088,8 +1161,8 @@ void mlp_features(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint32_
              (unsigned long long)es.M);
     scale_edges(c, m, es, true);
     if (feat_host) d2h(c, feat_host, es.feat.get(), es.M * MLP_F);
-    if (ei_host) d2h(c, ei_host, es.ei.get(), es.M);
-    if (ej_host) d2h(c, ej_host, es.ej.get(), es.M);
+    if (ei_host) d2h(c, ei_host, es.ei, es.M);
+    if (ej_host) d2h(c, ej_host, es.ej, es.M);
     sync(c);
 }
 
@@ -1103,7 +1176,7 @@ double mlp_train(Ctx& c, Mlp& m, const DevGraph& g, const uint32_t* d_memb, doub
     scale_edges(c, m, es, true);
     DBuf<uint8_t> lab(c, es.M);
     if (es.M) {
-        k_edge_labels<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), es.M, d_memb, lab.get());
+        k_edge_labels<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei, es.ej, es.M, d_memb, lab.get());
         SC_LAUNCH_CHECK();
         c.launches++;
     }
@@ -1160,9 +1233,9 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
     zero(c, deg.get(), n);
     zero(c, conf.get(), n);
     if (es.M) {
-        k_conf_degree<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
+        k_conf_degree<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei, es.ej, p.get(), es.M, (float)thr,
                                                                deg.get(), conf.get());
-        k_core_mask<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), p.get(), es.M, (float)thr,
+        k_core_mask<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei, es.ej, p.get(), es.M, (float)thr,
                                                              core_fraction, deg.get(), conf.get(), keep.get());
         SC_LAUNCH_CHECK();
         c.launches += 3;
@@ -1175,7 +1248,7 @@ uint64_t mlp_propose(Ctx& c, Mlp& m, const DevGraph& g, double gamma, const uint
     for (int round = 0; round < 4096 && !done; ++round) {
         zero(c, changed.get(), 1);
         if (es.M)
-            k_cc_hook<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei.get(), es.ej.get(), keep.get(), es.M, d_labels,
+            k_cc_hook<<<grid_for(es.M, TB), TB, 0, c.stream>>>(es.ei, es.ej, keep.get(), es.M, d_labels,
                                                                changed.get());
         for (int j = 0; j < 4; ++j) k_cc_jump<<<grid_for(n, TB), TB, 0, c.stream>>>(d_labels, n, changed.get());
         SC_LAUNCH_CHECK();
