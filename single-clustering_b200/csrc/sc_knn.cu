@@ -198,30 +198,6 @@ __device__ __noinline__ Worst cand_insert(float* cs, uint32_t* ci, int qrow, int
     return w;
 }
 
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]),
-          "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
-          "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-        : "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]),
-          "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]),
-          "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]),
-          "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]),
-          "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
-        : "r"(taddr + 32));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-}
-
 // ------------------------------------------------------------ prep
 template <int KA>
 __global__ void k_knn_prep(const float* __restrict__ X, uint64_t n, uint32_t d, __nv_bfloat16* A,
@@ -387,9 +363,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
     unsigned char* sB = smem + L::B_OFF;
     float* cs = (float*)(smem + L::C_OFF);
     uint32_t* ci = (uint32_t*)(smem + L::I_OFF);
-    constexpr int STG = L::STAGES;
     uint64_t* bars = (uint64_t*)(smem + L::BAR_OFF);
-    uint64_t* full = bars;                 // [STG] B tile landed
+    uint64_t* full = bars;                 // [L::STAGES] B tile landed
     uint64_t* empty = bars + L::STAGES;       // [L::STAGES] B tile consumed by the MMAs
     uint64_t* accfull = bars + 2 * L::STAGES;       // [2] accumulator ready
     uint64_t* accempty = bars + 2 * L::STAGES + 2;  // [2] accumulator drained
@@ -1368,7 +1343,12 @@ __global__ void k_cell_radius(const float* __restrict__ Xs, uint64_t n, uint32_t
 // Per pass-2 group (one block, a thread per query): the fine cells of the
 // group's candidate clusters (its own clusters and every cluster one of its
 // queries needs) that the ball bound |q - c_f| - r_f cannot exclude for at
-// least one query, as bits of the group's cell bitmap.
+// least one query, as bits of the group's cell bitmap. The group's queries
+// are neighbours in the sorted order (one or a few fine cells), so a ball
+// around them (centre: their mean, radius: the farthest of them) first
+// excludes, for all queries at once, every cell with
+// |g - c_f| - r_g - r_f > max kth; only the remaining cells are tested per
+// query. Both tests carry the same rounding margins, the group test twice.
 __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ ord,
                               const uint32_t* __restrict__ perm, const float* __restrict__ d2k, uint32_t k1,
                               const unsigned long long* __restrict__ gmask, const uint32_t* __restrict__ gown,
@@ -1384,14 +1364,61 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
     for (int j = 0; j < 64; ++j) x[j] = (uint32_t)j < d ? Xs[sq * d + j] : 0.0f;
     const float kd2 = d2k[(uint64_t)perm[sq] * k1 + (k1 - 1)];
     const float kth = isfinite(kd2) ? sqrtf(kd2) * (1.0f + 1e-5f) + eps : INFINITY;
-    extern __shared__ unsigned s_bits[];  // cwords
-    for (uint32_t w = threadIdx.x; w < cwords; w += blockDim.x) s_bits[w] = 0u;
+    extern __shared__ unsigned s_bits[];  // cwords: the result, then cwords: cells the group ball keeps
+    unsigned* s_maybe = s_bits + cwords;
+    __shared__ float s_c[64];
+    __shared__ unsigned s_r, s_k;  // group radius and max kth (ordered bits)
+    for (uint32_t w = threadIdx.x; w < cwords; w += blockDim.x) s_bits[w] = s_maybe[w] = 0u;
+    for (uint32_t j = threadIdx.x; j < 64; j += blockDim.x) s_c[j] = 0.0f;
+    if (threadIdx.x == 0) s_r = s_k = 0u;
     __syncthreads();
+    // group centre: the mean of its queries, summed in a fixed order (a warp
+    // per dimension, lanes over the queries, a fixed tree)
+    const uint64_t g0 = g * (QT * TILE), gcount = n - g0 < (uint64_t)(QT * TILE) ? n - g0 : (uint64_t)(QT * TILE);
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t j = wid; j < d; j += nw) {
+        float acc = 0.0f;
+        for (uint64_t t = lane; t < gcount; t += 32) acc += Xs[(uint64_t)ord[g0 + t] * d + j];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        if (lane == 0) s_c[j] = acc / (float)gcount;
+    }
+    __syncthreads();
+    if (ok) {
+        float dq = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 64; ++j)
+            if ((uint32_t)j < d) {
+                const float df = x[j] - s_c[j];
+                dq = __fmaf_rn(df, df, dq);
+            }
+        atomicMax(&s_r, ord32(sqrtf(dq)));
+        atomicMax(&s_k, ord32(kth));
+    }
+    __syncthreads();
+    const float rg = unord32(s_r) * (1.0f + 1e-5f), kmax = unord32(s_k);
     const uint32_t a0 = gown[2 * g], a1 = gown[2 * g + 1];
+    // the group-ball test, a thread per cell
     for (uint32_t b = 0; b < K; ++b) {
         const bool cand = (b >= a0 && b <= a1) || ((gmask[g * words + b / 64] >> (b % 64)) & 1ull);
         if (!cand) continue;  // uniform over the block
-        for (uint32_t f = fbase[b]; f < fbase[b + 1]; ++f) {
+        for (uint32_t f = fbase[b] + threadIdx.x; f < fbase[b + 1]; f += blockDim.x) {
+            const float* m = fcent + (uint64_t)f * d;
+            float dc = 0.0f;
+            for (uint32_t j = 0; j < d; ++j) {
+                const float df = s_c[j] - m[j];
+                dc = __fmaf_rn(df, df, dc);
+            }
+            if (!(sqrtf(dc) * (1.0f - 1e-5f) - rg - unord32(crad[f]) - 2.0f * eps > kmax))
+                atomicOr(s_maybe + f / 32, 1u << (f % 32));
+        }
+    }
+    __syncthreads();
+    // the per-query test on the cells the group ball kept
+    for (uint32_t wd = 0; wd < cwords; ++wd) {
+        unsigned bits = s_maybe[wd];  // uniform over the block
+        while (bits) {
+            const uint32_t f = wd * 32 + (uint32_t)(__ffs(bits) - 1);
+            bits &= bits - 1;
             const float* m = fcent + (uint64_t)f * d;
             float dc = 0.0f;
 #pragma unroll
@@ -1402,11 +1429,70 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
                 }
             const bool need = ok && sqrtf(dc) * (1.0f - 1e-5f) - unord32(crad[f]) - eps <= kth;
             // one shared OR per warp that needs the cell (most cells are needed by all or none)
-            if (__ballot_sync(0xFFFFFFFFu, need) && (threadIdx.x & 31) == 0) atomicOr(s_bits + f / 32, 1u << (f % 32));
+            if (__ballot_sync(0xFFFFFFFFu, need) && lane == 0) atomicOr(s_bits + f / 32, 1u << (f % 32));
         }
     }
     __syncthreads();
     for (uint32_t w = threadIdx.x; w < cwords; w += blockDim.x) gcell[g * cwords + w] = s_bits[w];
+}
+
+// The pass-2 tile ranges of every group (a thread per group) from its cell
+// bitmap: each run of consecutive set cells is a run of adjacent points
+// [cstart[first], cstart[last + 1]); those become tile ranges, merged where
+// they touch or overlap (the host helper tiles_of does the same for pass 1).
+// Without rptr it counts the ranges into cnt; with it, it writes them from
+// rptr[g] and adds the group's tile count to *tiles.
+__global__ void k_group_ranges(const unsigned* __restrict__ gcell, uint32_t cwords, uint32_t F,
+                               const uint64_t* __restrict__ cstart, uint64_t ngroups,
+                               const uint32_t* __restrict__ rptr, uint32_t* cnt, uint2* rngs,
+                               unsigned long long* tiles) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < ngroups;
+         g += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned* bits = gcell + g * cwords;
+        uint64_t cur_b = 0, cur_e = 0, sum = 0;
+        bool open = false;
+        uint32_t k = 0, out = rptr ? rptr[g] : 0;
+        auto emit = [&](uint64_t b, uint64_t e) {
+            if (rptr) rngs[out + k] = make_uint2((uint32_t)b, (uint32_t)(e - b));
+            sum += e - b;
+            ++k;
+        };
+        uint32_t f = 0;
+        while (f < F) {
+            const unsigned m = bits[f / 32] >> (f % 32);
+            if (m == 0) {  // no set bit left in this word
+                f = (f / 32 + 1) * 32;
+                continue;
+            }
+            f += (uint32_t)(__ffs(m) - 1);
+            const uint32_t run0 = f;
+            while (f < F) {
+                const uint32_t avail = 32 - f % 32;
+                const unsigned zeros = ~bits[f / 32] >> (f % 32);  // first clear bit at or after f
+                if (zeros == 0) {
+                    f += avail;
+                    continue;
+                }
+                f += (uint32_t)(__ffs(zeros) - 1);
+                break;
+            }
+            const uint32_t run1 = f < F ? f : F;
+            const uint64_t pb = cstart[run0], pe = cstart[run1];
+            if (pe <= pb) continue;
+            const uint64_t tb = pb / TILE, te = (pe + TILE - 1) / TILE;
+            if (open && tb <= cur_e) {
+                cur_e = cur_e > te ? cur_e : te;
+            } else {
+                if (open) emit(cur_b, cur_e);
+                cur_b = tb;
+                cur_e = te;
+                open = true;
+            }
+        }
+        if (open) emit(cur_b, cur_e);
+        if (rptr) atomicAdd(tiles, (unsigned long long)sum);
+        else cnt[g] = k;
+    }
 }
 
 // The pass-2 score bound of every query (row r of the pass-2 order is the
@@ -1542,31 +1628,6 @@ void launch_operands(Ctx& c, const TcOperands& op, uint64_t n, float* cscore, ui
     if (op.kind == 2) launch_tc<32, true>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else if (op.kind == 0) launch_tc<32, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else launch_tc<64, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
-}
-
-// The runs [first, last) of consecutive set bits among bits 0 .. nbits-1.
-std::vector<std::pair<uint32_t, uint32_t>> bit_runs(const unsigned* bits, uint32_t nbits) {
-    std::vector<std::pair<uint32_t, uint32_t>> out;
-    uint32_t f = 0;
-    while (f < nbits) {
-        const unsigned m = bits[f / 32] >> (f % 32);
-        if (m == 0) {  // no set bit left in this word
-            f = (f / 32 + 1) * 32;
-            continue;
-        }
-        f += (uint32_t)__builtin_ctz(m);
-        const uint32_t run0 = f;
-        while (f < nbits) {
-            const uint32_t avail = 32 - f % 32;                    // bits left in this word
-            const unsigned zeros = ~bits[f / 32] >> (f % 32);       // first clear bit at or after f
-            const uint32_t len = zeros ? (uint32_t)__builtin_ctz(zeros) : avail;
-            f += len;
-            if (len < avail) break;
-        }
-        if (f > nbits) f = nbits;
-        out.emplace_back(run0, f);
-    }
-    return out;
 }
 
 // Merged tile ranges of the point ranges [b, e) given in ascending order of b.
@@ -1821,6 +1882,15 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
         c.launches++;
         sync(c);  // the host arrays above must outlive the copies
     };
+    // the same with tile lists already on the device
+    auto run_pass_dev = [&](const TcOperands& o, const uint32_t* ord, const uint32_t* d_rptr, const uint2* d_rngs,
+                            uint32_t* out_idx, float* out_d2, const float* qcap) {
+        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr, d_rngs, qcap});
+        k_knn_rerank_sorted<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(Xs.get(), n, d, k, ord, perm.get(),
+                                                                        cidx.get(), out_idx, out_d2);
+        SC_LAUNCH_CHECK();
+        c.launches++;
+    };
     // 6. pass 1: every query group against its own clusters, starting at its own
     // tile (the nearest points come first, so the rows' thresholds tighten early
     // and fewer later scores take the insertion path; pass 1 only yields the
@@ -1882,15 +1952,13 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     const uint32_t cwords = (F + 31) / 32;
     DBuf<unsigned> gcell(c, ngroups * cwords);
     zero(c, gcell.get(), ngroups * cwords);
-    SC_CUDA(cudaFuncSetAttribute(k_group_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(cwords * 4)));
-    k_group_cells<<<(unsigned)ngroups, QT * TILE, cwords * 4, c.stream>>>(Xs.get(), n, d, ord.get(), perm.get(), d21.get(), k1,
+    SC_CUDA(cudaFuncSetAttribute(k_group_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(cwords * 8)));
+    k_group_cells<<<(unsigned)ngroups, QT * TILE, cwords * 8, c.stream>>>(Xs.get(), n, d, ord.get(), perm.get(), d21.get(), k1,
                                                                 gmask.get(), gown.get(), words, K, d_fbase.get(),
                                                                 fcent.get(), crad.get(), eps, cwords, gcell.get());
     SC_LAUNCH_CHECK();
     c.launches++;
     tm.mark();  // 8: group cells done
-    std::vector<unsigned> h_cell(ngroups * cwords);
-    d2h(c, h_cell.data(), gcell.get(), ngroups * cwords);
     // the query operand in pass-2 order
     TcOperands op2;
     {
@@ -1919,20 +1987,27 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     idx1.release();
     d21.release();
     mask.release();
-    // 8. pass 2: every cell a query of the group cannot exclude (cells in point order)
-    rngs.clear();
-    uint64_t tiles2 = 0;
-    std::vector<std::pair<uint64_t, uint64_t>> pts;
-    for (uint64_t g = 0; g < ngroups; ++g) {
-        pts.clear();
-        const unsigned* bits = h_cell.data() + g * cwords;
-        // runs of consecutive set bits are runs of adjacent cells: one point range each
-        for (const auto& run : bit_runs(bits, F)) pts.emplace_back(cstart[run.first], cstart[run.second]);
-        tiles_of(pts, rngs, tiles2);
-        rptr[g + 1] = (uint32_t)rngs.size();
-    }
+    // 8. pass 2: every cell a query of the group cannot exclude (cells in point
+    // order), the tile lists built on the device from the cell bitmaps
+    DBuf<uint64_t> d_cstart(c, F + 1);
+    h2d(c, d_cstart.get(), cstart.data(), F + 1);
+    DBuf<uint32_t> gcnt(c, ngroups + 1), d_rptr2(c, ngroups + 1);
+    zero(c, gcnt.get(), ngroups + 1);
+    DBuf<unsigned long long> d_tiles2(c, 1);
+    zero(c, d_tiles2.get(), 1);
+    k_group_ranges<<<grid_for(ngroups, 128), 128, 0, c.stream>>>(gcell.get(), cwords, F, d_cstart.get(), ngroups,
+                                                                 nullptr, gcnt.get(), nullptr, nullptr);
+    exclusive_sum(c, gcnt.get(), d_rptr2.get(), ngroups + 1);
+    const uint32_t nranges = to_host(c, d_rptr2.get() + ngroups);
+    DBuf<uint2> d_rngs2(c, std::max<uint32_t>(nranges, 1));
+    k_group_ranges<<<grid_for(ngroups, 128), 128, 0, c.stream>>>(gcell.get(), cwords, F, d_cstart.get(), ngroups,
+                                                                 d_rptr2.get(), nullptr, d_rngs2.get(),
+                                                                 d_tiles2.get());
+    SC_LAUNCH_CHECK();
+    c.launches += 2;
+    const uint64_t tiles2 = to_host(c, d_tiles2.get());
     tm.mark();  // 10: lists built
-    run_pass(op2, ord.get(), rptr, rngs, idx, d2, qcap.get());
+    run_pass_dev(op2, ord.get(), d_rptr2.get(), d_rngs2.get(), idx, d2, qcap.get());
     tm.mark();  // 11: pass 2
     c.knn_stats.ms_cluster = tm.ms(0, 3);
     c.knn_stats.ms_pass1 = tm.ms(3, 4);
