@@ -974,16 +974,22 @@ __global__ void k_km_assign(const float* __restrict__ X, uint64_t n, uint32_t d,
     for (uint32_t i = threadIdx.x; i < K * d; i += blockDim.x) s_cent[i] = cent[i];
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-        const float* x = X + i * d;
+        // the point in registers (d <= 62): the centroid loop then reads only
+        // shared memory, every lane the same word (a broadcast)
+        float x[64];
+#pragma unroll
+        for (int j = 0; j < 64; ++j) x[j] = (uint32_t)j < d ? X[i * d + j] : 0.0f;
         float best = INFINITY;
         uint32_t bc = 0;
         for (uint32_t c = 0; c < K; ++c) {
             const float* m = s_cent + c * d;
             float acc = 0.0f;
-            for (uint32_t j = 0; j < d; ++j) {
-                const float df = __fsub_rn(x[j], m[j]);
-                acc = __fmaf_rn(df, df, acc);
-            }
+#pragma unroll
+            for (int j = 0; j < 64; ++j)
+                if ((uint32_t)j < d) {
+                    const float df = __fsub_rn(x[j], m[j]);
+                    acc = __fmaf_rn(df, df, acc);
+                }
             if (acc < best) {
                 best = acc;
                 bc = c;
