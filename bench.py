@@ -935,6 +935,13 @@ def main():
                                          "1M-point run (profiles/local_move_dram_knn10_gmm1000000x30.md) x "
                                          "this run's algorithmic bytes",
                          "peak_kind": peak_kind},
+            "roofline_phases": {
+                ph: {"achieved": stats[f"alg_bytes_{key}"] / (stats[f"ms_{ms}"] / 1e3) / 1e9 if stats[f"ms_{ms}"] else None,
+                     "frac": (stats[f"alg_bytes_{key}"] / (stats[f"ms_{ms}"] / 1e3) / 1e9 / hbm
+                              if stats[f"ms_{ms}"] and hbm else None),
+                     "algorithmic_bytes": stats[f"alg_bytes_{key}"], "ms": stats[f"ms_{ms}"], "unit": "GB/s",
+                     "peak": hbm, "peak_kind": peak_kind}
+                for ph, key, ms in (("refine", "refine", "refine"), ("aggregate", "aggregate", "aggregate"))},
             "clocks": clk,
             "e2e": {"value": world * m / e2e_s, "unit": "edges/s", "s_per_run": e2e_s,
                     "graph_upload_s": graph_s / e2e_steps, "leiden_call_s": leiden_s / e2e_steps,
