@@ -1505,12 +1505,12 @@ __global__ void k_group_ranges(const unsigned* __restrict__ gcell, uint32_t cwor
 // sorted query ord[r]). Scores are |y|^2 - 2 x.y from BF16 operands with FP32
 // accumulation. A point that can reach the final list has an FP32 distance of
 // at most d21 (the query's (k+1)-th FP32 distance from pass 1), so |y| <= Y =
-// |x| + sqrt(d21), and its score lies within 2^-5 |x| Y + 2^-12 Y^2 of
-// d^2 - |x|^2: the BF16 roundings of x and y (unit roundoff 2^-8 each, so
-// 2 x.y moves by at most about 2^-6 |x| |y| by Cauchy-Schwarz over the
-// products), the two-term norm and up to 64 FP32 accumulations, with a factor
-// of two to spare. 2^-16 (d21 + |x|^2) covers the FP32 distances and norm; the
-// sum is rounded up.
+// |x| + sqrt(d21), and its score lies within 2^-6 (1 + 2^-6) |x| Y + 2^-14 Y^2
+// of d^2 - |x|^2. The terms: the BF16 roundings of x and y (unit roundoff
+// u = 2^-8 each) move 2 x.y by at most (4u + 2u^2) |x| |y| (Cauchy-Schwarz
+// over the products); the FP32 norm split into two BF16 terms and up to 64
+// FP32 accumulations add under 2^-15 (|x| |y| + |y|^2). 2^-16 (d21 + |x|^2)
+// covers the FP32 distances and norm; the sum is rounded up.
 __global__ void k_pass2_cap(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ ord,
                             const uint32_t* __restrict__ perm, const float* __restrict__ d21, uint32_t k1,
                             float* __restrict__ cap) {
@@ -1525,7 +1525,8 @@ __global__ void k_pass2_cap(const float* __restrict__ Xs, uint64_t n, uint32_t d
             continue;
         }
         const double nx = sqrt((double)nx2), Y = nx + sqrt((double)dk);
-        const double margin = ldexp(nx * Y, -5) + ldexp(Y * Y, -12) + ldexp((double)dk + (double)nx2, -16);
+        const double margin = ldexp(nx * Y, -6) * (1.0 + 0x1.0p-6) + ldexp(Y * Y, -14) +
+                              ldexp((double)dk + (double)nx2, -16);
         cap[r] = __double2float_ru((double)dk - (double)nx2 + 1.01 * margin);
     }
 }
