@@ -204,3 +204,25 @@ def test_graph_without_edges():
     assert loss == 0.0
     lab, k = m.propose(g, 1.0)
     assert list(lab) == [0, 1, 2, 3, 4] and k == 5
+
+
+def test_embedding_rows_must_match_nodes_and_features_follow_it():
+    """An embedding needs one row per node; replacing it changes only the
+    embedding feature (the graph's cached structural features are rebuilt)."""
+    import sc_gpu
+    from sc_gpu.learned import EdgeMlp
+    g, _ = _planted(600, 6)
+    n = g.node_count()
+    rng = np.random.default_rng(9)
+    with pytest.raises(sc_gpu.ClusteringError) as e:
+        g.set_embedding(rng.normal(size=(n - 1, 4)).astype(np.float32))
+    assert "embedding" in str(e.value)
+    m = EdgeMlp(seed=2)
+    f0, ei0, ej0 = m.features(g, 1.0)
+    g.set_embedding(rng.normal(size=(n, 4)).astype(np.float32))
+    f1, ei1, ej1 = m.features(g, 1.0)
+    assert np.array_equal(ei0, ei1) and np.array_equal(ej0, ej1)
+    assert np.array_equal(f0[:, :14], f1[:, :14])
+    assert not np.array_equal(f0[:, 14], f1[:, 14])
+    f2, _, _ = m.features(g, 1.0)  # the cached values again
+    assert np.array_equal(f1, f2)
