@@ -226,7 +226,9 @@ void sc_graph_destroy(sc_graph* g);
  * row-major host memory, n = node count) for the learned warm start's
  * features: the library keeps its projection to 16 components per node (a
  * fixed sign matrix), replacing any earlier one. The reference's Leiden takes
- * no embedding; its kNN builder (src/neighborhood/mod.rs) starts from one. */
+ * no embedding; its kNN builder (src/neighborhood/mod.rs) starts from one.
+ * This is the one call that changes a graph: make it before the graph is
+ * shared, not while another context uses the graph. */
 sc_status sc_graph_set_embedding(sc_ctx* ctx, sc_graph* g, const float* X, uint64_t n, uint64_t d);
 
 /* node_count, stored entries, edge_count, total_weight, has_self_loops
