@@ -1442,10 +1442,86 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
     for (uint32_t w = threadIdx.x; w < cwords; w += blockDim.x) gcell[g * cwords + w] = s_bits[w];
 }
 
+// Pass 1's tile order, a block per query group: the group's own-cluster tiles
+// [tb[g], te[g]) sorted by the distance from the group's centre (the mean of
+// its queries) to the centroid of the cell holding each tile's first point,
+// nearest first, ties by tile id; each tile one range of length 1 at
+// out[rptr[g] ..]. Nearest points first tighten the rows' thresholds within
+// the first tiles. More tiles than ORDER_CAP keep ascending order from the
+// group's own tile.
+constexpr int ORDER_CAP = 2048;
+__global__ void k_order_tiles(const float* __restrict__ Xs, uint64_t n, uint32_t d, const uint32_t* __restrict__ tb,
+                              const uint32_t* __restrict__ te, const uint32_t* __restrict__ tile_cell,
+                              const float* __restrict__ fcent, const uint32_t* __restrict__ rptr, uint2* out) {
+    __shared__ float s_c[64];
+    __shared__ float s_key[ORDER_CAP];
+    __shared__ uint32_t s_tile[ORDER_CAP];
+    const uint64_t g = blockIdx.x;
+    const uint64_t g0 = g * (QT * TILE), gcount = n - g0 < (uint64_t)(QT * TILE) ? n - g0 : (uint64_t)(QT * TILE);
+    const uint32_t t0 = tb[g], t1 = te[g], cnt = t1 - t0;
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (cnt > (uint32_t)ORDER_CAP) {  // ascending from the group's own tile, wrapping round
+        const uint32_t own = (uint32_t)(g0 / TILE);
+        const uint32_t first = own >= t0 && own < t1 ? own : t0;
+        for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) {
+            uint32_t t = first + k;
+            if (t >= t1) t -= cnt;
+            out[rptr[g] + k] = make_uint2(t, 1u);
+        }
+        return;
+    }
+    for (uint32_t j = wid; j < d; j += nw) {
+        float acc = 0.0f;
+        for (uint64_t t = lane; t < gcount; t += 32) acc += Xs[(g0 + t) * d + j];
+        for (int o = 16; o; o >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFu, acc, o);
+        if (lane == 0) s_c[j] = acc / (float)gcount;
+    }
+    __syncthreads();
+    uint32_t P = 1;
+    while (P < cnt) P <<= 1;
+    for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) {
+        float key = INFINITY;
+        uint32_t t = 0xFFFFFFFFu;
+        if (k < cnt) {
+            t = t0 + k;
+            const float* m = fcent + (uint64_t)tile_cell[t] * d;
+            key = 0.0f;
+            for (uint32_t j = 0; j < d; ++j) {
+                const float df = s_c[j] - m[j];
+                key = __fmaf_rn(df, df, key);
+            }
+        }
+        s_key[k] = key;
+        s_tile[k] = t;
+    }
+    __syncthreads();
+    // bitonic sort of (key, tile) ascending
+    for (uint32_t size = 2; size <= P; size <<= 1)
+        for (uint32_t stride = size >> 1; stride > 0; stride >>= 1) {
+            for (uint32_t k = threadIdx.x; k < P; k += blockDim.x) {
+                const uint32_t o = k ^ stride;
+                if (o > k) {
+                    const bool up = (k & size) == 0;
+                    const float ka = s_key[k], kb = s_key[o];
+                    const uint32_t ta = s_tile[k], tb2 = s_tile[o];
+                    const bool gt = ka > kb || (ka == kb && ta > tb2);
+                    if (gt == up) {
+                        s_key[k] = kb;
+                        s_key[o] = ka;
+                        s_tile[k] = tb2;
+                        s_tile[o] = ta;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) out[rptr[g] + k] = make_uint2(s_tile[k], 1u);
+}
+
 // The pass-2 tile ranges of every group (a thread per group) from its cell
 // bitmap: each run of consecutive set cells is a run of adjacent points
 // [cstart[first], cstart[last + 1]); those become tile ranges, merged where
-// they touch or overlap (the host helper tiles_of does the same for pass 1).
+// they touch or overlap.
 // Without rptr it counts the ranges into cnt; with it, it writes them from
 // rptr[g] and adds the group's tile count to *tiles.
 __global__ void k_group_ranges(const unsigned* __restrict__ gcell, uint32_t cwords, uint32_t F,
@@ -1635,27 +1711,6 @@ void launch_operands(Ctx& c, const TcOperands& op, uint64_t n, float* cscore, ui
     if (op.kind == 2) launch_tc<32, true>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else if (op.kind == 0) launch_tc<32, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else launch_tc<64, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
-}
-
-// Merged tile ranges of the point ranges [b, e) given in ascending order of b.
-void tiles_of(const std::vector<std::pair<uint64_t, uint64_t>>& pts, std::vector<uint2>& out, uint64_t& total) {
-    const size_t first = out.size();
-    uint64_t cur_b = 0, cur_e = 0;
-    bool open = false;
-    for (const auto& pe : pts) {
-        if (pe.second <= pe.first) continue;
-        const uint64_t tb = pe.first / TILE, te = (pe.second + TILE - 1) / TILE;
-        if (open && tb <= cur_e) {
-            cur_e = std::max(cur_e, te);
-        } else {
-            if (open) out.push_back(make_uint2((uint32_t)cur_b, (uint32_t)(cur_e - cur_b)));
-            cur_b = tb;
-            cur_e = te;
-            open = true;
-        }
-    }
-    if (open) out.push_back(make_uint2((uint32_t)cur_b, (uint32_t)(cur_e - cur_b)));
-    for (size_t i = first; i < out.size(); ++i) total += out[i].y;
 }
 
 // The exact k+1 nearest points of every point by the pruned search (see
@@ -1876,20 +1931,7 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     DBuf<float> cscore(c, n * RTOTAL);
     DBuf<uint32_t> cidx(c, n * RTOTAL);
     // queries in the order `ord` (nullable: the sorted order), operand `o`
-    auto run_pass = [&](const TcOperands& o, const uint32_t* ord, const std::vector<uint32_t>& rptr,
-                        const std::vector<uint2>& rngs, uint32_t* out_idx, float* out_d2, const float* qcap) {
-        DBuf<uint32_t> d_rptr(c, rptr.size());
-        DBuf<uint2> d_rngs(c, std::max<size_t>(rngs.size(), 1));
-        h2d(c, d_rptr.get(), rptr.data(), rptr.size());
-        h2d(c, d_rngs.get(), rngs.data(), rngs.size());
-        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr.get(), d_rngs.get(), qcap});
-        k_knn_rerank_sorted<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(Xs.get(), n, d, k, ord, perm.get(),
-                                                                        cidx.get(), out_idx, out_d2);
-        SC_LAUNCH_CHECK();
-        c.launches++;
-        sync(c);  // the host arrays above must outlive the copies
-    };
-    // the same with tile lists already on the device
+    // a scan and its re-rank, the tile lists on the device
     auto run_pass_dev = [&](const TcOperands& o, const uint32_t* ord, const uint32_t* d_rptr, const uint2* d_rngs,
                             uint32_t* out_idx, float* out_d2, const float* qcap) {
         launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr, d_rngs, qcap});
@@ -1898,29 +1940,43 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
         SC_LAUNCH_CHECK();
         c.launches++;
     };
-    // 6. pass 1: every query group against its own clusters, starting at its own
-    // tile (the nearest points come first, so the rows' thresholds tighten early
-    // and fewer later scores take the insertion path; pass 1 only yields the
-    // bounds of pass 2, which scans in point order)
+    // 6. pass 1: every query group against its own clusters, nearest cells first
+    // (k_order_tiles: the rows' thresholds tighten within the first tiles, so
+    // fewer later scores take the insertion path; pass 1 only yields the
+    // bounds of pass 2)
     std::vector<uint32_t> rptr(ngroups + 1, 0);
-    std::vector<uint2> rngs;
     uint64_t tiles1 = 0;
-    for (uint64_t g = 0; g < ngroups; ++g) {
-        std::vector<std::pair<uint64_t, uint64_t>> pts;
-        own(g, pts);
-        const size_t first = rngs.size();
-        tiles_of(pts, rngs, tiles1);
-        const uint32_t gt = (uint32_t)(g * QT * TILE / TILE);
-        if (rngs.size() == first + 1 && gt > rngs[first].x && gt < rngs[first].x + rngs[first].y) {
-            const uint2 r0 = rngs[first];
-            rngs[first] = make_uint2(gt, r0.x + r0.y - gt);
-            rngs.push_back(make_uint2(r0.x, gt - r0.x));
-        }
-        rptr[g + 1] = (uint32_t)rngs.size();
-    }
     DBuf<uint32_t> idx1(c, n * k1);
     DBuf<float> d21(c, n * k1);
-    run_pass(op, nullptr, rptr, rngs, idx1.get(), d21.get(), nullptr);
+    {
+        std::vector<uint32_t> h_tb(ngroups), h_te(ngroups);
+        std::vector<std::pair<uint64_t, uint64_t>> pts;
+        for (uint64_t g = 0; g < ngroups; ++g) {
+            pts.clear();
+            own(g, pts);
+            h_tb[g] = (uint32_t)(pts[0].first / TILE);
+            h_te[g] = (uint32_t)((pts[0].second + TILE - 1) / TILE);
+            rptr[g + 1] = rptr[g] + (h_te[g] - h_tb[g]);
+        }
+        tiles1 = rptr[ngroups];
+        std::vector<uint32_t> tile_cell(ntiles);
+        for (uint64_t t = 0, f = 0; t < ntiles; ++t) {
+            while (f + 1 < F && cstart[f + 1] <= t * TILE) ++f;
+            tile_cell[t] = (uint32_t)f;
+        }
+        DBuf<uint32_t> d_tb(c, ngroups), d_te(c, ngroups), d_tc(c, ntiles), d_rp(c, ngroups + 1);
+        DBuf<uint2> d_rg(c, std::max<uint64_t>(tiles1, 1));
+        h2d(c, d_tb.get(), h_tb.data(), ngroups);
+        h2d(c, d_te.get(), h_te.data(), ngroups);
+        h2d(c, d_tc.get(), tile_cell.data(), ntiles);
+        h2d(c, d_rp.get(), rptr.data(), ngroups + 1);
+        k_order_tiles<<<(unsigned)ngroups, 256, 0, c.stream>>>(Xs.get(), n, d, d_tb.get(), d_te.get(), d_tc.get(),
+                                                               fcent.get(), d_rp.get(), d_rg.get());
+        SC_LAUNCH_CHECK();
+        c.launches++;
+        run_pass_dev(op, nullptr, d_rp.get(), d_rg.get(), idx1.get(), d21.get(), nullptr);
+        sync(c);  // the host arrays above must outlive the copies
+    }
     tm.mark();  // 4: pass 1
     // 7. the clusters every group still needs
     const uint32_t words = (K + 63) / 64;
