@@ -178,6 +178,10 @@ def run_sweep_sharded(device_index, rank, world, dist, n_points=SWEEP_POINTS, n_
     timing = {}
 
     def run_local(ids, local_warm):
+        timing["instances"] = len(ids)
+        if not ids:  # more ranks than chains: this rank idles
+            timing["s"] = 0.0
+            return []
         torch.cuda.synchronize()
         t = time.perf_counter()
         out = sc_gpu.leiden_batch([g] * len(ids), [configs[i] for i in ids], local_warm, n_streams)
