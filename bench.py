@@ -888,10 +888,16 @@ def main():
     value = world * m / (ms_step / 1e3)
     q = sc_gpu.modularity(g, c.labels())
 
-    # e2e through the C ABI with host buffers
+    # e2e through the C ABI with host buffers. One untimed step first, as for
+    # the device-resident loop: the first graph uploaded beside the resident
+    # one grows the library's graph pool (a one-time cost per process, measured
+    # 0.02-0.3 s on different boxes), which every later upload reuses.
+    g2 = sc_gpu.CSRNetwork.from_csr_parts(ptr, nbr, w, device=local_rank)
+    sc_gpu.leiden(g2, cfg)
+    del g2
     torch.cuda.synchronize()
     t = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 2))
+    e2e_steps = max(1, min(args.steps, 3))
     graph_s = leiden_s = 0.0
     e2e_each = []
     for _ in range(e2e_steps):
