@@ -163,15 +163,28 @@ def run_sweep_sharded(device_index, rank, world, dist, n_points=SWEEP_POINTS, n_
     """The sweep's warm-started chains dealt across the ranks by cost (one
     chain per seed: parallel.run_sharded), each rank running its share on its
     own GPU; the only collective is one all-gather of the instances'
-    modularities after the runs. Every rank builds the same kNN graph. Timed
-    from a barrier to the end of the local runs, max over ranks."""
+    modularities after the runs. The kNN graph is built split by query rows
+    (parallel.knn_sharded), timed on its own. Both timed from a barrier, max
+    over ranks."""
     import torch
     import sc_gpu
     from sc_gpu import parallel, synth
     X, _ = synth.gaussian_mixture(n_points, SWEEP_DIMS, SWEEP_COMPONENTS, SWEEP_SEED, sigma=(0.7, 1.5))
-    r = sc_gpu.knn_gaussian(X, SWEEP_K, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    # the kNN graph split by query rows (parallel.knn_sharded): each rank
+    # searches its block against all points, one all-gather of the lists, then
+    # every rank builds the connectivities (the single build's bits)
+    sc_gpu.knn_search(X[:4096], SWEEP_K, 0, 4096, device=device_index)  # warm-up
+    dist.barrier()
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    idx, d2 = parallel.knn_sharded(lambda b, e: sc_gpu.knn_search(X, SWEEP_K, b, e, device=device_index),
+                                   n_points, rank, world)
+    r = sc_gpu.knn_connectivities(idx, d2, sigma=sc_gpu.SIGMA_KTH, sym=sc_gpu.SYM_UNION, device=device_index)
+    torch.cuda.synchronize()
+    tk = torch.tensor([time.perf_counter() - t], dtype=torch.float64, device=f"cuda:{device_index}")
+    dist.all_reduce(tk, op=dist.ReduceOp.MAX)
     g = sc_gpu.CSRNetwork.from_csr_parts(r.conn_ptrs, r.conn_nbrs, r.conn_w, device=device_index)
-    del X, r
+    del X, r, idx, d2
     res = np.geomspace(0.1, 3.0, SWEEP_RESOLUTIONS)
     configs, warm, keys = sc_gpu.sweep_plan(res, SWEEP_SEEDS, sc_gpu.Rb, True, None, 8, warm_passes)
     cost = [3.0 if w < 0 else 1.0 for w in warm]  # a singleton start costs about three warm runs
@@ -196,6 +209,9 @@ def run_sweep_sharded(device_index, rank, world, dist, n_points=SWEEP_POINTS, n_
     dist.all_reduce(tt, op=dist.ReduceOp.MAX)
     return {"workload": f"sweep_rb{SWEEP_RESOLUTIONS}x{len(SWEEP_SEEDS)}_knn{SWEEP_K}_gmm{n_points}x{SWEEP_DIMS}",
             "ranks": world, "s": float(tt.item()), "instances": len(configs),
+            "knn_sharded_s": float(tk.item()),
+            "knn_how": "parallel.knn_sharded: row blocks searched per rank (full scan), one all-gather of the "
+                       "k+1 lists, connectivities on every rank",
             "instances_rank0": timing["instances"], "units": "one warm chain per seed (its 8 pieces concurrent on the rank's streams), dealt by cost",
             "q_min": float(min(qs)), "q_max": float(max(qs)),
             "how": "parallel.run_sharded: no collective inside a run, one all-gather of modularities"}
