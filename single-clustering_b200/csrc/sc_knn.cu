@@ -183,12 +183,13 @@ struct Worst {
 // processed by the whole warp, row by row; denser chunks by each lane alone.
 constexpr int COOP_ROWS = 8;
 
+template <int R>
 __device__ __noinline__ Worst cand_insert(float* cs, uint32_t* ci, int qrow, int slot, float v, uint32_t idx) {
     constexpr int S = QT * HALVES * TILE;
     cs[slot * S + qrow] = v;
     ci[slot * S + qrow] = idx;
     Worst w{-INFINITY, 0};
-    for (int s = 0; s < RCAND; ++s) {
+    for (int s = 0; s < R; ++s) {
         const float x = cs[s * S + qrow];
         if (x > w.thr) {
             w.thr = x;
@@ -304,7 +305,7 @@ __global__ void k_knn_prep_f8(const float* __restrict__ X, uint64_t n, uint32_t 
 }
 
 // ------------------------------------------------------------ tensor-core candidate search
-template <int KA>
+template <int KA, int R = RCAND>
 struct KnnSmem {
     static constexpr int STAGES = stages_for<KA>();
     static constexpr uint32_t TILE_BYTES = TILE * KA * 2;
@@ -312,8 +313,8 @@ struct KnnSmem {
     static constexpr uint32_t A_OFF = 0;
     static constexpr uint32_t B_OFF = A_OFF + QT * TILE_BYTES;
     static constexpr uint32_t C_OFF = B_OFF + STAGES * TILE_BYTES;               // candidate scores
-    static constexpr uint32_t I_OFF = C_OFF + RCAND * SLOTS * 4;                 // candidate ids
-    static constexpr uint32_t BAR_OFF = I_OFF + RCAND * SLOTS * 4;
+    static constexpr uint32_t I_OFF = C_OFF + R * SLOTS * 4;                     // candidate ids
+    static constexpr uint32_t BAR_OFF = I_OFF + R * SLOTS * 4;
     static constexpr uint32_t NBAR = 2 * STAGES + 4 + 2;
     static constexpr uint32_t MISC_OFF = BAR_OFF + NBAR * 8;
     static constexpr uint32_t ROW_OFF = MISC_OFF + 64;                       // one staged row chunk per epilogue warp
@@ -350,13 +351,15 @@ struct TileWalk {
 // qcap (nullable): per query, a score no kept candidate reaches (a proven
 // bound of the pruned search's second pass); the rows start from it instead
 // of +inf, so far points never enter the insertion path.
-template <int KA, bool F8>
+// R: candidates kept per (query, half), RCAND or fewer (a pass that only
+// bounds the (k+1)-th distance); the slots past R are written empty.
+template <int KA, bool F8, int R = RCAND>
 __global__ void __launch_bounds__(KNN_THREADS, 1)
     k_knn_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB, uint32_t n,
              uint32_t nq, float* __restrict__ cand_score, uint32_t* __restrict__ cand_idx, uint32_t* status,
              uint32_t lim, uint32_t hold_tiles, const uint32_t* __restrict__ rptr, const uint2* __restrict__ rngs,
              const float* __restrict__ qcap) {
-    using L = KnnSmem<KA>;
+    using L = KnnSmem<KA, R>;
     extern __shared__ __align__(1024) unsigned char raw[];
     unsigned char* smem = (unsigned char*)(((uintptr_t)raw + 1023) & ~(uintptr_t)1023);
     unsigned char* sA = smem + L::A_OFF;
@@ -516,7 +519,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             const float capv = (qcap && qrow < nq) ? qcap[qrow] : INFINITY;
             float thr = capv;
             int thr_slot = 0;
-            for (int s2 = 0; s2 < RCAND; ++s2) {
+            for (int s2 = 0; s2 < R; ++s2) {
                 cs[s2 * S + owner] = INFINITY;
                 ci[s2 * S + owner] = 0xFFFFFFFFu;
             }
@@ -552,7 +555,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
 #pragma unroll
                             for (int j = 0; j < 32; ++j) {
                                 if (r[j] < thr && base_idx + j < n) {
-                                    const Worst w = cand_insert(cs, ci, owner, thr_slot, r[j], base_idx + j);
+                                    const Worst w = cand_insert<R>(cs, ci, owner, thr_slot, r[j], base_idx + j);
                                     thr = fminf(w.thr, capv);
                                     thr_slot = w.slot;
                                 }
@@ -587,7 +590,7 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
                                 }
                                 __syncwarp();
                                 // new worst of the row: highest score, lowest slot on ties
-                                float wv = cs[lane * S + ownerL];
+                                float wv = lane < R ? cs[lane * S + ownerL] : -INFINITY;
                                 int ws = lane;
 #pragma unroll
                                 for (int o = 16; o; o >>= 1) {
@@ -618,8 +621,8 @@ __global__ void __launch_bounds__(KNN_THREADS, 1)
             if (*abort_flag) break;
             if (qrow < nq) {
                 for (int s2 = 0; s2 < RCAND; ++s2) {
-                    cand_score[qrow * RTOTAL + h * RCAND + s2] = cs[s2 * S + owner];
-                    cand_idx[qrow * RTOTAL + h * RCAND + s2] = ci[s2 * S + owner];
+                    cand_score[qrow * RTOTAL + h * RCAND + s2] = s2 < R ? cs[s2 * S + owner] : INFINITY;
+                    cand_idx[qrow * RTOTAL + h * RCAND + s2] = s2 < R ? ci[s2 * S + owner] : 0xFFFFFFFFu;
                 }
             }
         }
@@ -909,14 +912,14 @@ struct TileLists {
     const float* cap = nullptr;      // per query (launch order): the score bound of k_knn_tc's qcap
 };
 
-template <int KA, bool F8>
+template <int KA, bool F8, int R = RCAND>
 void launch_tc(Ctx& c, const CUtensorMap& ta, const CUtensorMap& tb, uint64_t n, uint64_t nq, float* cand_score,
                uint32_t* cand_idx, const TileLists& tl = TileLists{}) {
-    using L = KnnSmem<KA>;
-    SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA, F8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
+    using L = KnnSmem<KA, R>;
+    SC_CUDA(cudaFuncSetAttribute(k_knn_tc<KA, F8, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L::BYTES));
     const uint32_t ngroups = (uint32_t)((nq + QT * TILE - 1) / (QT * TILE));
     const unsigned grid = std::min<unsigned>(ngroups, (unsigned)c.sm_count);
-    k_knn_tc<KA, F8><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
+    k_knn_tc<KA, F8, R><<<grid, KNN_THREADS, L::BYTES, c.stream>>>(ta, tb, (uint32_t)n, (uint32_t)nq, cand_score,
                                                                  cand_idx, c.d_status, c.wait_limit,
                                                                  c.knn_hold_tiles, tl.rptr, tl.rngs, tl.cap);
     SC_LAUNCH_CHECK();
@@ -1707,9 +1710,15 @@ void prep_operands(Ctx& c, const float* dX, uint64_t n, uint32_t d, int precisio
     op.tb = make_map(B, n, KA * 2, false);
 }
 
-void launch_operands(Ctx& c, const TcOperands& op, uint64_t n, float* cscore, uint32_t* cidx, const TileLists& tl) {
+// few: keep PASS1_CAND candidates per (query, half) instead of RCAND (BF16;
+// for a pass whose lists only bound the (k+1)-th distance).
+constexpr int PASS1_CAND = 16;
+void launch_operands(Ctx& c, const TcOperands& op, uint64_t n, float* cscore, uint32_t* cidx, const TileLists& tl,
+                     bool few = false) {
     if (op.kind == 2) launch_tc<32, true>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
+    else if (op.kind == 0 && few) launch_tc<32, false, PASS1_CAND>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else if (op.kind == 0) launch_tc<32, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
+    else if (few) launch_tc<64, false, PASS1_CAND>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
     else launch_tc<64, false>(c, op.ta, op.tb, n, n, cscore, cidx, tl);
 }
 
@@ -1933,8 +1942,8 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     // queries in the order `ord` (nullable: the sorted order), operand `o`
     // a scan and its re-rank, the tile lists on the device
     auto run_pass_dev = [&](const TcOperands& o, const uint32_t* ord, const uint32_t* d_rptr, const uint2* d_rngs,
-                            uint32_t* out_idx, float* out_d2, const float* qcap) {
-        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr, d_rngs, qcap});
+                            uint32_t* out_idx, float* out_d2, const float* qcap, bool few) {
+        launch_operands(c, o, n, cscore.get(), cidx.get(), TileLists{d_rptr, d_rngs, qcap}, few);
         k_knn_rerank_sorted<<<grid_for(n * 32, 256), 256, 0, c.stream>>>(Xs.get(), n, d, k, ord, perm.get(),
                                                                         cidx.get(), out_idx, out_d2);
         SC_LAUNCH_CHECK();
@@ -1974,7 +1983,10 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
                                                                fcent.get(), d_rp.get(), d_rg.get());
         SC_LAUNCH_CHECK();
         c.launches++;
-        run_pass_dev(op, nullptr, d_rp.get(), d_rg.get(), idx1.get(), d21.get(), nullptr);
+        // pass 1 only bounds the (k+1)-th distance: fewer kept candidates suffice
+        // (any k + 1 real points give a bound; 2 x PASS1_CAND of them are kept)
+        run_pass_dev(op, nullptr, d_rp.get(), d_rg.get(), idx1.get(), d21.get(), nullptr,
+                     2 * PASS1_CAND >= (int)k1 + 8);
         sync(c);  // the host arrays above must outlive the copies
     }
     tm.mark();  // 4: pass 1
@@ -2070,7 +2082,7 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     c.launches += 2;
     const uint64_t tiles2 = to_host(c, d_tiles2.get());
     tm.mark();  // 10: lists built
-    run_pass_dev(op2, ord.get(), d_rptr2.get(), d_rngs2.get(), idx, d2, qcap.get());
+    run_pass_dev(op2, ord.get(), d_rptr2.get(), d_rngs2.get(), idx, d2, qcap.get(), false);
     tm.mark();  // 11: pass 2
     c.knn_stats.ms_cluster = tm.ms(0, 3);
     c.knn_stats.ms_pass1 = tm.ms(3, 4);
