@@ -1363,7 +1363,8 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
                               const unsigned long long* __restrict__ gmask, const uint32_t* __restrict__ gown,
                               uint32_t words, uint32_t K, const uint32_t* __restrict__ fbase,
                               const float* __restrict__ fcent, const unsigned* __restrict__ crad, float eps,
-                              uint32_t cwords, unsigned* gcell) {
+                              uint32_t cwords, const unsigned long long* __restrict__ qmask,
+                              const uint32_t* __restrict__ qcl, unsigned* gcell) {
     const uint64_t g = blockIdx.x;
     const uint64_t r = g * (QT * TILE) + threadIdx.x;
     const bool ok = r < n;
@@ -1422,12 +1423,20 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
         }
     }
     __syncthreads();
-    // the per-query test on the cells the group ball kept
+    // the per-query test on the cells the group ball kept, for the queries
+    // whose own cluster or needs hold the cell's cluster (the group scans the
+    // union of its queries' needs; each query tests only its own)
+    const uint32_t myown = qcl[sq];
+    const unsigned long long* mym = qmask + sq * words;
+    uint32_t b = 0;  // the cluster of cell f (cells ascend, so does b)
     for (uint32_t wd = 0; wd < cwords; ++wd) {
         unsigned bits = s_maybe[wd];  // uniform over the block
         while (bits) {
             const uint32_t f = wd * 32 + (uint32_t)(__ffs(bits) - 1);
             bits &= bits - 1;
+            while (fbase[b + 1] <= f) ++b;
+            const bool mine = ok && (b == myown || ((mym[b / 64] >> (b % 64)) & 1ull));
+            if (!__any_sync(0xFFFFFFFFu, mine)) continue;
             const float* m = fcent + (uint64_t)f * d;
             float dc = 0.0f;
 #pragma unroll
@@ -1436,7 +1445,7 @@ __global__ void k_group_cells(const float* __restrict__ Xs, uint64_t n, uint32_t
                     const float df = x[j] - m[j];
                     dc = __fmaf_rn(df, df, dc);
                 }
-            const bool need = ok && sqrtf(dc) * (1.0f - 1e-5f) - unord32(crad[f]) - eps <= kth;
+            const bool need = mine && sqrtf(dc) * (1.0f - 1e-5f) - unord32(crad[f]) - eps <= kth;
             // one shared OR per warp that needs the cell (most cells are needed by all or none)
             if (__ballot_sync(0xFFFFFFFFu, need) && lane == 0) atomicOr(s_bits + f / 32, 1u << (f % 32));
         }
@@ -2030,7 +2039,8 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     SC_CUDA(cudaFuncSetAttribute(k_group_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(cwords * 8)));
     k_group_cells<<<(unsigned)ngroups, QT * TILE, cwords * 8, c.stream>>>(Xs.get(), n, d, ord.get(), perm.get(), d21.get(), k1,
                                                                 gmask.get(), gown.get(), words, K, d_fbase.get(),
-                                                                fcent.get(), crad.get(), eps, cwords, gcell.get());
+                                                                fcent.get(), crad.get(), eps, cwords, mask.get(),
+                                                                cl_s.get(), gcell.get());
     SC_LAUNCH_CHECK();
     c.launches++;
     tm.mark();  // 8: group cells done
