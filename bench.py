@@ -885,12 +885,14 @@ def main():
     torch.cuda.synchronize()
     clocks.mark()
     dev_ms = 0.0
+    ms_each = []
     stats = None
     t = time.perf_counter()
     for _ in range(args.steps):
         c = sc_gpu.leiden(g, cfg)
         stats = sc_gpu.last_run_stats(local_rank)
         dev_ms += stats["ms_total"]
+        ms_each.append(stats["ms_total"])
     torch.cuda.synchronize()
     wall = time.perf_counter() - t
     if dist:
@@ -947,7 +949,7 @@ def main():
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": workload,
             "s_per_run": ms_step / 1e3, "edge_count": m, "modularity": q, "n_clusters": c.n_clusters(),
-            "wall_s_per_step": wall / args.steps,
+            "wall_s_per_step": wall / args.steps, "ms_each": ms_each,
             "phases_ms": {k: stats[k] for k in ("ms_local_move", "ms_refine", "ms_aggregate", "ms_other")},
             "run_stats": {k: stats[k] for k in ("passes", "levels", "local_move_sweeps", "moves")},
             "autotune": tuned,
