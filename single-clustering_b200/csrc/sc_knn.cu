@@ -1530,6 +1530,11 @@ __global__ void k_order_tiles(const float* __restrict__ Xs, uint64_t n, uint32_t
     for (uint32_t k = threadIdx.x; k < cnt; k += blockDim.x) out[rptr[g] + k] = make_uint2(s_tile[k], 1u);
 }
 
+__global__ void k_u64_to_u32(const uint64_t* __restrict__ in, uint64_t n, uint32_t* out) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = (uint32_t)in[i];
+}
+
 // The pass-2 tile ranges of every group (a thread per group) from its cell
 // bitmap: each run of consecutive set cells is a run of adjacent points
 // [cstart[first], cstart[last + 1]); those become tile ranges, merged where
@@ -1538,7 +1543,7 @@ __global__ void k_order_tiles(const float* __restrict__ Xs, uint64_t n, uint32_t
 // rptr[g] and adds the group's tile count to *tiles.
 __global__ void k_group_ranges(const unsigned* __restrict__ gcell, uint32_t cwords, uint32_t F,
                                const uint64_t* __restrict__ cstart, uint64_t ngroups,
-                               const uint32_t* __restrict__ rptr, uint32_t* cnt, uint2* rngs,
+                               const uint32_t* __restrict__ rptr, uint64_t* cnt, uint2* rngs,
                                unsigned long long* tiles) {
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < ngroups;
          g += (uint64_t)gridDim.x * blockDim.x) {
@@ -1974,9 +1979,11 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
             own(g, pts);
             h_tb[g] = (uint32_t)(pts[0].first / TILE);
             h_te[g] = (uint32_t)((pts[0].second + TILE - 1) / TILE);
-            rptr[g + 1] = rptr[g] + (h_te[g] - h_tb[g]);
+            tiles1 += h_te[g] - h_tb[g];
+            if (tiles1 > 0xFFFFFFFFull)
+                fail(SC_E_UNSUPPORTED, "pruned kNN lists exceed 2^32 tiles: use more clusters or the full scan");
+            rptr[g + 1] = (uint32_t)tiles1;
         }
-        tiles1 = rptr[ngroups];
         std::vector<uint32_t> tile_cell(ntiles);
         for (uint64_t t = 0, f = 0; t < ntiles; ++t) {
             while (f + 1 < F && cstart[f + 1] <= t * TILE) ++f;
@@ -2076,20 +2083,24 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     // order), the tile lists built on the device from the cell bitmaps
     DBuf<uint64_t> d_cstart(c, F + 1);
     h2d(c, d_cstart.get(), cstart.data(), F + 1);
-    DBuf<uint32_t> gcnt(c, ngroups + 1), d_rptr2(c, ngroups + 1);
+    DBuf<uint64_t> gcnt(c, ngroups + 1), r64(c, ngroups + 1);
+    DBuf<uint32_t> d_rptr2(c, ngroups + 1);
     zero(c, gcnt.get(), ngroups + 1);
     DBuf<unsigned long long> d_tiles2(c, 1);
     zero(c, d_tiles2.get(), 1);
     k_group_ranges<<<grid_for(ngroups, 128), 128, 0, c.stream>>>(gcell.get(), cwords, F, d_cstart.get(), ngroups,
                                                                  nullptr, gcnt.get(), nullptr, nullptr);
-    exclusive_sum(c, gcnt.get(), d_rptr2.get(), ngroups + 1);
-    const uint32_t nranges = to_host(c, d_rptr2.get() + ngroups);
-    DBuf<uint2> d_rngs2(c, std::max<uint32_t>(nranges, 1));
+    exclusive_sum(c, gcnt.get(), r64.get(), ngroups + 1);
+    const uint64_t nranges = to_host(c, r64.get() + ngroups);
+    if (nranges > 0xFFFFFFFFull)
+        fail(SC_E_UNSUPPORTED, "pruned kNN lists exceed 2^32 ranges: use more clusters or the full scan");
+    k_u64_to_u32<<<grid_for(ngroups + 1, 256), 256, 0, c.stream>>>(r64.get(), ngroups + 1, d_rptr2.get());
+    DBuf<uint2> d_rngs2(c, std::max<uint64_t>(nranges, 1));
     k_group_ranges<<<grid_for(ngroups, 128), 128, 0, c.stream>>>(gcell.get(), cwords, F, d_cstart.get(), ngroups,
                                                                  d_rptr2.get(), nullptr, d_rngs2.get(),
                                                                  d_tiles2.get());
     SC_LAUNCH_CHECK();
-    c.launches += 2;
+    c.launches += 3;
     const uint64_t tiles2 = to_host(c, d_tiles2.get());
     tm.mark();  // 10: lists built
     run_pass_dev(op2, ord.get(), d_rptr2.get(), d_rngs2.get(), idx, d2, qcap.get(), false);
