@@ -973,25 +973,36 @@ constexpr uint32_t KM_SAMPLE = 65536;  // points the Lloyd steps run on
 // Nearest centroid of every point (squared FP32 distance, ties to the lower id).
 __global__ void k_km_assign(const float* __restrict__ X, uint64_t n, uint32_t d, const float* __restrict__ cent,
                             uint32_t K, uint32_t* assign) {
-    extern __shared__ float s_cent[];
-    for (uint32_t i = threadIdx.x; i < K * d; i += blockDim.x) s_cent[i] = cent[i];
+    // centroid rows padded to a multiple of 4 floats, read as float4
+    extern __shared__ __align__(16) float s_cent[];
+    const uint32_t dp = (d + 3) & ~3u;
+    for (uint32_t i = threadIdx.x; i < K * dp; i += blockDim.x) {
+        const uint32_t c = i / dp, j = i % dp;
+        s_cent[i] = j < d ? cent[(uint64_t)c * d + j] : 0.0f;
+    }
     __syncthreads();
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         // the point in registers (d <= 62): the centroid loop then reads only
-        // shared memory, every lane the same word (a broadcast)
+        // shared memory, every lane the same words (a broadcast)
         float x[64];
 #pragma unroll
         for (int j = 0; j < 64; ++j) x[j] = (uint32_t)j < d ? X[i * d + j] : 0.0f;
         float best = INFINITY;
         uint32_t bc = 0;
         for (uint32_t c = 0; c < K; ++c) {
-            const float* m = s_cent + c * d;
+            const float4* m4 = reinterpret_cast<const float4*>(s_cent + (uint64_t)c * dp);
             float acc = 0.0f;
 #pragma unroll
-            for (int j = 0; j < 64; ++j)
-                if ((uint32_t)j < d) {
-                    const float df = __fsub_rn(x[j], m[j]);
-                    acc = __fmaf_rn(df, df, acc);
+            for (int q = 0; q < 16; ++q)
+                if ((uint32_t)(4 * q) < d) {
+                    const float4 mv = m4[q];
+                    const float mm[4] = {mv.x, mv.y, mv.z, mv.w};
+#pragma unroll
+                    for (int t = 0; t < 4; ++t)
+                        if ((uint32_t)(4 * q + t) < d) {
+                            const float df = __fsub_rn(x[4 * q + t], mm[t]);
+                            acc = __fmaf_rn(df, df, acc);
+                        }
                 }
             if (acc < best) {
                 best = acc;
@@ -1811,7 +1822,7 @@ void knn_search_pruned(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint32_t
     DBuf<uint32_t> assign(c, n);
     DBuf<unsigned long long> sums(c, (uint64_t)K * d);
     DBuf<unsigned> cnt(c, K);
-    const size_t sm_assign = (size_t)K * d * 4, sm_accum = (size_t)K * d * 8 + (size_t)K * 4;
+    const size_t sm_assign = (size_t)K * ((d + 3) & ~3u) * 4, sm_accum = (size_t)K * d * 8 + (size_t)K * 4;
     SC_CUDA(cudaFuncSetAttribute(k_km_assign, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_assign));
     SC_CUDA(cudaFuncSetAttribute(k_km_accum, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_accum));
     for (int it = 0; it < KM_ITERS; ++it) {
