@@ -1141,16 +1141,20 @@ __global__ void k_fine_assign(const float* __restrict__ Xs, uint64_t n, uint32_t
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t b = cl[i];
         const uint64_t s0 = cstart[b], s1 = cstart[b + 1];
-        const float* x = Xs + i * d;
+        float x[64];  // the point in registers (d <= 62)
+#pragma unroll
+        for (int j = 0; j < 64; ++j) x[j] = (uint32_t)j < d ? Xs[i * d + j] : 0.0f;
         float best = INFINITY;
         uint32_t bf = 0, f = 0;
         for (uint64_t p = s0; p < s1; p += FINE, ++f) {
             const float* m = Xs + p * d;
             float acc = 0.0f;
-            for (uint32_t j = 0; j < d; ++j) {
-                const float df = __fsub_rn(x[j], m[j]);
-                acc = __fmaf_rn(df, df, acc);
-            }
+#pragma unroll
+            for (int j = 0; j < 64; ++j)
+                if ((uint32_t)j < d) {
+                    const float df = __fsub_rn(x[j], m[j]);
+                    acc = __fmaf_rn(df, df, acc);
+                }
             if (acc < best) {
                 best = acc;
                 bf = f;
