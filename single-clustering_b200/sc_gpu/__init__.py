@@ -640,12 +640,16 @@ def knn_gaussian(X, k: int, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_I
     opts = _lib.KnnOpts()
     lib().sc_knn_opts_default(C.byref(opts))
     opts.sigma, opts.sym, opts.precision, opts.squared_kiddo = sigma, sym, precision, int(squared)
-    idx = np.zeros((n, k + 1), np.uint32)
-    dist = np.zeros((n, k + 1), np.float32)
+    # outputs are written by the library in full: no zero fill. The entry
+    # arrays are sized for the most entries possible (2 n k) and returned as
+    # views of their first nnz; the unwritten tail is never touched, so it
+    # takes no memory, and no copy is made.
+    idx = np.empty((n, k + 1), np.uint32)
+    dist = np.empty((n, k + 1), np.float32)
     cap = 2 * n * k
-    ptrs = np.zeros(n + 1, np.uint64)
-    nbrs = np.zeros(cap, np.uint32)
-    w = np.zeros(cap, np.float32)
+    ptrs = np.empty(n + 1, np.uint64)
+    nbrs = np.empty(cap, np.uint32)
+    w = np.empty(cap, np.float32)
     nnz = C.c_uint64()
     gh = C.c_void_p()
     _check(lib().sc_knn_gaussian(ctx.h, _ptr(X, _lib.f32p), n, d, k, C.byref(opts), _ptr(idx, _lib.u32p),
@@ -654,7 +658,7 @@ def knn_gaussian(X, k: int, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_LOWER_I
                                  C.byref(gh) if build_graph else None), ctx)
     m = nnz.value
     graph = CSRNetwork(gh, ctx) if build_graph else None
-    return NeighborResult(idx, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), graph)
+    return NeighborResult(idx, dist, ptrs, nbrs[:m], w[:m], graph)
 
 
 def set_knn_clusters(clusters: int, device: int | None = None) -> None:
@@ -721,9 +725,9 @@ def knn_connectivities(index, d2, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_L
     ctx = context(device)
     opts = _knn_opts(sigma, sym, KNN_BF16, squared)
     cap = 2 * n * k
-    ptrs = np.zeros(n + 1, np.uint64)
-    nbrs = np.zeros(max(cap, 1), np.uint32)
-    w = np.zeros(max(cap, 1), np.float32)
+    ptrs = np.empty(n + 1, np.uint64)  # written in full by the library (see knn_gaussian)
+    nbrs = np.empty(max(cap, 1), np.uint32)
+    w = np.empty(max(cap, 1), np.float32)
     nnz = C.c_uint64()
     gh = C.c_void_p()
     _check(lib().sc_knn_connectivities(ctx.h, _ptr(index, _lib.u32p), _ptr(d2, _lib.f32p), n, k, C.byref(opts),
@@ -731,7 +735,7 @@ def knn_connectivities(index, d2, *, sigma: int = SIGMA_MEDIAN, sym: int = SYM_L
                                        C.byref(nnz), C.byref(gh) if build_graph else None), ctx)
     m = nnz.value
     dist = d2 if squared else np.sqrt(d2)
-    return NeighborResult(index, dist, ptrs, nbrs[:m].copy(), w[:m].copy(), CSRNetwork(gh, ctx) if build_graph else None)
+    return NeighborResult(index, dist, ptrs, nbrs[:m], w[:m], CSRNetwork(gh, ctx) if build_graph else None)
 
 
 __all__ += ["knn_search", "knn_connectivities"]
