@@ -36,7 +36,11 @@
 // accumulation, 16 edges per warp step, features and hidden gradients split
 // into two BF16 parts so the sums keep FP32-level accuracy); gradients
 // accumulate in registers, then per block in shared memory, then in a
-// fixed-order reduction over blocks (deterministic).
+// fixed-order reduction over blocks (deterministic). The features that depend
+// on neither gamma nor a context (EDGE_SF values per edge) are computed once
+// per graph, a warp per row (a block per hub row), and kept with the graph;
+// each call assembles them with log(gamma), the null term and the context
+// features (label shares from per-chunk label groups).
 #include <cuda_bf16.h>
 
 #include <algorithm>
