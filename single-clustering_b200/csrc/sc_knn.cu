@@ -964,9 +964,13 @@ void candidates_f8(Ctx& c, const float* dX, uint64_t n, uint32_t d, uint64_t q0,
 // and the slab bound of the direction u from the query's cluster centre to
 // c_b (every x in b projects into [lo, hi] on u, so |q - x| >= the distance
 // from <q, u> to [lo, hi]). The second pass scans the own tiles and those of
-// every cluster some query of the group cannot exclude; skipped points are
-// provably farther than the query's (k+1)-th neighbour, so the result is the
-// full search's.
+// every cluster some query of the group cannot exclude, narrowed to the fine
+// cells (~256 points) a ball bound cannot exclude; skipped points are provably
+// farther than the query's (k+1)-th neighbour, so the result is the full
+// search's. The first pass keeps fewer candidates (it only yields the bound)
+// and walks each group's nearest cells first; the second starts every query's
+// candidate rows from a proven score bound derived from the first pass's
+// distance (k_pass2_cap). Both passes take their tile lists from the device.
 constexpr int KM_ITERS = 8;
 constexpr uint32_t KM_SAMPLE = 65536;  // points the Lloyd steps run on
 
